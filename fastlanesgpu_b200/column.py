@@ -1,0 +1,135 @@
+"""Encoded FastLanes columns: host encoding (C++ encoders of the library) and
+device residency (torch tensors holding the packed words and metadata).
+
+An encoded column is a contiguous array of 1024-value vectors, each with a
+16-byte metadata entry {word offset, FOR base, scheme, bit width, aux}; the
+uniform form (one scheme/bit width/base for all vectors, no metadata) is the
+reference's layout (fastlanes/src/ssb/fls_q11.cu:202-223).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import (LAYOUT_NORMAL, LAYOUT_TRANSPOSED, SCHEME_DELTA, SCHEME_FOR, Column, check, lib)
+
+META_DTYPE = np.dtype([("offset", "<u8"), ("base", "<i4"), ("scheme", "u1"), ("bw", "u1"), ("aux", "<u2")])
+assert META_DTYPE.itemsize == 16
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def n_vectors(n_values: int) -> int:
+    return (n_values + 1023) // 1024
+
+
+@dataclass
+class EncodedColumn:
+    """A column encoded on the host."""
+    words: np.ndarray            # uint32 payload words
+    meta: np.ndarray | None      # META_DTYPE per vector, or None for a uniform column
+    n_values: int
+    layout: int
+    scheme: int = SCHEME_FOR     # uniform columns
+    bw: int = 0                  # uniform columns
+    base: int = 0                # uniform columns
+    max_vec_words: int = 0
+    scheme_mask: int = 0
+    payload_words: int = -1      # encoded words (words may carry padding past them)
+
+    @property
+    def n_vec(self) -> int:
+        return n_vectors(self.n_values)
+
+    @property
+    def nbytes(self) -> int:
+        """Encoded bytes a decode must read: payload plus per-vector metadata."""
+        pw = int(self.words.size) if self.payload_words < 0 else self.payload_words
+        return pw * 4 + (0 if self.meta is None else int(self.meta.size) * 16)
+
+    # -- encoders -----------------------------------------------------------
+    @classmethod
+    def uniform(cls, values: np.ndarray, scheme: int = SCHEME_FOR, layout: int = LAYOUT_NORMAL,
+                bw: int | None = None, base: int = 0) -> "EncodedColumn":
+        """One scheme, bit width and FOR base for every vector (the reference's
+        column format).  bw=None picks the smallest width that fits."""
+        v = np.ascontiguousarray(values, dtype=np.int32)
+        n = int(v.size)
+        out = np.zeros(int(lib().fls_encode_bound_words(n)), dtype=np.uint32)
+        n_words = ctypes.c_uint64()
+        out_bw = ctypes.c_uint8()
+        check(lib().fls_encode_uniform(_ptr(v), n, scheme, layout, 0xFF if bw is None else bw, base, _ptr(out),
+                                       ctypes.addressof(n_words), ctypes.addressof(out_bw)), "fls_encode_uniform")
+        words = out[:max(n_words.value, 4)].copy()
+        return cls(words=words, meta=None, n_values=n, layout=layout, scheme=scheme, bw=out_bw.value, base=base,
+                   max_vec_words=0, scheme_mask=1 << scheme, payload_words=int(n_words.value))
+
+    @classmethod
+    def encode(cls, values: np.ndarray, schemes: np.ndarray | int = SCHEME_FOR,
+               layout: int = LAYOUT_TRANSPOSED, round4: bool = False) -> "EncodedColumn":
+        """Per-vector encoding: `schemes` is one scheme for all vectors or an
+        array with one scheme per vector (e.g. from the selector)."""
+        v = np.ascontiguousarray(values, dtype=np.int32)
+        n = int(v.size)
+        nv = n_vectors(n)
+        out = np.zeros(int(lib().fls_encode_bound_words(n)), dtype=np.uint32)
+        meta = np.zeros(nv, dtype=META_DTYPE)
+        n_words, mvw, mask = ctypes.c_uint64(), ctypes.c_uint32(), ctypes.c_uint32()
+        if isinstance(schemes, (int, np.integer)):
+            sp, s0 = None, int(schemes)
+        else:
+            sch = np.ascontiguousarray(schemes, dtype=np.uint8)
+            assert sch.size == nv
+            sp, s0 = _ptr(sch), 0
+        check(lib().fls_encode_column(_ptr(v), n, sp, s0, layout, int(round4), _ptr(out), ctypes.addressof(n_words),
+                                      _ptr(meta), ctypes.addressof(mvw), ctypes.addressof(mask)),
+              "fls_encode_column")
+        words = out[:max(n_words.value, 4)].copy()
+        return cls(words=words, meta=meta, n_values=n, layout=layout, max_vec_words=mvw.value,
+                   scheme_mask=mask.value, payload_words=int(n_words.value))
+
+    def to_device(self, device=None) -> "DeviceColumn":
+        return DeviceColumn(self, device)
+
+
+class DeviceColumn:
+    """An EncodedColumn resident in device memory, with its C descriptor."""
+
+    def __init__(self, col: EncodedColumn, device=None):
+        import torch
+        dev = torch.device("cuda") if device is None else torch.device(device)
+        self.host = col
+        self.data = torch.from_numpy(col.words.view(np.int32)).to(dev)
+        self.meta = None if col.meta is None else torch.from_numpy(col.meta.view(np.int32).reshape(-1)).to(dev)
+        self.desc = Column(data=self.data.data_ptr(), meta=0 if self.meta is None else self.meta.data_ptr(),
+                           n_values=col.n_values, n_words=int(col.words.size), layout=col.layout,
+                           scheme=col.scheme, bw=col.bw, base=col.base, max_vec_words=col.max_vec_words,
+                           scheme_mask=col.scheme_mask)
+
+    @property
+    def n_values(self) -> int:
+        return self.host.n_values
+
+    @property
+    def n_vec(self) -> int:
+        return self.host.n_vec
+
+    @property
+    def nbytes(self) -> int:
+        return self.host.nbytes
+
+
+def columns_array(cols) -> ctypes.Array:
+    arr = (Column * len(cols))()
+    for i, c in enumerate(cols):
+        arr[i] = c.desc
+    return arr
+
+
+__all__ = ["EncodedColumn", "DeviceColumn", "META_DTYPE", "columns_array", "n_vectors", "_lib",
+           "SCHEME_DELTA", "LAYOUT_TRANSPOSED"]

@@ -1,0 +1,112 @@
+// fls_decode.cu -- decode-to-HBM and decode-fused-sum operators.
+//
+// Reference counterparts: unpack_global (fastlanes/src/include/fls_gen/unpack/
+// unpack.cuh:3436), QueryKernel of bitpack_shared_memory.cu:21 /
+// bitpack_register.cu:21 (decode + sum), delta_shared_memory.cu:24 (delta +
+// sum) and delta_global_memory.cu:24 (delta to global memory).
+#include "fls_pipeline.cuh"
+
+namespace fls {
+namespace {
+
+struct NoState {};
+
+// Decode to HBM.  Values of a vector are written as 32 coalesced 128-byte rows
+// with streaming stores; transposed columns can instead be reordered through a
+// padded shared-memory tile (33 words per chunk, conflict-free) into original
+// order.
+struct DecodeOp {
+	using State = NoState;
+	uint32_t* out;
+	uint32_t  original;
+	__device__ void cta_setup(State&, uint32_t*, const StageCfg&) const {}
+	__device__ void process(State&, uint64_t v, const WarpStage& ws, uint32_t st, uint32_t lane,
+	                        const StageCfg&) const {
+		uint32_t vals[32];
+		if (!stage_decode(ws, st, 0, lane, vals)) { return; }
+		uint32_t* dst = out + v * 1024u;
+		if (original) {
+			uint32_t*      tb = ws.extra();
+			const uint32_t cb = 33u * dev::chunk_of_lane(lane);
+#pragma unroll
+			for (uint32_t r = 0; r < 32; ++r) { tb[cb + dev::step_of_row(r)] = vals[r]; }
+			__syncwarp();
+#pragma unroll
+			for (uint32_t r = 0; r < 32; ++r) { dev::st_stream(dst + 32u * r + lane, tb[33u * r + lane]); }
+			__syncwarp();
+		} else {
+#pragma unroll
+			for (uint32_t r = 0; r < 32; ++r) { dev::st_stream(dst + 32u * r + lane, vals[r]); }
+		}
+	}
+	__device__ void finish(State&, uint32_t, const StageCfg&) const {}
+};
+
+struct AccState {
+	unsigned long long acc;
+};
+
+// Decode fused with a uint64 sum; one atomic per warp at the end.
+struct DecodeSumOp {
+	using State = AccState;
+	unsigned long long* sum;
+	__device__ void cta_setup(State&, uint32_t*, const StageCfg&) const {}
+	__device__ void process(State& S, uint64_t v, const WarpStage& ws, uint32_t st, uint32_t lane,
+	                        const StageCfg& cfg) const {
+		uint32_t vals[32];
+		if (!stage_decode(ws, st, 0, lane, vals)) { return; }
+		const uint32_t m = valid_rows(cfg, v, lane);
+		// 32 values of < 2^32 each: accumulate low and high parts in 32 bits.
+		uint32_t lo = 0, hi = 0;
+#pragma unroll
+		for (uint32_t r = 0; r < 32; ++r) {
+			const uint32_t x = ((m >> r) & 1u) ? vals[r] : 0u;
+			const uint32_t t = lo + x;
+			hi += t < lo ? 1u : 0u;
+			lo = t;
+		}
+		S.acc += (static_cast<unsigned long long>(hi) << 32) | lo;
+	}
+	__device__ void finish(State& S, uint32_t lane, const StageCfg&) const {
+		const unsigned long long s = warp_sum_u64(S.acc);
+		if (lane == 0 && s) { atomicAdd(sum, s); }
+	}
+};
+
+} // namespace
+} // namespace fls
+
+using namespace fls;
+
+extern "C" {
+
+fls_status fls_decode_u32(const fls_column* col, uint32_t* d_out, uint32_t order, fls_stream_t stream) {
+	if (!col || !d_out) { return set_error(FLS_ERR_INVALID_ARG, "fls_decode_u32: null pointer"); }
+	if (order > FLS_ORDER_ORIGINAL) { return set_error(FLS_ERR_INVALID_ARG, "fls_decode_u32: bad order"); }
+	StageCfg   cfg;
+	uint32_t   grid, threads;
+	size_t     smem;
+	const bool orig = order == FLS_ORDER_ORIGINAL && col->layout == FLS_LAYOUT_TRANSPOSED;
+	fls_status s    = plan_stages(col, 1, orig ? kTBufWords : 0u, 0u, cfg, grid, threads, smem);
+	if (s != FLS_OK) { return s; }
+	DecodeOp op {};
+	op.out      = d_out;
+	op.original = orig ? 1u : 0u;
+	return launch_staged(cfg, op, grid, threads, smem, reinterpret_cast<cudaStream_t>(stream));
+}
+
+fls_status fls_decode_sum_u32(const fls_column* col, uint64_t* d_sum, fls_stream_t stream) {
+	if (!col || !d_sum) { return set_error(FLS_ERR_INVALID_ARG, "fls_decode_sum_u32: null pointer"); }
+	StageCfg   cfg;
+	uint32_t   grid, threads;
+	size_t     smem;
+	fls_status s = plan_stages(col, 1, 0u, 0u, cfg, grid, threads, smem);
+	if (s != FLS_OK) { return s; }
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	if ((s = cuda_check(cudaMemsetAsync(d_sum, 0, sizeof(uint64_t), st), "cudaMemsetAsync")) != FLS_OK) { return s; }
+	DecodeSumOp op {};
+	op.sum = reinterpret_cast<unsigned long long*>(d_sum);
+	return launch_staged(cfg, op, grid, threads, smem, st);
+}
+
+} // extern "C"

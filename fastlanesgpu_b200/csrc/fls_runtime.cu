@@ -1,0 +1,240 @@
+// fls_runtime.cu -- host runtime of the library: device properties, the device
+// error word, launch configuration, shared-memory planning of the staged
+// pipeline, and the C ABI entry points that are not operators.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <mutex>
+#include <vector>
+
+#include "fls_pipeline.cuh"
+
+namespace fls {
+
+// One error word per device (a module-scope variable exists once per device
+// context); kernels receive its address as a parameter.
+__device__ uint32_t g_err_word = 0;
+
+namespace {
+std::atomic<uint64_t> g_launches {0};
+
+struct LaunchCfg {
+	uint32_t warps = 8, stages = 3, ctas_per_sm = 1;
+};
+std::mutex g_cfg_mu;
+LaunchCfg  g_cfg;
+
+LaunchCfg launch_cfg() {
+	std::lock_guard<std::mutex> lk(g_cfg_mu);
+	return g_cfg;
+}
+
+uint32_t round4(uint32_t w) { return (w + 3u) & ~3u; }
+
+std::mutex              g_dev_mu;
+std::vector<DeviceInfo> g_dev_cache;
+std::vector<uint32_t*>  g_err_addr;
+} // namespace
+
+void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+fls_status cuda_check(cudaError_t e, const char* what) {
+	if (e == cudaSuccess) { return FLS_OK; }
+	return set_error(FLS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+fls_status device_info(DeviceInfo& di) {
+	int dev = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess) {
+		cudaGetLastError();
+		return set_error(FLS_ERR_NO_DEVICE, "no CUDA device");
+	}
+	std::lock_guard<std::mutex> lk(g_dev_mu);
+	if (static_cast<int>(g_dev_cache.size()) <= dev) {
+		g_dev_cache.resize(dev + 1);
+		g_err_addr.resize(dev + 1, nullptr);
+	}
+	if (g_dev_cache[dev].sms == 0) {
+		cudaDeviceProp p;
+		if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) {
+			return set_error(FLS_ERR_NO_DEVICE, "cudaGetDeviceProperties failed");
+		}
+		void* addr = nullptr;
+		if (cudaGetSymbolAddress(&addr, g_err_word) != cudaSuccess) {
+			return set_error(FLS_ERR_CUDA, "cannot resolve the device error word");
+		}
+		g_err_addr[dev]           = static_cast<uint32_t*>(addr);
+		g_dev_cache[dev].sms      = p.multiProcessorCount;
+		g_dev_cache[dev].max_smem = static_cast<int>(p.sharedMemPerBlockOptin);
+		g_dev_cache[dev].major    = p.major;
+	}
+	di = g_dev_cache[dev];
+	if (di.major < 10) { return set_error(FLS_ERR_NO_DEVICE, "device is not sm_100 class"); }
+	return FLS_OK;
+}
+
+uint32_t* device_error_word() {
+	int dev = 0;
+	cudaGetDevice(&dev);
+	std::lock_guard<std::mutex> lk(g_dev_mu);
+	return dev < static_cast<int>(g_err_addr.size()) ? g_err_addr[dev] : nullptr;
+}
+
+namespace {
+// Validates one column descriptor and converts it for the kernel.
+fls_status make_devcol(const fls_column& c, DevCol& d) {
+	if (!c.data && c.n_words) { return set_error(FLS_ERR_INVALID_ARG, "column data is null"); }
+	if (reinterpret_cast<uintptr_t>(c.data) & 15u) {
+		return set_error(FLS_ERR_ALIGNMENT, "column data must be 16-byte aligned");
+	}
+	if (reinterpret_cast<uintptr_t>(c.meta) & 15u) {
+		return set_error(FLS_ERR_ALIGNMENT, "column metadata must be 16-byte aligned");
+	}
+	if (c.layout > FLS_LAYOUT_TRANSPOSED) { return set_error(FLS_ERR_INVALID_ARG, "bad column layout"); }
+	if (c.n_values == 0) { return set_error(FLS_ERR_INVALID_ARG, "column has no values"); }
+	d.data    = c.data;
+	d.meta    = c.meta;
+	d.n_words = c.n_words;
+	d.layout  = c.layout;
+	d.pad_    = 0;
+	if (c.meta == nullptr) {
+		if (c.scheme != FLS_SCHEME_FOR && c.scheme != FLS_SCHEME_DELTA) {
+			return set_error(FLS_ERR_INVALID_ARG, "uniform columns must be FOR or DELTA");
+		}
+		if (c.bw > 32) { return set_error(FLS_ERR_BAD_BW, "bit width > 32"); }
+		if (c.scheme == FLS_SCHEME_DELTA && c.layout != FLS_LAYOUT_TRANSPOSED) {
+			return set_error(FLS_ERR_INVALID_ARG, "DELTA columns are stored transposed");
+		}
+		d.scheme             = c.scheme;
+		d.bw                 = c.bw;
+		d.base               = c.base;
+		d.slot_words         = dev::payload_words(c.scheme, c.bw, 0);
+		const uint64_t n_vec = (c.n_values + 1023u) / 1024u;
+		if (static_cast<uint64_t>(d.slot_words) * n_vec > c.n_words) {
+			return set_error(FLS_ERR_CAPACITY, "column data smaller than n_values at this bit width");
+		}
+	} else {
+		if (c.max_vec_words > kMaxVecWords) { return set_error(FLS_ERR_INVALID_ARG, "max_vec_words too large"); }
+		if ((c.scheme_mask & ((1u << FLS_SCHEME_DELTA) | (1u << FLS_SCHEME_RLE))) && c.layout != FLS_LAYOUT_TRANSPOSED) {
+			return set_error(FLS_ERR_INVALID_ARG, "DELTA/RLE vectors need the transposed layout");
+		}
+		d.scheme     = 0;
+		d.bw         = 0;
+		d.base       = 0;
+		d.slot_words = round4(c.max_vec_words);
+	}
+	return FLS_OK;
+}
+
+bool needs_dict(const fls_column& c) {
+	return c.meta != nullptr && (c.scheme_mask & ((1u << FLS_SCHEME_RLE) | (1u << FLS_SCHEME_DICT)));
+}
+} // namespace
+
+fls_status plan_stages(const fls_column* cols, uint32_t n_cols, uint32_t extra_words, uint32_t cta_words,
+                       StageCfg& cfg, uint32_t& grid, uint32_t& threads, size_t& smem_bytes) {
+	if (!cols || n_cols == 0 || n_cols > kMaxCols) { return set_error(FLS_ERR_INVALID_ARG, "1..8 columns per query"); }
+	DeviceInfo di;
+	fls_status s = device_info(di);
+	if (s != FLS_OK) { return s; }
+	std::memset(&cfg, 0, sizeof(cfg));
+	bool dict    = false;
+	cfg.n_values = cols[0].n_values;
+	cfg.layout   = cols[0].layout;
+	for (uint32_t c = 0; c < n_cols; ++c) {
+		if ((s = make_devcol(cols[c], cfg.cols[c])) != FLS_OK) { return s; }
+		if (cols[c].n_values != cfg.n_values) { return set_error(FLS_ERR_INVALID_ARG, "columns differ in length"); }
+		if (cols[c].layout != cfg.layout) {
+			return set_error(FLS_ERR_UNSUPPORTED, "all columns of a query must share one layout");
+		}
+		cfg.col_off[c] = cfg.stage_words;
+		cfg.stage_words += cfg.cols[c].slot_words;
+		dict = dict || needs_dict(cols[c]);
+	}
+	cfg.n_cols    = n_cols;
+	cfg.n_vec     = (cfg.n_values + 1023u) / 1024u;
+	cfg.err       = device_error_word();
+	LaunchCfg lc  = launch_cfg();
+	uint32_t  W = lc.warps, S = lc.stages;
+	// Shrink the pipeline until it fits the shared-memory budget.
+	for (;;) {
+		uint32_t w = S * cfg.stage_words;
+		cfg.dict_off = w;
+		w += dict ? kDictWords : 0u;
+		cfg.extra_off = w;
+		w += round4(extra_words);
+		cfg.info_off = w;
+		w += 2u * kMaxCols * S;
+		cfg.bar_off = w;
+		w += 2u * S;
+		w                   = round4(w);
+		cfg.warp_smem_words = w;
+		smem_bytes          = 4ull * (static_cast<size_t>(w) * W + cta_words);
+		if (smem_bytes <= static_cast<size_t>(di.max_smem)) { break; }
+		if (S > 2) {
+			--S;
+		} else if (W > 1) {
+			W /= 2;
+		} else {
+			return set_error(FLS_ERR_CAPACITY, "vectors too large for shared-memory staging");
+		}
+	}
+	cfg.stages               = S;
+	cfg.warps                = W;
+	cfg.cta_extra_off        = cfg.warp_smem_words * W;
+	const uint64_t need_ctas = (cfg.n_vec + W - 1) / W;
+	grid    = static_cast<uint32_t>(std::min<uint64_t>(need_ctas, static_cast<uint64_t>(di.sms) * lc.ctas_per_sm));
+	threads = 32u * W;
+	return FLS_OK;
+}
+
+} // namespace fls
+
+using namespace fls;
+
+extern "C" {
+
+fls_status fls_check_device_error(fls_stream_t stream) {
+	fls_status s = cuda_check(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)), "cudaStreamSynchronize");
+	if (s != FLS_OK) { return s; }
+	uint32_t word = 0, zero = 0;
+	if ((s = cuda_check(cudaMemcpyFromSymbol(&word, g_err_word, sizeof(word)), "read error word")) != FLS_OK) {
+		return s;
+	}
+	if (word == 0) { return FLS_OK; }
+	cudaMemcpyToSymbol(g_err_word, &zero, sizeof(zero));
+	std::string msg = "device error:";
+	if (word & kErrBadMeta) { msg += " bad-vector-metadata"; }
+	if (word & kErrBounds) { msg += " vector-out-of-bounds"; }
+	if (word & kErrHash) { msg += " hash-out-of-table"; }
+	if (word & kErrCapacity) { msg += " vector-exceeds-slot"; }
+	if (word & kErrTimeout) {
+		msg += " wait-timeout";
+		return set_error(FLS_ERR_TIMEOUT, msg);
+	}
+	return set_error(FLS_ERR_DEVICE, msg);
+}
+
+fls_status fls_set_launch_config(uint32_t warps_per_cta, uint32_t stages, uint32_t ctas_per_sm) {
+	if (warps_per_cta > 8 || stages > 8 || ctas_per_sm > 8 || (stages != 0 && stages < 2)) {
+		return set_error(FLS_ERR_INVALID_ARG, "launch config out of range (warps <= 8, 2 <= stages <= 8, ctas <= 8)");
+	}
+	std::lock_guard<std::mutex> lk(g_cfg_mu);
+	g_cfg.warps       = warps_per_cta ? warps_per_cta : 8u;
+	g_cfg.stages      = stages ? stages : 3u;
+	g_cfg.ctas_per_sm = ctas_per_sm ? ctas_per_sm : 1u;
+	return FLS_OK;
+}
+
+fls_status fls_get_launch_config(uint32_t* warps_per_cta, uint32_t* stages, uint32_t* ctas_per_sm) {
+	LaunchCfg c = launch_cfg();
+	if (warps_per_cta) { *warps_per_cta = c.warps; }
+	if (stages) { *stages = c.stages; }
+	if (ctas_per_sm) { *ctas_per_sm = c.ctas_per_sm; }
+	return FLS_OK;
+}
+
+uint64_t fls_kernel_launch_count(void) { return g_launches.load(); }
+
+} // extern "C"

@@ -1,0 +1,108 @@
+"""Seeded synthetic inputs with the shapes, sizes and value distributions of the
+workloads the reference measures (its SSB data is not available; these stand
+in for it).  All generators use numpy's PCG64 with an explicit seed.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+# Day ids 0..2555 cover 1992-01-01 .. 1998-12-30 (the SSB date dimension);
+# first day id of each year 1992..1998 and one past the end.
+YEAR_START = np.array([0, 366, 731, 1096, 1461, 1827, 2192, 2556], dtype=np.int32)
+N_DAYS = 2556
+
+
+def year_of_day(day: np.ndarray) -> np.ndarray:
+    return (1992 + np.searchsorted(YEAR_START, day, side="right") - 1).astype(np.int32)
+
+
+def rng(seed: int) -> np.random.Generator:
+    return np.random.default_rng(seed)
+
+
+def for_bitpack_mixed(n: int, seed: int = 1, widths=(3, 7, 11, 16, 21)) -> np.ndarray:
+    """Per 1024-value vector a seeded width w from `widths`, base U[0,2^20),
+    values base + U[0,2^w)."""
+    g = rng(seed)
+    nv = (n + 1023) // 1024
+    w = g.choice(np.asarray(widths), size=nv)
+    base = g.integers(0, 1 << 20, size=nv)
+    off = (g.integers(0, 1 << 32, size=(nv, 1024), dtype=np.uint64) & ((np.uint64(1) << w.astype(np.uint64)[:, None])
+                                                                       - np.uint64(1))).astype(np.int64)
+    return (base[:, None] + off).reshape(-1)[:n].astype(np.int32)
+
+
+def uniform_bits(n: int, bw: int, seed: int = 2) -> np.ndarray:
+    """Uniform values in [0, 2^bw) (bw 32 uses the full uint32 range)."""
+    g = rng(seed)
+    x = g.integers(0, 1 << 32, size=n, dtype=np.uint64)
+    if bw < 32:
+        x &= np.uint64((1 << bw) - 1)
+    return x.astype(np.uint32).view(np.int32)
+
+
+def sorted_geometric(n: int, p: float = 0.3, seed: int = 3) -> np.ndarray:
+    """Sorted keys with geometric(p) gaps (delta workload)."""
+    g = rng(seed)
+    return np.cumsum(g.geometric(p, size=n), dtype=np.int64).astype(np.int32)
+
+
+def geometric_runs(n: int, mean_run: float = 16.0, value_bits: int = 16, seed: int = 4) -> np.ndarray:
+    """Runs with geometric lengths (mean `mean_run`) of uniform values in [0, 2^value_bits)."""
+    g = rng(seed)
+    n_runs = int(n / mean_run * 1.2) + 16
+    lens = g.geometric(1.0 / mean_run, size=n_runs)
+    while lens.sum() < n:
+        lens = np.concatenate([lens, g.geometric(1.0 / mean_run, size=n_runs)])
+    vals = g.integers(0, 1 << value_bits, size=lens.size)
+    return np.repeat(vals, lens)[:n].astype(np.int32)
+
+
+def zipf_values(n: int, s: float = 1.1, domain: int = 1 << 20, seed: int = 5) -> np.ndarray:
+    """Zipf(s) ranks folded into [0, domain)."""
+    g = rng(seed)
+    z = g.zipf(s, size=n)
+    return ((z - 1) % domain).astype(np.int32)
+
+
+def lineorder_q11(n: int, seed: int = 11) -> dict:
+    """Fact table of the filter-aggregate workload: date day id U[0,2556)
+    (12 bit), discount U[0,10] (4 bit), quantity U[1,50] (6 bit), price
+    U[90000,10.5M] (24 bit)."""
+    g = rng(seed)
+    return {
+        "date": g.integers(0, N_DAYS, size=n).astype(np.int32),
+        "discount": g.integers(0, 11, size=n).astype(np.int32),
+        "quantity": g.integers(1, 51, size=n).astype(np.int32),
+        "price": g.integers(90000, 10_500_001, size=n).astype(np.int32),
+    }
+
+
+# Q1.1-shape predicate on the synthetic table: year 1993, discount in [1,3],
+# quantity < 25 (fls_q11.cu:20-26 on SSB), ~1/7 * 3/11 * 24/50 = 1.87 %.
+Q11_FILTER = {"date": (int(YEAR_START[1]), int(YEAR_START[2]) - 1), "discount": (1, 3), "quantity": (-2**31, 24)}
+Q11_BITS = {"date": 12, "discount": 4, "quantity": 6, "price": 24}
+
+
+def q21_tables(n: int, seed: int = 21, part_ids: int = 1 << 19, supp_ids: int = 1 << 17) -> dict:
+    """Join workload: fact foreign keys (part 19 bit, supplier 17 bit, date
+    12 bit, revenue 24 bit) and uniform dimension attributes; part filter
+    category == 1 of 5, supplier filter region == 1 of 25, brand in [0,1000)."""
+    g = rng(seed)
+    return {
+        "lo_partkey": g.integers(0, part_ids, size=n).astype(np.int32),
+        "lo_suppkey": g.integers(0, supp_ids, size=n).astype(np.int32),
+        "lo_orderdate": g.integers(0, N_DAYS, size=n).astype(np.int32),
+        "lo_revenue": g.integers(90000, 10_500_001, size=n).astype(np.int32),
+        "p_partkey": np.arange(part_ids, dtype=np.int32),
+        "p_category": g.integers(0, 5, size=part_ids).astype(np.int32),
+        "p_brand1": g.integers(0, 1000, size=part_ids).astype(np.int32),
+        "s_suppkey": np.arange(supp_ids, dtype=np.int32),
+        "s_region": g.integers(0, 25, size=supp_ids).astype(np.int32),
+        "d_datekey": np.arange(N_DAYS, dtype=np.int32),
+        "d_year": year_of_day(np.arange(N_DAYS)),
+    }
+
+
+Q21_BITS = {"lo_suppkey": 17, "lo_partkey": 19, "lo_orderdate": 12, "lo_revenue": 24}
+N_GROUPS = (1998 - 1992 + 1) * (5 * 5 * 40)

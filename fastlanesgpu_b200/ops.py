@@ -1,0 +1,195 @@
+"""Operators of the B200 FastLanes library (Python face of include/fls_gpu.h).
+
+Every call enqueues CUDA work on the current torch stream and returns device
+tensors; nothing here computes on the CPU.  Names follow the reference's
+operators:
+
+=============================  ==============================================
+this module                    reference (FastLanesGPU)
+=============================  ==============================================
+``pack`` / ``transpose_i`` /   fastlanes/src/pack.cpp:29607, transpose.cpp:4110,
+``unrsum`` / ``vector_rle``    unrsum.cpp:120, fls_gen/rle/rle.hpp:29 (host)
+``unpack_global``              fls_gen/unpack/unpack.cuh:3436 and
+                               delta_global_memory.cu:24 (decode to HBM)
+``query_aggregate``            bitpack_shared_memory.cu:21 QueryKernel (decode+sum)
+``query_filter_agg``           ssb/fls_q11.cu:29 QueryKernel_v1
+``build_pht``                  ssb/fls_q21.cu:197-263 build_hashtable_{s,p,d}
+``probe_groupby``              ssb/fls_q21.cu:21 probe_v1
+=============================  ==============================================
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import (MAX_FILTERS, MAX_PROBES, ORDER_STORED, FilterAggDesc, JoinAggDesc, check, lib)
+from .column import DeviceColumn, columns_array
+
+
+def _stream():
+    import torch
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+# ---------------------------------------------------------------- host side
+
+def pack(vec: np.ndarray, bw: int) -> np.ndarray:
+    """FastLanes 32-bit bit-packing of one 1024-value vector (32*bw words)."""
+    v = np.ascontiguousarray(vec, dtype=np.uint32)
+    assert v.size == 1024
+    out = np.zeros(max(32 * bw, 1), dtype=np.uint32)
+    check(lib().fls_pack_u32(_p(v), _p(out), bw), "fls_pack_u32")
+    return out[:32 * bw]
+
+
+def transpose_i(vec: np.ndarray) -> np.ndarray:
+    v = np.ascontiguousarray(vec, dtype=np.uint32)
+    out = np.empty(1024, dtype=np.uint32)
+    check(lib().fls_transpose_i_u32(_p(v), _p(out)), "fls_transpose_i_u32")
+    return out
+
+
+def untranspose(vec: np.ndarray) -> np.ndarray:
+    v = np.ascontiguousarray(vec, dtype=np.uint32)
+    out = np.empty(1024, dtype=np.uint32)
+    check(lib().fls_untranspose_u32(_p(v), _p(out)), "fls_untranspose_u32")
+    return out
+
+
+def unrsum(vec: np.ndarray) -> np.ndarray:
+    v = np.ascontiguousarray(vec, dtype=np.uint32)
+    out = np.empty(1024, dtype=np.uint32)
+    check(lib().fls_unrsum_u32(_p(v), _p(out)), "fls_unrsum_u32")
+    return out
+
+
+def vector_rle(vec: np.ndarray):
+    """rle.hpp VECTOR_RLE: (n_dict, idx[1024] uint8, dict[n_dict], dict4[4])."""
+    v = np.ascontiguousarray(vec, dtype=np.int32)
+    idx = np.zeros(1024, np.uint8)
+    dic = np.zeros(1024, np.int32)
+    d4 = np.zeros(4, np.uint16)
+    n = ctypes.c_uint32()
+    check(lib().fls_vector_rle(_p(v), _p(idx), _p(dic), _p(d4), ctypes.addressof(n)), "fls_vector_rle")
+    return n.value, idx, dic[:n.value].copy(), d4
+
+
+def encode_exhaustive(values: np.ndarray, n_threads: int = 0):
+    """Exact per-vector sizes of all 5 schemes and the argmin (n_vec x 5, n_vec)."""
+    v = np.ascontiguousarray(values, dtype=np.int32)
+    nv = (v.size + 1023) // 1024
+    sizes = np.zeros((nv, 5), np.uint32)
+    best = np.zeros(nv, np.uint8)
+    check(lib().fls_encode_exhaustive(_p(v), v.size, _p(sizes), _p(best), n_threads), "fls_encode_exhaustive")
+    return sizes, best
+
+
+def vector_stats(values: np.ndarray, n_threads: int = 0) -> np.ndarray:
+    v = np.ascontiguousarray(values, dtype=np.int32)
+    nv = (v.size + 1023) // 1024
+    out = np.zeros((nv, 16), np.float32)
+    check(lib().fls_vector_stats(_p(v), v.size, _p(out), n_threads), "fls_vector_stats")
+    return out
+
+
+# -------------------------------------------------------------- device side
+
+def unpack_global(col: DeviceColumn, order: int = ORDER_STORED, out=None):
+    """Decode every vector to HBM (n_vec*1024 int32 values, device)."""
+    import torch
+    if out is None:
+        out = torch.empty(col.n_vec * 1024, dtype=torch.int32, device=col.data.device)
+    check(lib().fls_decode_u32(ctypes.byref(col.desc), out.data_ptr(), order, _stream()), "fls_decode_u32")
+    return out
+
+
+def query_aggregate(col: DeviceColumn, out=None):
+    """Decode fused with a uint64 sum of all values (device int64[1])."""
+    import torch
+    if out is None:
+        out = torch.empty(1, dtype=torch.int64, device=col.data.device)
+    check(lib().fls_decode_sum_u32(ctypes.byref(col.desc), out.data_ptr(), _stream()), "fls_decode_sum_u32")
+    return out
+
+
+def query_filter_agg(cols, filters, agg_a: int = -1, agg_b: int = -1, out=None):
+    """Filters [(col, lo, hi)] (inclusive int32 ranges) ANDed; returns the int64
+    sum of cols[agg_a] (* cols[agg_b]) over the selected rows, or the count."""
+    import torch
+    if len(filters) > MAX_FILTERS:
+        raise ValueError("at most 4 filters")
+    arr = columns_array(cols)
+    d = FilterAggDesc()
+    d.cols = arr
+    d.n_cols = len(cols)
+    for i, (c, lo, hi) in enumerate(filters):
+        d.filters[i].col, d.filters[i].lo, d.filters[i].hi = c, lo, hi
+    d.n_filters = len(filters)
+    d.agg_a, d.agg_b = agg_a, agg_b
+    if out is None:
+        out = torch.empty(1, dtype=torch.int64, device=cols[0].data.device)
+    check(lib().fls_query_filter_agg(ctypes.byref(d), out.data_ptr(), _stream()), "fls_query_filter_agg")
+    return out
+
+
+def build_pht(keys, ht_len: int, vals=None, filt=None, filter_eq: int = 1, keys_min: int = 0, out=None):
+    """Selective perfect-hash table on device int32 columns: PHT_1 (vals None,
+    ht_len slots) or PHT_2 (2*ht_len slots)."""
+    import torch
+    size = ht_len if vals is None else 2 * ht_len
+    if out is None:
+        out = torch.zeros(size, dtype=torch.int32, device=keys.device)
+    else:
+        out.zero_()
+    check(lib().fls_pht_build(0 if filt is None else filt.data_ptr(), filter_eq, keys.data_ptr(),
+                              0 if vals is None else vals.data_ptr(), keys.numel(), out.data_ptr(), ht_len,
+                              keys_min, _stream()), "fls_pht_build")
+    return out
+
+
+def probe_groupby(cols, probes, agg_col: int, key_a: int, key_b: int, group_mul: int, group_sub: int,
+                  n_groups: int, out=None):
+    """probes: [(col, ht tensor, ht_len, keys_min, kind)].  Returns the
+    reference's result array int32[4*n_groups]: [key_b value, key_a value,
+    int64 sum (2 words)] per group."""
+    import torch
+    if len(probes) > MAX_PROBES:
+        raise ValueError("at most 4 probes")
+    arr = columns_array(cols)
+    d = JoinAggDesc()
+    d.cols = arr
+    d.n_cols = len(cols)
+    for i, (c, ht, ln, kmin, kind) in enumerate(probes):
+        d.probes[i].col, d.probes[i].ht, d.probes[i].ht_len = c, ht.data_ptr(), ln
+        d.probes[i].keys_min, d.probes[i].kind = kmin, kind
+    d.n_probes = len(probes)
+    d.agg_col, d.key_a, d.key_b = agg_col, key_a, key_b
+    d.group_mul, d.group_sub, d.n_groups = group_mul, group_sub, n_groups
+    if out is None:
+        out = torch.empty(4 * n_groups, dtype=torch.int32, device=cols[0].data.device)
+    check(lib().fls_query_probe_groupby(ctypes.byref(d), out.data_ptr(), _stream()), "fls_query_probe_groupby")
+    return out
+
+
+def check_device_error() -> None:
+    """Synchronise the current stream and raise if a kernel flagged bad input."""
+    check(lib().fls_check_device_error(_stream()), "device")
+
+
+def set_launch_config(warps: int = 0, stages: int = 0, ctas_per_sm: int = 0) -> None:
+    check(lib().fls_set_launch_config(warps, stages, ctas_per_sm), "fls_set_launch_config")
+
+
+def get_launch_config():
+    w, s, c = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    lib().fls_get_launch_config(ctypes.addressof(w), ctypes.addressof(s), ctypes.addressof(c))
+    return w.value, s.value, c.value
+
+
+def kernel_launch_count() -> int:
+    return int(lib().fls_kernel_launch_count())

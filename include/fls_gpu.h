@@ -1,0 +1,237 @@
+/*
+ * fls_gpu.h -- C ABI of the B200 (sm_100a) FastLanes decode + fused query library.
+ *
+ * Drop-in boundary for the hot path of FastLanesGPU: FastLanes vector decode
+ * (1024-value interleaved bit-packing, FOR, delta over the transposed layout,
+ * RLE) fused into Crystal-style tile query kernels.  The reference exposes this
+ * path only as header templates and host functions; every entry point below
+ * names the reference interface it replaces (paths relative to the reference
+ * project root).
+ *
+ * Conventions
+ *  - The caller owns every buffer.  Pointers documented as "device" must be
+ *    device memory of the current device; "host" pointers are host memory.
+ *  - Device calls are asynchronous and stream-ordered on `stream`
+ *    (0 = legacy default stream).  They never allocate device memory.
+ *  - Every call returns an fls_status.  Nothing calls exit(), traps the GPU or
+ *    throws across the ABI.  Kernels validate per-vector metadata and record
+ *    violations in a device error word instead of reading out of bounds;
+ *    fls_check_device_error() synchronises `stream` and reports it.
+ *  - Packed data buffers must be 16-byte aligned; every vector starts on a
+ *    16-byte boundary (vector word offsets are multiples of 4).
+ */
+#ifndef FLS_GPU_H
+#define FLS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* fls_stream_t; /* == cudaStream_t */
+
+typedef enum fls_status {
+	FLS_OK                = 0,
+	FLS_ERR_INVALID_ARG   = 1, /* null pointer, bad enum, inconsistent sizes  */
+	FLS_ERR_BAD_BW        = 2, /* bit width > 32 (or > 10 for dictionary codes) */
+	FLS_ERR_ALIGNMENT     = 3, /* packed buffer or vector not 16-byte aligned  */
+	FLS_ERR_CUDA          = 4, /* a CUDA runtime call failed (see message)      */
+	FLS_ERR_DEVICE        = 5, /* a kernel reported bad metadata / bad input    */
+	FLS_ERR_TIMEOUT       = 6, /* a bounded device wait gave up                 */
+	FLS_ERR_UNSUPPORTED   = 7, /* combination not supported (e.g. layouts mix)  */
+	FLS_ERR_CAPACITY      = 8, /* output / workspace too small                  */
+	FLS_ERR_NO_DEVICE     = 9  /* no CUDA device, or not an sm_100 device       */
+} fls_status;
+
+/* Per-vector encodings.  FOR with bw 0 is a constant vector too; CONST is the
+ * explicit zero-payload form. */
+typedef enum fls_scheme {
+	FLS_SCHEME_FOR   = 0, /* FOR base + FastLanes bit-packing (pack.cpp)             */
+	FLS_SCHEME_DELTA = 1, /* 32 lane bases + packed deltas (transpose+unrsum+pack)   */
+	FLS_SCHEME_RLE   = 2, /* run index as bw-1 transposed delta + packed run values  */
+	FLS_SCHEME_CONST = 3, /* single value, no payload                                */
+	FLS_SCHEME_DICT  = 4, /* bit-packed codes + packed sorted dictionary             */
+	FLS_N_SCHEMES    = 5
+} fls_scheme;
+
+/* Row order of a column's 1024-value vectors.  NORMAL: lane i, row r holds
+ * value 32r+i (pack.cpp).  TRANSPOSED: FastLanes transposed order
+ * (transpose.cpp:4110); DELTA and RLE vectors are always transposed.  All
+ * columns of one query must share a layout so that rows line up. */
+typedef enum fls_layout { FLS_LAYOUT_NORMAL = 0, FLS_LAYOUT_TRANSPOSED = 1 } fls_layout;
+
+/* Order of fls_decode_u32 output for transposed columns. */
+typedef enum fls_order { FLS_ORDER_STORED = 0, FLS_ORDER_ORIGINAL = 1 } fls_order;
+
+/* Per-vector metadata (16 bytes), the generalisation of the reference's
+ * per-vector {bw, base, offset} arrays (fastlanes/src/ssb/compress_ssb.cu:372-454). */
+typedef struct fls_vec_meta {
+	uint64_t offset; /* word offset of the vector's payload (multiple of 4) */
+	int32_t  base;   /* FOR base / minimum of the dictionary              */
+	uint8_t  scheme; /* fls_scheme                                        */
+	uint8_t  bw;     /* bit width of the packed values / deltas / dict    */
+	uint16_t aux;    /* RLE: number of runs; DICT: dictionary size        */
+} fls_vec_meta;
+
+/* An encoded column resident in device memory.  With meta == NULL the column
+ * is "uniform" like the reference's (one scheme/bw/base for all vectors,
+ * vector v at word 32*bw*v for FOR, (32+32*bw)*v for DELTA). */
+typedef struct fls_column {
+	const uint32_t*     data;          /* device, 16-byte aligned packed words   */
+	const fls_vec_meta* meta;          /* device, n_vec entries, or NULL         */
+	uint64_t            n_values;      /* rows (the last vector may be partial)  */
+	uint64_t            n_words;       /* size of data in words (bounds checks)  */
+	uint32_t            layout;        /* fls_layout                             */
+	uint32_t            scheme;        /* uniform columns: FOR or DELTA          */
+	uint32_t            bw;            /* uniform columns                        */
+	int32_t             base;          /* uniform columns (FOR)                  */
+	uint32_t            max_vec_words; /* largest vector payload, in words       */
+	uint32_t            scheme_mask;   /* bit s set if scheme s occurs           */
+} fls_column;
+
+/* ---------------------------------------------------------------- errors */
+
+/* Human-readable text of the last error raised on this host thread. */
+const char* fls_last_error(void);
+/* Synchronise `stream`, then read and clear the device error word.
+ * Returns FLS_OK, FLS_ERR_DEVICE or FLS_ERR_TIMEOUT. */
+fls_status fls_check_device_error(fls_stream_t stream);
+
+/* ------------------------------------------------- host encoders (CPU) */
+
+/* fastlanes/src/pack.cpp:29607 generated::pack::fallback::scalar::pack(u32):
+ * packs one 1024-value vector into 32*bw words. */
+fls_status fls_pack_u32(const uint32_t* in, uint32_t* out, uint8_t bw);
+/* fastlanes/src/transpose.cpp:4110 transpose_i (u32). */
+fls_status fls_transpose_i_u32(const uint32_t* in, uint32_t* out);
+/* Inverse of transpose_i.  (The reference's transpose_o, transpose.cpp:5136,
+ * applies the same permutation as transpose_i and is not its inverse.) */
+fls_status fls_untranspose_u32(const uint32_t* in, uint32_t* out);
+/* fastlanes/src/unrsum.cpp:120 unrsum (u32). */
+fls_status fls_unrsum_u32(const uint32_t* in, uint32_t* out);
+/* fastlanes/src/include/fls_gen/rle/rle.hpp:29 VECTOR_RLE; returns the total
+ * dictionary size in *n_dict. */
+fls_status fls_vector_rle(const int32_t* vec, uint8_t* idx, int32_t* dict, uint16_t* dict4, uint32_t* n_dict);
+
+/* Worst-case payload words of a column of n values (any scheme mix). */
+uint64_t fls_encode_bound_words(uint64_t n_values);
+
+/* Encodes a uniform (reference-style) column: FOR with one base and bit width
+ * for all vectors (fls_q11.cu:187-223), or DELTA with one delta bit width
+ * (delta_shared_memory.cu:142-157).  bw = 0xff picks the smallest bit width
+ * that fits; base is the FOR base (ignored for DELTA).  Values past n are
+ * padded with the last value.  out: host, fls_encode_bound_words(n) words. */
+fls_status fls_encode_uniform(const int32_t* values, uint64_t n, uint32_t scheme, uint32_t layout, uint8_t bw,
+                              int32_t base, uint32_t* out, uint64_t* out_words, uint8_t* out_bw);
+
+/* Encodes a column vector by vector with the given per-vector schemes
+ * (schemes == NULL: every vector uses `scheme`).  Writes payload words and one
+ * fls_vec_meta per vector (offsets relative to `out`).  round4 rounds FOR bit
+ * widths up to a multiple of 4 (ssb_utils.h:222-239 find_bw).  A scheme that
+ * cannot represent a vector (CONST on a non-constant vector) falls back to FOR. */
+fls_status fls_encode_column(const int32_t* values, uint64_t n, const uint8_t* schemes, uint32_t scheme,
+                             uint32_t layout, int round4, uint32_t* out, uint64_t* out_words, fls_vec_meta* meta,
+                             uint32_t* max_vec_words, uint32_t* scheme_mask);
+
+/* Exhaustive per-vector encoder (the selector's judge): exact encoded size in
+ * bytes (payload + 16 B metadata) of every scheme for every vector
+ * (sizes: n_vec*5, UINT32_MAX = not representable) and the argmin scheme, ties
+ * broken by the decode-cost order CONST < FOR < DICT < RLE < DELTA. */
+fls_status fls_encode_exhaustive(const int32_t* values, uint64_t n, uint32_t* sizes, uint8_t* best, int n_threads);
+
+/* The 16 per-vector statistics the learned selector reads (n_vec*16 floats). */
+fls_status fls_vector_stats(const int32_t* values, uint64_t n, float* stats16, int n_threads);
+
+/* ------------------------------------------------------ decode (device) */
+
+/* fastlanes/src/include/fls_gen/unpack/unpack.cuh:3436 unpack_global and
+ * fastlanes/src/delta_global_memory.cu:24 (delta to global memory): decodes
+ * every vector of `col` into d_out (n_vec*1024 values, device).  Transposed
+ * columns are written in stored (transposed) order, as the reference does, or
+ * in original order. */
+fls_status fls_decode_u32(const fls_column* col, uint32_t* d_out, uint32_t order, fls_stream_t stream);
+
+/* fastlanes/src/bitpack_shared_memory.cu:21 / bitpack_register.cu:21 /
+ * delta_shared_memory.cu:24 QueryKernel: decode fused with a sum; *d_sum
+ * (device) receives the uint64 sum of all n_values decoded values. */
+fls_status fls_decode_sum_u32(const fls_column* col, uint64_t* d_sum, fls_stream_t stream);
+
+/* ------------------------------------------------------ queries (device) */
+
+#define FLS_MAX_QUERY_COLS 8
+#define FLS_MAX_FILTERS    4
+#define FLS_MAX_PROBES     4
+
+typedef struct fls_filter {
+	uint32_t col; /* index into cols                        */
+	int32_t  lo;  /* keep rows with lo <= value <= hi (int32) */
+	int32_t  hi;
+} fls_filter;
+
+/* fastlanes/src/ssb/fls_q11.cu:29-81 QueryKernel_v1: filters (BlockPred*,
+ * crystal-opt/pred.cuh) ANDed together, then sum(a) or sum(a*b) in int64
+ * over the selected rows (BlockSum, crystal-opt/reduce.cuh:26). */
+typedef struct fls_filter_agg_desc {
+	const fls_column* cols; /* host array of n_cols column descriptors */
+	uint32_t          n_cols;
+	fls_filter        filters[FLS_MAX_FILTERS];
+	uint32_t          n_filters;
+	int32_t           agg_a; /* column summed; -1 = count rows            */
+	int32_t           agg_b; /* if >= 0: sum of a*b                       */
+} fls_filter_agg_desc;
+
+/* *d_result (device int64) receives the aggregate. */
+fls_status fls_query_filter_agg(const fls_filter_agg_desc* desc, int64_t* d_result, fls_stream_t stream);
+
+/* crystal-opt/join.cuh:190-334 BlockBuildSelectivePHT_1/_2 as driven by
+ * fls_q21.cu:197-263 build_hashtable_{s,p,d}: rows with
+ * (d_filter == NULL || d_filter[i] == filter_eq) insert key (PHT_1, d_vals ==
+ * NULL: ht[h] = key) or (key, value) (PHT_2: ht[2h] = key, ht[2h+1] = value) at
+ * h = (key - keys_min) % ht_len.  d_ht (device, ht_len or 2*ht_len int32) must
+ * be zeroed by the caller (fls_q21.cu:293-297). */
+fls_status fls_pht_build(const int32_t* d_filter, int32_t filter_eq, const int32_t* d_keys, const int32_t* d_vals,
+                         uint64_t n, int32_t* d_ht, int32_t ht_len, int32_t keys_min, fls_stream_t stream);
+
+typedef struct fls_probe {
+	uint32_t       col;      /* probed foreign-key column                        */
+	const int32_t* ht;       /* device hash table                                */
+	int32_t        ht_len;   /* slots                                            */
+	int32_t        keys_min; /* HASH(X,Y,Z) = (X-Z)%Y, crystal-opt/join.cuh:26     */
+	int32_t        kind;     /* 1 = PHT_1 (semi-join), 2 = PHT_2 (returns value)  */
+} fls_probe;
+
+/* fastlanes/src/ssb/fls_q21.cu:21-78 probe_v1: probes in order (each AND-ed
+ * into the selection), then group g = (val[key_a]*group_mul + val[key_b] -
+ * group_sub) % n_groups with val[] the PHT_2 payloads, and the reference's
+ * result layout: d_res[4g] = val[key_b], d_res[4g+1] = val[key_a], and an
+ * int64 sum of column agg at d_res[4g+2..3].  d_res (device, 4*n_groups int32)
+ * is zeroed by this call. */
+typedef struct fls_join_agg_desc {
+	const fls_column* cols;
+	uint32_t          n_cols;
+	fls_probe         probes[FLS_MAX_PROBES];
+	uint32_t          n_probes;
+	uint32_t          agg_col;
+	int32_t           key_a, key_b; /* indices into probes (kind 2)  */
+	int32_t           group_mul, group_sub, n_groups;
+} fls_join_agg_desc;
+
+fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res, fls_stream_t stream);
+
+/* --------------------------------------------------------- tuning */
+
+/* Launch shape of the staged decode/query kernels: warps per CTA, pipeline
+ * stages per warp and CTAs per SM (0 = library default).  Used by the
+ * autotuner; applies to subsequent calls from all threads. */
+fls_status fls_set_launch_config(uint32_t warps_per_cta, uint32_t stages, uint32_t ctas_per_sm);
+fls_status fls_get_launch_config(uint32_t* warps_per_cta, uint32_t* stages, uint32_t* ctas_per_sm);
+
+/* Number of kernels this library has launched in this process (all threads). */
+uint64_t fls_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLS_GPU_H */

@@ -1,0 +1,455 @@
+/*
+ * fls_oracle.c -- TEST INFRASTRUCTURE ONLY.  CPU restatement of the reference's
+ * FastLanes decode + Crystal query path; see fls_oracle.h for what pins it.
+ * Loaded only by tests/, the smoke entry point and bench.py's CPU baseline.
+ */
+#include "fls_oracle.h"
+
+#include <stdlib.h>
+#include <string.h>
+
+/* ---- layout ------------------------------------------------------------ */
+
+static const uint32_t k_row_quad[4] = {0, 2, 1, 3};
+
+uint32_t orc_tpos(uint32_t j) {
+	/* transpose.cpp:4110-4135 (and the row order of rsum.cuh:4-107): chunk c of
+	 * 32 consecutive values lands in one lane, visited in rsum row order. */
+	uint32_t c    = j >> 5, s = j & 31u;
+	uint32_t lane = (c >> 1) | ((c & 1u) << 4);
+	uint32_t row  = 4u * (s & 7u) + k_row_quad[s >> 3];
+	return 32u * row + lane;
+}
+
+void orc_transpose_i(const uint32_t* in, uint32_t* out) {
+	for (uint32_t j = 0; j < 1024; ++j) { out[orc_tpos(j)] = in[j]; }
+}
+
+void orc_untranspose(const uint32_t* in, uint32_t* out) {
+	for (uint32_t j = 0; j < 1024; ++j) { out[j] = in[orc_tpos(j)]; }
+}
+
+/* ---- bit-packing -------------------------------------------------------- */
+
+unsigned orc_bit_width(uint32_t v) {
+	unsigned bw = 0;
+	while (v) { ++bw; v >>= 1; }
+	return bw;
+}
+
+static uint32_t mask_of(unsigned bw) { return bw >= 32 ? 0xffffffffu : ((1u << bw) - 1u); }
+
+void orc_pack(const uint32_t* in, uint32_t* out, unsigned bw) {
+	/* pack.cpp:1954-1990: lane i packs rows r = 0..31 of in[32r+i] LSB-first into
+	 * its own word stream; word k of lane i is out[32k+i]. */
+	if (bw == 0) { return; }
+	const uint32_t m = mask_of(bw);
+	memset(out, 0, sizeof(uint32_t) * 32u * bw);
+	for (uint32_t lane = 0; lane < 32; ++lane) {
+		for (uint32_t r = 0; r < 32; ++r) {
+			uint64_t v   = in[32u * r + lane] & m;
+			uint32_t bit = r * bw, k = bit >> 5, sh = bit & 31u;
+			out[32u * k + lane] |= (uint32_t)(v << sh);
+			if (sh + bw > 32) { out[32u * (k + 1) + lane] |= (uint32_t)(v >> (32u - sh)); }
+		}
+	}
+}
+
+void orc_unpack(const uint32_t* in, uint32_t* out, unsigned bw) {
+	/* unpack.cuh:201-279: inverse of orc_pack; a value that straddles words k and
+	 * k+1 takes its high bits from the low bits of word k+1. */
+	const uint32_t m = mask_of(bw);
+	for (uint32_t lane = 0; lane < 32; ++lane) {
+		for (uint32_t r = 0; r < 32; ++r) {
+			if (bw == 0) { out[32u * r + lane] = 0; continue; }
+			uint32_t bit = r * bw, k = bit >> 5, sh = bit & 31u;
+			uint64_t w   = in[32u * k + lane];
+			if (sh + bw > 32) { w |= (uint64_t)in[32u * (k + 1) + lane] << 32; }
+			out[32u * r + lane] = (uint32_t)(w >> sh) & m;
+		}
+	}
+}
+
+void orc_unpack_quarter(const uint32_t* in_quarter, uint32_t* out256, unsigned bw) {
+	/* hardcoded_16.cuh:436-786 decodes rows 8q..8q+7 from in = vec + q*bw*8; for
+	 * bw % 4 == 0 those rows start on a word boundary of every lane stream. */
+	const uint32_t m = mask_of(bw);
+	for (uint32_t lane = 0; lane < 32; ++lane) {
+		for (uint32_t r = 0; r < 8; ++r) {
+			if (bw == 0) { out256[32u * r + lane] = 0; continue; }
+			uint32_t bit = r * bw, k = bit >> 5, sh = bit & 31u;
+			uint64_t w   = in_quarter[32u * k + lane];
+			if (sh + bw > 32) { w |= (uint64_t)in_quarter[32u * (k + 1) + lane] << 32; }
+			out256[32u * r + lane] = (uint32_t)(w >> sh) & m;
+		}
+	}
+}
+
+/* ---- delta over the transposed layout ----------------------------------- */
+
+/* Row visited at step s of a lane's running sum (rsum.cuh:4-107). */
+static uint32_t rsum_row(uint32_t s) { return 4u * (s & 7u) + k_row_quad[s >> 3]; }
+
+void orc_unrsum(const uint32_t* in, uint32_t* out) {
+	/* unrsum.cpp:120-256: per lane, the difference to the previous row in rsum
+	 * order; row 0 gets 0 (its value is the lane's base). */
+	for (uint32_t lane = 0; lane < 32; ++lane) {
+		uint32_t prev = in[lane];
+		out[lane]     = 0;
+		for (uint32_t s = 1; s < 32; ++s) {
+			uint32_t p = 32u * rsum_row(s) + lane;
+			out[p]     = in[p] - prev;
+			prev       = in[p];
+		}
+	}
+}
+
+void orc_rsum(const uint32_t* deltas, uint32_t* out, const uint32_t* base) {
+	/* rsum.cuh:4-107: lane i starts at base[i] and accumulates in rsum order. */
+	for (uint32_t lane = 0; lane < 32; ++lane) {
+		uint32_t acc = base[lane];
+		for (uint32_t s = 0; s < 32; ++s) {
+			uint32_t p = 32u * rsum_row(s) + lane;
+			acc += deltas[p];
+			out[p] = acc;
+		}
+	}
+}
+
+/* ---- reference RLE ------------------------------------------------------- */
+
+static uint32_t rle_minivec(const int32_t* v, uint8_t* idx, int32_t* dict) {
+	/* rle.hpp:8-25 */
+	int32_t  cur = v[0];
+	uint32_t ci  = 0;
+	idx[0]       = 0;
+	dict[0]      = cur;
+	for (uint32_t i = 1; i < 256; ++i) {
+		if (v[i] != cur) {
+			++ci;
+			dict[ci] = v[i];
+			cur      = v[i];
+		}
+		idx[i] = (uint8_t)ci;
+	}
+	return ci + 1;
+}
+
+int orc_vector_rle(const int32_t* vec, uint8_t* idx, int32_t* dict, uint16_t* dict4) {
+	/* rle.hpp:28-41: four 256-value mini-vectors, dictionaries concatenated. */
+	dict4[0] = 0;
+	for (uint32_t m = 0; m < 4; ++m) {
+		uint32_t n = rle_minivec(vec + 256u * m, idx + 256u * m, dict + dict4[m]);
+		if (m < 3) {
+			dict4[m + 1] = (uint16_t)(dict4[m] + n);
+		} else {
+			return (int)(dict4[3] + n);
+		}
+	}
+	return 0;
+}
+
+/* ---- encoded-vector schemes ---------------------------------------------- */
+
+static uint32_t pad4(uint32_t w) { return (w + 3u) & ~3u; }
+
+static unsigned round_up4(unsigned bw) { return bw == 0 ? 0 : ((bw + 3u) & ~3u); }
+
+/* Sequential LSB-first bit-packing of n values (the dictionary stream). */
+static uint32_t pack_seq(const uint32_t* v, uint32_t n, unsigned bw, uint32_t* out) {
+	uint32_t words = pad4((n * bw + 31u) / 32u);
+	memset(out, 0, sizeof(uint32_t) * words);
+	if (bw == 0) { return words; }
+	for (uint32_t k = 0; k < n; ++k) {
+		uint64_t x   = v[k] & mask_of(bw);
+		uint32_t bit = k * bw, w = bit >> 5, sh = bit & 31u;
+		out[w] |= (uint32_t)(x << sh);
+		if (sh + bw > 32) { out[w + 1] |= (uint32_t)(x >> (32u - sh)); }
+	}
+	return words;
+}
+
+static uint32_t unpack_seq_one(const uint32_t* in, uint32_t k, unsigned bw) {
+	if (bw == 0) { return 0; }
+	uint32_t bit = k * bw, w = bit >> 5, sh = bit & 31u;
+	uint64_t x   = in[w];
+	if (sh + bw > 32) { x |= (uint64_t)in[w + 1] << 32; }
+	return (uint32_t)(x >> sh) & mask_of(bw);
+}
+
+static int cmp_i32(const void* a, const void* b) {
+	int32_t x = *(const int32_t*)a, y = *(const int32_t*)b;
+	return (x > y) - (x < y);
+}
+
+static void min_max(const int32_t* in, uint32_t n, int32_t* mn, int32_t* mx) {
+	*mn = in[0];
+	*mx = in[0];
+	for (uint32_t i = 1; i < n; ++i) {
+		if (in[i] < *mn) { *mn = in[i]; }
+		if (in[i] > *mx) { *mx = in[i]; }
+	}
+}
+
+/* Global run index of every value: rle.hpp's local index plus the offset of
+ * its mini-vector's dictionary. */
+static uint32_t rle_global(const int32_t* in, uint32_t* gidx, int32_t* dict) {
+	uint8_t  idx[1024];
+	uint16_t d4[4];
+	uint32_t n = (uint32_t)orc_vector_rle(in, idx, dict, d4);
+	for (uint32_t j = 0; j < 1024; ++j) { gidx[j] = (uint32_t)d4[j >> 8] + idx[j]; }
+	return n;
+}
+
+int orc_encode_vec(const int32_t* in, uint32_t scheme, int transposed, int round4, uint32_t* out, orc_vec* meta) {
+	int32_t mn, mx;
+	min_max(in, 1024, &mn, &mx);
+	memset(meta, 0, sizeof(*meta));
+	meta->scheme = scheme;
+	uint32_t tmp[1024], tr[1024];
+	switch (scheme) {
+	case ORC_CONST:
+		if (mn != mx) { return -1; }
+		meta->base = mn;
+		return 0;
+	case ORC_FOR: {
+		/* FOR (subtract the vector minimum, ssb_utils.h:187-205) then bit-pack
+		 * at the range's bit width (optionally rounded up as find_bw does,
+		 * ssb_utils.h:222-239). */
+		unsigned bw = orc_bit_width((uint32_t)mx - (uint32_t)mn);
+		if (round4) { bw = round_up4(bw); }
+		for (uint32_t j = 0; j < 1024; ++j) { tmp[j] = (uint32_t)in[j] - (uint32_t)mn; }
+		if (transposed) {
+			orc_transpose_i(tmp, tr);
+			memcpy(tmp, tr, sizeof(tmp));
+		}
+		orc_pack(tmp, out, bw);
+		meta->base    = mn;
+		meta->bw      = bw;
+		meta->n_words = 32u * bw;
+		return 0;
+	}
+	case ORC_DELTA: {
+		/* delta_shared_memory.cu:142-157: transpose_i, unrsum, bases = first 32
+		 * transposed values, pack the deltas. */
+		uint32_t d[1024];
+		orc_transpose_i((const uint32_t*)in, tr);
+		orc_unrsum(tr, d);
+		uint32_t mxd = 0;
+		for (uint32_t j = 0; j < 1024; ++j) {
+			if (d[j] > mxd) { mxd = d[j]; }
+		}
+		unsigned bw = orc_bit_width(mxd);
+		memcpy(out, tr, sizeof(uint32_t) * 32);
+		orc_pack(d, out + 32, bw);
+		meta->bw      = bw;
+		meta->n_words = 32u + 32u * bw;
+		return 0;
+	}
+	case ORC_RLE: {
+		/* Run index (rle.hpp) as a transposed delta at bit width 1 with 16-bit
+		 * lane bases, followed by the FOR'd run values packed sequentially. */
+		uint32_t gidx[1024], d[1024];
+		int32_t  dict[1024];
+		uint32_t n = rle_global(in, gidx, dict);
+		orc_transpose_i(gidx, tr);
+		orc_unrsum(tr, d);
+		uint16_t* b16 = (uint16_t*)out;
+		for (uint32_t l = 0; l < 32; ++l) { b16[l] = (uint16_t)tr[l]; }
+		orc_pack(d, out + 16, 1);
+		int32_t dmn, dmx;
+		min_max(dict, n, &dmn, &dmx);
+		unsigned bw = orc_bit_width((uint32_t)dmx - (uint32_t)dmn);
+		for (uint32_t k = 0; k < n; ++k) { tmp[k] = (uint32_t)dict[k] - (uint32_t)dmn; }
+		uint32_t dw   = pack_seq(tmp, n, bw, out + 48);
+		meta->base    = dmn;
+		meta->bw      = bw;
+		meta->aux     = n;
+		meta->n_words = 48u + dw;
+		return 0;
+	}
+	case ORC_DICT: {
+		/* Sorted distinct values as a FOR'd sequentially packed dictionary,
+		 * codes FastLanes bit-packed at bit_width(n_dict - 1). */
+		int32_t sorted[1024];
+		memcpy(sorted, in, sizeof(sorted));
+		qsort(sorted, 1024, sizeof(int32_t), cmp_i32);
+		uint32_t n = 0;
+		for (uint32_t j = 0; j < 1024; ++j) {
+			if (j == 0 || sorted[j] != sorted[j - 1]) { sorted[n++] = sorted[j]; }
+		}
+		unsigned cbw = orc_bit_width(n - 1);
+		for (uint32_t j = 0; j < 1024; ++j) {
+			uint32_t lo = 0, hi = n - 1;
+			while (lo < hi) {
+				uint32_t mid = (lo + hi) >> 1;
+				if (sorted[mid] < in[j]) {
+					lo = mid + 1;
+				} else {
+					hi = mid;
+				}
+			}
+			tmp[j] = lo;
+		}
+		if (transposed) {
+			orc_transpose_i(tmp, tr);
+			memcpy(tmp, tr, sizeof(tmp));
+		}
+		orc_pack(tmp, out, cbw);
+		unsigned bw = orc_bit_width((uint32_t)sorted[n - 1] - (uint32_t)sorted[0]);
+		for (uint32_t k = 0; k < n; ++k) { tmp[k] = (uint32_t)sorted[k] - (uint32_t)sorted[0]; }
+		uint32_t dw   = pack_seq(tmp, n, bw, out + 32u * cbw);
+		meta->base    = sorted[0];
+		meta->bw      = bw;
+		meta->aux     = n;
+		meta->n_words = 32u * cbw + dw;
+		return 0;
+	}
+	default: return -1;
+	}
+}
+
+void orc_decode_vec(const uint32_t* in, const orc_vec* meta, int transposed, int32_t* out) {
+	uint32_t v[1024], t[1024];
+	switch (meta->scheme) {
+	case ORC_CONST:
+		for (uint32_t j = 0; j < 1024; ++j) { out[j] = meta->base; }
+		return;
+	case ORC_FOR:
+		orc_unpack(in, v, meta->bw);
+		if (transposed) {
+			orc_untranspose(v, t);
+			memcpy(v, t, sizeof(v));
+		}
+		for (uint32_t j = 0; j < 1024; ++j) { out[j] = (int32_t)(v[j] + (uint32_t)meta->base); }
+		return;
+	case ORC_DELTA:
+		orc_unpack(in + 32, v, meta->bw);
+		orc_rsum(v, t, in);
+		orc_untranspose(t, (uint32_t*)out);
+		return;
+	case ORC_RLE: {
+		uint32_t        base[32];
+		const uint16_t* b16 = (const uint16_t*)in;
+		for (uint32_t l = 0; l < 32; ++l) { base[l] = b16[l]; }
+		orc_unpack(in + 16, v, 1);
+		orc_rsum(v, t, base);
+		orc_untranspose(t, v);
+		for (uint32_t j = 0; j < 1024; ++j) {
+			out[j] = (int32_t)(unpack_seq_one(in + 48, v[j], meta->bw) + (uint32_t)meta->base);
+		}
+		return;
+	}
+	case ORC_DICT: {
+		unsigned cbw = orc_bit_width(meta->aux - 1);
+		orc_unpack(in, v, cbw);
+		if (transposed) {
+			orc_untranspose(v, t);
+			memcpy(v, t, sizeof(v));
+		}
+		for (uint32_t j = 0; j < 1024; ++j) {
+			out[j] = (int32_t)(unpack_seq_one(in + 32u * cbw, v[j], meta->bw) + (uint32_t)meta->base);
+		}
+		return;
+	}
+	default: memset(out, 0, sizeof(int32_t) * 1024);
+	}
+}
+
+void orc_scheme_sizes(const int32_t* in, uint32_t* size5) {
+	uint32_t buf[4096];
+	orc_vec  m;
+	for (uint32_t s = 0; s < 5; ++s) {
+		if (orc_encode_vec(in, s, 1, 0, buf, &m) != 0) {
+			size5[s] = 0xffffffffu;
+		} else {
+			size5[s] = 4u * m.n_words + 16u;
+		}
+	}
+}
+
+/* ---- query path ---------------------------------------------------------- */
+
+int64_t orc_filter_agg(const int32_t* date, const int32_t* disc, const int32_t* qty, const int32_t* price,
+                       uint64_t n, int32_t date_lo, int32_t date_hi, int32_t disc_lo, int32_t disc_hi,
+                       int32_t qty_lt) {
+	/* fls_q11.cu:49-72: predicates on date, quantity and discount, then
+	 * sum += price * discount over the selected rows (64-bit products). */
+	int64_t sum = 0;
+	for (uint64_t t = 0; t < n; ++t) {
+		int f = date[t] >= date_lo && date[t] <= date_hi;
+		f     = f && qty[t] < qty_lt;
+		f     = f && disc[t] >= disc_lo && disc[t] <= disc_hi;
+		if (f) { sum += (int64_t)price[t] * (int64_t)disc[t]; }
+	}
+	return sum;
+}
+
+/* HASH(X,Y,Z) ((X-Z) % Y), join.cuh:26; a negative remainder is out of the
+ * table in the reference (undefined there) and a miss here. */
+static int pht_hash(int32_t key, int32_t len, int32_t keys_min, int32_t* h) {
+	int32_t x = (int32_t)((uint32_t)key - (uint32_t)keys_min) % len;
+	if (x < 0) { return 0; }
+	*h = x;
+	return 1;
+}
+
+void orc_pht1_build(const int32_t* filter, int32_t filter_eq, const int32_t* keys, uint64_t n, int32_t* ht,
+                    int32_t len, int32_t keys_min) {
+	/* join.cuh:190-245: atomicCAS(&ht[hash], 0, key) for selected rows. */
+	for (uint64_t t = 0; t < n; ++t) {
+		int32_t h;
+		if (filter && filter[t] != filter_eq) { continue; }
+		if (!pht_hash(keys[t], len, keys_min, &h)) { continue; }
+		if (ht[h] == 0) { ht[h] = keys[t]; }
+	}
+}
+
+void orc_pht2_build(const int32_t* filter, int32_t filter_eq, const int32_t* keys, const int32_t* vals, uint64_t n,
+                    int32_t* ht, int32_t len, int32_t keys_min) {
+	/* join.cuh:255-275: atomicCAS on the key word, then store the value.  With
+	 * distinct keys (a perfect hash) the outcome does not depend on order. */
+	for (uint64_t t = 0; t < n; ++t) {
+		int32_t h;
+		if (filter && filter[t] != filter_eq) { continue; }
+		if (!pht_hash(keys[t], len, keys_min, &h)) { continue; }
+		if (ht[2 * h] == 0) { ht[2 * h] = keys[t]; }
+		ht[2 * h + 1] = vals[t];
+	}
+}
+
+void orc_probe_groupby(const int32_t* supp, const int32_t* part, const int32_t* date, const int32_t* rev, uint64_t n,
+                       const int32_t* ht_s, int32_t s_len, const int32_t* ht_p, int32_t p_len, const int32_t* ht_d,
+                       int32_t d_len, int32_t d_keys_min, int32_t* res) {
+	/* fls_q21.cu:50-77 with the probes of join.cuh:28-188 (PHT_1: slot != 0;
+	 * PHT_2: the (key,value) pair read as one u64, value = slot >> 32). */
+	const int32_t n_grp = (1998 - 1992 + 1) * (5 * 5 * 40);
+	for (uint64_t t = 0; t < n; ++t) {
+		int32_t  h;
+		uint64_t slot;
+		if (!pht_hash(supp[t], s_len, 0, &h) || ht_s[h] == 0) { continue; }
+		if (!pht_hash(part[t], p_len, 0, &h)) { continue; }
+		memcpy(&slot, &ht_p[2 * (int64_t)h], 8);
+		if (slot == 0) { continue; }
+		int32_t brand = (int32_t)(slot >> 32);
+		if (!pht_hash(date[t], d_len, d_keys_min, &h)) { continue; }
+		memcpy(&slot, &ht_d[2 * (int64_t)h], 8);
+		if (slot == 0) { continue; }
+		int32_t year = (int32_t)(slot >> 32);
+		int32_t g    = (brand * 7 + (year - 1992)) % n_grp;
+		if (g < 0) { continue; }
+		res[4 * g]     = year;
+		res[4 * g + 1] = brand;
+		uint64_t acc;
+		memcpy(&acc, &res[4 * g + 2], 8);
+		acc += (uint64_t)(int64_t)rev[t];
+		memcpy(&res[4 * g + 2], &acc, 8);
+	}
+}
+
+uint64_t orc_splitmix64(uint64_t* state) {
+	uint64_t z = (*state += 0x9e3779b97f4a7c15ull);
+	z          = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+	z          = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+	return z ^ (z >> 31);
+}

@@ -1,0 +1,100 @@
+/*
+ * fls_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatement of the reference's FastLanes decode + Crystal query path, used
+ * as the parity checker for the CUDA library.  Only tests/, the smoke entry point
+ * and bench.py's CPU-baseline leg may load it; the product never does.
+ *
+ * Parity is pinned against the reference itself: tests compare every function
+ * here with the reference's own code compiled from its sources
+ * (oracle/_ref/libflsref.so: pack.cpp, transpose.cpp, unrsum.cpp, unpack.cuh,
+ * unpack_fused.cuh, hardcoded_16.cuh, rsum.cuh, rle.hpp) and with its golden
+ * arrays (generated/cuda/normal_t32_uf1/..._unpack_helper.hpp), and the
+ * committed fixtures under tests/golden/ were produced by that library.
+ *
+ * All functions work on one 1024-value vector unless stated otherwise.
+ */
+#ifndef FLS_ORACLE_H
+#define FLS_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- layout ------------------------------------------------------------ */
+/* Position of original index j (0..1023) in the FastLanes transposed order
+ * (transpose.cpp:4110): lane (c>>1)|((c&1)<<4) holds chunk c = j/32 and
+ * s = j%32 sits at row 4*(s&7) + {0,2,1,3}[s>>3]; position = 32*row + lane. */
+uint32_t orc_tpos(uint32_t j);
+void     orc_transpose_i(const uint32_t* in, uint32_t* out);   /* out[tpos(j)] = in[j] */
+void     orc_untranspose(const uint32_t* in, uint32_t* out);   /* out[j] = in[tpos(j)] */
+
+/* ---- bit-packing (pack.cpp:1954-1990, unpack.cuh:201-279) --------------- */
+unsigned orc_bit_width(uint32_t max_value);
+void     orc_pack(const uint32_t* in, uint32_t* out, unsigned bw);   /* out: 32*bw words */
+void     orc_unpack(const uint32_t* in, uint32_t* out, unsigned bw); /* out: 1024 values */
+/* rows [8q, 8q+8) of every lane from a quarter pointer in = vec + q*bw*8
+ * (hardcoded_16.cuh:436-786; valid for bw % 4 == 0) */
+void     orc_unpack_quarter(const uint32_t* in_quarter, uint32_t* out256, unsigned bw);
+
+/* ---- delta over the transposed layout (unrsum.cpp:120, rsum.cuh:4) ------ */
+void orc_unrsum(const uint32_t* in_transposed, uint32_t* out_deltas);
+void orc_rsum(const uint32_t* deltas, uint32_t* out_transposed, const uint32_t* base32);
+
+/* ---- reference RLE (rle.hpp:8-44) ---------------------------------------- */
+/* Returns the number of dictionary entries; idx[j] is the per-256 local run
+ * index, dict4[m] the dictionary offset of mini-vector m. */
+int orc_vector_rle(const int32_t* vec, uint8_t* idx, int32_t* dict, uint16_t* dict4);
+
+/* ---- per-vector schemes of the encoded-column format --------------------- */
+enum {
+	ORC_FOR = 0,   /* FOR + FastLanes bit-packing                          */
+	ORC_DELTA = 1, /* transposed delta: 32 base words + packed deltas       */
+	ORC_RLE = 2,   /* run index as bw-1 transposed delta + packed dict      */
+	ORC_CONST = 3, /* one value, no payload                                 */
+	ORC_DICT = 4   /* FastLanes bit-packed codes + packed sorted dictionary */
+};
+
+/* Encoded vector: payload words and the fields of its metadata entry.  The
+ * payload word counts are always multiples of 4 (16-byte aligned vectors). */
+typedef struct orc_vec {
+	uint32_t scheme, bw, aux, n_words;
+	int32_t  base;
+} orc_vec;
+
+/* Encode one vector with a given scheme (transposed selects the transposed
+ * layout for FOR/DICT codes; DELTA and RLE are always transposed).  Returns 0
+ * on success, -1 if the scheme cannot represent the vector (CONST). */
+int orc_encode_vec(const int32_t* in, uint32_t scheme, int transposed, int round4, uint32_t* out, orc_vec* meta);
+/* Decode one vector to ORIGINAL order. */
+void orc_decode_vec(const uint32_t* in, const orc_vec* meta, int transposed, int32_t* out);
+/* Exact encoded size in bytes (payload + 16 B metadata) of every scheme;
+ * size[s] = UINT32_MAX when the scheme cannot represent the vector. */
+void orc_scheme_sizes(const int32_t* in, uint32_t* size5);
+
+/* ---- query path (fls_q11.cu:49-72, fls_q21.cu:50-77, join.cuh) ----------- */
+/* Filter-aggregate over decoded int32 columns: sum of price*disc over rows with
+ * date in [date_lo,date_hi], qty < qty_lt, disc in [disc_lo,disc_hi]. */
+int64_t orc_filter_agg(const int32_t* date, const int32_t* disc, const int32_t* qty, const int32_t* price,
+                       uint64_t n, int32_t date_lo, int32_t date_hi, int32_t disc_lo, int32_t disc_hi,
+                       int32_t qty_lt);
+/* Selective perfect-hash builds (join.cuh:190-334): PHT_1 stores the key,
+ * PHT_2 stores (key, value) pairs; slot = (key - keys_min) % len. */
+void orc_pht1_build(const int32_t* filter, int32_t filter_eq, const int32_t* keys, uint64_t n, int32_t* ht,
+                    int32_t len, int32_t keys_min);
+void orc_pht2_build(const int32_t* filter, int32_t filter_eq, const int32_t* keys, const int32_t* vals, uint64_t n,
+                    int32_t* ht, int32_t len, int32_t keys_min);
+/* Probe + group-by of fls_q21.cu probe_v1: res is int32[4*7000]; group g gets
+ * res[4g]=year, res[4g+1]=brand and a uint64 revenue sum at res[4g+2]. */
+void orc_probe_groupby(const int32_t* supp, const int32_t* part, const int32_t* date, const int32_t* rev, uint64_t n,
+                       const int32_t* ht_s, int32_t s_len, const int32_t* ht_p, int32_t p_len, const int32_t* ht_d,
+                       int32_t d_len, int32_t d_keys_min, int32_t* res);
+
+/* ---- synthetic inputs (SplitMix64; shared with the Python tests) --------- */
+uint64_t orc_splitmix64(uint64_t* state);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
