@@ -52,7 +52,8 @@ struct StageCfg {
 	uint32_t  cta_extra_off;   // CTA-level scratch after all warp regions (words)
 	uint64_t  n_vec, n_values;
 	uint32_t  layout;
-	uint32_t* err; // device error word
+	uint32_t  has_dict; // per-warp dictionary scratch planned (RLE / DICT allowed)
+	uint32_t* err;      // device error word
 };
 
 __device__ __forceinline__ void raise_err(uint32_t* err, uint32_t bits) { atomicOr(err, bits); }
@@ -79,6 +80,8 @@ __device__ __forceinline__ void issue_stage(const StageCfg& cfg, const WarpStage
 	bool     ok = true;
 	if (lane < cfg.n_cols) {
 		ok = dev::vec_info(cfg.cols[lane], v, raw, vi);
+		// RLE / DICT vectors need the dictionary scratch; reject them otherwise.
+		if (ok && !cfg.has_dict && (vi.scheme == FLS_SCHEME_RLE || vi.scheme == FLS_SCHEME_DICT)) { ok = false; }
 		uint2 x;
 		if (ok) {
 			bytes = vi.words * 4u;

@@ -153,6 +153,7 @@ fls_status plan_stages(const fls_column* cols, uint32_t n_cols, uint32_t extra_w
 		dict = dict || needs_dict(cols[c]);
 	}
 	cfg.n_cols    = n_cols;
+	cfg.has_dict  = dict ? 1u : 0u;
 	cfg.n_vec     = (cfg.n_values + 1023u) / 1024u;
 	cfg.err       = device_error_word();
 	LaunchCfg lc  = launch_cfg();

@@ -47,6 +47,7 @@ def cuda():
     import torch
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
-    from fastlanesgpu_b200 import build
-    build.build()
+    from fastlanesgpu_b200 import _lib, build
+    if not os.path.exists(_lib.LIB_PATH):
+        build.build()
     return torch.device("cuda:0")
