@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Benchmark of the fused FastLanes decode + query path on B200.
+
+Headline workload (one "step" = one pass of the hot path over the table):
+fused decode + filter-aggregate over a synthetic 2^27-row fact table
+(date 12 bit, discount 4 bit, quantity 6 bit, price 24 bit, FastLanes
+bit-packed; year-1993 AND discount in [1,3] AND quantity < 25; exact int64
+sum(price*discount)) -- the Q1.1 shape of fastlanes/src/ssb/fls_q11.cu.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload q11|q21|decode]
+
+Prints ONE JSON line on rank 0.  With --gpus N > 1 it is launched under
+torchrun: each rank holds its own shard of 2^27 rows (weak scaling) and the
+per-step int64 partial aggregates are summed with one NCCL all-reduce.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["q11", "q21", "decode"], default="q11")
+    ap.add_argument("--rows", type=int, default=1 << 27)
+    ap.add_argument("--decode-bw", type=int, default=16, help="bit width of the decode workload")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+
+    def init(self, backend="nccl"):
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(self.local)
+        if self.world > 1:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples of this rank's GPU."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        import torch
+        self.proc = None
+        self.window = None
+        try:
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            sel = uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"
+        except Exception:
+            sel = str(device_index)
+        self.cmd = ["nvidia-smi", "-i", sel, f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                    "-lms", "50"]
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(self.cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        self.t_start = time.time()
+
+    def mark(self, t0: float, t1: float):
+        self.window = (t0, t1)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        rows = [r for r in csv.reader(io.StringIO(out)) if len(r) >= 9]
+        n = len(rows)
+        if n == 0:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        # nvidia-smi -lms emits at a fixed period; map samples to wall time.
+        t_end = time.time()
+        period = (t_end - self.t_start) / n
+        stamps = [self.t_start + (i + 1) * period for i in range(n)]
+        sel = [r for r, t in zip(rows, stamps) if self.window and self.window[0] <= t <= self.window[1]]
+        scope = "timed"
+        if not sel:
+            sel, scope = rows, "run"
+        sm = [float(r[1]) for r in sel if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in sel if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in sel for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sel), "window": scope}
+
+
+def measured_peak_gbs():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(key: str):
+    """DRAM bytes per launch of the dominant kernel from a committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get(key)
+    except Exception:
+        return None
+
+
+# --------------------------------------------------------------- workloads
+
+def build_q11(rows: int, seed: int):
+    from fastlanesgpu_b200 import EncodedColumn, datagen
+    t = datagen.lineorder_q11(rows, seed=seed)
+    names = ["date", "discount", "quantity", "price"]
+    cols = [EncodedColumn.uniform(t[k], bw=datagen.Q11_BITS[k]) for k in names]
+    f = datagen.Q11_FILTER
+    filters = [(0, *f["date"]), (1, *f["discount"]), (2, *f["quantity"])]
+    return t, cols, filters
+
+
+def build_q21(rows: int, seed: int):
+    from fastlanesgpu_b200 import EncodedColumn, datagen
+    t = datagen.q21_tables(rows, seed=seed)
+    names = ["lo_suppkey", "lo_partkey", "lo_orderdate", "lo_revenue"]
+    cols = [EncodedColumn.uniform(t[k], bw=datagen.Q21_BITS[k]) for k in names]
+    return t, cols
+
+
+def run_ours(a, dist: Dist):
+    import torch
+
+    from fastlanesgpu_b200 import EncodedColumn, datagen, ops
+    dev = torch.device("cuda", dist.local)
+    stream = torch.cuda.current_stream()
+    seed = 1000 * (dist.rank + 1)
+    # ---------------------------------------------------------------- setup
+    if a.workload == "q11":
+        t, hcols, filters = build_q11(a.rows, seed)
+        dcols = [c.to_device(dev) for c in hcols]
+        res = torch.zeros(1, dtype=torch.int64, device=dev)
+
+        def step():
+            ops.query_filter_agg(dcols, filters, agg_a=3, agg_b=1, out=res)
+            return res
+        workload = {"workload": "fused decode + filter-aggregate (Q1.1 shape)", "rows_per_gpu": a.rows,
+                    "columns": "date 12b, discount 4b, quantity 6b, price 24b (FastLanes bit-packed, uniform)",
+                    "predicate": "date in year 1993 AND discount in [1,3] AND quantity < 25",
+                    "aggregate": "int64 sum(price*discount)"}
+        metric_key = "q11"
+    elif a.workload == "q21":
+        t, hcols = build_q21(a.rows, seed)
+        dcols = [c.to_device(dev) for c in hcols]
+        dt = {k: torch.from_numpy(v).to(dev) for k, v in t.items() if not k.startswith("lo_")}
+        ht_s = ops.build_pht(dt["s_suppkey"], dt["s_suppkey"].numel(), filt=dt["s_region"], filter_eq=1)
+        ht_p = ops.build_pht(dt["p_partkey"], dt["p_partkey"].numel(), vals=dt["p_brand1"], filt=dt["p_category"],
+                             filter_eq=1)
+        ht_d = ops.build_pht(dt["d_datekey"], datagen.N_DAYS, vals=dt["d_year"])
+        probes = [(0, ht_s, ht_s.numel(), 0, 1), (1, ht_p, ht_p.numel() // 2, 0, 2),
+                  (2, ht_d, ht_d.numel() // 2, 0, 2)]
+        res = torch.zeros(4 * datagen.N_GROUPS, dtype=torch.int32, device=dev)
+
+        def step():
+            ops.probe_groupby(dcols, probes, 3, 1, 2, 7, 1992, datagen.N_GROUPS, out=res)
+            return res
+        workload = {"workload": "fused decode + 3-way perfect-hash probe + 7000-group int64 group-by (Q2.1 shape)",
+                    "rows_per_gpu": a.rows, "columns": "supp 17b, part 19b, date 12b, revenue 24b",
+                    "filters": "part category 1/5, supplier region 1/25"}
+        metric_key = "q21"
+    else:
+        vals = datagen.uniform_bits(a.rows, a.decode_bw, seed=seed)
+        hcols = [EncodedColumn.uniform(vals, bw=a.decode_bw)]
+        dcols = [c.to_device(dev) for c in hcols]
+        res = torch.zeros(1, dtype=torch.int64, device=dev)
+
+        def step():
+            ops.query_aggregate(dcols[0], out=res)
+            return res
+        workload = {"workload": f"decode fused with sum, bit-pack bw {a.decode_bw}", "rows_per_gpu": a.rows}
+        metric_key = f"decode_sum_bw{a.decode_bw}"
+    comp_bytes = sum(c.nbytes for c in hcols)
+
+    def collective():
+        if dist.pg:
+            dist.pg.all_reduce(res.view(torch.int64) if a.workload != "q21" else res)
+
+    # -------------------------------------------------- device-resident timing
+    clocks = ClockSampler(dist.local)
+    clocks.start()
+    for _ in range(a.warmup):
+        step()
+        collective()
+    torch.cuda.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    l0 = ops.kernel_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
+    e0.record(stream)
+    for _ in range(a.steps):
+        step()
+        collective()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    w1 = time.time()
+    dist.barrier()
+    launches = ops.kernel_launch_count() - l0
+    clocks.mark(w0, w1)
+    ms_local = e0.elapsed_time(e1)
+    ms = dist.max(ms_local)
+    ops.check_device_error()
+
+    # ------------------------------------------- end-to-end through the C ABI
+    pinned = [torch.from_numpy(c.words.view("int32")).pin_memory() for c in hcols]
+    h2d = sum(p.numel() * 4 for p in pinned)
+    d2h = res.numel() * res.element_size()
+    host_res = torch.empty_like(res, device="cpu").pin_memory()
+    n_e2e = max(3, min(a.e2e_steps, a.steps))
+    torch.cuda.synchronize()
+    dist.barrier()
+    x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    x0.record(stream)
+    for _ in range(n_e2e):
+        for dc, hp in zip(dcols, pinned):
+            dc.data.copy_(hp, non_blocking=True)
+        step()
+        collective()
+        host_res.copy_(res, non_blocking=True)
+    x1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = dist.max(x0.elapsed_time(x1)) / n_e2e
+    clk = clocks.stop()
+
+    rows_total = a.rows * dist.world
+    value = rows_total * a.steps / (ms / 1e3)
+    ms_step = ms / a.steps
+    peak, peak_src = measured_peak_gbs()
+    achieved = comp_bytes / (ms_local / a.steps / 1e3) / 1e9
+    traffic = profiled_traffic(metric_key)
+    out = {
+        "metric": "fused decode+query rows/s", "value": value, "unit": "rows/s", "n_gpus": dist.world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32->int64", "data": "synthetic (seeded)",
+        "config": {**workload, "rows_total": rows_total, "compressed_bytes_per_gpu": comp_bytes,
+                   "l2": "inputs larger than L2 (126 MB), no flush",
+                   "parallelism": f"row shards x{dist.world}, one int64 all-reduce per step" if dist.world > 1
+                   else "1 GPU"},
+        "e2e": {"value": rows_total / (e2e_ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                "path": "pinned host encoded columns -> H2D -> fused kernel (C ABI) -> D2H result"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
+                     else "fallback 6650 GB/s",
+                     "traffic": traffic, "algorithmic_bytes_per_launch": comp_bytes},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    return out, t if a.workload == "q11" else None, hcols
+
+
+def cpu_baseline_q11(a, hcols, budget_s: float):
+    """The reference's CPU implementation (its own unpack compiled from its
+    sources + the fls_q11.cu scalar loop), all host threads, on a bounded
+    prefix sample of the same table."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as orc
+    from fastlanesgpu_b200 import datagen
+    R = orc.Reference()
+    threads = os.cpu_count() or 1
+    sample = min(a.rows, 1 << 24)
+    n_vec = (sample + 1023) // 1024
+    words = [np.ascontiguousarray(c.words[:n_vec * 32 * c.bw + 4]) for c in hcols]
+    bws = [c.bw for c in hcols]
+    f = datagen.Q11_FILTER
+    args = (words, bws, sample, *f["date"], *f["discount"], f["quantity"][1] + 1, threads)
+    R.q11_sum(*args)  # warm-up
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while time.perf_counter() < t_end or len(times) < 3:
+        t0 = time.perf_counter()
+        R.q11_sum(*args)
+        times.append(time.perf_counter() - t0)
+    med = statistics.median(times)
+    return {"value": sample / med, "unit": "rows/s", "cores": threads, "kind": "reference",
+            "sample": f"first {sample} rows of the table, {len(times)} repetitions, median; reference unpack "
+                      f"(unpack_fused.cuh host-compiled) + fls_q11.cu loop, OpenMP {threads} threads"}
+
+
+def run_reference(a, dist: Dist):
+    """--impl reference: the reference's own CPU implementation of the path."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    from fastlanesgpu_b200 import datagen
+    R = orc.Reference()
+    threads = os.cpu_count() or 1
+    sample = min(a.rows, 1 << 24)
+    if a.workload != "q11":
+        raise SystemExit("--impl reference supports the q11 workload")
+    t = datagen.lineorder_q11(sample, seed=1000)
+    names = ["date", "discount", "quantity", "price"]
+    words = [R.pack_column(t[k], datagen.Q11_BITS[k], threads) for k in names]
+    bws = [datagen.Q11_BITS[k] for k in names]
+    f = datagen.Q11_FILTER
+    args = (words, bws, sample, *f["date"], *f["discount"], f["quantity"][1] + 1, threads)
+    for _ in range(max(1, min(a.warmup, 3))):
+        R.q11_sum(*args)
+    steps = max(1, min(a.steps, 10))
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        R.q11_sum(*args)
+        times.append(time.perf_counter() - t0)
+    value = sample * len(times) / sum(times)
+    return {
+        "impl": "reference", "metric": "fused decode+query rows/s", "value": value, "unit": "rows/s",
+        "n_gpus": a.gpus, "steps": steps, "warmup": max(1, min(a.warmup, 3)),
+        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32->int64", "data": "synthetic (seeded)",
+        "config": {"workload": "fused decode + filter-aggregate (Q1.1 shape)", "rows_per_gpu": a.rows,
+                   "sample_rows_per_step": sample},
+        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "reference",
+                         "sample": f"{sample} rows per step of the same table shape; the reference's unpack "
+                                   f"(host-compiled from its sources) + fls_q11.cu loop, OpenMP {threads} threads"},
+        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    a = parse_args()
+    dist = Dist()
+    if a.impl == "reference":
+        if dist.rank == 0:
+            print(json.dumps(run_reference(a, dist)), flush=True)
+        return
+    dist.init()
+    try:
+        out, _, hcols = run_ours(a, dist)
+        if dist.rank == 0:
+            if dist.world == 1 and a.workload == "q11" and not a.no_cpu_baseline:
+                out["cpu_baseline"] = cpu_baseline_q11(a, hcols, a.cpu_seconds)
+            print(json.dumps(out), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

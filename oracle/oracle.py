@@ -196,6 +196,8 @@ class Reference:
                                       + [_i32p, ctypes.c_int32] * 3 + [ctypes.c_int32, _i32p, ctypes.c_int])
         L.ref_decode_sum.restype = ctypes.c_uint64
         L.ref_decode_sum.argtypes = [_u32p, ctypes.c_uint, ctypes.c_uint64, ctypes.c_int]
+        L.ref_pack_column.restype = None
+        L.ref_pack_column.argtypes = [_u32p, ctypes.c_uint64, ctypes.c_uint, _u32p, ctypes.c_int]
         L.ref_decode.restype = ctypes.c_uint64
         L.ref_decode.argtypes = [_u32p, ctypes.c_uint, ctypes.c_uint64, _u32p, ctypes.c_int]
 
@@ -275,6 +277,12 @@ class Reference:
         self.L.ref_q21_groupby(*args, n_rows, _p(ht_s, _i32p), ht_s.size, _p(ht_p, _i32p), ht_p.size // 2,
                                _p(ht_d, _i32p), ht_d.size // 2, d_keys_min, _p(res, _i32p), threads)
         return res
+
+    def pack_column(self, values, bw, threads):
+        v = np.ascontiguousarray(values).view(np.uint32)
+        out = np.zeros(((v.size + 1023) // 1024) * 32 * bw + 4, dtype=np.uint32)
+        self.L.ref_pack_column(_p(v, _u32p), v.size, bw, _p(out, _u32p), threads)
+        return out
 
     def decode_sum(self, packed, bw, n_vec, threads):
         return int(self.L.ref_decode_sum(_p(packed, _u32p), bw, n_vec, threads))

@@ -51,6 +51,7 @@ void ref_q21_groupby(const uint32_t* supp_p, unsigned supp_bw, const uint32_t* p
                      const uint32_t* date_p, unsigned date_bw, const uint32_t* rev_p, unsigned rev_bw,
                      uint64_t n_rows, const int32_t* ht_s, int32_t s_len, const int32_t* ht_p, int32_t p_len,
                      const int32_t* ht_d, int32_t d_len, int32_t d_keys_min, int32_t* res, int n_threads);
+void ref_pack_column(const uint32_t* values, uint64_t n, unsigned bw, uint32_t* out, int n_threads);
 uint64_t ref_decode_sum(const uint32_t* packed, unsigned bw, uint64_t n_vec, int n_threads);
 uint64_t ref_decode(const uint32_t* packed, unsigned bw, uint64_t n_vec, uint32_t* out, int n_threads);
 

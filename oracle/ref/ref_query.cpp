@@ -126,3 +126,17 @@ extern "C" uint64_t ref_decode(const uint32_t* packed, unsigned bw, uint64_t n_v
 	for (uint64_t v = 0; v < n_vec; ++v) { ref_unpack_u32(packed + v * 32ull * bw, out + v * 1024, bw); }
 	return n_vec * 1024;
 }
+
+// Packs a whole column with the reference's pack.cpp, vector by vector
+// (fls_q11.cu:207-223); a partial last vector is padded with its last value.
+extern "C" void ref_pack_column(const uint32_t* values, uint64_t n, unsigned bw, uint32_t* out, int n_threads) {
+	const uint64_t n_vec = (n + 1023) / 1024;
+#pragma omp parallel for schedule(static) num_threads(n_threads)
+	for (uint64_t v = 0; v < n_vec; ++v) {
+		uint32_t       buf[1024];
+		const uint64_t cnt = (v + 1 == n_vec) ? n - v * 1024 : 1024;
+		std::memcpy(buf, values + v * 1024, cnt * sizeof(uint32_t));
+		for (uint64_t j = cnt; j < 1024; ++j) { buf[j] = buf[cnt - 1]; }
+		ref_pack_u32(buf, out + v * 32ull * bw, bw);
+	}
+}
