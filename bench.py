@@ -44,6 +44,8 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--launch", default="", help="warps,stages,ctas_per_sm,tile_bytes (0 = default)")
+    ap.add_argument("--sparse-rows", type=int, default=0, help="FLS_TUNE_SPARSE_ROWS (0 = default)")
     return ap.parse_args()
 
 
@@ -182,6 +184,10 @@ def run_ours(a, dist: Dist):
     from fastlanesgpu_b200 import EncodedColumn, datagen, ops
     dev = torch.device("cuda", dist.local)
     stream = torch.cuda.current_stream()
+    if a.launch:
+        ops.set_launch_config(*[int(x) for x in a.launch.split(",")])
+    if a.sparse_rows:
+        ops.set_tuning(0, a.sparse_rows)
     seed = 1000 * (dist.rank + 1)
     # ---------------------------------------------------------------- setup
     if a.workload == "q11":
@@ -302,6 +308,8 @@ def run_ours(a, dist: Dist):
                      else "fallback 6650 GB/s",
                      "traffic": traffic, "algorithmic_bytes_per_launch": comp_bytes},
         "gpu_launches": int(launches),
+        "launch_config": dict(zip(["warps", "stages", "ctas_per_sm", "tile_bytes"], ops.get_launch_config()),
+                              sparse_rows=ops.get_tuning(0)),
         "clocks": clk,
     }
     return out, t if a.workload == "q11" else None, hcols

@@ -22,6 +22,7 @@ SCHEME_NAMES = ["FOR", "DELTA", "RLE", "CONST", "DICT"]
 LAYOUT_NORMAL, LAYOUT_TRANSPOSED = 0, 1
 ORDER_STORED, ORDER_ORIGINAL = 0, 1
 MAX_QUERY_COLS, MAX_FILTERS, MAX_PROBES = 8, 4, 4
+TUNE_SPARSE_ROWS = 0
 
 
 class FlsError(RuntimeError):
@@ -92,9 +93,11 @@ _SIGS = {
     "fls_pht_build": (ctypes.c_int, [_VP, ctypes.c_int32, _VP, _VP, ctypes.c_uint64, _VP, ctypes.c_int32,
                                      ctypes.c_int32, _VP]),
     "fls_query_probe_groupby": (ctypes.c_int, [ctypes.POINTER(JoinAggDesc), _VP, _VP]),
-    "fls_set_launch_config": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
-    "fls_get_launch_config": (ctypes.c_int, [_VP, _VP, _VP]),
+    "fls_set_launch_config": (ctypes.c_int, [ctypes.c_uint32] * 4),
+    "fls_get_launch_config": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
     "fls_kernel_launch_count": (ctypes.c_uint64, []),
+    "fls_set_tuning": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_int64]),
+    "fls_get_tuning": (ctypes.c_int, [ctypes.c_uint32, _VP]),
 }
 
 _LIB = None

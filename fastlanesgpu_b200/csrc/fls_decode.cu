@@ -20,10 +20,12 @@ struct DecodeOp {
 	uint32_t* out;
 	uint32_t  original;
 	__device__ void cta_setup(State&, uint32_t*, const StageCfg&) const {}
-	__device__ void process(State&, uint64_t v, const WarpStage& ws, uint32_t st, uint32_t lane,
+	__device__ void process(State&, uint64_t v, const WarpStage& ws, uint32_t st, uint32_t i, uint32_t lane,
 	                        const StageCfg&) const {
+		const StagedVec sv = staged(ws, st, i, 0);
+		if (sv.bad()) { return; }
 		uint32_t vals[32];
-		if (!stage_decode(ws, st, 0, lane, vals)) { return; }
+		dev::decode_vals(sv.s, sv.vi, ws.dict(), lane, vals);
 		uint32_t* dst = out + v * 1024u;
 		if (original) {
 			uint32_t*      tb = ws.extra();
@@ -46,26 +48,24 @@ struct AccState {
 	unsigned long long acc;
 };
 
-// Decode fused with a uint64 sum; one atomic per warp at the end.
+// Decode fused with a uint64 sum; four independent partial sums per lane, one
+// atomic per warp at the end.
 struct DecodeSumOp {
 	using State = AccState;
 	unsigned long long* sum;
 	__device__ void cta_setup(State&, uint32_t*, const StageCfg&) const {}
-	__device__ void process(State& S, uint64_t v, const WarpStage& ws, uint32_t st, uint32_t lane,
+	__device__ void process(State& S, uint64_t v, const WarpStage& ws, uint32_t st, uint32_t i, uint32_t lane,
 	                        const StageCfg& cfg) const {
+		const StagedVec sv = staged(ws, st, i, 0);
+		if (sv.bad()) { return; }
 		uint32_t vals[32];
-		if (!stage_decode(ws, st, 0, lane, vals)) { return; }
-		const uint32_t m = valid_rows(cfg, v, lane);
-		// 32 values of < 2^32 each: accumulate low and high parts in 32 bits.
-		uint32_t lo = 0, hi = 0;
+		// Values are summed as uint32 (base added per value: it may wrap).
+		dev::decode_vals(sv.s, sv.vi, ws.dict(), lane, vals);
+		const uint32_t     m = valid_rows(cfg, v, lane);
+		unsigned long long p[4] = {0, 0, 0, 0};
 #pragma unroll
-		for (uint32_t r = 0; r < 32; ++r) {
-			const uint32_t x = ((m >> r) & 1u) ? vals[r] : 0u;
-			const uint32_t t = lo + x;
-			hi += t < lo ? 1u : 0u;
-			lo = t;
-		}
-		S.acc += (static_cast<unsigned long long>(hi) << 32) | lo;
+		for (uint32_t r = 0; r < 32; ++r) { p[r & 3] += ((m >> r) & 1u) ? vals[r] : 0u; }
+		S.acc += (p[0] + p[1]) + (p[2] + p[3]);
 	}
 	__device__ void finish(State& S, uint32_t lane, const StageCfg&) const {
 		const unsigned long long s = warp_sum_u64(S.acc);

@@ -39,37 +39,56 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+	asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
 	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
 	             : "memory");
 }
 
+// L2 policy for data read exactly once (the streamed column payloads): evict
+// first, so it does not displace hash tables and group arrays kept in L2.
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+	uint64_t pol;
+	asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+	return pol;
+}
+
 // 1-D bulk copy global -> shared (no multicast); size and both addresses are
 // multiples of 16 bytes.  Completion is signalled on `bar`.
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar, uint64_t pol) {
 	asm volatile(
-	    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
-	    "l"(src), "r"(bytes), "r"(smem_u32(bar))
+	    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+	        smem_u32(dst)),
+	    "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
 	    : "memory");
 }
 
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+// One poll of the stage barrier.  The thread may be suspended in hardware until
+// the phase completes or `hint_ns` elapses, so waiting warps do not spin on the
+// issue slots that decoding warps need.
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
 	uint32_t ok;
 	asm volatile(
 	    "{\n\t.reg .pred p;\n\t"
-	    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+	    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
 	    "selp.u32 %0, 1, 0, p;\n\t}"
 	    : "=r"(ok)
-	    : "r"(smem_u32(bar)), "r"(parity)
+	    : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
 	    : "memory");
 	return ok != 0;
 }
 
-// Bounded wait: gives up after `limit` polls (each poll may itself suspend the
-// thread for a short, hardware-chosen time).
+// Bounded wait: gives up after `limit` polls of at most ~20 us each.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t limit) {
 	for (uint32_t i = 0; i < limit; ++i) {
-		if (mbar_try_wait(bar, parity)) { return true; }
+		if (mbar_try_wait(bar, parity, 20000u)) { return true; }
 	}
 	return false;
 }
@@ -222,7 +241,7 @@ struct DevCol {
 	int32_t             base;
 	uint32_t            slot_words; // staging slot (multiple of 4, >= largest vector)
 	uint32_t            layout;
-	uint32_t            pad_;
+	uint32_t            vec_words; // uniform columns: payload words of every vector
 };
 
 // Raw metadata for vector v (one 16-byte load; uniform columns need none).
@@ -264,14 +283,23 @@ __device__ __forceinline__ bool vec_info(const DevCol& c, uint64_t v, uint4 raw,
 	    X(20) X(21) X(22) X(23) X(24) X(25) X(26) X(27) X(28) X(29) X(30) X(31) X(32)
 #define FLS_BW_CASES_0_10(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
 
+// With AddBase = false, FOR vectors yield the packed value p (the caller adds
+// value_offset(m) = base, or folds it into its constants); every other scheme
+// always yields final values.
+__host__ __device__ __forceinline__ uint32_t value_offset(const VecInfo& m) {
+	return m.scheme == FLS_SCHEME_FOR ? static_cast<uint32_t>(m.base) : 0u;
+}
+
+template <bool AddBase = true>
 __device__ __forceinline__ void decode_vals(const uint32_t* __restrict__ s, const VecInfo& m,
                                             uint32_t* __restrict__ dict, uint32_t lane, uint32_t (&vals)[32]) {
 	const uint32_t base = static_cast<uint32_t>(m.base);
+	const uint32_t fadd = AddBase ? base : 0u;
 	switch (m.scheme) {
 	case FLS_SCHEME_FOR:
 		switch (m.bw) {
 #define FLS_FOR_CASE(B)                                                                                                \
-	case B: unpack_rows<B>(s, lane, [&](int r, uint32_t p) { vals[r] = p + base; }); break;
+	case B: unpack_rows<B>(s, lane, [&](int r, uint32_t p) { vals[r] = p + fadd; }); break;
 			FLS_BW_CASES_0_32(FLS_FOR_CASE)
 #undef FLS_FOR_CASE
 		default: break;
@@ -310,6 +338,119 @@ __device__ __forceinline__ void decode_vals(const uint32_t* __restrict__ s, cons
 	}
 	default: break;
 	}
+}
+
+// Callback form of decode_vals: f(r, value) for r = 0..31, with the consumer
+// inlined into each unrolled scheme / bit-width case so no value array is
+// materialised.  Use it only with cheap consumers (the code is replicated once
+// per case).
+template <bool AddBase, class F>
+__device__ __forceinline__ void decode_each(const uint32_t* __restrict__ s, const VecInfo& m,
+                                            uint32_t* __restrict__ dict, uint32_t lane, F&& f) {
+	const uint32_t base = static_cast<uint32_t>(m.base);
+	const uint32_t fadd = AddBase ? base : 0u;
+	switch (m.scheme) {
+	case FLS_SCHEME_FOR:
+		switch (m.bw) {
+#define FLS_FOR_CASE(B)                                                                                                \
+	case B: unpack_rows<B>(s, lane, [&](int r, uint32_t p) { f(r, p + fadd); }); break;
+			FLS_BW_CASES_0_32(FLS_FOR_CASE)
+#undef FLS_FOR_CASE
+		default: break;
+		}
+		break;
+	case FLS_SCHEME_DELTA:
+		switch (m.bw) {
+#define FLS_DELTA_CASE(B)                                                                                              \
+	case B: rsum_rows<B>(s, lane, f); break;
+			FLS_BW_CASES_0_32(FLS_DELTA_CASE)
+#undef FLS_DELTA_CASE
+		default: break;
+		}
+		break;
+	case FLS_SCHEME_RLE:
+		unpack_dict(s + 48, m.aux, m.bw, m.base, dict, lane);
+		rle_rows(s, lane, dict, f);
+		__syncwarp();
+		break;
+	case FLS_SCHEME_CONST:
+#pragma unroll
+		for (int r = 0; r < 32; ++r) { f(r, base); }
+		break;
+	case FLS_SCHEME_DICT: {
+		const uint32_t cbw = bits_of(m.aux - 1u);
+		unpack_dict(s + 32u * cbw, m.aux, m.bw, m.base, dict, lane);
+		switch (cbw) {
+#define FLS_DICT_CASE(B)                                                                                               \
+	case B: unpack_rows<B>(s, lane, [&](int r, uint32_t c) { f(r, dict[c & 1023u]); }); break;
+			FLS_BW_CASES_0_10(FLS_DICT_CASE)
+#undef FLS_DICT_CASE
+		default: break;
+		}
+		__syncwarp();
+		break;
+	}
+	default: break;
+	}
+}
+
+// ------------------------------------------------- single-row extraction
+
+// A FOR vector prepared for reading single rows: the lane's word column in
+// shared memory, bit width, mask and base.  get(r) reads two words (the second
+// may lie past the payload: the pipeline leaves slack after every slot, and
+// the bits read from it are masked off unless the field straddles).
+struct ForRows {
+	const uint32_t* s;
+	uint32_t        bw, mask, base;
+	__device__ __forceinline__ void init(const uint32_t* slot, const VecInfo& m, uint32_t lane) {
+		s    = slot + lane;
+		bw   = m.bw;
+		mask = m.bw >= 32 ? 0xffffffffu : ((1u << m.bw) - 1u);
+		base = static_cast<uint32_t>(m.base);
+	}
+	__device__ __forceinline__ uint32_t get(uint32_t r) const {
+		const uint32_t bit = r * bw, w = bit >> 5, sh = bit & 31u;
+		const uint32_t* p  = s + 32u * w;
+		return (__funnelshift_r(p[0], p[32], sh) & mask) + base;
+	}
+};
+
+// Schemes whose rows can be read at random (no running sum): FOR, CONST, DICT.
+__device__ __forceinline__ bool random_access(uint32_t scheme) {
+	return scheme == FLS_SCHEME_FOR || scheme == FLS_SCHEME_CONST || scheme == FLS_SCHEME_DICT;
+}
+
+// Field of row r (runtime) of this lane's bit-packed stream.
+__device__ __forceinline__ uint32_t extract_rt(const uint32_t* __restrict__ s, uint32_t bw, uint32_t lane, uint32_t r) {
+	if (bw == 0) { return 0u; }
+	const uint32_t bit = r * bw, w = bit >> 5, sh = bit & 31u;
+	const uint32_t lo  = s[32u * w + lane];
+	const uint32_t hi  = (sh + bw > 32u) ? s[32u * (w + 1u) + lane] : 0u;
+	const uint32_t m   = bw >= 32 ? 0xffffffffu : ((1u << bw) - 1u);
+	return __funnelshift_r(lo, hi, sh) & m;
+}
+
+// Entry k of a sequentially packed dictionary.
+__device__ __forceinline__ uint32_t dict_entry(const uint32_t* __restrict__ d, uint32_t bw, uint32_t k) {
+	if (bw == 0) { return 0u; }
+	const uint32_t bit = k * bw, w = bit >> 5, sh = bit & 31u;
+	const uint32_t hi  = (sh + bw > 32u) ? d[w + 1u] : 0u;
+	const uint32_t m   = bw >= 32 ? 0xffffffffu : ((1u << bw) - 1u);
+	return __funnelshift_r(d[w], hi, sh) & m;
+}
+
+// Final value of row r of a random-access (FOR / CONST / DICT) vector.
+__device__ __forceinline__ uint32_t value_at(const uint32_t* __restrict__ s, const VecInfo& m, uint32_t lane,
+                                             uint32_t r) {
+	const uint32_t base = static_cast<uint32_t>(m.base);
+	if (m.scheme == FLS_SCHEME_FOR) { return extract_rt(s, m.bw, lane, r) + base; }
+	if (m.scheme == FLS_SCHEME_DICT) {
+		const uint32_t cbw  = bits_of(m.aux - 1u);
+		const uint32_t code = extract_rt(s, cbw, lane, r);
+		return dict_entry(s + 32u * cbw, m.bw, code < m.aux ? code : 0u) + base;
+	}
+	return base; // CONST
 }
 
 } // namespace dev

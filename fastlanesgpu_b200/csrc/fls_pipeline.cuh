@@ -3,16 +3,17 @@
 //
 // Execution model:
 //   * persistent grid: ctas_per_sm CTAs per SM, W warps per CTA;
-//   * each warp owns vectors w, w + total_warps, ... of the table;
-//   * each warp stages its next S vectors (all referenced columns of one vector
-//     form one stage) into private shared-memory slots with cp.async.bulk,
-//     tracked by one mbarrier per stage, so HBM reads run S vectors ahead of
-//     the decode;
+//   * the table is cut into tiles of k consecutive 1024-value vectors (k is
+//     chosen so a tile is a few KB: 32 vectors at bit width 1, one vector for
+//     a 4-column 46-bit row); warp w owns tiles w, w + total_warps, ...;
+//   * each warp stages its next S tiles into private shared-memory slots, one
+//     cp.async.bulk per column per tile, tracked by one mbarrier per stage, so
+//     HBM reads run S tiles ahead of the decode;
 //   * decode happens lane-parallel out of shared memory into registers
 //     (fls_device.cuh); predicates become a 32-bit row mask per lane;
 //     aggregates are warp-reduced and committed with one atomic per warp.
 // Nothing spins without a bound, traps or reads outside a buffer: bad metadata
-// or a timed-out wait sets a bit in the device error word and skips the vector.
+// or a timed-out wait sets a bit in the device error word and skips the tile.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -29,11 +30,13 @@ namespace fls {
 using dev::DevCol;
 using dev::VecInfo;
 
-constexpr uint32_t kMaxCols   = FLS_MAX_QUERY_COLS;
-constexpr uint32_t kWaitPolls = 1u << 22; // bounded mbarrier waits
-constexpr uint32_t kDictWords = 1024;     // per-warp dictionary scratch
-constexpr uint32_t kTBufWords = 33 * 32;  // per-warp transpose buffer
-constexpr uint32_t kBadScheme = 0xffu;
+constexpr uint32_t kMaxCols    = FLS_MAX_QUERY_COLS;
+constexpr uint32_t kMaxTile    = 32;       // vectors per tile (one lane per vector at issue)
+constexpr uint32_t kMaxWarps   = 16;       // warps per CTA
+constexpr uint32_t kWaitPolls  = 1u << 17; // bounded mbarrier waits (x <= 20 us each)
+constexpr uint32_t kDictWords  = 1024;     // per-warp dictionary scratch
+constexpr uint32_t kTBufWords  = 33 * 32;  // per-warp transpose buffer
+constexpr uint32_t kBadScheme  = 0xffu;
 
 // ------------------------------------------------------------ parameters
 
@@ -41,67 +44,128 @@ struct StageCfg {
 	DevCol    cols[kMaxCols];
 	uint32_t  col_off[kMaxCols]; // word offset of column c's slot inside a stage
 	uint32_t  n_cols;
+	uint32_t  tile;            // k vectors per tile
 	uint32_t  stage_words;     // words per stage (multiple of 4)
 	uint32_t  stages;          // S
 	uint32_t  warps;           // W
 	uint32_t  warp_smem_words; // per-warp region (multiple of 4)
 	uint32_t  dict_off;        // per-warp dictionary scratch (words)
-	uint32_t  extra_off;       // per-warp kernel-specific scratch (words)
-	uint32_t  info_off;        // per-warp stage info (uint2 per stage per column)
+	uint32_t  extra_off;       // per-warp operator scratch (words)
+	uint32_t  info_off;        // per-warp vector info: uint4 per (stage, vector, column)
 	uint32_t  bar_off;         // per-warp mbarriers (uint64 per stage)
 	uint32_t  cta_extra_off;   // CTA-level scratch after all warp regions (words)
-	uint64_t  n_vec, n_values;
+	uint64_t  n_vec, n_values, n_tiles;
 	uint32_t  layout;
-	uint32_t  has_dict; // per-warp dictionary scratch planned (RLE / DICT allowed)
-	uint32_t* err;      // device error word
+	uint32_t  has_dict;    // per-warp dictionary scratch planned (RLE / DICT allowed)
+	uint32_t  all_uniform; // every column uniform (no metadata): host-validated, no per-vector info
+	uint32_t* err;         // device error word
 };
+
+// Words of slack after the staged slots of a warp (single-row reads may look
+// one word row past a vector's payload).
+constexpr uint32_t kSlotSlackWords = 32;
 
 __device__ __forceinline__ void raise_err(uint32_t* err, uint32_t bits) { atomicOr(err, bits); }
 
 // ------------------------------------------------------- staged pipeline
 
-// Per-warp view of its shared-memory region.
+// Per-warp view of its shared-memory region.  Vector info entries are
+// {base, scheme | bw<<8 | aux<<16, word offset inside the column's slot, 0}.
 struct WarpStage {
 	uint32_t*       base;
 	const StageCfg* cfg;
 	__device__ uint32_t* slot(uint32_t st, uint32_t c) const { return base + st * cfg->stage_words + cfg->col_off[c]; }
-	__device__ uint2*    info(uint32_t st) const { return reinterpret_cast<uint2*>(base + cfg->info_off) + st * kMaxCols; }
+	__device__ uint4*    info(uint32_t st, uint32_t i, uint32_t c) const {
+        return reinterpret_cast<uint4*>(base + cfg->info_off) + (st * cfg->tile + i) * cfg->n_cols + c;
+	}
 	__device__ uint64_t* bar(uint32_t st) const { return reinterpret_cast<uint64_t*>(base + cfg->bar_off) + st; }
 	__device__ uint32_t* dict() const { return base + cfg->dict_off; }
 	__device__ uint32_t* extra() const { return base + cfg->extra_off; }
 };
 
-// Issues the bulk copies of vector v into stage st.  All lanes participate:
-// lane c handles column c; `raw` is lane c's metadata entry for v.
-__device__ __forceinline__ void issue_stage(const StageCfg& cfg, const WarpStage& ws, uint32_t st, uint64_t v,
-                                            uint4 raw, uint32_t lane) {
-	uint32_t bytes = 0;
-	VecInfo  vi {};
-	bool     ok = true;
-	if (lane < cfg.n_cols) {
-		ok = dev::vec_info(cfg.cols[lane], v, raw, vi);
-		// RLE / DICT vectors need the dictionary scratch; reject them otherwise.
-		if (ok && !cfg.has_dict && (vi.scheme == FLS_SCHEME_RLE || vi.scheme == FLS_SCHEME_DICT)) { ok = false; }
-		uint2 x;
-		if (ok) {
-			bytes = vi.words * 4u;
-			x     = make_uint2(static_cast<uint32_t>(vi.base), vi.scheme | (vi.bw << 8) | (vi.aux << 16));
-		} else {
-			x = make_uint2(0u, kBadScheme);
-			raise_err(cfg.err, kErrBadMeta);
-		}
-		ws.info(st)[lane] = x;
-	}
-	const uint32_t total = __reduce_add_sync(0xffffffffu, bytes);
-	if (lane == 0) { dev::mbar_arrive_expect_tx(ws.bar(st), total); }
-	__syncwarp();
-	if (lane < cfg.n_cols && ok && bytes) {
-		dev::bulk_g2s(ws.slot(st, lane), cfg.cols[lane].data + vi.offset, bytes, ws.bar(st));
-	}
+// Issues the bulk copies of tile t into stage st.  All lanes participate in
+// one pass: lane l handles vector l / n_cols of the tile for column
+// l % n_cols (the planner keeps tile * n_cols <= 32).  The lane holding a
+// column's first vector issues one bulk copy covering the tile's payload range
+// of that column, after adding its byte count to the stage barrier's
+// transaction count; lane 0 arrives last.
+struct LaneRole {
+	uint32_t i, c;     // tile vector and column of this lane
+	uint32_t col_mask; // lanes that work on column c
+};
+
+__device__ __forceinline__ LaneRole lane_role(const StageCfg& cfg, uint32_t lane) {
+	LaneRole role;
+	role.i        = lane / cfg.n_cols;
+	role.c        = lane - role.i * cfg.n_cols;
+	uint32_t m    = 0;
+	for (uint32_t l = role.c; l < 32; l += cfg.n_cols) { m |= 1u << l; }
+	role.col_mask = m;
+	return role;
 }
 
-__device__ __forceinline__ VecInfo stage_info(const WarpStage& ws, uint32_t st, uint32_t c) {
-	const uint2 x = ws.info(st)[c];
+__device__ __forceinline__ void issue_stage(const StageCfg& cfg, const WarpStage& ws, uint32_t st, uint64_t t,
+                                            uint32_t lane, const LaneRole& role, uint64_t pol) {
+	const uint64_t v0     = t * cfg.tile;
+	const uint32_t kk     = static_cast<uint32_t>(min(static_cast<uint64_t>(cfg.tile), cfg.n_vec - v0));
+	if (cfg.all_uniform) {
+		// Uniform columns: vector v sits at v * vec_words; the host checked that
+		// the data buffer covers every vector.  Lane c copies column c.
+		if (lane < cfg.n_cols) {
+			const DevCol&  col   = cfg.cols[lane];
+			const uint32_t bytes = kk * col.vec_words * 4u;
+			if (bytes) {
+				dev::mbar_expect_tx(ws.bar(st), bytes);
+				dev::bulk_g2s(ws.slot(st, lane), col.data + v0 * col.vec_words, bytes, ws.bar(st), pol);
+			}
+		}
+		__syncwarp();
+		if (lane == 0) { dev::mbar_arrive(ws.bar(st)); }
+		__syncwarp();
+		return;
+	}
+	const uint32_t active = kk * cfg.n_cols; // lanes with a (vector, column) pair
+	const bool     mine   = lane < active;
+	const DevCol&  col    = cfg.cols[mine ? role.c : 0];
+	VecInfo        vi {};
+	bool           ok = true;
+	if (mine) {
+		const uint4 raw = dev::load_meta(col, v0 + role.i);
+		ok              = dev::vec_info(col, v0 + role.i, raw, vi);
+		// RLE / DICT vectors need the dictionary scratch; reject them otherwise.
+		if (ok && !cfg.has_dict && (vi.scheme == FLS_SCHEME_RLE || vi.scheme == FLS_SCHEME_DICT)) { ok = false; }
+	}
+	// The column's payload range [start, end) over the tile.
+	const uint32_t first_lane = role.c;
+	const uint32_t last_lane  = (kk - 1u) * cfg.n_cols + role.c;
+	const uint64_t start      = __shfl_sync(0xffffffffu, vi.offset, first_lane);
+	const uint64_t end        = __shfl_sync(0xffffffffu, vi.offset + vi.words, last_lane);
+	if (mine) { ok = ok && vi.offset >= start && vi.offset + vi.words <= end && end - start <= col.slot_words; }
+	const uint32_t bad   = __ballot_sync(0xffffffffu, !ok);
+	const bool     good  = (bad & role.col_mask & ((active >= 32u) ? 0xffffffffu : ((1u << active) - 1u))) == 0u;
+	if (mine) {
+		*ws.info(st, role.i, role.c) = good ? make_uint4(static_cast<uint32_t>(vi.base),
+		                                                 vi.scheme | (vi.bw << 8) | (vi.aux << 16),
+		                                                 static_cast<uint32_t>(vi.offset - start), 0u)
+		                                    : make_uint4(0u, kBadScheme, 0u, 0u);
+		if (role.i == 0) {
+			if (!good) {
+				raise_err(cfg.err, kErrBadMeta);
+			} else if (end > start) {
+				const uint32_t bytes = static_cast<uint32_t>(end - start) * 4u;
+				dev::mbar_expect_tx(ws.bar(st), bytes);
+				dev::bulk_g2s(ws.slot(st, role.c), col.data + start, bytes, ws.bar(st), pol);
+			}
+		}
+	}
+	__syncwarp();
+	if (lane == 0) { dev::mbar_arrive(ws.bar(st)); }
+	__syncwarp();
+}
+
+__device__ __forceinline__ VecInfo stage_info(const WarpStage& ws, uint32_t st, uint32_t i, uint32_t c,
+                                              uint32_t& rel_off) {
+	const uint4 x = *ws.info(st, i, c);
 	VecInfo     vi;
 	vi.offset = 0;
 	vi.base   = static_cast<int32_t>(x.x);
@@ -109,17 +173,34 @@ __device__ __forceinline__ VecInfo stage_info(const WarpStage& ws, uint32_t st, 
 	vi.bw     = (x.y >> 8) & 0xffu;
 	vi.aux    = x.y >> 16;
 	vi.words  = 0;
+	rel_off   = x.z;
 	return vi;
 }
 
-// Decodes column c of the staged vector in stage st into vals; false if the
-// vector's metadata was rejected at issue time.
-__device__ __forceinline__ bool stage_decode(const WarpStage& ws, uint32_t st, uint32_t c, uint32_t lane,
-                                             uint32_t (&vals)[32]) {
-	const VecInfo vi = stage_info(ws, st, c);
-	if (vi.scheme == kBadScheme) { return false; }
-	dev::decode_vals(ws.slot(st, c), vi, ws.dict(), lane, vals);
-	return true;
+// A staged vector of one column: its info and where its payload sits.
+struct StagedVec {
+	VecInfo         vi;
+	const uint32_t* s;
+	__device__ bool bad() const { return vi.scheme == kBadScheme; }
+};
+
+__device__ __forceinline__ StagedVec staged(const WarpStage& ws, uint32_t st, uint32_t i, uint32_t c) {
+	StagedVec sv;
+	if (ws.cfg->all_uniform) {
+		const DevCol& col = ws.cfg->cols[c];
+		sv.vi.offset      = 0;
+		sv.vi.base        = col.base;
+		sv.vi.scheme      = col.scheme;
+		sv.vi.bw          = col.bw;
+		sv.vi.aux         = 0;
+		sv.vi.words       = col.vec_words;
+		sv.s              = ws.slot(st, c) + i * col.vec_words;
+		return sv;
+	}
+	uint32_t rel;
+	sv.vi = stage_info(ws, st, i, c, rel);
+	sv.s  = ws.slot(st, c) + rel;
+	return sv;
 }
 
 __device__ __forceinline__ uint32_t valid_rows(const StageCfg& cfg, uint64_t v, uint32_t lane) {
@@ -131,12 +212,12 @@ __device__ __forceinline__ uint32_t valid_rows(const StageCfg& cfg, uint64_t v, 
 // The persistent staged loop.  Op provides
 //   struct State                                                    (per-thread mutable state)
 //   __device__ void cta_setup(State&, uint32_t* cta_smem, const StageCfg&) const   (all threads)
-//   __device__ void process(State&, uint64_t v, const WarpStage&, uint32_t st, uint32_t lane,
-//                           const StageCfg&) const
+//   __device__ void process(State&, uint64_t v, const WarpStage&, uint32_t st, uint32_t i, uint32_t lane,
+//                           const StageCfg&) const      (vector v = tile vector i in stage st)
 //   __device__ void finish(State&, uint32_t lane, const StageCfg&) const
 // The Op itself is a read-only kernel parameter.
 template <class Op>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(kMaxWarps * 32, 1)
     staged_kernel(const __grid_constant__ StageCfg cfg, const __grid_constant__ Op op) {
 	extern __shared__ __align__(128) uint32_t smem[];
 	const uint32_t     lane = threadIdx.x & 31u;
@@ -154,21 +235,19 @@ __global__ void __launch_bounds__(256, 1)
 		dev::fence_mbar_init();
 	}
 	__syncwarp();
+	const LaneRole role = lane_role(cfg, lane);
+	const uint64_t pol  = dev::l2_evict_first_policy();
 
 	// Prologue: fill the pipeline.
 	for (uint32_t s = 0; s < cfg.stages; ++s) {
-		const uint64_t v = first + s * total;
-		if (v >= cfg.n_vec) { break; }
-		const uint4 raw = lane < cfg.n_cols ? dev::load_meta(cfg.cols[lane], v) : make_uint4(0, 0, 0, 0);
-		issue_stage(cfg, ws, s, v, raw, lane);
+		const uint64_t t = first + s * total;
+		if (t >= cfg.n_tiles) { break; }
+		issue_stage(cfg, ws, s, t, lane, role, pol);
 	}
-	// Metadata of the next vector to issue, fetched one iteration early.
 	uint64_t next_issue = first + static_cast<uint64_t>(cfg.stages) * total;
-	uint4    next_raw   = (lane < cfg.n_cols && next_issue < cfg.n_vec) ? dev::load_meta(cfg.cols[lane], next_issue)
-	                                                                   : make_uint4(0, 0, 0, 0);
 
 	uint32_t st = 0, phase = 0;
-	for (uint64_t v = first; v < cfg.n_vec; v += total) {
+	for (uint64_t t = first; t < cfg.n_tiles; t += total) {
 		if (!dev::mbar_wait_bounded(ws.bar(st), phase, kWaitPolls)) {
 			raise_err(cfg.err, kErrTimeout);
 			// Give the copies still in flight a bounded chance to land before exit.
@@ -178,14 +257,14 @@ __global__ void __launch_bounds__(256, 1)
 			}
 			return;
 		}
-		op.process(state, v, ws, st, lane, cfg);
+		const uint64_t v0 = t * cfg.tile;
+		const uint32_t kk = static_cast<uint32_t>(min(static_cast<uint64_t>(cfg.tile), cfg.n_vec - v0));
+		for (uint32_t i = 0; i < kk; ++i) { op.process(state, v0 + i, ws, st, i, lane, cfg); }
 		__syncwarp();
-		if (next_issue < cfg.n_vec) {
+		if (next_issue < cfg.n_tiles) {
 			dev::fence_proxy_async_smem();
-			issue_stage(cfg, ws, st, next_issue, next_raw, lane);
+			issue_stage(cfg, ws, st, next_issue, lane, role, pol);
 			next_issue += total;
-			next_raw = (lane < cfg.n_cols && next_issue < cfg.n_vec) ? dev::load_meta(cfg.cols[lane], next_issue)
-			                                                         : make_uint4(0, 0, 0, 0);
 		}
 		if (++st == cfg.stages) {
 			st = 0;
@@ -211,6 +290,7 @@ fls_status device_info(DeviceInfo& di);
 fls_status cuda_check(cudaError_t e, const char* what);
 uint32_t*  device_error_word(); // device address of this device's error word
 void       count_launch(uint64_t n = 1);
+int        tuning_sparse_rows();
 
 // Lays out shared memory for a set of columns; extra_words per warp and
 // cta_words per CTA are operator-specific scratch.

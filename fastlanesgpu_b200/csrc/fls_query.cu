@@ -4,6 +4,10 @@
 // Reference counterparts: QueryKernel_v1/_v2 (fastlanes/src/ssb/fls_q11.cu:29-135),
 // build_hashtable_{s,p,d} and probe_v1..v3 (fls_q21.cu:21-263), with the tile
 // primitives of fastlanes/src/include/crystal-opt/{pred,load,reduce,join}.cuh.
+#include <algorithm>
+#include <cmath>
+#include <utility>
+
 #include "fls_pipeline.cuh"
 
 namespace fls {
@@ -12,6 +16,10 @@ namespace {
 struct AccState {
 	unsigned long long acc;
 };
+
+__device__ __forceinline__ int max_rows(uint32_t mask) { return __reduce_max_sync(0xffffffffu, __popc(mask)); }
+
+__device__ __forceinline__ bool in_range(uint32_t x, uint32_t lo, uint32_t range) { return x - lo <= range; }
 
 // Range filters ANDed into a per-lane row mask (bit r = row r), then sum(a),
 // sum(a*b) or count over the selected rows, in int64.
@@ -23,46 +31,182 @@ struct FilterAggOp {
 	uint32_t   f_range[FLS_MAX_FILTERS]; // hi - lo (unsigned)
 	int32_t    agg_a, agg_b;
 	long long* result;
+	// Above this many selected rows in some lane, whole vectors are evaluated
+	// (dense); at or below it a loop over the set bits of the row mask reads
+	// only the selected rows' fields (FLS_TUNE_SPARSE_ROWS).
+	int32_t sparse_rows;
 
 	__device__ void cta_setup(State&, uint32_t*, const StageCfg&) const {}
-	__device__ void process(State& S, uint64_t v, const WarpStage& ws, uint32_t st, uint32_t lane,
+
+	// Dense pass of filter f: whole vector, FOR base folded into the bound.
+	__device__ bool dense_filter(uint32_t f, uint32_t& mask, const WarpStage& ws, uint32_t st, uint32_t i,
+	                             uint32_t lane) const {
+		const StagedVec sv = staged(ws, st, i, f_col[f]);
+		if (sv.bad()) { return false; }
+		const uint32_t lo = f_lo[f] - dev::value_offset(sv.vi), range = f_range[f];
+		uint32_t       m[4] = {0, 0, 0, 0};
+		dev::decode_each<false>(sv.s, sv.vi, ws.dict(), lane,
+		                        [&](int r, uint32_t x) { m[r & 3] |= (in_range(x, lo, range) ? 1u : 0u) << r; });
+		mask &= (m[0] | m[1]) | (m[2] | m[3]);
+		return true;
+	}
+
+	__device__ void process(State& S, uint64_t v, const WarpStage& ws, uint32_t st, uint32_t i, uint32_t lane,
 	                        const StageCfg& cfg) const {
 		uint32_t mask = valid_rows(cfg, v, lane);
-		uint32_t vals[32];
-		for (uint32_t f = 0; f < n_filters; ++f) {
-			if (!stage_decode(ws, st, f_col[f], lane, vals)) { return; }
-			const uint32_t lo = f_lo[f], range = f_range[f];
-			uint32_t       fm = 0;
-			// lo <= x <= hi  <=>  (x - lo) <= (hi - lo) in wrapping unsigned arithmetic.
-#pragma unroll
-			for (uint32_t r = 0; r < 32; ++r) { fm |= (vals[r] - lo <= range ? 1u : 0u) << r; }
-			mask &= fm;
-			if (!__any_sync(0xffffffffu, mask)) { return; }
+		uint32_t f    = 0;
+		for (; f < n_filters; ++f) {
+			if (max_rows(mask) <= sparse_rows) { break; }
+			if (!dense_filter(f, mask, ws, st, i, lane)) { return; }
 		}
-		if (agg_a < 0) {
-			S.acc += static_cast<unsigned long long>(__popc(mask));
+		if (!__any_sync(0xffffffffu, mask)) { return; }
+		// Can the rest be read row by row?
+		bool rnd = true;
+		for (uint32_t g = f; g < n_filters; ++g) { rnd = rnd && dev::random_access(staged(ws, st, i, f_col[g]).vi.scheme); }
+		if (agg_a >= 0) { rnd = rnd && dev::random_access(staged(ws, st, i, static_cast<uint32_t>(agg_a)).vi.scheme); }
+		if (agg_b >= 0) { rnd = rnd && dev::random_access(staged(ws, st, i, static_cast<uint32_t>(agg_b)).vi.scheme); }
+		if (rnd) {
+			S.acc += all_for(f, ws, st, i) ? sparse_rest_for(f, mask, ws, st, i, lane)
+			                                : sparse_rest(f, mask, ws, st, i, lane);
 			return;
 		}
-		long long a = 0;
-		if (agg_b >= 0) {
-			int32_t bv[32];
-			if (!stage_decode(ws, st, static_cast<uint32_t>(agg_b), lane, vals)) { return; }
+		for (; f < n_filters; ++f) {
+			if (!dense_filter(f, mask, ws, st, i, lane)) { return; }
+			if (!__any_sync(0xffffffffu, mask)) { return; }
+		}
+		S.acc += dense_agg(mask, ws, st, i, lane);
+	}
+
+	__device__ bool all_for(uint32_t f0, const WarpStage& ws, uint32_t st, uint32_t i) const {
+		bool ok = true;
+		for (uint32_t f = f0; f < n_filters; ++f) { ok = ok && staged(ws, st, i, f_col[f]).vi.scheme == FLS_SCHEME_FOR; }
+		if (agg_a >= 0) { ok = ok && staged(ws, st, i, static_cast<uint32_t>(agg_a)).vi.scheme == FLS_SCHEME_FOR; }
+		if (agg_b >= 0) { ok = ok && staged(ws, st, i, static_cast<uint32_t>(agg_b)).vi.scheme == FLS_SCHEME_FOR; }
+		return ok;
+	}
+
+	// Row-at-a-time rest when every remaining column is FOR: per field two
+	// shared-memory loads, a funnel shift, a mask and the base.
+	__device__ unsigned long long sparse_rest_for(uint32_t f0, uint32_t mask, const WarpStage& ws, uint32_t st,
+	                                              uint32_t i, uint32_t lane) const {
+		dev::ForRows fr[FLS_MAX_FILTERS];
+		uint32_t     lo[FLS_MAX_FILTERS], range[FLS_MAX_FILTERS];
 #pragma unroll
-			for (uint32_t r = 0; r < 32; ++r) { bv[r] = ((mask >> r) & 1u) ? static_cast<int32_t>(vals[r]) : 0; }
-			if (!stage_decode(ws, st, static_cast<uint32_t>(agg_a), lane, vals)) { return; }
-#pragma unroll
-			for (uint32_t r = 0; r < 32; ++r) {
-				a += static_cast<long long>(static_cast<int32_t>(vals[r])) * static_cast<long long>(bv[r]);
-			}
-		} else {
-			if (!stage_decode(ws, st, static_cast<uint32_t>(agg_a), lane, vals)) { return; }
-#pragma unroll
-			for (uint32_t r = 0; r < 32; ++r) {
-				a += ((mask >> r) & 1u) ? static_cast<long long>(static_cast<int32_t>(vals[r])) : 0ll;
+		for (uint32_t f = 0; f < FLS_MAX_FILTERS; ++f) {
+			if (f >= f0 && f < n_filters) {
+				const StagedVec sv = staged(ws, st, i, f_col[f]);
+				fr[f].init(sv.s, sv.vi, lane);
+				// fold the base into the bound: x + base - lo = x - (lo - base)
+				lo[f]        = f_lo[f] - fr[f].base;
+				range[f]     = f_range[f];
+				fr[f].base   = 0;
 			}
 		}
-		S.acc += static_cast<unsigned long long>(a);
+		dev::ForRows ra {}, rb {};
+		if (agg_a >= 0) {
+			const StagedVec sv = staged(ws, st, i, static_cast<uint32_t>(agg_a));
+			ra.init(sv.s, sv.vi, lane);
+		}
+		if (agg_b >= 0) {
+			const StagedVec sv = staged(ws, st, i, static_cast<uint32_t>(agg_b));
+			rb.init(sv.s, sv.vi, lane);
+		}
+		// Warp-uniform trip count (the largest per-lane row count); the body is
+		// branch-free: lanes without a row left read row 0 and discard it.
+		const int n_it = max_rows(mask);
+		long long acc  = 0;
+		for (int it = 0; it < n_it; ++it) {
+			const bool     have = mask != 0u;
+			const uint32_t r    = have ? static_cast<uint32_t>(__ffs(mask)) - 1u : 0u;
+			mask &= mask - 1u;
+			bool pass = have;
+#pragma unroll
+			for (uint32_t f = 0; f < FLS_MAX_FILTERS; ++f) {
+				if (f >= f0 && f < n_filters) { pass &= in_range(fr[f].get(r), lo[f], range[f]); }
+			}
+			long long x;
+			if (agg_a < 0) {
+				x = 1;
+			} else if (agg_b >= 0) {
+				x = static_cast<long long>(static_cast<int32_t>(ra.get(r))) *
+				    static_cast<long long>(static_cast<int32_t>(rb.get(r)));
+			} else {
+				x = static_cast<int32_t>(ra.get(r));
+			}
+			acc += pass ? x : 0ll;
+		}
+		return static_cast<unsigned long long>(acc);
 	}
+
+	// Remaining filters and the aggregate, one selected row at a time.  The
+	// staged-vector descriptors are read once; the row loop only extracts.
+	__device__ unsigned long long sparse_rest(uint32_t f0, uint32_t mask, const WarpStage& ws, uint32_t st,
+	                                          uint32_t i, uint32_t lane) const {
+		StagedVec fv[FLS_MAX_FILTERS];
+#pragma unroll
+		for (uint32_t f = 0; f < FLS_MAX_FILTERS; ++f) {
+			if (f >= f0 && f < n_filters) {
+				fv[f] = staged(ws, st, i, f_col[f]);
+				if (fv[f].bad()) { return 0; }
+			}
+		}
+		StagedVec sa {}, sb {};
+		if (agg_a >= 0) {
+			sa = staged(ws, st, i, static_cast<uint32_t>(agg_a));
+			if (sa.bad()) { return 0; }
+		}
+		if (agg_b >= 0) {
+			sb = staged(ws, st, i, static_cast<uint32_t>(agg_b));
+			if (sb.bad()) { return 0; }
+		}
+		long long acc = 0;
+		while (mask) {
+			const uint32_t r = static_cast<uint32_t>(__ffs(mask)) - 1u;
+			mask &= mask - 1u;
+			bool pass = true;
+#pragma unroll
+			for (uint32_t f = 0; f < FLS_MAX_FILTERS; ++f) {
+				if (pass && f >= f0 && f < n_filters) {
+					pass = in_range(dev::value_at(fv[f].s, fv[f].vi, lane, r), f_lo[f], f_range[f]);
+				}
+			}
+			if (!pass) { continue; }
+			if (agg_a < 0) {
+				acc += 1;
+			} else if (agg_b >= 0) {
+				acc += static_cast<long long>(static_cast<int32_t>(dev::value_at(sa.s, sa.vi, lane, r))) *
+				       static_cast<long long>(static_cast<int32_t>(dev::value_at(sb.s, sb.vi, lane, r)));
+			} else {
+				acc += static_cast<int32_t>(dev::value_at(sa.s, sa.vi, lane, r));
+			}
+		}
+		return static_cast<unsigned long long>(acc);
+	}
+
+	__device__ unsigned long long dense_agg(uint32_t mask, const WarpStage& ws, uint32_t st, uint32_t i,
+	                                        uint32_t lane) const {
+		if (agg_a < 0) { return static_cast<unsigned long long>(__popc(mask)); }
+		long long       p[4] = {0, 0, 0, 0};
+		const StagedVec sa   = staged(ws, st, i, static_cast<uint32_t>(agg_a));
+		if (sa.bad()) { return 0; }
+		if (agg_b >= 0) {
+			const StagedVec sb = staged(ws, st, i, static_cast<uint32_t>(agg_b));
+			if (sb.bad()) { return 0; }
+			int32_t bv[32];
+			dev::decode_each<true>(sb.s, sb.vi, ws.dict(), lane, [&](int r, uint32_t x) {
+				bv[r] = ((mask >> r) & 1u) ? static_cast<int32_t>(x) : 0;
+			});
+			dev::decode_each<true>(sa.s, sa.vi, ws.dict(), lane, [&](int r, uint32_t x) {
+				p[r & 3] += static_cast<long long>(static_cast<int32_t>(x)) * static_cast<long long>(bv[r]);
+			});
+		} else {
+			dev::decode_each<true>(sa.s, sa.vi, ws.dict(), lane, [&](int r, uint32_t x) {
+				p[r & 3] += ((mask >> r) & 1u) ? static_cast<long long>(static_cast<int32_t>(x)) : 0ll;
+			});
+		}
+		return static_cast<unsigned long long>((p[0] + p[1]) + (p[2] + p[3]));
+	}
+
 	__device__ void finish(State& S, uint32_t lane, const StageCfg&) const {
 		const unsigned long long s = warp_sum_u64(S.acc);
 		if (lane == 0 && s) { atomicAdd(reinterpret_cast<unsigned long long*>(result), s); }
@@ -73,11 +217,8 @@ struct TableState {
 	const uint32_t* tables;
 };
 
-// Probe + group-by.  Small hash tables are staged into shared memory once per
-// CTA: PHT_1 tables as a presence bitmap (the probe only tests slot != 0,
-// crystal-opt/join.cuh:42-47), small PHT_2 tables verbatim.
-struct ProbeGroupByOp {
-	using State = TableState;
+// Shared parameters of the probe + group-by operators (fls_q21.cu probe_v1).
+struct ProbeParams {
 	uint32_t       n_probes;
 	uint32_t       p_col[FLS_MAX_PROBES];
 	const int32_t* p_ht[FLS_MAX_PROBES];
@@ -88,8 +229,12 @@ struct ProbeGroupByOp {
 	int32_t        key_a, key_b, mul, sub, n_groups;
 	uint32_t       agg_col;
 	int32_t*       res;
+	int32_t        sparse_rows; // see FilterAggOp
 
-	__device__ void cta_setup(State& S, uint32_t* cta_smem, const StageCfg&) const {
+	// Small hash tables are staged into shared memory once per CTA: PHT_1 tables
+	// as a presence bitmap (the probe only tests slot != 0, crystal-opt/
+	// join.cuh:42-47), small PHT_2 tables verbatim.
+	__device__ void stage_tables(TableState& S, uint32_t* cta_smem) const {
 		S.tables            = cta_smem;
 		const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 		for (uint32_t p = 0; p < n_probes; ++p) {
@@ -98,83 +243,211 @@ struct ProbeGroupByOp {
 			const int32_t* ht  = p_ht[p];
 			const uint32_t len = static_cast<uint32_t>(p_len[p]);
 			if (p_kind[p] == 1) {
+				// Presence bitmap, 8 independent coalesced loads in flight per warp.
 				const uint32_t n_words = (len + 31u) / 32u;
-				for (uint32_t w = warp; w < n_words; w += nw) {
-					const uint32_t i   = 32u * w + lane;
-					const bool     set = i < len && __ldg(ht + i) != 0;
-					const uint32_t b   = __ballot_sync(0xffffffffu, set);
-					if (lane == 0) { dst[w] = b; }
+				for (uint32_t w0 = warp * 8u; w0 < n_words; w0 += nw * 8u) {
+					int32_t x[8];
+#pragma unroll
+					for (uint32_t j = 0; j < 8; ++j) {
+						const uint32_t idx = 32u * (w0 + j) + lane;
+						x[j]               = (w0 + j < n_words && idx < len) ? __ldg(ht + idx) : 0;
+					}
+#pragma unroll
+					for (uint32_t j = 0; j < 8; ++j) {
+						const uint32_t b = __ballot_sync(0xffffffffu, x[j] != 0);
+						if (lane == 0 && w0 + j < n_words) { dst[w0 + j] = b; }
+					}
 				}
 			} else {
-				for (uint32_t i = threadIdx.x; i < 2u * len; i += blockDim.x) {
-					dst[i] = static_cast<uint32_t>(__ldg(ht + i));
+				const uint32_t n = 2u * len;
+				for (uint32_t i0 = threadIdx.x; i0 < n; i0 += 4u * blockDim.x) {
+					int32_t x[4];
+#pragma unroll
+					for (uint32_t j = 0; j < 4; ++j) {
+						const uint32_t idx = i0 + j * blockDim.x;
+						x[j]               = idx < n ? __ldg(ht + idx) : 0;
+					}
+#pragma unroll
+					for (uint32_t j = 0; j < 4; ++j) {
+						const uint32_t idx = i0 + j * blockDim.x;
+						if (idx < n) { dst[idx] = static_cast<uint32_t>(x[j]); }
+					}
 				}
 			}
 		}
 	}
 
-	__device__ void process(State& S, uint64_t v, const WarpStage& ws, uint32_t st, uint32_t lane,
+	// HASH(X,Y,Z) = (X-Z) % Y (join.cuh:26): d = key - keys_min; in-range keys
+	// skip the division; a negative remainder is flagged and misses.
+	__device__ __forceinline__ bool slot_of(uint32_t p, uint32_t key, int32_t& h, uint32_t* err) const {
+		const int32_t d = static_cast<int32_t>(key - static_cast<uint32_t>(p_min[p]));
+		h               = d;
+		if (static_cast<uint32_t>(d) >= static_cast<uint32_t>(p_len[p])) {
+			h = d % p_len[p];
+			if (h < 0) {
+				raise_err(err, kErrHash);
+				return false;
+			}
+		}
+		return true;
+	}
+
+	// Probe of one key: hit?  PHT_2 hits return their value in *val.
+	__device__ __forceinline__ bool probe(const TableState& S, uint32_t p, uint32_t key, int32_t* val,
+	                                      uint32_t* err) const {
+		int32_t h;
+		if (!slot_of(p, key, h, err)) { return false; }
+		const bool in_smem = p_smem_off[p] != ~0u;
+		if (p_kind[p] == 1) {
+			return in_smem ? ((S.tables[p_smem_off[p] + (h >> 5)] >> (h & 31)) & 1u) != 0u : __ldg(p_ht[p] + h) != 0;
+		}
+		const uint2 s = in_smem ? reinterpret_cast<const uint2*>(S.tables + p_smem_off[p])[h]
+		                        : __ldg(reinterpret_cast<const uint2*>(p_ht[p]) + h);
+		*val = static_cast<int32_t>(s.y);
+		return (s.x | s.y) != 0u;
+	}
+
+	// Group-by epilogue of one selected row (fls_q21.cu:67-77).
+	__device__ __forceinline__ void emit(int32_t a, int32_t b, uint32_t measure, uint32_t* err) const {
+		// (a*mul + (b - sub)) % n_groups in wrapping 32-bit arithmetic.
+		const int32_t key = static_cast<int32_t>(static_cast<uint32_t>(a) * static_cast<uint32_t>(mul) +
+		                                         (static_cast<uint32_t>(b) - static_cast<uint32_t>(sub)));
+		const int32_t g   = static_cast<uint32_t>(key) < static_cast<uint32_t>(n_groups) ? key : key % n_groups;
+		if (g < 0) {
+			raise_err(err, kErrHash);
+			return;
+		}
+		res[4 * g]     = b;
+		res[4 * g + 1] = a;
+		atomicAdd(reinterpret_cast<unsigned long long*>(res + 4 * g + 2),
+		          static_cast<unsigned long long>(static_cast<long long>(static_cast<int32_t>(measure))));
+	}
+};
+
+// Random-access form: leading PHT_1 probes run dense over the whole vector;
+// from the first PHT_2 probe on (or once few rows remain) every selected row is
+// probed and aggregated on its own, reading only its fields.  Used when every
+// probed / summed column holds only FOR, CONST or DICT vectors.
+struct ProbeGroupByRowOp : ProbeParams {
+	using State = TableState;
+
+	__device__ void cta_setup(State& S, uint32_t* cta_smem, const StageCfg&) const { stage_tables(S, cta_smem); }
+
+	__device__ void process(State& S, uint64_t v, const WarpStage& ws, uint32_t st, uint32_t i, uint32_t lane,
+	                        const StageCfg& cfg) const {
+		uint32_t mask = valid_rows(cfg, v, lane);
+		uint32_t p    = 0;
+		for (; p < n_probes && p_kind[p] == 1; ++p) {
+			if (max_rows(mask) <= sparse_rows) { break; }
+			const StagedVec sv = staged(ws, st, i, p_col[p]);
+			if (sv.bad() || !dev::random_access(sv.vi.scheme)) { return; }
+			uint32_t vals[32];
+			dev::decode_vals(sv.s, sv.vi, ws.dict(), lane, vals);
+			uint32_t hit[4] = {0, 0, 0, 0};
+#pragma unroll
+			for (uint32_t r = 0; r < 32; ++r) {
+				int32_t unused;
+				hit[r & 3] |= (probe(S, p, vals[r], &unused, cfg.err) ? 1u : 0u) << r;
+			}
+			mask &= (hit[0] | hit[1]) | (hit[2] | hit[3]);
+		}
+		// Row-at-a-time rest; FOR vectors use the hoisted fast field reader.
+		bool fast = staged(ws, st, i, agg_col).vi.scheme == FLS_SCHEME_FOR;
+		for (uint32_t q = p; q < n_probes; ++q) { fast = fast && staged(ws, st, i, p_col[q]).vi.scheme == FLS_SCHEME_FOR; }
+		if (fast) {
+			dev::ForRows kr[FLS_MAX_PROBES], mr;
+#pragma unroll
+			for (uint32_t q = 0; q < FLS_MAX_PROBES; ++q) {
+				if (q >= p && q < n_probes) {
+					const StagedVec sv = staged(ws, st, i, p_col[q]);
+					kr[q].init(sv.s, sv.vi, lane);
+				}
+			}
+			{
+				const StagedVec sv = staged(ws, st, i, agg_col);
+				mr.init(sv.s, sv.vi, lane);
+			}
+			const int n_it = max_rows(mask);
+			for (int it = 0; it < n_it; ++it) {
+				const bool     have = mask != 0u;
+				const uint32_t r    = have ? static_cast<uint32_t>(__ffs(mask)) - 1u : 0u;
+				mask &= mask - 1u;
+				int32_t a = 0, b = 0;
+				bool    pass = have;
+#pragma unroll
+				for (uint32_t q = 0; q < FLS_MAX_PROBES; ++q) {
+					if (q >= p && q < n_probes) {
+						int32_t val = 0;
+						const uint32_t key = kr[q].get(r);
+						if (pass) { pass = probe(S, q, key, &val, cfg.err); }
+						if (static_cast<int32_t>(q) == key_a) { a = val; }
+						if (static_cast<int32_t>(q) == key_b) { b = val; }
+					}
+				}
+				const uint32_t m = mr.get(r);
+				if (pass) { emit(a, b, m, cfg.err); }
+			}
+			return;
+		}
+		while (mask) {
+			const uint32_t r = static_cast<uint32_t>(__ffs(mask)) - 1u;
+			mask &= mask - 1u;
+			int32_t a = 0, b = 0;
+			bool    pass = true;
+			for (uint32_t q = p; q < n_probes && pass; ++q) {
+				const StagedVec sv = staged(ws, st, i, p_col[q]);
+				int32_t         val = 0;
+				pass = !sv.bad() && probe(S, q, dev::value_at(sv.s, sv.vi, lane, r), &val, cfg.err);
+				if (static_cast<int32_t>(q) == key_a) { a = val; }
+				if (static_cast<int32_t>(q) == key_b) { b = val; }
+			}
+			if (!pass) { continue; }
+			const StagedVec sm = staged(ws, st, i, agg_col);
+			if (sm.bad()) { continue; }
+			emit(a, b, dev::value_at(sm.s, sm.vi, lane, r), cfg.err);
+		}
+	}
+	__device__ void finish(State&, uint32_t, const StageCfg&) const {}
+};
+
+// General form (any scheme, including the running-sum schemes DELTA / RLE):
+// every probe and the aggregate are evaluated over whole vectors.
+struct ProbeGroupByDenseOp : ProbeParams {
+	using State = TableState;
+
+	__device__ void cta_setup(State& S, uint32_t* cta_smem, const StageCfg&) const { stage_tables(S, cta_smem); }
+
+	__device__ void process(State& S, uint64_t v, const WarpStage& ws, uint32_t st, uint32_t i, uint32_t lane,
 	                        const StageCfg& cfg) const {
 		uint32_t mask = valid_rows(cfg, v, lane);
 		uint32_t vals[32];
 		int32_t  pa[32], pb[32];
 		for (uint32_t p = 0; p < n_probes; ++p) {
-			if (!stage_decode(ws, st, p_col[p], lane, vals)) { return; }
-			const int32_t   len = p_len[p], kmin = p_min[p];
-			const bool      one     = p_kind[p] == 1;
-			const bool      in_smem = p_smem_off[p] != ~0u;
-			const uint32_t* tab     = S.tables + (in_smem ? p_smem_off[p] : 0u);
-			const int32_t*  ght     = p_ht[p];
-			const bool      wa = static_cast<int32_t>(p) == key_a, wb = static_cast<int32_t>(p) == key_b;
-			uint32_t        hit = 0;
+			const StagedVec sv = staged(ws, st, i, p_col[p]);
+			if (sv.bad()) { return; }
+			dev::decode_vals(sv.s, sv.vi, ws.dict(), lane, vals);
+			const bool wa = static_cast<int32_t>(p) == key_a, wb = static_cast<int32_t>(p) == key_b;
+			uint32_t   hit = 0;
 #pragma unroll
 			for (uint32_t r = 0; r < 32; ++r) {
 				if ((mask >> r) & 1u) {
-					// HASH(X,Y,Z) = (X-Z) % Y (join.cuh:26); in-range keys skip the division.
-					const int32_t d = static_cast<int32_t>(vals[r] - static_cast<uint32_t>(kmin));
-					int32_t       h = d;
-					bool          ok = true;
-					if (static_cast<uint32_t>(d) >= static_cast<uint32_t>(len)) {
-						h  = d % len;
-						ok = h >= 0;
-						if (!ok) { raise_err(cfg.err, kErrHash); }
-					}
-					if (ok) {
-						if (one) {
-							const bool f = in_smem ? ((tab[h >> 5] >> (h & 31)) & 1u) != 0u : (__ldg(ght + h) != 0);
-							hit |= (f ? 1u : 0u) << r;
-						} else {
-							const uint2 s = in_smem ? reinterpret_cast<const uint2*>(tab)[h]
-							                        : __ldg(reinterpret_cast<const uint2*>(ght) + h);
-							if (s.x | s.y) {
-								hit |= 1u << r;
-								if (wa) { pa[r] = static_cast<int32_t>(s.y); }
-								if (wb) { pb[r] = static_cast<int32_t>(s.y); }
-							}
-						}
+					int32_t val = 0;
+					if (probe(S, p, vals[r], &val, cfg.err)) {
+						hit |= 1u << r;
+						if (wa) { pa[r] = val; }
+						if (wb) { pb[r] = val; }
 					}
 				}
 			}
 			mask &= hit;
 			if (!__any_sync(0xffffffffu, mask)) { return; }
 		}
-		if (!stage_decode(ws, st, agg_col, lane, vals)) { return; }
+		const StagedVec sm = staged(ws, st, i, agg_col);
+		if (sm.bad()) { return; }
+		dev::decode_vals(sm.s, sm.vi, ws.dict(), lane, vals);
 #pragma unroll
 		for (uint32_t r = 0; r < 32; ++r) {
-			if ((mask >> r) & 1u) {
-				// (a*mul + (b - sub)) % n_groups in wrapping 32-bit arithmetic.
-				const int32_t key = static_cast<int32_t>(static_cast<uint32_t>(pa[r]) * static_cast<uint32_t>(mul) +
-				                                         (static_cast<uint32_t>(pb[r]) - static_cast<uint32_t>(sub)));
-				const int32_t g   = key % n_groups;
-				if (g < 0) {
-					raise_err(cfg.err, kErrHash);
-				} else {
-					res[4 * g]     = pb[r];
-					res[4 * g + 1] = pa[r];
-					atomicAdd(reinterpret_cast<unsigned long long*>(res + 4 * g + 2),
-					          static_cast<unsigned long long>(static_cast<long long>(static_cast<int32_t>(vals[r]))));
-				}
-			}
+			if ((mask >> r) & 1u) { emit(pa[r], pb[r], vals[r], cfg.err); }
 		}
 	}
 	__device__ void finish(State&, uint32_t, const StageCfg&) const {}
@@ -221,17 +494,42 @@ fls_status fls_query_filter_agg(const fls_filter_agg_desc* desc, int64_t* d_resu
 	FilterAggOp op {};
 	op.n_filters = desc->n_filters;
 	bool empty   = false;
+	// Evaluate the most selective filter first (the result does not depend on
+	// the order).  Selectivity is estimated for uniform FOR columns as the share
+	// of the column's value domain [base, base + 2^bw) inside the range; other
+	// columns keep their position.
+	fls_filter order[FLS_MAX_FILTERS];
+	double     sel[FLS_MAX_FILTERS];
 	for (uint32_t f = 0; f < desc->n_filters; ++f) {
-		const fls_filter& fl = desc->filters[f];
+		order[f] = desc->filters[f];
+		sel[f]   = 1.0;
+		if (order[f].col < desc->n_cols) {
+			const fls_column& c = desc->cols[order[f].col];
+			if (!c.meta && c.scheme == FLS_SCHEME_FOR && c.bw < 32) {
+				const double lo = std::max<double>(order[f].lo, c.base);
+				const double hi = std::min<double>(order[f].hi, static_cast<double>(c.base) + std::ldexp(1.0, c.bw) - 1);
+				sel[f]          = hi < lo ? 0.0 : (hi - lo + 1.0) / std::ldexp(1.0, c.bw);
+			}
+		}
+	}
+	for (uint32_t f = 1; f < desc->n_filters; ++f) { // stable insertion sort
+		for (uint32_t g = f; g > 0 && sel[g] < sel[g - 1]; --g) {
+			std::swap(sel[g], sel[g - 1]);
+			std::swap(order[g], order[g - 1]);
+		}
+	}
+	for (uint32_t f = 0; f < desc->n_filters; ++f) {
+		const fls_filter& fl = order[f];
 		if (fl.col >= desc->n_cols) { return set_error(FLS_ERR_INVALID_ARG, "filter column out of range"); }
 		empty         = empty || fl.lo > fl.hi;
 		op.f_col[f]   = fl.col;
 		op.f_lo[f]    = static_cast<uint32_t>(fl.lo);
 		op.f_range[f] = static_cast<uint32_t>(fl.hi) - static_cast<uint32_t>(fl.lo);
 	}
-	op.agg_a  = desc->agg_a;
-	op.agg_b  = desc->agg_b;
-	op.result = reinterpret_cast<long long*>(d_result);
+	op.agg_a       = desc->agg_a;
+	op.agg_b       = desc->agg_b;
+	op.result      = reinterpret_cast<long long*>(d_result);
+	op.sparse_rows = tuning_sparse_rows();
 	StageCfg   cfg;
 	uint32_t   grid, threads;
 	size_t     smem;
@@ -273,7 +571,7 @@ fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res
 	    desc->probes[desc->key_a].kind != 2 || desc->probes[desc->key_b].kind != 2) {
 		return set_error(FLS_ERR_INVALID_ARG, "group keys must name PHT_2 probes");
 	}
-	ProbeGroupByOp op {};
+	ProbeParams op {};
 	op.n_probes = desc->n_probes;
 	// Small tables go to shared memory, first come first served.
 	uint32_t       cta_words = 0;
@@ -305,8 +603,17 @@ fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res
 	op.mul      = desc->group_mul;
 	op.sub      = desc->group_sub;
 	op.n_groups = desc->n_groups;
-	op.agg_col  = desc->agg_col;
-	op.res      = d_res;
+	op.agg_col     = desc->agg_col;
+	op.res         = d_res;
+	op.sparse_rows = tuning_sparse_rows();
+	// The row-at-a-time form needs random access to every column it reads.
+	const uint32_t seq_schemes = (1u << FLS_SCHEME_DELTA) | (1u << FLS_SCHEME_RLE);
+	bool           rnd         = true;
+	for (uint32_t c = 0; c < desc->n_cols; ++c) {
+		const fls_column& col = desc->cols[c];
+		const uint32_t    mask = col.meta ? col.scheme_mask : (1u << col.scheme);
+		rnd                   = rnd && !(mask & seq_schemes);
+	}
 	StageCfg   cfg;
 	uint32_t   grid, threads;
 	size_t     smem;
@@ -316,7 +623,14 @@ fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res
 	s = cuda_check(cudaMemsetAsync(d_res, 0, sizeof(int32_t) * 4u * static_cast<size_t>(desc->n_groups), st),
 	               "cudaMemsetAsync");
 	if (s != FLS_OK) { return s; }
-	return launch_staged(cfg, op, grid, threads, smem, st);
+	if (rnd) {
+		ProbeGroupByRowOp rop;
+		static_cast<ProbeParams&>(rop) = op;
+		return launch_staged(cfg, rop, grid, threads, smem, st);
+	}
+	ProbeGroupByDenseOp dop;
+	static_cast<ProbeParams&>(dop) = op;
+	return launch_staged(cfg, dop, grid, threads, smem, st);
 }
 
 } // extern "C"

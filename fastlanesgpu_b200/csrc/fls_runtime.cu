@@ -20,7 +20,7 @@ namespace {
 std::atomic<uint64_t> g_launches {0};
 
 struct LaunchCfg {
-	uint32_t warps = 8, stages = 3, ctas_per_sm = 1;
+	uint32_t warps = 16, stages = 2, ctas_per_sm = 1, tile_bytes = 6144;
 };
 std::mutex g_cfg_mu;
 LaunchCfg  g_cfg;
@@ -38,6 +38,13 @@ std::vector<uint32_t*>  g_err_addr;
 } // namespace
 
 void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+namespace {
+constexpr int    kDefaultSparseRows = 4;
+std::atomic<int> g_sparse_rows {kDefaultSparseRows};
+} // namespace
+
+int tuning_sparse_rows() { return g_sparse_rows.load(std::memory_order_relaxed); }
 
 fls_status cuda_check(cudaError_t e, const char* what) {
 	if (e == cudaSuccess) { return FLS_OK; }
@@ -96,8 +103,8 @@ fls_status make_devcol(const fls_column& c, DevCol& d) {
 	d.data    = c.data;
 	d.meta    = c.meta;
 	d.n_words = c.n_words;
-	d.layout  = c.layout;
-	d.pad_    = 0;
+	d.layout    = c.layout;
+	d.vec_words = 0;
 	if (c.meta == nullptr) {
 		if (c.scheme != FLS_SCHEME_FOR && c.scheme != FLS_SCHEME_DELTA) {
 			return set_error(FLS_ERR_INVALID_ARG, "uniform columns must be FOR or DELTA");
@@ -110,6 +117,7 @@ fls_status make_devcol(const fls_column& c, DevCol& d) {
 		d.bw                 = c.bw;
 		d.base               = c.base;
 		d.slot_words         = dev::payload_words(c.scheme, c.bw, 0);
+		d.vec_words          = d.slot_words;
 		const uint64_t n_vec = (c.n_values + 1023u) / 1024u;
 		if (static_cast<uint64_t>(d.slot_words) * n_vec > c.n_words) {
 			return set_error(FLS_ERR_CAPACITY, "column data smaller than n_values at this bit width");
@@ -139,41 +147,60 @@ fls_status plan_stages(const fls_column* cols, uint32_t n_cols, uint32_t extra_w
 	fls_status s = device_info(di);
 	if (s != FLS_OK) { return s; }
 	std::memset(&cfg, 0, sizeof(cfg));
-	bool dict    = false;
-	cfg.n_values = cols[0].n_values;
-	cfg.layout   = cols[0].layout;
+	bool     dict     = false;
+	bool     uniform  = true;
+	uint32_t vec_words[kMaxCols];
+	uint32_t sum_vec  = 0;
+	cfg.n_values      = cols[0].n_values;
+	cfg.layout        = cols[0].layout;
 	for (uint32_t c = 0; c < n_cols; ++c) {
 		if ((s = make_devcol(cols[c], cfg.cols[c])) != FLS_OK) { return s; }
 		if (cols[c].n_values != cfg.n_values) { return set_error(FLS_ERR_INVALID_ARG, "columns differ in length"); }
 		if (cols[c].layout != cfg.layout) {
 			return set_error(FLS_ERR_UNSUPPORTED, "all columns of a query must share one layout");
 		}
-		cfg.col_off[c] = cfg.stage_words;
-		cfg.stage_words += cfg.cols[c].slot_words;
-		dict = dict || needs_dict(cols[c]);
+		vec_words[c] = cfg.cols[c].slot_words; // one vector's slot
+		sum_vec += vec_words[c];
+		dict    = dict || needs_dict(cols[c]);
+		uniform = uniform && cols[c].meta == nullptr;
 	}
-	cfg.n_cols    = n_cols;
-	cfg.has_dict  = dict ? 1u : 0u;
-	cfg.n_vec     = (cfg.n_values + 1023u) / 1024u;
-	cfg.err       = device_error_word();
-	LaunchCfg lc  = launch_cfg();
+	cfg.n_cols      = n_cols;
+	cfg.all_uniform = uniform ? 1u : 0u;
+	cfg.has_dict = dict ? 1u : 0u;
+	cfg.n_vec    = (cfg.n_values + 1023u) / 1024u;
+	cfg.err      = device_error_word();
+	LaunchCfg lc = launch_cfg();
 	uint32_t  W = lc.warps, S = lc.stages;
+	// Tile: enough consecutive vectors for ~tile_bytes per stage, but keep at
+	// least 4 tiles per warp of the grid for load balance.
+	const uint64_t total_warps = static_cast<uint64_t>(di.sms) * lc.ctas_per_sm * W;
+	uint32_t       k           = sum_vec ? std::max<uint32_t>(1u, lc.tile_bytes / (4u * sum_vec)) : kMaxTile;
+	k                          = std::min<uint32_t>(k, kMaxTile / n_cols); // one lane per (vector, column) at issue
+	while (k > 1 && (cfg.n_vec + k - 1) / k < 4 * total_warps) { k /= 2; }
 	// Shrink the pipeline until it fits the shared-memory budget.
 	for (;;) {
-		uint32_t w = S * cfg.stage_words;
+		cfg.stage_words = 0;
+		for (uint32_t c = 0; c < n_cols; ++c) {
+			cfg.cols[c].slot_words = k * vec_words[c];
+			cfg.col_off[c]         = cfg.stage_words;
+			cfg.stage_words += cfg.cols[c].slot_words;
+		}
+		uint32_t w   = S * cfg.stage_words + kSlotSlackWords;
 		cfg.dict_off = w;
 		w += dict ? kDictWords : 0u;
 		cfg.extra_off = w;
 		w += round4(extra_words);
 		cfg.info_off = w;
-		w += 2u * kMaxCols * S;
+		w += 4u * S * k * n_cols;
 		cfg.bar_off = w;
 		w += 2u * S;
 		w                   = round4(w);
 		cfg.warp_smem_words = w;
 		smem_bytes          = 4ull * (static_cast<size_t>(w) * W + cta_words);
 		if (smem_bytes <= static_cast<size_t>(di.max_smem)) { break; }
-		if (S > 2) {
+		if (k > 1) {
+			k /= 2;
+		} else if (S > 2) {
 			--S;
 		} else if (W > 1) {
 			W /= 2;
@@ -181,10 +208,12 @@ fls_status plan_stages(const fls_column* cols, uint32_t n_cols, uint32_t extra_w
 			return set_error(FLS_ERR_CAPACITY, "vectors too large for shared-memory staging");
 		}
 	}
+	cfg.tile                 = k;
+	cfg.n_tiles              = (cfg.n_vec + k - 1) / k;
 	cfg.stages               = S;
 	cfg.warps                = W;
 	cfg.cta_extra_off        = cfg.warp_smem_words * W;
-	const uint64_t need_ctas = (cfg.n_vec + W - 1) / W;
+	const uint64_t need_ctas = (cfg.n_tiles + W - 1) / W;
 	grid    = static_cast<uint32_t>(std::min<uint64_t>(need_ctas, static_cast<uint64_t>(di.sms) * lc.ctas_per_sm));
 	threads = 32u * W;
 	return FLS_OK;
@@ -217,25 +246,49 @@ fls_status fls_check_device_error(fls_stream_t stream) {
 	return set_error(FLS_ERR_DEVICE, msg);
 }
 
-fls_status fls_set_launch_config(uint32_t warps_per_cta, uint32_t stages, uint32_t ctas_per_sm) {
-	if (warps_per_cta > 8 || stages > 8 || ctas_per_sm > 8 || (stages != 0 && stages < 2)) {
-		return set_error(FLS_ERR_INVALID_ARG, "launch config out of range (warps <= 8, 2 <= stages <= 8, ctas <= 8)");
+fls_status fls_set_launch_config(uint32_t warps_per_cta, uint32_t stages, uint32_t ctas_per_sm, uint32_t tile_bytes) {
+	if (warps_per_cta > kMaxWarps || stages > 8 || ctas_per_sm > 4 || (stages != 0 && stages < 2) ||
+	    tile_bytes > 65536) {
+		return set_error(FLS_ERR_INVALID_ARG,
+		                 "launch config out of range (warps <= 16, 2 <= stages <= 8, ctas <= 4, tile_bytes <= 64K)");
 	}
+	const LaunchCfg d;
 	std::lock_guard<std::mutex> lk(g_cfg_mu);
-	g_cfg.warps       = warps_per_cta ? warps_per_cta : 8u;
-	g_cfg.stages      = stages ? stages : 3u;
-	g_cfg.ctas_per_sm = ctas_per_sm ? ctas_per_sm : 1u;
+	g_cfg.warps       = warps_per_cta ? warps_per_cta : d.warps;
+	g_cfg.stages      = stages ? stages : d.stages;
+	g_cfg.ctas_per_sm = ctas_per_sm ? ctas_per_sm : d.ctas_per_sm;
+	g_cfg.tile_bytes  = tile_bytes ? tile_bytes : d.tile_bytes;
 	return FLS_OK;
 }
 
-fls_status fls_get_launch_config(uint32_t* warps_per_cta, uint32_t* stages, uint32_t* ctas_per_sm) {
+fls_status fls_get_launch_config(uint32_t* warps_per_cta, uint32_t* stages, uint32_t* ctas_per_sm,
+                                 uint32_t* tile_bytes) {
 	LaunchCfg c = launch_cfg();
 	if (warps_per_cta) { *warps_per_cta = c.warps; }
 	if (stages) { *stages = c.stages; }
 	if (ctas_per_sm) { *ctas_per_sm = c.ctas_per_sm; }
+	if (tile_bytes) { *tile_bytes = c.tile_bytes; }
 	return FLS_OK;
 }
 
 uint64_t fls_kernel_launch_count(void) { return g_launches.load(); }
+
+fls_status fls_set_tuning(uint32_t param, int64_t value) {
+	switch (param) {
+	case FLS_TUNE_SPARSE_ROWS:
+		if (value < 0 || value > 32) { return set_error(FLS_ERR_INVALID_ARG, "sparse rows must be in [0, 32]"); }
+		g_sparse_rows.store(value ? static_cast<int>(value) : kDefaultSparseRows);
+		return FLS_OK;
+	default: return set_error(FLS_ERR_INVALID_ARG, "unknown tuning parameter");
+	}
+}
+
+fls_status fls_get_tuning(uint32_t param, int64_t* value) {
+	if (!value) { return set_error(FLS_ERR_INVALID_ARG, "fls_get_tuning: null pointer"); }
+	switch (param) {
+	case FLS_TUNE_SPARSE_ROWS: *value = tuning_sparse_rows(); return FLS_OK;
+	default: return set_error(FLS_ERR_INVALID_ARG, "unknown tuning parameter");
+	}
+}
 
 } // extern "C"

@@ -181,14 +181,25 @@ def check_device_error() -> None:
     check(lib().fls_check_device_error(_stream()), "device")
 
 
-def set_launch_config(warps: int = 0, stages: int = 0, ctas_per_sm: int = 0) -> None:
-    check(lib().fls_set_launch_config(warps, stages, ctas_per_sm), "fls_set_launch_config")
+def set_launch_config(warps: int = 0, stages: int = 0, ctas_per_sm: int = 0, tile_bytes: int = 0) -> None:
+    """0 keeps the library default of that field."""
+    check(lib().fls_set_launch_config(warps, stages, ctas_per_sm, tile_bytes), "fls_set_launch_config")
 
 
 def get_launch_config():
-    w, s, c = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
-    lib().fls_get_launch_config(ctypes.addressof(w), ctypes.addressof(s), ctypes.addressof(c))
-    return w.value, s.value, c.value
+    w, s, c, t = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    lib().fls_get_launch_config(ctypes.addressof(w), ctypes.addressof(s), ctypes.addressof(c), ctypes.addressof(t))
+    return w.value, s.value, c.value, t.value
+
+
+def set_tuning(param: int, value: int) -> None:
+    check(lib().fls_set_tuning(param, value), "fls_set_tuning")
+
+
+def get_tuning(param: int) -> int:
+    v = ctypes.c_int64()
+    check(lib().fls_get_tuning(param, ctypes.addressof(v)), "fls_get_tuning")
+    return v.value
 
 
 def kernel_launch_count() -> int:

@@ -222,11 +222,23 @@ fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res
 
 /* --------------------------------------------------------- tuning */
 
-/* Launch shape of the staged decode/query kernels: warps per CTA, pipeline
- * stages per warp and CTAs per SM (0 = library default).  Used by the
+/* Launch shape of the staged decode/query kernels: warps per CTA (<= 16),
+ * pipeline stages per warp, CTAs per SM and the target bytes of one staged
+ * tile of consecutive vectors (0 = library default for each).  Used by the
  * autotuner; applies to subsequent calls from all threads. */
-fls_status fls_set_launch_config(uint32_t warps_per_cta, uint32_t stages, uint32_t ctas_per_sm);
-fls_status fls_get_launch_config(uint32_t* warps_per_cta, uint32_t* stages, uint32_t* ctas_per_sm);
+fls_status fls_set_launch_config(uint32_t warps_per_cta, uint32_t stages, uint32_t ctas_per_sm, uint32_t tile_bytes);
+fls_status fls_get_launch_config(uint32_t* warps_per_cta, uint32_t* stages, uint32_t* ctas_per_sm,
+                                 uint32_t* tile_bytes);
+
+/* Other tuning parameters of the operators (0 restores the default). */
+typedef enum fls_tune_param {
+	/* Operators evaluate whole vectors while some lane of a warp still has more
+	 * than this many selected rows in its 32; at or below it they switch to a
+	 * loop over the selected rows that reads only their fields.  Default 4. */
+	FLS_TUNE_SPARSE_ROWS = 0
+} fls_tune_param;
+fls_status fls_set_tuning(uint32_t param, int64_t value);
+fls_status fls_get_tuning(uint32_t param, int64_t* value);
 
 /* Number of kernels this library has launched in this process (all threads). */
 uint64_t fls_kernel_launch_count(void);

@@ -32,7 +32,7 @@ def test_argument_errors_are_status_codes():
     assert L.fls_pack_u32(x.ctypes.data, out.ctypes.data, 33) == 2
     assert b"bit width" in L.fls_last_error()
     assert L.fls_pack_u32(None, out.ctypes.data, 3) == 1
-    assert L.fls_set_launch_config(99, 3, 1) == 1
+    assert L.fls_set_launch_config(99, 3, 1, 0) == 1
     assert L.fls_decode_u32(None, None, 0, None) == 1
 
 

@@ -145,7 +145,7 @@ def test_sizes_and_tails(cuda, n):
         assert int(_np(ops.query_aggregate(d))[0]) == int(vals.view(np.uint32).astype(np.uint64).sum())
 
 
-@pytest.mark.parametrize("cfg", [(1, 2, 1), (2, 2, 2), (4, 3, 1), (8, 4, 1), (8, 2, 2)])
+@pytest.mark.parametrize("cfg", [(1, 2, 1, 0), (2, 2, 2, 512), (4, 3, 1, 0), (8, 4, 1, 4096), (16, 2, 1, 16384), (16, 3, 1, 65536), (8, 2, 2, 2048)])
 def test_launch_configs_agree(cuda, cfg):
     vals = datagen.for_bitpack_mixed(300 * 1024 + 5, seed=8)
     d = EncodedColumn.encode(vals, 0).to_device()
@@ -154,7 +154,7 @@ def test_launch_configs_agree(cuda, cfg):
         assert np.array_equal(_np(ops.unpack_global(d, ORDER_ORIGINAL))[:vals.size], vals)
         assert int(_np(ops.query_aggregate(d))[0]) == int(vals.view(np.uint32).astype(np.uint64).sum())
     finally:
-        ops.set_launch_config(0, 0, 0)
+        ops.set_launch_config(0, 0, 0, 0)
 
 
 def test_bad_metadata_is_reported_not_read(cuda):

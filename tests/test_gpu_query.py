@@ -165,3 +165,25 @@ def test_probe_out_of_range_keys_flagged(cuda, oracle):
     with pytest.raises(FlsError):
         ops.check_device_error()
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("sparse_rows", [1, 4, 8, 32])
+def test_sparse_threshold_does_not_change_results(cuda, oracle, sparse_rows):
+    """Dense and row-at-a-time evaluation give identical answers."""
+    n = 100 * 1024 + 1
+    t = datagen.lineorder_q11(n, seed=9)
+    f = datagen.Q11_FILTER
+    want = oracle.filter_agg(t["date"], t["discount"], t["quantity"], t["price"], *f["date"], *f["discount"],
+                             f["quantity"][1] + 1)
+    tq, ht_s, ht_p, ht_d = _q21(n, 25, 1 << 14, 1 << 10)
+    want21 = oracle.probe_groupby(tq["lo_suppkey"], tq["lo_partkey"], tq["lo_orderdate"], tq["lo_revenue"],
+                                  ht_s.cpu().numpy(), ht_p.cpu().numpy(), ht_d.cpu().numpy())
+    try:
+        ops.set_tuning(0, sparse_rows)
+        for per_vector in (False, True):
+            cols = [c.to_device() for c in _q11_cols(t, per_vector=per_vector)]
+            assert int(_q11(cols).cpu()[0]) == want
+            _, got = _q21_run(tq, (ht_s, ht_p, ht_d), per_vector=per_vector)
+            assert np.array_equal(got, want21)
+    finally:
+        ops.set_tuning(0, 0)
