@@ -23,6 +23,8 @@ LAYOUT_NORMAL, LAYOUT_TRANSPOSED = 0, 1
 ORDER_STORED, ORDER_ORIGINAL = 0, 1
 MAX_QUERY_COLS, MAX_FILTERS, MAX_PROBES = 8, 4, 4
 TUNE_SPARSE_ROWS = 0
+MLP_IN, MLP_HIDDEN, MLP_OUT = 16, 64, 5
+MLP_N_PARAMS = 64 * 16 + 64 + 64 * 64 + 64 + 5 * 64 + 5
 
 
 class FlsError(RuntimeError):
@@ -53,6 +55,11 @@ class FilterAggDesc(ctypes.Structure):
     _fields_ = [("cols", ctypes.POINTER(Column)), ("n_cols", ctypes.c_uint32),
                 ("filters", Filter * MAX_FILTERS), ("n_filters", ctypes.c_uint32),
                 ("agg_a", ctypes.c_int32), ("agg_b", ctypes.c_int32)]
+
+
+class BatchQuery(ctypes.Structure):
+    _fields_ = [("col", ctypes.c_uint32), ("lo", ctypes.c_int32), ("hi", ctypes.c_int32), ("agg_col", ctypes.c_uint32),
+                ("n_values", ctypes.c_uint64)]
 
 
 class Probe(ctypes.Structure):
@@ -96,7 +103,25 @@ _SIGS = {
     "fls_set_launch_config": (ctypes.c_int, [ctypes.c_uint32] * 4),
     "fls_get_launch_config": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
     "fls_kernel_launch_count": (ctypes.c_uint64, []),
+    "fls_crystal_q11": (ctypes.c_int, [_VP, ctypes.c_uint32] * 4 + [ctypes.c_uint64] + [ctypes.c_int32] * 5
+                        + [_VP, _VP]),
+    "fls_crystal_q21_probe": (ctypes.c_int, [_VP, ctypes.c_uint32] * 4 + [ctypes.c_uint64]
+                              + [_VP, ctypes.c_int32] * 3 + [ctypes.c_int32, _VP, _VP]),
     "fls_set_tuning": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_int64]),
+    "fls_vector_stats_gpu": (ctypes.c_int, [_VP, ctypes.c_uint64, _VP, _VP]),
+    "fls_batch_create": (ctypes.c_int, [ctypes.POINTER(Column), ctypes.c_uint32, ctypes.POINTER(BatchQuery),
+                                        ctypes.c_uint32, ctypes.c_uint32, _VP]),
+    "fls_batch_workspace_bytes": (ctypes.c_uint64, [_VP]),
+    "fls_batch_items": (ctypes.c_uint32, [_VP]),
+    "fls_batch_upload": (ctypes.c_int, [_VP, _VP, ctypes.c_uint64, _VP]),
+    "fls_batch_run": (ctypes.c_int, [_VP, _VP, _VP]),
+    "fls_batch_destroy": (None, [_VP]),
+    "fls_mlp_init": (ctypes.c_int, [_VP, ctypes.c_uint64, _VP]),
+    "fls_mlp_workspace_bytes": (ctypes.c_uint64, [ctypes.c_uint32]),
+    "fls_mlp_gradients": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_uint32, _VP, ctypes.c_uint64, _VP, _VP, _VP]),
+    "fls_mlp_adam_step": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                         ctypes.c_float, ctypes.c_uint32, _VP]),
+    "fls_mlp_infer": (ctypes.c_int, [_VP, _VP, ctypes.c_uint64, _VP, _VP, _VP, _VP]),
     "fls_get_tuning": (ctypes.c_int, [ctypes.c_uint32, _VP]),
 }
 

@@ -1,0 +1,86 @@
+"""Autotuner of the staged kernels' launch shape.
+
+Sweeps warps per CTA, pipeline stages, tile bytes (vectors per staged tile)
+and the dense/row-at-a-time threshold for a workload, times each candidate
+with CUDA events after warm-up, keeps the fastest and caches it in a JSON file
+keyed by the workload's signature (default ~/.cache/fastlanesgpu_b200/
+autotune.json, or $FLS_AUTOTUNE_CACHE)."""
+from __future__ import annotations
+
+import itertools
+import json
+import os
+
+from . import ops
+
+DEFAULT_SPACE = {
+    "warps": [8, 16],
+    "stages": [2, 3],
+    "tile_bytes": [2048, 6144, 16384],
+    "sparse_rows": [2, 4, 8],
+}
+
+
+def cache_path() -> str:
+    return os.environ.get("FLS_AUTOTUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "fastlanesgpu_b200", "autotune.json"))
+
+
+def _load(path):
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def apply(cfg: dict) -> None:
+    ops.set_launch_config(cfg["warps"], cfg["stages"], 0, cfg["tile_bytes"])
+    ops.set_tuning(0, cfg["sparse_rows"])
+
+
+def time_ms(fn, warmup: int = 3, iters: int = 10) -> float:
+    import torch
+    for _ in range(warmup):
+        fn()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(iters):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / iters
+
+
+def tune(signature: str, fn, space: dict | None = None, iters: int = 10, use_cache: bool = True,
+         path: str | None = None) -> dict:
+    """Best launch configuration for `fn` (a callable enqueueing the workload);
+    applies it and returns {config, ms, candidates}."""
+    path = path or cache_path()
+    cache = _load(path) if use_cache else {}
+    if use_cache and signature in cache:
+        apply(cache[signature]["config"])
+        return cache[signature]
+    space = space or DEFAULT_SPACE
+    keys = list(space)
+    results = []
+    for combo in itertools.product(*[space[k] for k in keys]):
+        cfg = dict(zip(keys, combo))
+        apply(cfg)
+        results.append((time_ms(fn, iters=iters), cfg))
+    results.sort(key=lambda x: x[0])
+    best = {"config": results[0][1], "ms": results[0][0],
+            "candidates": [{"ms": m, **c} for m, c in results]}
+    apply(best["config"])
+    if use_cache:
+        cache[signature] = best
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        with open(path, "w") as f:
+            json.dump(cache, f, indent=1)
+    return best
+
+
+def reset() -> None:
+    ops.set_launch_config(0, 0, 0, 0)
+    ops.set_tuning(0, 0)

@@ -1,0 +1,346 @@
+// fls_batch.cu -- batched persistent execution of many filter-aggregate queries
+// over many columns of uneven length and bit width in one launch.
+//
+// The host cuts every query (filter lo <= x <= hi on one column, sum of
+// another column of the same length) into work items of `chunk` consecutive
+// vectors.  One persistent kernel runs all items: each warp pulls the next item
+// from a global counter (dynamic load balancing across columns of very
+// different lengths), streams the item's vectors through its own two-slot
+// bulk-copy pipeline, and adds the item's sum and count into the query's
+// result with one atomic each.  fls_batch_run only resets the counter and
+// launches, so it can be captured into a CUDA graph and replayed.
+//
+// No reference counterpart: the reference launches one grid per query
+// (fls_q11.cu:150-160).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "fls_pipeline.cuh"
+
+struct fls_batch {
+	std::vector<fls::DevCol>    cols;
+	std::vector<fls_batch_query> queries;
+	std::vector<uint4>           items; // {query, first vector, end vector, 0}
+	uint32_t                     slot_words = 0;
+	uint32_t                     has_dict   = 0;
+	void*                        ws         = nullptr; // device workspace after upload
+	uint64_t                     ws_bytes   = 0;
+};
+
+namespace fls {
+namespace {
+
+constexpr uint32_t kBatchStages = 3;
+
+struct BatchParams {
+	const DevCol*          cols;
+	const fls_batch_query* queries;
+	const uint4*           items;
+	uint32_t               n_items;
+	uint32_t*              counter;
+	long long*             results; // 2 per query: sum, count
+	uint32_t               slot_words;
+	uint32_t               has_dict;
+	uint32_t               warps;
+	uint32_t*              err;
+};
+
+// Per warp shared memory: kBatchStages x {filter slot, aggregate slot},
+// slack, dictionary scratch, stage infos and barriers.
+struct BatchLayout {
+	uint32_t slots, dict, info, bars, total;
+	__host__ __device__ BatchLayout(uint32_t slot_words) {
+		slots = 0;
+		dict  = slots + kBatchStages * 2u * slot_words + kSlotSlackWords;
+		info  = dict + kDictWords;
+		bars  = info + kBatchStages * 2u * 4u;
+		total = (bars + 2u * kBatchStages + 3u) & ~3u;
+	}
+};
+
+// Stages vector v of the filter column (slot 0) and, unless it is the same
+// column, of the aggregated column (slot 1).
+__device__ __forceinline__ bool batch_issue(const BatchParams& P, uint32_t* base, const BatchLayout& L, uint32_t st,
+                                            const DevCol& cf, const DevCol& ca, bool same, uint64_t v, uint32_t lane,
+                                            uint64_t pol) {
+	uint4*    info = reinterpret_cast<uint4*>(base + L.info) + st * 2u;
+	uint64_t* bar  = reinterpret_cast<uint64_t*>(base + L.bars) + st;
+	bool      ok   = true;
+	if (lane < (same ? 1u : 2u)) {
+		const DevCol& c  = lane == 0 ? cf : ca;
+		VecInfo       vi {};
+		ok               = dev::vec_info(c, v, dev::load_meta(c, v), vi);
+		if (ok && !P.has_dict && (vi.scheme == FLS_SCHEME_RLE || vi.scheme == FLS_SCHEME_DICT)) { ok = false; }
+		info[lane] = ok ? make_uint4(static_cast<uint32_t>(vi.base), vi.scheme | (vi.bw << 8) | (vi.aux << 16), 0u, 0u)
+		                : make_uint4(0u, kBadScheme, 0u, 0u);
+		if (!ok) { raise_err(P.err, kErrBadMeta); }
+		if (ok && vi.words) {
+			dev::mbar_expect_tx(bar, vi.words * 4u);
+			dev::bulk_g2s(base + L.slots + (st * 2u + lane) * P.slot_words, c.data + vi.offset, vi.words * 4u, bar, pol);
+		}
+	}
+	__syncwarp();
+	if (lane == 0) { dev::mbar_arrive(bar); }
+	__syncwarp();
+	return ok;
+}
+
+__global__ void __launch_bounds__(kMaxWarps * 32, 1) batch_kernel(const __grid_constant__ BatchParams P) {
+	extern __shared__ __align__(128) uint32_t smem[];
+	const uint32_t    lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+	const BatchLayout L(P.slot_words);
+	uint32_t*         base = smem + warp * L.total;
+	uint64_t*         bars = reinterpret_cast<uint64_t*>(base + L.bars);
+	if (lane == 0) {
+		for (uint32_t s = 0; s < kBatchStages; ++s) { dev::mbar_init(bars + s, 1); }
+		dev::fence_mbar_init();
+	}
+	__syncwarp();
+	const uint64_t pol   = dev::l2_evict_first_policy();
+	uint32_t       phase = 0, st = 0; // running stage / phase across items
+	for (;;) {
+		uint32_t item = 0;
+		if (lane == 0) { item = atomicAdd(P.counter, 1u); }
+		item = __shfl_sync(0xffffffffu, item, 0);
+		if (item >= P.n_items) { break; }
+		const uint4            it = P.items[item];
+		const fls_batch_query& q  = P.queries[it.x];
+		const DevCol&          cf = P.cols[q.col];
+		const DevCol&          ca = P.cols[q.agg_col];
+		const uint64_t         v0 = it.y, v1 = it.z;
+		const uint32_t         lo = static_cast<uint32_t>(q.lo), range = static_cast<uint32_t>(q.hi) - lo;
+		const bool             empty = q.lo > q.hi;
+		const bool             same  = q.col == q.agg_col;
+		// prologue
+		uint32_t s_issue = st;
+		for (uint32_t k = 0; k < kBatchStages && v0 + k < v1; ++k) {
+			batch_issue(P, base, L, s_issue, cf, ca, same, v0 + k, lane, pol);
+			s_issue = (s_issue + 1u == kBatchStages) ? 0u : s_issue + 1u;
+		}
+		long long          sum = 0;
+		unsigned long long cnt = 0;
+		for (uint64_t v = v0; v < v1; ++v) {
+			if (!dev::mbar_wait_bounded(bars + st, phase, kWaitPolls)) {
+				raise_err(P.err, kErrTimeout);
+				for (uint32_t s = 0; s < kBatchStages; ++s) {
+					dev::mbar_wait_bounded(bars + s, phase, 1u << 10);
+					dev::mbar_wait_bounded(bars + s, phase ^ 1u, 1u << 10);
+				}
+				return;
+			}
+			const uint4* info = reinterpret_cast<const uint4*>(base + L.info) + st * 2u;
+			const uint4  fi = info[0], ai = same ? info[0] : info[1];
+			if ((fi.y & 0xffu) != kBadScheme && (ai.y & 0xffu) != kBadScheme && !empty) {
+				VecInfo vf {}, va {};
+				vf.base = static_cast<int32_t>(fi.x), vf.scheme = fi.y & 0xffu, vf.bw = (fi.y >> 8) & 0xffu;
+				vf.aux  = fi.y >> 16;
+				va.base = static_cast<int32_t>(ai.x), va.scheme = ai.y & 0xffu, va.bw = (ai.y >> 8) & 0xffu;
+				va.aux  = ai.y >> 16;
+				const uint32_t* sf = base + L.slots + (st * 2u) * P.slot_words;
+				const uint32_t* sa = same ? sf : sf + P.slot_words;
+				// rows of a partial last vector
+				const uint64_t rows  = q.n_values;
+				uint32_t       mask  = 0xffffffffu;
+				if ((v + 1) * 1024u > rows) {
+					mask = dev::tail_rows(cf.layout, lane, static_cast<uint32_t>(rows - v * 1024u));
+				}
+				const uint32_t flo = lo - dev::value_offset(vf);
+				uint32_t       m[4] = {0, 0, 0, 0};
+				dev::decode_each<false>(sf, vf, base + L.dict, lane,
+				                        [&](int r, uint32_t x) { m[r & 3] |= (x - flo <= range ? 1u : 0u) << r; });
+				mask &= (m[0] | m[1]) | (m[2] | m[3]);
+				cnt += static_cast<unsigned>(__popc(mask));
+				if (__reduce_max_sync(0xffffffffu, __popc(mask)) <= 4 && va.scheme == FLS_SCHEME_FOR) {
+					dev::ForRows ra;
+					ra.init(sa, va, lane);
+					const int n_it = __reduce_max_sync(0xffffffffu, __popc(mask));
+					uint32_t  mm   = mask;
+					for (int k = 0; k < n_it; ++k) {
+						const bool     have = mm != 0u;
+						const uint32_t r    = have ? static_cast<uint32_t>(__ffs(mm)) - 1u : 0u;
+						mm &= mm - 1u;
+						const long long x = static_cast<int32_t>(ra.get(r));
+						sum += have ? x : 0ll;
+					}
+				} else if (__any_sync(0xffffffffu, mask)) {
+					long long p[4] = {0, 0, 0, 0};
+					dev::decode_each<true>(sa, va, base + L.dict, lane, [&](int r, uint32_t x) {
+						p[r & 3] += ((mask >> r) & 1u) ? static_cast<long long>(static_cast<int32_t>(x)) : 0ll;
+					});
+					sum += (p[0] + p[1]) + (p[2] + p[3]);
+				}
+			}
+			__syncwarp();
+			if (v + kBatchStages < v1) {
+				dev::fence_proxy_async_smem();
+				batch_issue(P, base, L, st, cf, ca, same, v + kBatchStages, lane, pol);
+			}
+			if (++st == kBatchStages) {
+				st = 0;
+				phase ^= 1u;
+			}
+		}
+		const unsigned long long s = warp_sum_u64(static_cast<unsigned long long>(sum));
+		const unsigned long long c = warp_sum_u64(cnt);
+		if (lane == 0) {
+			if (s) { atomicAdd(reinterpret_cast<unsigned long long*>(P.results + 2u * it.x), s); }
+			if (c) { atomicAdd(reinterpret_cast<unsigned long long*>(P.results + 2u * it.x + 1u), c); }
+		}
+	}
+}
+
+size_t ws_align(size_t x) { return (x + 255u) & ~static_cast<size_t>(255u); }
+
+struct WsLayout {
+	size_t cols, queries, items, counter, total;
+	explicit WsLayout(const fls_batch& b) {
+		cols    = 0;
+		queries = cols + ws_align(b.cols.size() * sizeof(DevCol));
+		items   = queries + ws_align(b.queries.size() * sizeof(fls_batch_query));
+		counter = items + ws_align(b.items.size() * sizeof(uint4));
+		total   = counter + 256;
+	}
+};
+
+} // namespace
+
+// Shared by fls_batch_run and its static-scratch variant.
+fls_status batch_launch(const fls_batch* b, const DevCol* cols, const fls_batch_query* queries, const uint4* items,
+                        uint32_t* counter, int64_t* d_results, cudaStream_t st) {
+	DeviceInfo di;
+	fls_status s = device_info(di);
+	if (s != FLS_OK) { return s; }
+	if ((s = cuda_check(cudaMemsetAsync(counter, 0, sizeof(uint32_t), st), "cudaMemsetAsync")) != FLS_OK) { return s; }
+	if ((s = cuda_check(cudaMemsetAsync(d_results, 0, sizeof(int64_t) * 2u * b->queries.size(), st), "cudaMemsetAsync")) !=
+	    FLS_OK) {
+		return s;
+	}
+	if (b->items.empty()) { return FLS_OK; }
+	uint32_t          warps, stages, ctas, tile;
+	fls_get_launch_config(&warps, &stages, &ctas, &tile);
+	const BatchLayout L(b->slot_words);
+	while (warps > 1 && 4ull * L.total * warps > static_cast<uint64_t>(di.max_smem)) { warps /= 2; }
+	if (4ull * L.total * warps > static_cast<uint64_t>(di.max_smem)) {
+		return set_error(FLS_ERR_CAPACITY, "batch vectors too large for shared-memory staging");
+	}
+	{
+		static std::mutex mu;
+		static uint64_t   configured = 0; // bit d: device d's shared-memory attribute raised
+		int               dev        = 0;
+		cudaGetDevice(&dev);
+		std::lock_guard<std::mutex> lk(mu);
+		if (dev >= 64 || !(configured & (1ull << dev))) {
+			if ((s = cuda_check(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, di.max_smem),
+			                    "cudaFuncSetAttribute")) != FLS_OK) {
+				return s;
+			}
+			if (dev < 64) { configured |= 1ull << dev; }
+		}
+	}
+	BatchParams P;
+	P.cols       = cols;
+	P.queries    = queries;
+	P.items      = items;
+	P.n_items    = static_cast<uint32_t>(b->items.size());
+	P.counter    = counter;
+	P.results    = reinterpret_cast<long long*>(d_results);
+	P.slot_words = b->slot_words;
+	P.has_dict   = b->has_dict;
+	P.warps      = warps;
+	P.err        = device_error_word();
+	const uint64_t want = (b->items.size() + warps - 1) / warps;
+	const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>(want, static_cast<uint64_t>(di.sms) * ctas));
+	batch_kernel<<<grid, 32u * warps, 4ull * L.total * warps, st>>>(P);
+	count_launch();
+	return cuda_check(cudaGetLastError(), "batch_kernel launch");
+}
+
+} // namespace fls
+
+using namespace fls;
+
+extern "C" {
+
+fls_status fls_batch_create(const fls_column* cols, uint32_t n_cols, const fls_batch_query* queries,
+                            uint32_t n_queries, uint32_t chunk_vectors, fls_batch** out) {
+	if (!cols || !queries || !out || n_cols == 0 || chunk_vectors == 0) {
+		return set_error(FLS_ERR_INVALID_ARG, "fls_batch_create: bad arguments");
+	}
+	fls_batch* b = new (std::nothrow) fls_batch;
+	if (!b) { return set_error(FLS_ERR_CAPACITY, "out of host memory"); }
+	b->cols.resize(n_cols);
+	uint32_t slot = 0;
+	for (uint32_t c = 0; c < n_cols; ++c) {
+		fls_status s = make_devcol(cols[c], b->cols[c]);
+		if (s != FLS_OK) {
+			delete b;
+			return s;
+		}
+		slot = std::max(slot, b->cols[c].slot_words);
+		if (cols[c].meta && (cols[c].scheme_mask & ((1u << FLS_SCHEME_RLE) | (1u << FLS_SCHEME_DICT)))) {
+			b->has_dict = 1u;
+		}
+	}
+	b->slot_words = (slot + 3u) & ~3u;
+	b->queries.assign(queries, queries + n_queries);
+	for (uint32_t q = 0; q < n_queries; ++q) {
+		fls_batch_query& bq = b->queries[q];
+		if (bq.col >= n_cols || bq.agg_col >= n_cols || cols[bq.col].n_values != cols[bq.agg_col].n_values ||
+		    cols[bq.col].layout != cols[bq.agg_col].layout) {
+			delete b;
+			return set_error(FLS_ERR_INVALID_ARG, "batch query names missing or mismatched columns");
+		}
+		bq.n_values          = cols[bq.col].n_values;
+		const uint64_t n_vec = (bq.n_values + 1023u) / 1024u;
+		for (uint64_t v = 0; v < n_vec; v += chunk_vectors) {
+			b->items.push_back(make_uint4(q, static_cast<uint32_t>(v),
+			                              static_cast<uint32_t>(std::min<uint64_t>(n_vec, v + chunk_vectors)), 0u));
+		}
+	}
+	*out = b;
+	return FLS_OK;
+}
+
+uint64_t fls_batch_workspace_bytes(const fls_batch* b) { return b ? WsLayout(*b).total : 0; }
+
+uint32_t fls_batch_items(const fls_batch* b) { return b ? static_cast<uint32_t>(b->items.size()) : 0u; }
+
+fls_status fls_batch_upload(fls_batch* b, void* d_workspace, uint64_t workspace_bytes, fls_stream_t stream) {
+	if (!b || !d_workspace) { return set_error(FLS_ERR_INVALID_ARG, "fls_batch_upload: bad arguments"); }
+	const WsLayout L(*b);
+	if (workspace_bytes < L.total) { return set_error(FLS_ERR_CAPACITY, "batch workspace too small"); }
+	char*        w  = static_cast<char*>(d_workspace);
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	fls_status   s  = cuda_check(cudaMemcpyAsync(w + L.cols, b->cols.data(), b->cols.size() * sizeof(DevCol),
+	                                             cudaMemcpyHostToDevice, st), "upload columns");
+	if (s == FLS_OK) {
+		s = cuda_check(cudaMemcpyAsync(w + L.queries, b->queries.data(), b->queries.size() * sizeof(fls_batch_query),
+		                               cudaMemcpyHostToDevice, st), "upload queries");
+	}
+	if (s == FLS_OK && !b->items.empty()) {
+		s = cuda_check(cudaMemcpyAsync(w + L.items, b->items.data(), b->items.size() * sizeof(uint4),
+		                               cudaMemcpyHostToDevice, st), "upload items");
+	}
+	if (s == FLS_OK) { s = cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize"); }
+	if (s == FLS_OK) {
+		b->ws       = d_workspace;
+		b->ws_bytes = workspace_bytes;
+	}
+	return s;
+}
+
+fls_status fls_batch_run(const fls_batch* b, int64_t* d_results, fls_stream_t stream) {
+	if (!b || !d_results || !b->ws) { return set_error(FLS_ERR_INVALID_ARG, "fls_batch_run: not uploaded"); }
+	const WsLayout L(*b);
+	char*          w = static_cast<char*>(b->ws);
+	return batch_launch(b, reinterpret_cast<const DevCol*>(w + L.cols), reinterpret_cast<const fls_batch_query*>(w + L.queries),
+	                    reinterpret_cast<const uint4*>(w + L.items), reinterpret_cast<uint32_t*>(w + L.counter), d_results,
+	                    reinterpret_cast<cudaStream_t>(stream));
+}
+
+void fls_batch_destroy(fls_batch* b) { delete b; }
+
+} // extern "C"

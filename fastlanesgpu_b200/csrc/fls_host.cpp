@@ -283,15 +283,31 @@ uint8_t best_scheme(const uint32_t* size5) {
 	return best;
 }
 
-// 16 per-vector statistics for the learned selector, all in [0, ~1].
+// 16 per-vector statistics for the learned selector, all in [0, 1].  Every
+// feature is an integer count or bit width divided by a power of two, so the
+// CPU and GPU (fls_mlp.cu) computations agree bit for bit.
+//   0 bit width of max-min              8 bit width of mean |delta| (sum >> 10)
+//   1 bit width of the largest transposed delta (DELTA payload width)
+//   2 runs (rle.hpp, restarts every 256)  9 values < 2^(rbw/2) above min
+//   3 rising neighbours                10 values < 2^(rbw-4) above min
+//   4 falling neighbours               11 bit width of |min|
+//   5 equal neighbours                 12 constant vector
+//   6 occupied slots of a 1024-bit hash bitmap (distinct-value proxy)
+//   7 bit width of that occupancy      13 bit width of the run count
+//   14 constant 32-value chunks        15 bias (1)
 void vector_stats(const int32_t* v, float* f) {
 	const MinMax   mm  = min_max(v);
 	const uint32_t rng = static_cast<uint32_t>(mm.mx) - static_cast<uint32_t>(mm.mn);
 	const unsigned rbw = bits_of(rng);
-	uint32_t       max_d = 0, n_runs = 0, n_up = 0, n_down = 0, n_eq = 0;
-	double         sum_abs_d = 0.0;
-	uint32_t       low_half = 0, low_quarter = 0;
+	uint32_t       max_d = 0, n_runs = 0, n_up = 0, n_down = 0, n_eq = 0, low_half = 0, low_quarter = 0;
+	uint64_t       sum_abs_d = 0;
 	uint32_t       bitmap[32] = {0};
+	uint32_t       const_chunks = 0;
+	for (uint32_t c = 0; c < 32; ++c) {
+		bool same = true;
+		for (uint32_t s2 = 1; s2 < 32; ++s2) { same = same && v[32 * c + s2] == v[32 * c]; }
+		const_chunks += same ? 1u : 0u;
+	}
 	for (uint32_t j = 0; j < 1024; ++j) {
 		const uint32_t x = static_cast<uint32_t>(v[j]) - static_cast<uint32_t>(mm.mn);
 		if (rbw == 0 || x < (1u << (rbw / 2))) { ++low_half; }
@@ -303,7 +319,7 @@ void vector_stats(const int32_t* v, float* f) {
 			continue;
 		}
 		const int64_t dd = static_cast<int64_t>(v[j]) - static_cast<int64_t>(v[j - 1]);
-		sum_abs_d += static_cast<double>(dd < 0 ? -dd : dd);
+		sum_abs_d += static_cast<uint64_t>(dd < 0 ? -dd : dd);
 		n_up += dd > 0;
 		n_down += dd < 0;
 		n_eq += dd == 0;
@@ -312,26 +328,23 @@ void vector_stats(const int32_t* v, float* f) {
 	}
 	uint32_t set = 0;
 	for (uint32_t w = 0; w < 32; ++w) { set += static_cast<uint32_t>(__builtin_popcount(bitmap[w])); }
-	// Linear counting estimate of the number of distinct values (m = 1024 bits).
-	const double zeros  = static_cast<double>(1024 - set);
-	const double d_est  = zeros > 0 ? -1024.0 * std::log(zeros / 1024.0) : 1024.0 * 8.0;
-	const double d_bits = std::log2(1.0 + d_est);
-	const double mean_d = sum_abs_d / 1023.0;
-	f[0]  = rbw / 32.0f;
-	f[1]  = bits_of(max_d) / 32.0f;
-	f[2]  = n_runs / 1024.0f;
-	f[3]  = n_up / 1023.0f;
-	f[4]  = n_down / 1023.0f;
-	f[5]  = n_eq / 1023.0f;
-	f[6]  = static_cast<float>(d_bits / 13.0);
-	f[7]  = static_cast<float>(std::min(d_est, 1024.0) / 1024.0);
-	f[8]  = static_cast<float>(std::log2(1.0 + mean_d) / 32.0);
-	f[9]  = low_half / 1024.0f;
-	f[10] = low_quarter / 1024.0f;
-	f[11] = bits_of(static_cast<uint32_t>(mm.mn < 0 ? -static_cast<int64_t>(mm.mn) : mm.mn)) / 32.0f;
+	const uint64_t mean_d = sum_abs_d >> 10;
+	const uint32_t amin   = mm.mn < 0 ? static_cast<uint32_t>(-static_cast<int64_t>(mm.mn)) : static_cast<uint32_t>(mm.mn);
+	f[0]  = static_cast<float>(rbw) / 32.0f;
+	f[1]  = static_cast<float>(bits_of(max_d)) / 32.0f;
+	f[2]  = static_cast<float>(n_runs) / 1024.0f;
+	f[3]  = static_cast<float>(n_up) / 1024.0f;
+	f[4]  = static_cast<float>(n_down) / 1024.0f;
+	f[5]  = static_cast<float>(n_eq) / 1024.0f;
+	f[6]  = static_cast<float>(set) / 1024.0f;
+	f[7]  = static_cast<float>(bits_of(set)) / 16.0f;
+	f[8]  = static_cast<float>(bits_of(static_cast<uint32_t>(std::min<uint64_t>(mean_d, 0xffffffffu)))) / 32.0f;
+	f[9]  = static_cast<float>(low_half) / 1024.0f;
+	f[10] = static_cast<float>(low_quarter) / 1024.0f;
+	f[11] = static_cast<float>(bits_of(amin)) / 32.0f;
 	f[12] = (mm.mn == mm.mx) ? 1.0f : 0.0f;
-	f[13] = static_cast<float>(std::max(0.0, static_cast<double>(rbw) - std::ceil(d_bits)) / 32.0);
-	f[14] = static_cast<float>(std::log2(1.0 + n_runs) / 10.0);
+	f[13] = static_cast<float>(bits_of(n_runs)) / 16.0f;
+	f[14] = static_cast<float>(const_chunks) / 32.0f;
 	f[15] = 1.0f;
 }
 

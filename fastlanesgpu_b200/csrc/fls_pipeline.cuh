@@ -292,6 +292,9 @@ uint32_t*  device_error_word(); // device address of this device's error word
 void       count_launch(uint64_t n = 1);
 int        tuning_sparse_rows();
 
+// Validates one column descriptor and converts it for a kernel.
+fls_status make_devcol(const fls_column& c, DevCol& d);
+
 // Lays out shared memory for a set of columns; extra_words per warp and
 // cta_words per CTA are operator-specific scratch.
 fls_status plan_stages(const fls_column* cols, uint32_t n_cols, uint32_t extra_words, uint32_t cta_words,

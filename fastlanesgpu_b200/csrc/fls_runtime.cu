@@ -88,7 +88,6 @@ uint32_t* device_error_word() {
 	return dev < static_cast<int>(g_err_addr.size()) ? g_err_addr[dev] : nullptr;
 }
 
-namespace {
 // Validates one column descriptor and converts it for the kernel.
 fls_status make_devcol(const fls_column& c, DevCol& d) {
 	if (!c.data && c.n_words) { return set_error(FLS_ERR_INVALID_ARG, "column data is null"); }
@@ -135,6 +134,7 @@ fls_status make_devcol(const fls_column& c, DevCol& d) {
 	return FLS_OK;
 }
 
+namespace {
 bool needs_dict(const fls_column& c) {
 	return c.meta != nullptr && (c.scheme_mask & ((1u << FLS_SCHEME_RLE) | (1u << FLS_SCHEME_DICT)));
 }

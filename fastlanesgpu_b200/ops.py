@@ -176,6 +176,35 @@ def probe_groupby(cols, probes, agg_col: int, key_a: int, key_b: int, group_mul:
     return out
 
 
+def crystal_q11(cols, n_rows: int, date_gt: int, date_lt: int, qty_lt: int, disc_ge: int, disc_le: int, out=None):
+    """fls_q11.cu QueryKernel_v1 on the drop-in primitive API.  cols: uniform
+    DeviceColumns (date, discount, quantity, price)."""
+    import torch
+    if out is None:
+        out = torch.empty(1, dtype=torch.int64, device=cols[0].data.device)
+    args = []
+    for c in cols:
+        args += [c.data.data_ptr(), c.host.bw]
+    check(lib().fls_crystal_q11(*args, n_rows, date_gt, date_lt, qty_lt, disc_ge, disc_le, out.data_ptr(),
+                                _stream()), "fls_crystal_q11")
+    return out
+
+
+def crystal_q21_probe(cols, n_rows: int, ht_s, ht_p, ht_d, d_keys_min: int = 0, out=None):
+    """fls_q21.cu probe_v1 on the drop-in primitive API.  cols: uniform
+    DeviceColumns (suppkey, partkey, orderdate, revenue)."""
+    import torch
+    if out is None:
+        out = torch.empty(4 * 7000, dtype=torch.int32, device=cols[0].data.device)
+    args = []
+    for c in cols:
+        args += [c.data.data_ptr(), c.host.bw]
+    check(lib().fls_crystal_q21_probe(*args, n_rows, ht_s.data_ptr(), ht_s.numel(), ht_p.data_ptr(), ht_p.numel() // 2,
+                                      ht_d.data_ptr(), ht_d.numel() // 2, d_keys_min, out.data_ptr(), _stream()),
+          "fls_crystal_q21_probe")
+    return out
+
+
 def check_device_error() -> None:
     """Synchronise the current stream and raise if a kernel flagged bad input."""
     check(lib().fls_check_device_error(_stream()), "device")

@@ -220,6 +220,89 @@ typedef struct fls_join_agg_desc {
 
 fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res, fls_stream_t stream);
 
+/* ------------------------------------ batched persistent execution (device) */
+
+/* One filter-aggregate query of a batch: rows with lo <= cols[col] <= hi,
+ * sum of cols[agg_col] (same length and layout) and the row count. */
+typedef struct fls_batch_query {
+	uint32_t col;
+	int32_t  lo, hi;
+	uint32_t agg_col;
+	uint64_t n_values; /* filled in by fls_batch_create */
+} fls_batch_query;
+
+/* Host-side plan of a batch: the queries cut into work items of chunk_vectors
+ * vectors.  No reference counterpart (the reference launches one grid per
+ * query, fls_q11.cu:150-160). */
+typedef struct fls_batch fls_batch;
+fls_status fls_batch_create(const fls_column* cols, uint32_t n_cols, const fls_batch_query* queries,
+                            uint32_t n_queries, uint32_t chunk_vectors, fls_batch** out);
+uint64_t   fls_batch_workspace_bytes(const fls_batch* batch);
+uint32_t   fls_batch_items(const fls_batch* batch);
+/* Copies the plan into a caller-provided device workspace (synchronises
+ * `stream`); the batch keeps using that workspace. */
+fls_status fls_batch_upload(fls_batch* batch, void* d_workspace, uint64_t workspace_bytes, fls_stream_t stream);
+/* Runs every query in one persistent launch: d_results (device int64[2*n_queries])
+ * receives {sum, count} per query.  Only memsets and one kernel launch are
+ * enqueued, so the call can be captured into a CUDA graph. */
+fls_status fls_batch_run(const fls_batch* batch, int64_t* d_results, fls_stream_t stream);
+void       fls_batch_destroy(fls_batch* batch);
+
+/* ----------------------------------- learned encoding selection (device) */
+
+/* A 16-64-64-5 FP32 MLP reads 16 per-vector statistics and scores the five
+ * schemes; the exhaustive encoder (fls_encode_exhaustive) labels its training
+ * vectors and remains the fallback for low-confidence picks.  Any pick is
+ * lossless: the encoder recomputes bit widths exactly.  No reference
+ * counterpart (the reference picks encodings by hand, ssb_utils.h:37-83).
+ * Parameters: W1[64][16], b1[64], W2[64][64], b2[64], W3[5][64], b3[5]. */
+#define FLS_MLP_IN       16
+#define FLS_MLP_HIDDEN   64
+#define FLS_MLP_OUT      5
+#define FLS_MLP_N_PARAMS (64 * 16 + 64 + 64 * 64 + 64 + 5 * 64 + 5)
+
+/* The statistics of fls_vector_stats, computed on the device from device
+ * values (n_vec*16 floats, bit-identical to the host version). */
+fls_status fls_vector_stats_gpu(const int32_t* d_values, uint64_t n, float* d_stats, fls_stream_t stream);
+/* He-uniform initialisation from a seed. */
+fls_status fls_mlp_init(float* d_params, uint64_t seed, fls_stream_t stream);
+/* Device workspace needed by fls_mlp_gradients for a batch. */
+uint64_t fls_mlp_workspace_bytes(uint32_t batch);
+/* Mean softmax cross-entropy of a batch and its gradient w.r.t. every
+ * parameter (d_grads: FLS_MLP_N_PARAMS floats; d_loss optional). */
+fls_status fls_mlp_gradients(const float* d_params, const float* d_x, const uint8_t* d_labels, uint32_t batch,
+                             void* d_workspace, uint64_t workspace_bytes, float* d_grads, float* d_loss,
+                             fls_stream_t stream);
+/* One Adam update (t = 1-based step; d_m, d_v: moment buffers). */
+fls_status fls_mlp_adam_step(float* d_params, const float* d_grads, float* d_m, float* d_v, float lr, float beta1,
+                             float beta2, float eps, uint32_t t, fls_stream_t stream);
+/* Inference: optional softmax probabilities (n*5), argmax scheme and its
+ * probability (the confidence used for the exhaustive fallback). */
+fls_status fls_mlp_infer(const float* d_params, const float* d_x, uint64_t n, float* d_probs, uint8_t* d_best,
+                         float* d_conf, fls_stream_t stream);
+
+/* ------------------------------------- reference-shaped kernels (device) */
+
+/* fastlanes/src/ssb/fls_q11.cu:29-81 QueryKernel_v1, written against the
+ * drop-in primitive API (include/fls_crystal.cuh) and launched like the
+ * reference: one 32-thread CTA per 1024-value vector.  Columns are uniform
+ * bit-packed int32 columns (device, n_vec*32*bw words each).  Selection:
+ * date > date_gt AND date < date_lt AND qty < qty_lt AND disc >= disc_ge AND
+ * disc <= disc_le; *d_revenue = sum(price * disc) over selected rows. */
+fls_status fls_crystal_q11(const int32_t* date, uint32_t date_bw, const int32_t* disc, uint32_t disc_bw,
+                           const int32_t* qty, uint32_t qty_bw, const int32_t* price, uint32_t price_bw,
+                           uint64_t n_rows, int32_t date_gt, int32_t date_lt, int32_t qty_lt, int32_t disc_ge,
+                           int32_t disc_le, uint64_t* d_revenue, fls_stream_t stream);
+
+/* fastlanes/src/ssb/fls_q21.cu:21-78 probe_v1 on the drop-in primitive API:
+ * supplier PHT_1, part PHT_2 (brand), date PHT_2 (year), group
+ * (brand*7 + year-1992) % 7000 into d_res (device int32[4*7000], zeroed here). */
+fls_status fls_crystal_q21_probe(const int32_t* suppkey, uint32_t supp_bw, const int32_t* partkey, uint32_t part_bw,
+                                 const int32_t* orderdate, uint32_t date_bw, const int32_t* revenue, uint32_t rev_bw,
+                                 uint64_t n_rows, const int32_t* ht_s, int32_t s_len, const int32_t* ht_p,
+                                 int32_t p_len, const int32_t* ht_d, int32_t d_len, int32_t d_keys_min, int32_t* d_res,
+                                 fls_stream_t stream);
+
 /* --------------------------------------------------------- tuning */
 
 /* Launch shape of the staged decode/query kernels: warps per CTA (<= 16),

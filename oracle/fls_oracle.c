@@ -6,6 +6,7 @@
 #include "fls_oracle.h"
 
 #include <stdlib.h>
+#include <math.h>
 #include <string.h>
 
 /* ---- layout ------------------------------------------------------------ */
@@ -445,6 +446,122 @@ void orc_probe_groupby(const int32_t* supp, const int32_t* part, const int32_t* 
 		acc += (uint64_t)(int64_t)rev[t];
 		memcpy(&res[4 * g + 2], &acc, 8);
 	}
+}
+
+/* ---- learned selector ------------------------------------------------------ */
+
+double orc_mlp_loss_grad(const float* P, const float* x, const uint8_t* y, uint32_t B, double* g) {
+	enum { I = 16, H = 64, O = 5, W1 = 0, B1 = W1 + H * I, W2 = B1 + H, B2 = W2 + H * H, W3 = B2 + H, B3 = W3 + O * H };
+	memset(g, 0, sizeof(double) * ORC_MLP_N_PARAMS);
+	double loss = 0.0;
+	for (uint32_t b = 0; b < B; ++b) {
+		const float* xb = x + (size_t)b * I;
+		double       h1[H], h2[H], z[O], d2[H], d1[H];
+		for (int j = 0; j < H; ++j) {
+			double a = P[B1 + j];
+			for (int i = 0; i < I; ++i) { a += (double)P[W1 + j * I + i] * xb[i]; }
+			h1[j] = a > 0 ? a : 0;
+		}
+		for (int j = 0; j < H; ++j) {
+			double a = P[B2 + j];
+			for (int i = 0; i < H; ++i) { a += (double)P[W2 + j * H + i] * h1[i]; }
+			h2[j] = a > 0 ? a : 0;
+		}
+		double m = -1e300, s = 0;
+		for (int k = 0; k < O; ++k) {
+			double a = P[B3 + k];
+			for (int j = 0; j < H; ++j) { a += (double)P[W3 + k * H + j] * h2[j]; }
+			z[k] = a;
+			if (a > m) { m = a; }
+		}
+		for (int k = 0; k < O; ++k) {
+			z[k] = exp(z[k] - m);
+			s += z[k];
+		}
+		const int t = y[b] < O ? y[b] : 0;
+		loss += -log(z[t] / s) / B;
+		double dz[O];
+		for (int k = 0; k < O; ++k) { dz[k] = (z[k] / s - (k == t)) / B; }
+		for (int k = 0; k < O; ++k) {
+			g[B3 + k] += dz[k];
+			for (int j = 0; j < H; ++j) { g[W3 + k * H + j] += dz[k] * h2[j]; }
+		}
+		for (int j = 0; j < H; ++j) {
+			double a = 0;
+			for (int k = 0; k < O; ++k) { a += (double)P[W3 + k * H + j] * dz[k]; }
+			d2[j] = h2[j] > 0 ? a : 0;
+			g[B2 + j] += d2[j];
+			for (int i = 0; i < H; ++i) { g[W2 + j * H + i] += d2[j] * h1[i]; }
+		}
+		for (int i = 0; i < H; ++i) {
+			double a = 0;
+			for (int j = 0; j < H; ++j) { a += (double)P[W2 + j * H + i] * d2[j]; }
+			d1[i] = h1[i] > 0 ? a : 0;
+			g[B1 + i] += d1[i];
+			for (int f = 0; f < I; ++f) { g[W1 + i * I + f] += d1[i] * xb[f]; }
+		}
+	}
+	return loss;
+}
+
+static unsigned bw_u32(uint32_t v) {
+	unsigned b = 0;
+	while (v) { ++b; v >>= 1; }
+	return b;
+}
+
+void orc_vector_stats(const int32_t* v, float* f) {
+	int32_t mn, mx;
+	min_max(v, 1024, &mn, &mx);
+	const uint32_t rbw = bw_u32((uint32_t)mx - (uint32_t)mn);
+	uint32_t max_d = 0, runs = 0, up = 0, down = 0, eq = 0, lh = 0, lq = 0, bitmap[32] = {0}, cc = 0;
+	uint64_t sabs  = 0;
+	for (uint32_t c = 0; c < 32; ++c) {
+		int same = 1;
+		for (uint32_t s = 1; s < 32; ++s) { same = same && v[32 * c + s] == v[32 * c]; }
+		cc += (uint32_t)same;
+	}
+	for (uint32_t j = 0; j < 1024; ++j) {
+		const uint32_t u = (uint32_t)v[j] - (uint32_t)mn;
+		lh += (rbw == 0 || u < (1u << (rbw / 2))) ? 1u : 0u;
+		lq += (rbw <= 4 || u < (1u << (rbw - 4))) ? 1u : 0u;
+		const uint32_t h = ((uint32_t)v[j] * 0x9e3779b1u) >> 22;
+		bitmap[h >> 5] |= 1u << (h & 31u);
+		if (j == 0) {
+			++runs;
+			continue;
+		}
+		const int64_t d = (int64_t)v[j] - (int64_t)v[j - 1];
+		sabs += (uint64_t)(d < 0 ? -d : d);
+		up += d > 0;
+		down += d < 0;
+		eq += d == 0;
+		if (j & 31u) {
+			const uint32_t dd = (uint32_t)v[j] - (uint32_t)v[j - 1];
+			if (dd > max_d) { max_d = dd; }
+		}
+		runs += ((j & 255u) == 0 || d != 0) ? 1u : 0u;
+	}
+	uint32_t occ = 0;
+	for (int w = 0; w < 32; ++w) { occ += (uint32_t)__builtin_popcount(bitmap[w]); }
+	const uint64_t md   = sabs >> 10;
+	const uint32_t amin = mn < 0 ? (uint32_t)(-(int64_t)mn) : (uint32_t)mn;
+	f[0]  = (float)rbw / 32.0f;
+	f[1]  = (float)bw_u32(max_d) / 32.0f;
+	f[2]  = (float)runs / 1024.0f;
+	f[3]  = (float)up / 1024.0f;
+	f[4]  = (float)down / 1024.0f;
+	f[5]  = (float)eq / 1024.0f;
+	f[6]  = (float)occ / 1024.0f;
+	f[7]  = (float)bw_u32(occ) / 16.0f;
+	f[8]  = (float)bw_u32((uint32_t)(md > 0xffffffffull ? 0xffffffffull : md)) / 32.0f;
+	f[9]  = (float)lh / 1024.0f;
+	f[10] = (float)lq / 1024.0f;
+	f[11] = (float)bw_u32(amin) / 32.0f;
+	f[12] = mn == mx ? 1.0f : 0.0f;
+	f[13] = (float)bw_u32(runs) / 16.0f;
+	f[14] = (float)cc / 32.0f;
+	f[15] = 1.0f;
 }
 
 uint64_t orc_splitmix64(uint64_t* state) {

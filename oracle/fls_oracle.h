@@ -91,6 +91,15 @@ void orc_probe_groupby(const int32_t* supp, const int32_t* part, const int32_t* 
                        const int32_t* ht_s, int32_t s_len, const int32_t* ht_p, int32_t p_len, const int32_t* ht_d,
                        int32_t d_len, int32_t d_keys_min, int32_t* res);
 
+/* ---- learned selector MLP, double precision (the gradient checker) ------- */
+/* Parameter layout W1[64][16], b1[64], W2[64][64], b2[64], W3[5][64], b3[5];
+ * ReLU hidden layers, mean softmax cross-entropy over the batch.  Writes the
+ * loss and d(loss)/d(param) for every parameter (5573 doubles). */
+#define ORC_MLP_N_PARAMS 5573
+double orc_mlp_loss_grad(const float* params, const float* x, const uint8_t* y, uint32_t batch, double* grads);
+/* 16 selector statistics of one vector (the same definitions as the library). */
+void orc_vector_stats(const int32_t* v, float* f16);
+
 /* ---- synthetic inputs (SplitMix64; shared with the Python tests) --------- */
 uint64_t orc_splitmix64(uint64_t* state);
 

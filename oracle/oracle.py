@@ -143,6 +143,23 @@ class Oracle:
         self.L.orc_scheme_sizes(_p(vec, _i32p), _p(out, _u32p))
         return out
 
+    def vector_stats(self, vec) -> np.ndarray:
+        vec = np.ascontiguousarray(vec, dtype=np.int32)
+        out = np.zeros(16, np.float32)
+        self.L.orc_vector_stats(_p(vec, _i32p), out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+        return out
+
+    def mlp_loss_grad(self, params, x, y):
+        params = np.ascontiguousarray(params, np.float32)
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.uint8)
+        g = np.zeros(5573, np.float64)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self.L.orc_mlp_loss_grad.restype = ctypes.c_double
+        loss = self.L.orc_mlp_loss_grad(params.ctypes.data_as(fp), x.ctypes.data_as(fp), _p(y, _u8p),
+                                        ctypes.c_uint32(y.size), g.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return float(loss), g
+
     # -- query path ----------------------------------------------------------
     def filter_agg(self, date, disc, qty, price, date_lo, date_hi, disc_lo, disc_hi, qty_lt) -> int:
         cols = [np.ascontiguousarray(c, dtype=np.int32) for c in (date, disc, qty, price)]

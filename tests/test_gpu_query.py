@@ -187,3 +187,23 @@ def test_sparse_threshold_does_not_change_results(cuda, oracle, sparse_rows):
             assert np.array_equal(got, want21)
     finally:
         ops.set_tuning(0, 0)
+
+
+@pytest.mark.parametrize("n", [1000, (1 << 20) + 77])
+def test_crystal_api_kernels(cuda, oracle, n):
+    """Kernels written against the drop-in primitive API (fls_crystal.cuh),
+    launched one CTA per vector like the reference, match the oracle."""
+    t = datagen.lineorder_q11(n, seed=31)
+    cols = [c.to_device() for c in _q11_cols(t)]
+    f = datagen.Q11_FILTER
+    got = int(ops.crystal_q11(cols, n, f["date"][0] - 1, f["date"][1] + 1, f["quantity"][1] + 1, *f["discount"]).cpu()[0])
+    want = oracle.filter_agg(t["date"], t["discount"], t["quantity"], t["price"], *f["date"], *f["discount"],
+                             f["quantity"][1] + 1)
+    assert got == want
+    tq, ht_s, ht_p, ht_d = _q21(n, 32, 1 << 16, 1 << 14)
+    names = ["lo_suppkey", "lo_partkey", "lo_orderdate", "lo_revenue"]
+    qcols = [EncodedColumn.uniform(tq[k], bw=datagen.Q21_BITS[k]).to_device() for k in names]
+    got21 = ops.crystal_q21_probe(qcols, n, ht_s, ht_p, ht_d).cpu().numpy()
+    want21 = oracle.probe_groupby(tq["lo_suppkey"], tq["lo_partkey"], tq["lo_orderdate"], tq["lo_revenue"],
+                                  ht_s.cpu().numpy(), ht_p.cpu().numpy(), ht_d.cpu().numpy())
+    assert np.array_equal(got21, want21)
