@@ -188,7 +188,8 @@ def run_ours(a, dist: Dist):
         ops.set_launch_config(*[int(x) for x in a.launch.split(",")])
     if a.sparse_rows:
         ops.set_tuning(0, a.sparse_rows)
-    seed = 1000 * (dist.rank + 1)
+    from fastlanesgpu_b200.shard import allreduce_sum, shard_seed
+    seed = shard_seed(1000, dist.rank)
     # ---------------------------------------------------------------- setup
     if a.workload == "q11":
         t, hcols, filters = build_q11(a.rows, seed)
@@ -236,8 +237,19 @@ def run_ours(a, dist: Dist):
     comp_bytes = sum(c.nbytes for c in hcols)
 
     def collective():
-        if dist.pg:
-            dist.pg.all_reduce(res.view(torch.int64) if a.workload != "q21" else res)
+        # the one exchange of the sharded query: combine the ranks' partial aggregates
+        if not dist.pg:
+            return
+        if a.workload == "q21":
+            # reference layout per group: (year, brand) int32 pair + uint64 sum
+            r64 = res.view(torch.int64).view(-1, 2)
+            keys, sums = r64[:, 0].contiguous(), r64[:, 1].contiguous()
+            dist.pg.all_reduce(keys, op=dist.pg.ReduceOp.MAX)
+            allreduce_sum(sums)
+            r64[:, 0].copy_(keys)
+            r64[:, 1].copy_(sums)
+        else:
+            allreduce_sum(res)
 
     # -------------------------------------------------- device-resident timing
     clocks = ClockSampler(dist.local)
