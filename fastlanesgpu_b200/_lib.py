@@ -119,6 +119,7 @@ _SIGS = {
     "fls_mlp_init": (ctypes.c_int, [_VP, ctypes.c_uint64, _VP]),
     "fls_mlp_workspace_bytes": (ctypes.c_uint64, [ctypes.c_uint32]),
     "fls_mlp_gradients": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_uint32, _VP, ctypes.c_uint64, _VP, _VP, _VP]),
+    "fls_mlp_gradients_static": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_uint32, _VP, _VP, _VP]),
     "fls_mlp_adam_step": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                          ctypes.c_float, ctypes.c_uint32, _VP]),
     "fls_mlp_infer": (ctypes.c_int, [_VP, _VP, ctypes.c_uint64, _VP, _VP, _VP, _VP]),

@@ -10,6 +10,9 @@
 // b2[64], W3[5][64], b3[5]; ReLU after layers 1 and 2, softmax cross-entropy.
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <vector>
+
 #include "fls_pipeline.cuh"
 
 namespace fls {
@@ -340,6 +343,38 @@ __global__ void mlp_adam_kernel(float* __restrict__ p, const float* __restrict__
 
 size_t align256(size_t x) { return (x + 255u) & ~static_cast<size_t>(255u); }
 
+// Scratch of fls_mlp_gradients_static: h1, h2, dh1, dh2 (each
+// FLS_MLP_STATIC_MAX_BATCH x 64 floats) and dz (FLS_MLP_STATIC_MAX_BATCH x 5
+// floats), about 2.1 MB held by every device that loads this library.
+constexpr uint32_t kStaticBatch        = FLS_MLP_STATIC_MAX_BATCH;
+constexpr size_t   kStaticScratchFloats = 4u * kStaticBatch * kH + kStaticBatch * kOut;
+static __device__ __align__(256) float g_mlp_static_scratch[kStaticScratchFloats];
+
+// Device address of g_mlp_static_scratch, resolved once per device (host
+// code may not use the symbol itself as a device pointer).
+std::mutex          g_static_mu;
+std::vector<float*> g_static_ptr;
+
+fls_status static_scratch(float** out) {
+	int dev = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess) {
+		cudaGetLastError();
+		return set_error(FLS_ERR_NO_DEVICE, "no CUDA device");
+	}
+	std::lock_guard<std::mutex> lk(g_static_mu);
+	if (static_cast<int>(g_static_ptr.size()) <= dev) { g_static_ptr.resize(dev + 1, nullptr); }
+	if (!g_static_ptr[dev]) {
+		float*      ptr = nullptr;
+		cudaError_t e   = cudaGetSymbolAddress(reinterpret_cast<void**>(&ptr), g_mlp_static_scratch);
+		if (e != cudaSuccess || !ptr) {
+			return set_error(FLS_ERR_CUDA, std::string("cudaGetSymbolAddress(static MLP scratch): ") + cudaGetErrorString(e));
+		}
+		g_static_ptr[dev] = ptr;
+	}
+	*out = g_static_ptr[dev];
+	return FLS_OK;
+}
+
 } // namespace
 } // namespace fls
 
@@ -400,6 +435,40 @@ fls_status fls_mlp_gradients(const float* d_params, const float* d_x, const uint
 	mlp_grad_kernel<<<2 * kH + kOut, 256, 0, st>>>(d_x, batch, H1, H2, dZ, dH1, dH2, d_grads);
 	count_launch(3);
 	return cuda_check(cudaGetLastError(), "MLP gradient kernels launch");
+}
+
+// Same result as fls_mlp_gradients, for callers that cannot allocate device
+// memory: the activation scratch lives in a fixed static device array instead
+// of a caller workspace.  See include/fls_gpu.h.
+fls_status fls_mlp_gradients_static(const float* d_params, const float* d_x, const uint8_t* d_labels, uint32_t batch,
+                                    float* d_grads, float* d_loss, fls_stream_t stream) {
+	if (!d_params || !d_x || !d_labels || !d_grads || batch == 0) {
+		return set_error(FLS_ERR_INVALID_ARG, "fls_mlp_gradients_static: bad arguments");
+	}
+	if (batch > kStaticBatch) {
+		return set_error(FLS_ERR_CAPACITY, "fls_mlp_gradients_static: batch " + std::to_string(batch) +
+		                                       " exceeds FLS_MLP_STATIC_MAX_BATCH (" + std::to_string(kStaticBatch) + ")");
+	}
+	DeviceInfo di;
+	fls_status s = device_info(di);
+	if (s != FLS_OK) { return s; }
+	float* scratch = nullptr;
+	if ((s = static_scratch(&scratch)) != FLS_OK) { return s; }
+	float*       H1  = scratch;
+	float*       H2  = H1 + static_cast<size_t>(kStaticBatch) * kH;
+	float*       dH1 = H2 + static_cast<size_t>(kStaticBatch) * kH;
+	float*       dH2 = dH1 + static_cast<size_t>(kStaticBatch) * kH;
+	float*       dZ  = dH2 + static_cast<size_t>(kStaticBatch) * kH;
+	cudaStream_t st  = reinterpret_cast<cudaStream_t>(stream);
+	if (d_loss && (s = cuda_check(cudaMemsetAsync(d_loss, 0, sizeof(float), st), "cudaMemsetAsync")) != FLS_OK) {
+		return s;
+	}
+	const uint32_t g = (batch + 255u) / 256u;
+	mlp_train_fwd_kernel<<<g, 256, 0, st>>>(d_params, d_x, d_labels, batch, H1, H2, dZ, d_loss);
+	mlp_train_bwd_kernel<<<g, 256, 0, st>>>(d_params, batch, H1, H2, dZ, dH1, dH2);
+	mlp_grad_kernel<<<2 * kH + kOut, 256, 0, st>>>(d_x, batch, H1, H2, dZ, dH1, dH2, d_grads);
+	count_launch(3);
+	return cuda_check(cudaGetLastError(), "static-scratch MLP gradient kernels launch");
 }
 
 fls_status fls_mlp_adam_step(float* d_params, const float* d_grads, float* d_m, float* d_v, float lr, float beta1,

@@ -273,6 +273,24 @@ uint64_t fls_mlp_workspace_bytes(uint32_t batch);
 fls_status fls_mlp_gradients(const float* d_params, const float* d_x, const uint8_t* d_labels, uint32_t batch,
                              void* d_workspace, uint64_t workspace_bytes, float* d_grads, float* d_loss,
                              fls_stream_t stream);
+/* fls_mlp_gradients without a workspace argument: no counterpart in the
+ * reference.  It is for callers that cannot allocate device memory -- for
+ * example a host engine whose device memory all comes from its own fixed pool,
+ * or an ingest loop that must not pay cudaMalloc's implicit device-wide
+ * synchronisation.  The activation scratch is a static device array of this
+ * library, FLS_MLP_STATIC_MAX_BATCH x 261 floats (about 2.1 MB), which every
+ * device that loads the library holds until the process exits.  The caller
+ * still passes the parameters, inputs, labels and the gradient / loss outputs.
+ *   - batch > FLS_MLP_STATIC_MAX_BATCH returns FLS_ERR_CAPACITY (nothing runs).
+ *   - The first call on a device looks up the array's device address (with
+ *     that device current); make that first call before any stream capture.
+ *   - It calls no cudaMalloc / cudaFree.  All calls share the one array: each
+ *     call writes every scratch element it later reads, so nothing carries
+ *     over between calls, but calls that overlap on the GPU (other streams,
+ *     other host threads) race on it and must be serialised by the caller. */
+#define FLS_MLP_STATIC_MAX_BATCH 2048
+fls_status fls_mlp_gradients_static(const float* d_params, const float* d_x, const uint8_t* d_labels, uint32_t batch,
+                                    float* d_grads, float* d_loss, fls_stream_t stream);
 /* One Adam update (t = 1-based step; d_m, d_v: moment buffers). */
 fls_status fls_mlp_adam_step(float* d_params, const float* d_grads, float* d_m, float* d_v, float lr, float beta1,
                              float beta2, float eps, uint32_t t, fls_stream_t stream);
