@@ -46,6 +46,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch", default="", help="warps,stages,ctas_per_sm,tile_bytes (0 = default)")
     ap.add_argument("--sparse-rows", type=int, default=0, help="FLS_TUNE_SPARSE_ROWS (0 = default)")
+    ap.add_argument("--jit", type=int, choices=[0, 1], default=1,
+                    help="FLS_TUNE_JIT: 1 = kernel specialised to the query's shape, 0 = general kernel")
     return ap.parse_args()
 
 
@@ -188,6 +190,7 @@ def run_ours(a, dist: Dist):
         ops.set_launch_config(*[int(x) for x in a.launch.split(",")])
     if a.sparse_rows:
         ops.set_tuning(0, a.sparse_rows)
+    ops.set_tuning(1, a.jit)
     from fastlanesgpu_b200.shard import allreduce_sum, shard_seed
     seed = shard_seed(1000, dist.rank)
     # ---------------------------------------------------------------- setup
@@ -321,7 +324,8 @@ def run_ours(a, dist: Dist):
                      "traffic": traffic, "algorithmic_bytes_per_launch": comp_bytes},
         "gpu_launches": int(launches),
         "launch_config": dict(zip(["warps", "stages", "ctas_per_sm", "tile_bytes"], ops.get_launch_config()),
-                              sparse_rows=ops.get_tuning(0)),
+                              sparse_rows=ops.get_tuning(0), jit=ops.get_tuning(1),
+                              jit_launches=int(ops.jit_stats()["launches"])),
         "clocks": clk,
     }
     return out, t if a.workload == "q11" else None, hcols

@@ -22,7 +22,7 @@ SCHEME_NAMES = ["FOR", "DELTA", "RLE", "CONST", "DICT"]
 LAYOUT_NORMAL, LAYOUT_TRANSPOSED = 0, 1
 ORDER_STORED, ORDER_ORIGINAL = 0, 1
 MAX_QUERY_COLS, MAX_FILTERS, MAX_PROBES = 8, 4, 4
-TUNE_SPARSE_ROWS = 0
+TUNE_SPARSE_ROWS, TUNE_JIT = 0, 1
 MLP_IN, MLP_HIDDEN, MLP_OUT = 16, 64, 5
 MLP_N_PARAMS = 64 * 16 + 64 + 64 * 64 + 64 + 5 * 64 + 5
 
@@ -72,6 +72,11 @@ class JoinAggDesc(ctypes.Structure):
                 ("probes", Probe * MAX_PROBES), ("n_probes", ctypes.c_uint32), ("agg_col", ctypes.c_uint32),
                 ("key_a", ctypes.c_int32), ("key_b", ctypes.c_int32), ("group_mul", ctypes.c_int32),
                 ("group_sub", ctypes.c_int32), ("n_groups", ctypes.c_int32)]
+
+
+class JitStats(ctypes.Structure):
+    _fields_ = [("compiled", ctypes.c_uint64), ("launches", ctypes.c_uint64), ("failures", ctypes.c_uint64),
+                ("cached", ctypes.c_uint64)]
 
 
 _u32p = ctypes.POINTER(ctypes.c_uint32)
@@ -124,6 +129,9 @@ _SIGS = {
                                          ctypes.c_float, ctypes.c_uint32, _VP]),
     "fls_mlp_infer": (ctypes.c_int, [_VP, _VP, ctypes.c_uint64, _VP, _VP, _VP, _VP]),
     "fls_get_tuning": (ctypes.c_int, [ctypes.c_uint32, _VP]),
+    "fls_get_jit_stats": (ctypes.c_int, [ctypes.POINTER(JitStats)]),
+    "fls_jit_last_log": (ctypes.c_char_p, []),
+    "fls_jit_precompile": (ctypes.c_int, [ctypes.POINTER(FilterAggDesc)]),
 }
 
 _LIB = None

@@ -17,6 +17,12 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OBJ = os.path.join(ROOT, "_build", "obj")
+GEN = os.path.join(ROOT, "_build", "gen")
+# Headers compiled again at run time by NVRTC (query specialisation), embedded
+# as text under the names their #include lines use.
+JIT_HEADERS = [("fls_fixed.cuh", os.path.join(CSRC, "fls_fixed.cuh")),
+               ("fls_device.cuh", os.path.join(CSRC, "fls_device.cuh")),
+               ("../../include/fls_gpu.h", os.path.join(ROOT, "include", "fls_gpu.h"))]
 LIB = os.path.join(PKG, "libfls_gpu.so")
 
 NVCC = os.environ.get("NVCC", "nvcc")
@@ -36,6 +42,26 @@ def _headers():
     hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     hs.append(os.path.join(ROOT, "include", "fls_gpu.h"))
     return hs
+
+
+def _gen_jit_headers() -> None:
+    """Writes _build/gen/fls_jit_headers.inc (only when its text changes)."""
+    os.makedirs(GEN, exist_ok=True)
+    delim = "FLSJIT"
+    out = ["// generated by fastlanesgpu_b200/build.py from the headers it names",
+           "struct JitHeader { const char* name; const char* text; };",
+           "static const JitHeader kJitHeaders[] = {"]
+    for name, path in JIT_HEADERS:
+        text = open(path).read()
+        if ")" + delim + '"' in text:
+            raise RuntimeError(f"{path} contains the raw-string delimiter")
+        out.append(f'\t{{"{name}", R"{delim}(' + text + f'){delim}"}},')
+    out.append("};")
+    body = "\n".join(out) + "\n"
+    dst = os.path.join(GEN, "fls_jit_headers.inc")
+    if not os.path.exists(dst) or open(dst).read() != body:
+        with open(dst, "w") as f:
+            f.write(body)
 
 
 def _stale(obj: str, src: str, headers) -> bool:
@@ -58,13 +84,14 @@ def build(clean: bool = False, verbose: bool = False) -> str:
         shutil.rmtree(OBJ)
     os.makedirs(OBJ, exist_ok=True)
     cu, cpp = _sources()
+    _gen_jit_headers()
     headers = _headers()
     jobs, objs = [], []
     for f in cu:
         src, obj = os.path.join(CSRC, f), os.path.join(OBJ, f + ".o")
         objs.append(obj)
         if _stale(obj, src, headers):
-            jobs.append([NVCC, *NVCC_FLAGS, "-Xptxas", "-v", "-c", src, "-o", obj])
+            jobs.append([NVCC, *NVCC_FLAGS, "-I", GEN, "-Xptxas", "-v", "-c", src, "-o", obj])
     for f in cpp:
         src, obj = os.path.join(CSRC, f), os.path.join(OBJ, f + ".o")
         objs.append(obj)
@@ -76,7 +103,8 @@ def build(clean: bool = False, verbose: bool = False) -> str:
                 if verbose and log:
                     print(log, file=sys.stderr)
     if jobs or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        link = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-Xcompiler", "-fopenmp", "-lgomp", "-cudart", "static"]
+        link = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-Xcompiler", "-fopenmp", "-lgomp", "-ldl", "-cudart",
+                "static"]
         _compile(link)
     return LIB
 

@@ -398,21 +398,24 @@ __device__ __forceinline__ void decode_each(const uint32_t* __restrict__ s, cons
 
 // A FOR vector prepared for reading single rows: the lane's word column in
 // shared memory, bit width, mask and base.  get(r) reads two words (the second
-// may lie past the payload: the pipeline leaves slack after every slot, and
-// the bits read from it are masked off unless the field straddles).
+// may lie up to 31 words past the payload: the pipeline leaves 32 words of
+// slack after the stages, and the bits read from it are masked off unless the
+// field straddles).  A 0-bit vector has no payload: both reads then fall on
+// the slot's first word row (within the slack) and the mask drops them.
 struct ForRows {
 	const uint32_t* s;
-	uint32_t        bw, mask, base;
+	uint32_t        bw, mask, base, next;
 	__device__ __forceinline__ void init(const uint32_t* slot, const VecInfo& m, uint32_t lane) {
 		s    = slot + lane;
 		bw   = m.bw;
 		mask = m.bw >= 32 ? 0xffffffffu : ((1u << m.bw) - 1u);
 		base = static_cast<uint32_t>(m.base);
+		next = m.bw ? 32u : 0u;
 	}
 	__device__ __forceinline__ uint32_t get(uint32_t r) const {
 		const uint32_t bit = r * bw, w = bit >> 5, sh = bit & 31u;
 		const uint32_t* p  = s + 32u * w;
-		return (__funnelshift_r(p[0], p[32], sh) & mask) + base;
+		return (__funnelshift_r(p[0], p[next], sh) & mask) + base;
 	}
 };
 

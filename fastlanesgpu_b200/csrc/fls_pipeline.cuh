@@ -291,9 +291,31 @@ fls_status cuda_check(cudaError_t e, const char* what);
 uint32_t*  device_error_word(); // device address of this device's error word
 void       count_launch(uint64_t n = 1);
 int        tuning_sparse_rows();
+int        tuning_jit();
 
 // Validates one column descriptor and converts it for a kernel.
 fls_status make_devcol(const fls_column& c, DevCol& d);
+
+// Query specialisation of filter-aggregate (fls_jit.cu).  A shape: the staged
+// columns (filter columns in evaluation order, then aggregate-only columns),
+// the aggregate columns' staged slots and the key naming the kernel.
+struct JitShape {
+	uint32_t    staged[FLS_MAX_QUERY_COLS];
+	uint32_t    n_staged = 0;
+	int         agg_a = -1, agg_b = -1;
+	std::string key;
+};
+// False when the query does not qualify (a non-FOR or non-uniform column,
+// two ranges on one column, no column read).
+bool jit_shape(const fls_column* cols, const fls_filter* filters, uint32_t n_filters, int32_t agg_a, int32_t agg_b,
+               JitShape& sh);
+// NVRTC compile of a shape (cached; no device needed).  False on failure.
+bool jit_compile(const JitShape& sh);
+// Filter-aggregate through the specialised kernel (filters in evaluation
+// order).  used = false, with FLS_OK, when the shape does not qualify or its
+// specialisation is unavailable: run the general kernel then.
+fls_status jit_filter_agg(const fls_column* cols, const fls_filter* filters, uint32_t n_filters, int32_t agg_a,
+                          int32_t agg_b, int64_t* d_result, int32_t sparse_rows, cudaStream_t stream, bool& used);
 
 // Lays out shared memory for a set of columns; extra_words per warp and
 // cta_words per CTA are operator-specific scratch.

@@ -480,36 +480,32 @@ __global__ void pht_build_kernel(const int32_t* __restrict__ filter, int32_t fil
 
 using namespace fls;
 
-extern "C" {
+namespace {
 
-fls_status fls_query_filter_agg(const fls_filter_agg_desc* desc, int64_t* d_result, fls_stream_t stream) {
-	if (!desc || !d_result || !desc->cols) {
-		return set_error(FLS_ERR_INVALID_ARG, "fls_query_filter_agg: null pointer");
-	}
+// Validates a filter-aggregate descriptor and puts its filters in evaluation
+// order: most selective first (the result does not depend on the order).
+// Selectivity is estimated for uniform FOR columns as the share of the
+// column's value domain [base, base + 2^bw) inside the range; other columns
+// keep their position.  empty: some range is empty, so nothing is selected.
+fls_status order_filters(const fls_filter_agg_desc* desc, fls_filter (&order)[FLS_MAX_FILTERS], bool& empty) {
+	if (!desc || !desc->cols) { return set_error(FLS_ERR_INVALID_ARG, "fls_query_filter_agg: null pointer"); }
 	if (desc->n_filters > FLS_MAX_FILTERS) { return set_error(FLS_ERR_INVALID_ARG, "too many filters"); }
 	const int32_t nc = static_cast<int32_t>(desc->n_cols);
 	if (desc->agg_a >= nc || desc->agg_b >= nc || (desc->agg_b >= 0 && desc->agg_a < 0)) {
 		return set_error(FLS_ERR_INVALID_ARG, "aggregate column out of range");
 	}
-	FilterAggOp op {};
-	op.n_filters = desc->n_filters;
-	bool empty   = false;
-	// Evaluate the most selective filter first (the result does not depend on
-	// the order).  Selectivity is estimated for uniform FOR columns as the share
-	// of the column's value domain [base, base + 2^bw) inside the range; other
-	// columns keep their position.
-	fls_filter order[FLS_MAX_FILTERS];
-	double     sel[FLS_MAX_FILTERS];
+	empty = false;
+	double sel[FLS_MAX_FILTERS];
 	for (uint32_t f = 0; f < desc->n_filters; ++f) {
 		order[f] = desc->filters[f];
 		sel[f]   = 1.0;
-		if (order[f].col < desc->n_cols) {
-			const fls_column& c = desc->cols[order[f].col];
-			if (!c.meta && c.scheme == FLS_SCHEME_FOR && c.bw < 32) {
-				const double lo = std::max<double>(order[f].lo, c.base);
-				const double hi = std::min<double>(order[f].hi, static_cast<double>(c.base) + std::ldexp(1.0, c.bw) - 1);
-				sel[f]          = hi < lo ? 0.0 : (hi - lo + 1.0) / std::ldexp(1.0, c.bw);
-			}
+		if (order[f].col >= desc->n_cols) { return set_error(FLS_ERR_INVALID_ARG, "filter column out of range"); }
+		empty               = empty || order[f].lo > order[f].hi;
+		const fls_column& c = desc->cols[order[f].col];
+		if (!c.meta && c.scheme == FLS_SCHEME_FOR && c.bw < 32) {
+			const double lo = std::max<double>(order[f].lo, c.base);
+			const double hi = std::min<double>(order[f].hi, static_cast<double>(c.base) + std::ldexp(1.0, c.bw) - 1);
+			sel[f]          = hi < lo ? 0.0 : (hi - lo + 1.0) / std::ldexp(1.0, c.bw);
 		}
 	}
 	for (uint32_t f = 1; f < desc->n_filters; ++f) { // stable insertion sort
@@ -518,27 +514,60 @@ fls_status fls_query_filter_agg(const fls_filter_agg_desc* desc, int64_t* d_resu
 			std::swap(order[g], order[g - 1]);
 		}
 	}
+	return FLS_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+fls_status fls_query_filter_agg(const fls_filter_agg_desc* desc, int64_t* d_result, fls_stream_t stream) {
+	if (!d_result) { return set_error(FLS_ERR_INVALID_ARG, "fls_query_filter_agg: null pointer"); }
+	fls_filter order[FLS_MAX_FILTERS];
+	bool       empty = false;
+	fls_status s     = order_filters(desc, order, empty);
+	if (s != FLS_OK) { return s; }
+	FilterAggOp op {};
+	op.n_filters = desc->n_filters;
 	for (uint32_t f = 0; f < desc->n_filters; ++f) {
-		const fls_filter& fl = order[f];
-		if (fl.col >= desc->n_cols) { return set_error(FLS_ERR_INVALID_ARG, "filter column out of range"); }
-		empty         = empty || fl.lo > fl.hi;
-		op.f_col[f]   = fl.col;
-		op.f_lo[f]    = static_cast<uint32_t>(fl.lo);
-		op.f_range[f] = static_cast<uint32_t>(fl.hi) - static_cast<uint32_t>(fl.lo);
+		op.f_col[f]   = order[f].col;
+		op.f_lo[f]    = static_cast<uint32_t>(order[f].lo);
+		op.f_range[f] = static_cast<uint32_t>(order[f].hi) - static_cast<uint32_t>(order[f].lo);
 	}
 	op.agg_a       = desc->agg_a;
 	op.agg_b       = desc->agg_b;
 	op.result      = reinterpret_cast<long long*>(d_result);
 	op.sparse_rows = tuning_sparse_rows();
-	StageCfg   cfg;
-	uint32_t   grid, threads;
-	size_t     smem;
-	fls_status s = plan_stages(desc->cols, desc->n_cols, 0u, 0u, cfg, grid, threads, smem);
+	StageCfg cfg;
+	uint32_t grid, threads;
+	size_t   smem;
+	s = plan_stages(desc->cols, desc->n_cols, 0u, 0u, cfg, grid, threads, smem);
 	if (s != FLS_OK) { return s; }
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
 	if ((s = cuda_check(cudaMemsetAsync(d_result, 0, sizeof(int64_t), st), "cudaMemsetAsync")) != FLS_OK) { return s; }
 	if (empty) { return FLS_OK; } // an empty range selects nothing
+	if (tuning_jit()) {
+		bool used = false;
+		s = jit_filter_agg(desc->cols, order, desc->n_filters, desc->agg_a, desc->agg_b, d_result, op.sparse_rows, st,
+		                   used);
+		if (s != FLS_OK || used) { return s; }
+	}
 	return launch_staged(cfg, op, grid, threads, smem, st);
+}
+
+fls_status fls_jit_precompile(const fls_filter_agg_desc* desc) {
+	fls_filter order[FLS_MAX_FILTERS];
+	bool       empty = false;
+	fls_status s     = order_filters(desc, order, empty);
+	if (s != FLS_OK) { return s; }
+	JitShape sh;
+	if (!jit_shape(desc->cols, order, desc->n_filters, desc->agg_a, desc->agg_b, sh)) {
+		return set_error(FLS_ERR_UNSUPPORTED, "query does not qualify for specialisation (uniform FOR columns only)");
+	}
+	if (!jit_compile(sh)) {
+		return set_error(FLS_ERR_UNSUPPORTED, std::string("specialisation failed: ") + fls_jit_last_log());
+	}
+	return FLS_OK;
 }
 
 fls_status fls_pht_build(const int32_t* d_filter, int32_t filter_eq, const int32_t* d_keys, const int32_t* d_vals,

@@ -42,9 +42,11 @@ void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxe
 namespace {
 constexpr int    kDefaultSparseRows = 4;
 std::atomic<int> g_sparse_rows {kDefaultSparseRows};
+std::atomic<int> g_jit {1};
 } // namespace
 
 int tuning_sparse_rows() { return g_sparse_rows.load(std::memory_order_relaxed); }
+int tuning_jit() { return g_jit.load(std::memory_order_relaxed); }
 
 fls_status cuda_check(cudaError_t e, const char* what) {
 	if (e == cudaSuccess) { return FLS_OK; }
@@ -279,6 +281,10 @@ fls_status fls_set_tuning(uint32_t param, int64_t value) {
 		if (value < 0 || value > 32) { return set_error(FLS_ERR_INVALID_ARG, "sparse rows must be in [0, 32]"); }
 		g_sparse_rows.store(value ? static_cast<int>(value) : kDefaultSparseRows);
 		return FLS_OK;
+	case FLS_TUNE_JIT:
+		if (value < 0 || value > 1) { return set_error(FLS_ERR_INVALID_ARG, "jit must be 0 or 1"); }
+		g_jit.store(static_cast<int>(value));
+		return FLS_OK;
 	default: return set_error(FLS_ERR_INVALID_ARG, "unknown tuning parameter");
 	}
 }
@@ -287,6 +293,7 @@ fls_status fls_get_tuning(uint32_t param, int64_t* value) {
 	if (!value) { return set_error(FLS_ERR_INVALID_ARG, "fls_get_tuning: null pointer"); }
 	switch (param) {
 	case FLS_TUNE_SPARSE_ROWS: *value = tuning_sparse_rows(); return FLS_OK;
+	case FLS_TUNE_JIT: *value = tuning_jit(); return FLS_OK;
 	default: return set_error(FLS_ERR_INVALID_ARG, "unknown tuning parameter");
 	}
 }

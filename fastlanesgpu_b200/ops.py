@@ -23,7 +23,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import (MAX_FILTERS, MAX_PROBES, ORDER_STORED, FilterAggDesc, JoinAggDesc, check, lib)
+from ._lib import (MAX_FILTERS, MAX_PROBES, ORDER_STORED, Column, FilterAggDesc, JitStats, JoinAggDesc, check, lib)
 from .column import DeviceColumn, columns_array
 
 
@@ -121,20 +121,44 @@ def query_filter_agg(cols, filters, agg_a: int = -1, agg_b: int = -1, out=None):
     """Filters [(col, lo, hi)] (inclusive int32 ranges) ANDed; returns the int64
     sum of cols[agg_a] (* cols[agg_b]) over the selected rows, or the count."""
     import torch
-    if len(filters) > MAX_FILTERS:
-        raise ValueError("at most 4 filters")
-    arr = columns_array(cols)
-    d = FilterAggDesc()
-    d.cols = arr
-    d.n_cols = len(cols)
-    for i, (c, lo, hi) in enumerate(filters):
-        d.filters[i].col, d.filters[i].lo, d.filters[i].hi = c, lo, hi
-    d.n_filters = len(filters)
-    d.agg_a, d.agg_b = agg_a, agg_b
+    d, _keep = _filter_agg_desc(columns_array(cols), len(cols), filters, agg_a, agg_b)
     if out is None:
         out = torch.empty(1, dtype=torch.int64, device=cols[0].data.device)
     check(lib().fls_query_filter_agg(ctypes.byref(d), out.data_ptr(), _stream()), "fls_query_filter_agg")
     return out
+
+
+def _filter_agg_desc(arr, n_cols: int, filters, agg_a: int, agg_b: int):
+    if len(filters) > MAX_FILTERS:
+        raise ValueError("at most 4 filters")
+    d = FilterAggDesc()
+    d.cols = arr
+    d.n_cols = n_cols
+    for i, (c, lo, hi) in enumerate(filters):
+        d.filters[i].col, d.filters[i].lo, d.filters[i].hi = c, lo, hi
+    d.n_filters = len(filters)
+    d.agg_a, d.agg_b = agg_a, agg_b
+    return d, arr
+
+
+def jit_precompile(col_descs, filters, agg_a: int = -1, agg_b: int = -1) -> None:
+    """Compiles the specialised filter-aggregate kernel for this query shape
+    (column descriptors: `Column` structs, or DeviceColumns).  Needs no GPU."""
+    descs = [c.desc if hasattr(c, "desc") else c for c in col_descs]
+    arr = (Column * len(descs))(*descs)
+    d, _keep = _filter_agg_desc(arr, len(descs), filters, agg_a, agg_b)
+    check(lib().fls_jit_precompile(ctypes.byref(d)), "fls_jit_precompile")
+
+
+def jit_stats() -> dict:
+    """Counters of the specialised-kernel cache."""
+    s = JitStats()
+    check(lib().fls_get_jit_stats(ctypes.byref(s)), "fls_get_jit_stats")
+    return {"compiled": s.compiled, "launches": s.launches, "failures": s.failures, "cached": s.cached}
+
+
+def jit_last_log() -> str:
+    return (lib().fls_jit_last_log() or b"").decode(errors="replace")
 
 
 def build_pht(keys, ht_len: int, vals=None, filt=None, filter_eq: int = 1, keys_min: int = 0, out=None):

@@ -331,15 +331,39 @@ fls_status fls_set_launch_config(uint32_t warps_per_cta, uint32_t stages, uint32
 fls_status fls_get_launch_config(uint32_t* warps_per_cta, uint32_t* stages, uint32_t* ctas_per_sm,
                                  uint32_t* tile_bytes);
 
-/* Other tuning parameters of the operators (0 restores the default). */
+/* Other tuning parameters of the operators. */
 typedef enum fls_tune_param {
 	/* Operators evaluate whole vectors while some lane of a warp still has more
 	 * than this many selected rows in its 32; at or below it they switch to a
-	 * loop over the selected rows that reads only their fields.  Default 4. */
-	FLS_TUNE_SPARSE_ROWS = 0
+	 * loop over the selected rows that reads only their fields.  Default 4;
+	 * 0 restores the default. */
+	FLS_TUNE_SPARSE_ROWS = 0,
+	/* 1 (default): fls_query_filter_agg on uniform FOR columns runs a kernel
+	 * compiled at first use (NVRTC) for the query's exact bit widths, filter
+	 * count and aggregate, cached per shape in the process; any compile or
+	 * load failure falls back to the general kernel.  0: always the general
+	 * kernel.  Results are identical either way. */
+	FLS_TUNE_JIT = 1
 } fls_tune_param;
 fls_status fls_set_tuning(uint32_t param, int64_t value);
 fls_status fls_get_tuning(uint32_t param, int64_t* value);
+
+/* Counters of the specialised-kernel cache (all threads of the process). */
+typedef struct fls_jit_stats {
+	uint64_t compiled; /* shapes compiled and loaded */
+	uint64_t launches; /* launches of specialised kernels */
+	uint64_t failures; /* shapes whose compile or load failed (general kernel used) */
+	uint64_t cached;   /* shapes currently cached */
+} fls_jit_stats;
+fls_status fls_get_jit_stats(fls_jit_stats* out);
+/* Compile log of the most recent failed specialisation ("" if none). */
+const char* fls_jit_last_log(void);
+/* Compiles (NVRTC, no device needed) the specialised kernel that
+ * fls_query_filter_agg would run for this query, so that the first query does
+ * not pay for it (e.g. before capturing a CUDA graph).  FLS_ERR_UNSUPPORTED if
+ * the query does not qualify or the compile failed (fls_last_error has the
+ * log). */
+fls_status fls_jit_precompile(const fls_filter_agg_desc* desc);
 
 /* Number of kernels this library has launched in this process (all threads). */
 uint64_t fls_kernel_launch_count(void);

@@ -1,0 +1,150 @@
+"""GPU parity of the specialised (NVRTC-compiled) filter-aggregate kernel:
+against the oracle on Q1.1, and against a numpy evaluation and the general
+kernel on seeded random query shapes (bit widths 0..32, both layouts, 0-4
+filters, count / sum / sum of products, ragged lengths)."""
+import numpy as np
+import pytest
+
+from fastlanesgpu_b200 import LAYOUT_NORMAL, LAYOUT_TRANSPOSED, EncodedColumn, datagen, ops
+from fastlanesgpu_b200._lib import TUNE_JIT, TUNE_SPARSE_ROWS
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture
+def jit_on(cuda):
+    ops.set_tuning(TUNE_JIT, 1)
+    yield
+    ops.set_tuning(TUNE_JIT, 1)
+    ops.set_tuning(TUNE_SPARSE_ROWS, 0)
+
+
+def _launches():
+    return ops.jit_stats()["launches"]
+
+
+def _run(cols, filters, a, b, jit):
+    ops.set_tuning(TUNE_JIT, 1 if jit else 0)
+    before = _launches()
+    got = int(ops.query_filter_agg(cols, filters, agg_a=a, agg_b=b).cpu()[0])
+    ops.check_device_error()
+    return got, _launches() - before
+
+
+def _numpy(vals, filters, a, b):
+    sel = np.ones(vals[0].size, bool)
+    for c, lo, hi in filters:
+        sel &= (vals[c] >= lo) & (vals[c] <= hi)
+    if a < 0:
+        return int(sel.sum())
+    x = vals[a][sel].astype(np.int64)
+    if b >= 0:
+        x = x * vals[b][sel].astype(np.int64)
+    return int(x.sum())
+
+
+@pytest.mark.parametrize("n", [1, 1000, 1 << 20, (1 << 20) + 333, 1 << 24])
+def test_jit_q11_against_oracle(jit_on, oracle, n):
+    t = datagen.lineorder_q11(n, seed=n)
+    order = ["date", "discount", "quantity", "price"]
+    cols = [EncodedColumn.uniform(t[k], bw=datagen.Q11_BITS[k]).to_device() for k in order]
+    f = datagen.Q11_FILTER
+    filters = [(0, *f["date"]), (1, *f["discount"]), (2, *f["quantity"])]
+    want = oracle.filter_agg(t["date"], t["discount"], t["quantity"], t["price"], *f["date"], *f["discount"],
+                             f["quantity"][1] + 1)
+    got, used = _run(cols, filters, 3, 1, jit=True)
+    assert used == 1 and got == want
+    assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
+
+
+def _random_case(g, n):
+    n_cols = int(g.integers(1, 6))
+    layout = LAYOUT_TRANSPOSED if g.random() < 0.3 else LAYOUT_NORMAL
+    vals, cols = [], []
+    for _ in range(n_cols):
+        bw = int(g.choice([0, 1, 3, 4, 7, 8, 12, 16, 17, 24, 31, 32]))
+        if bw == 32:
+            v = g.integers(-2**31, 2**31, n, dtype=np.int64).astype(np.int32)
+            base = 0
+        else:
+            base = int(g.integers(-(1 << 20), 1 << 20))
+            v = (g.integers(0, 1 << bw, n, dtype=np.int64) + base).astype(np.int32) if bw else np.full(n, base, np.int32)
+        vals.append(v)
+        cols.append(EncodedColumn.uniform(v, bw=bw, base=base, layout=layout).to_device())
+    n_f = int(g.integers(0, min(4, n_cols) + 1))
+    fcols = g.permutation(n_cols)[:n_f]
+    filters = []
+    for c in fcols:
+        q = np.sort(g.random(2))
+        if g.random() < 0.3:  # a selective range
+            q[1] = q[0] + (q[1] - q[0]) * 0.05
+        lo, hi = (int(x) for x in np.quantile(vals[c], q))
+        filters.append((int(c), lo, hi))
+    r = g.random()
+    if r < 0.2:
+        a, b = -1, -1
+    elif r < 0.6:
+        a, b = int(g.integers(0, n_cols)), -1
+    else:
+        a, b = int(g.integers(0, n_cols)), int(g.integers(0, n_cols))
+    return vals, cols, filters, a, b
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_jit_random_shapes(jit_on, seed):
+    g = np.random.default_rng(1000 + seed)
+    n = int(g.choice([1, 17, 1024, 1025, 40 * 1024 + 511, 300 * 1024]))
+    vals, cols, filters, a, b = _random_case(g, n)
+    want = _numpy(vals, filters, a, b)
+    got_jit, used = _run(cols, filters, a, b, jit=True)
+    got_gen, used_gen = _run(cols, filters, a, b, jit=False)
+    assert used_gen == 0
+    assert got_gen == want
+    assert got_jit == want, (filters, a, b, [c.desc.bw for c in cols])
+    assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
+
+
+@pytest.mark.parametrize("sparse_rows", [1, 4, 12, 32])
+def test_jit_sparse_threshold_does_not_change_results(jit_on, sparse_rows):
+    n = 500 * 1024 + 3
+    t = datagen.lineorder_q11(n, seed=11)
+    order = ["date", "discount", "quantity", "price"]
+    cols = [EncodedColumn.uniform(t[k], bw=datagen.Q11_BITS[k]).to_device() for k in order]
+    vals = [t[k] for k in order]
+    for filters in ([(0, 366, 730), (1, 1, 3), (2, -2**31, 24)], [(2, 0, 40)], [(0, 0, 2000), (1, 0, 9)]):
+        ops.set_tuning(TUNE_SPARSE_ROWS, sparse_rows)
+        got, used = _run(cols, filters, 3, 1, jit=True)
+        assert used == 1
+        assert got == _numpy(vals, filters, 3, 1)
+
+
+def test_jit_falls_back_where_it_does_not_apply(jit_on):
+    n = 64 * 1024 + 5
+    g = np.random.default_rng(7)
+    a = g.integers(0, 1000, n).astype(np.int32)
+    b = g.integers(0, 50, n).astype(np.int32)
+    ua, ub = EncodedColumn.uniform(a, bw=10).to_device(), EncodedColumn.uniform(b, bw=6).to_device()
+    # two ranges on one column
+    got, used = _run([ua, ub], [(0, 100, 900), (0, 200, 950)], 1, -1, jit=True)
+    assert used == 0 and got == _numpy([a, b], [(0, 100, 900), (0, 200, 950)], 1, -1)
+    # a per-vector column
+    pb = EncodedColumn.encode(b, 0, layout=LAYOUT_NORMAL).to_device()
+    got, used = _run([ua, pb], [(0, 100, 900)], 1, 0, jit=True)
+    assert used == 0 and got == _numpy([a, b], [(0, 100, 900)], 1, 0)
+    # no column read at all
+    got, used = _run([ua], [], -1, -1, jit=True)
+    assert used == 0 and got == n
+    # switched off
+    got, used = _run([ua, ub], [(0, 100, 900)], 1, -1, jit=False)
+    assert used == 0 and got == _numpy([a, b], [(0, 100, 900)], 1, -1)
+
+
+def test_jit_unused_columns_are_not_read(jit_on):
+    n = 100 * 1024
+    g = np.random.default_rng(9)
+    a = g.integers(0, 1 << 12, n).astype(np.int32)
+    c = g.integers(0, 1 << 20, n).astype(np.int32)
+    cols = [EncodedColumn.uniform(a, bw=12).to_device(), EncodedColumn.uniform(c, bw=20).to_device(),
+            EncodedColumn.uniform(a, bw=12).to_device()]
+    got, used = _run(cols, [(2, 10, 2000)], 1, -1, jit=True)
+    assert used == 1 and got == _numpy([a, c, a], [(2, 10, 2000)], 1, -1)

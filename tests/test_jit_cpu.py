@@ -1,0 +1,48 @@
+"""Query specialisation without a GPU: NVRTC compiles the specialised
+filter-aggregate kernel for the Q1.1 shape and for edge shapes, and queries
+that do not qualify are refused with FLS_ERR_UNSUPPORTED."""
+import pytest
+
+from fastlanesgpu_b200 import FlsError, datagen, ops
+from fastlanesgpu_b200._lib import LAYOUT_NORMAL, LAYOUT_TRANSPOSED, SCHEME_DELTA, SCHEME_FOR, Column
+
+N = (1 << 20) + 7
+
+
+def _col(bw, layout=LAYOUT_NORMAL, scheme=SCHEME_FOR, base=0):
+    nv = (N + 1023) // 1024
+    return Column(data=0x100000, meta=0, n_values=N, n_words=32 * bw * nv + 32 * nv, layout=layout, scheme=scheme,
+                  bw=bw, base=base, max_vec_words=0, scheme_mask=1 << scheme)
+
+
+def test_precompile_q11_shape():
+    bits = datagen.Q11_BITS
+    f = datagen.Q11_FILTER
+    cols = [_col(bits[k]) for k in ("date", "discount", "quantity", "price")]
+    before = ops.jit_stats()
+    ops.jit_precompile(cols, [(0, *f["date"]), (1, *f["discount"]), (2, *f["quantity"])], 3, 1)
+    after = ops.jit_stats()
+    assert after["failures"] == before["failures"], ops.jit_last_log()
+    assert after["cached"] >= 1
+
+
+@pytest.mark.parametrize("bws,filters,a,b,layout", [
+    ([0, 32], [(0, 0, 0), (1, -5, 5)], 1, 1, LAYOUT_NORMAL),
+    ([1, 2, 3, 4, 5], [(0, 0, 0), (1, 0, 1), (2, 0, 2), (3, 0, 3)], 4, 0, LAYOUT_TRANSPOSED),
+    ([17], [], 0, -1, LAYOUT_NORMAL),
+    ([31, 9], [(1, 3, 300)], -1, -1, LAYOUT_TRANSPOSED),
+])
+def test_precompile_edge_shapes(bws, filters, a, b, layout):
+    ops.jit_precompile([_col(x, layout) for x in bws], filters, a, b)
+    assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
+
+
+def test_precompile_refuses_unqualified_queries():
+    with pytest.raises(FlsError) as e:
+        ops.jit_precompile([_col(8, LAYOUT_TRANSPOSED, SCHEME_DELTA)], [(0, 1, 2)], 0, -1)
+    assert e.value.status == 7
+    with pytest.raises(FlsError) as e:
+        ops.jit_precompile([_col(8), _col(9)], [(0, 1, 2), (0, 3, 4)], 1, -1)
+    assert e.value.status == 7
+    with pytest.raises(FlsError):
+        ops.jit_precompile([_col(8)], [(3, 1, 2)], 0, -1)  # filter column out of range
