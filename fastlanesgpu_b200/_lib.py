@@ -132,6 +132,7 @@ _SIGS = {
     "fls_get_jit_stats": (ctypes.c_int, [ctypes.POINTER(JitStats)]),
     "fls_jit_last_log": (ctypes.c_char_p, []),
     "fls_jit_precompile": (ctypes.c_int, [ctypes.POINTER(FilterAggDesc)]),
+    "fls_jit_precompile_probe": (ctypes.c_int, [ctypes.POINTER(JoinAggDesc)]),
 }
 
 _LIB = None

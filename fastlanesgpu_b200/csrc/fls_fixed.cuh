@@ -1,17 +1,18 @@
-// fls_fixed.cuh -- filter-aggregate kernel specialised to one query shape.
+// fls_fixed.cuh -- query kernels specialised to one query shape.
 //
 // For queries whose columns are all uniform FOR columns (the reference's
 // column format: one bit width and base per column, fls_q11.cu:202-223), the
-// library compiles this template at first use with NVRTC for the exact shape
-// (bit width of every column, number of filters, aggregate kind) and caches
-// the kernel (fls_jit.cu).  Everything that the generic operator decides per
-// vector at run time -- which decoder, how many filters, where the aggregate
-// columns are, which filters remain in the row-at-a-time loop -- becomes a
-// compile-time constant here.  Results are identical to the generic operator.
+// library compiles these templates at first use with NVRTC for the exact shape
+// and caches the kernel (fls_jit.cu).  Everything the general operators decide
+// per vector at run time -- which decoder, how many filters or probes, where
+// the aggregate columns are, which table lives in shared memory, which
+// predicates remain for the row-at-a-time loop -- becomes a compile-time
+// constant here.  Results are identical to the general operators.
 //
-// Columns are staged in filter order (column f holds filter f), followed by
-// aggregate columns that are not filter columns; Query's template arguments
-// name the aggregate columns by staged index (-1 = none).
+//  * filter-aggregate (FilterQuery): columns staged in filter order (column f
+//    holds filter f), then aggregate columns no filter reads;
+//  * probe + group-by (ProbeQuery): columns staged in probe order (column q
+//    holds the key of probe q), then the measure column if no probe reads it.
 #pragma once
 
 #include "fls_device.cuh"
@@ -19,35 +20,55 @@
 namespace fls {
 namespace fixed {
 
-constexpr uint32_t kSlack     = 32;       // words after the stages (row reads look one word row ahead)
-constexpr uint32_t kWaitPolls = 1u << 17; // bounded stage waits (each <= ~20 us)
+constexpr uint32_t kSlack         = 32;      // words after the stages (row reads look one word row ahead)
+constexpr uint32_t kWaitPolls     = 1u << 17; // bounded stage waits (each <= ~20 us)
 constexpr uint32_t kErrTimeoutBit = 1u << 2;
-constexpr int      kDenseAggRows  = 16;      // above this many rows in some lane, aggregate whole vectors
+constexpr uint32_t kErrHashBit    = 1u << 3;
+constexpr int      kDenseAggRows  = 16; // above this many rows in some lane, aggregate whole vectors
+constexpr int      kRowBatch      = 8;  // selected rows per lane whose table reads are in flight together
 
-struct FixedParams {
-	const uint32_t*     data[FLS_MAX_QUERY_COLS];
+// The staged pipeline's parameters (shared by both operators).
+struct StageParams {
+	const uint32_t* data[FLS_MAX_QUERY_COLS];
+	uint64_t        n_values, n_vec, n_tiles;
+	uint32_t        tile, stages, warps, warp_smem_words, stage_words, bar_off;
+	uint32_t*       err;
+	uint32_t        cta_off; // words: CTA-wide scratch (hash tables) after the warps' areas
+	uint32_t        pad_;
+};
+
+struct FilterParams {
+	StageParams         S;
 	uint32_t            base[FLS_MAX_QUERY_COLS]; // FOR base of each staged column
 	uint32_t            lo[FLS_MAX_FILTERS];      // filter lower bound (unsigned wrap)
 	uint32_t            range[FLS_MAX_FILTERS];   // hi - lo
-	uint64_t            n_values, n_vec, n_tiles;
-	uint32_t            tile, stages, warps, warp_smem_words, stage_words, bar_off;
 	int32_t             sparse_rows;
 	uint32_t            pad_;
 	unsigned long long* result;
-	uint32_t*           err;
 };
 
-// The host (nvcc + host compiler) and NVRTC must agree on the parameter block.
-// Every field is naturally aligned and padded explicitly, so equal sizes mean
-// equal offsets.
-static_assert(sizeof(FixedParams) == 200 && alignof(FixedParams) == 8, "FixedParams layout");
+struct ProbeParams {
+	StageParams    S;
+	uint32_t       base[FLS_MAX_QUERY_COLS];
+	const int32_t* ht[FLS_MAX_PROBES];
+	int32_t        len[FLS_MAX_PROBES];
+	int32_t        kmin[FLS_MAX_PROBES];
+	uint32_t       smem_off[FLS_MAX_PROBES]; // words into the CTA scratch (tables flagged as shared)
+	int32_t        mul, sub, n_groups, sparse_rows;
+	int32_t*       res;
+};
 
-template <int LAYOUT, int NF, int AGG_A, int AGG_B, int... BWS>
-struct Query {
-	static constexpr int NC     = sizeof...(BWS);
-	static constexpr int kNF    = NF;
-	static constexpr int kAggA  = AGG_A;
-	static constexpr int kAggB  = AGG_B;
+// The host (nvcc + host compiler) and NVRTC must agree on the parameter
+// blocks.  Every field is naturally aligned and padded explicitly, so equal
+// sizes mean equal offsets.
+static_assert(sizeof(StageParams) == 128 && alignof(StageParams) == 8, "StageParams layout");
+static_assert(sizeof(FilterParams) == 208, "FilterParams layout");
+static_assert(sizeof(ProbeParams) == 264, "ProbeParams layout");
+
+// Bit widths of the staged columns and where they sit in a stage.
+template <int LAYOUT, int... BWS>
+struct Shape {
+	static constexpr int NC      = sizeof...(BWS);
 	static constexpr int kLayout = LAYOUT;
 	__host__ __device__ static constexpr int bw(int c) {
 		int i = 0, r = 0;
@@ -60,8 +81,29 @@ struct Query {
 		for (int i = 0; i < c; ++i) { s += 32 * bw(i); }
 		return s;
 	}
-	static_assert(NF >= 0 && NF <= FLS_MAX_FILTERS && NC <= FLS_MAX_QUERY_COLS, "query shape");
+	static_assert(NC >= 1 && NC <= FLS_MAX_QUERY_COLS, "1..8 staged columns");
+};
+
+template <int LAYOUT, int NF, int AGG_A, int AGG_B, int... BWS>
+struct FilterQuery : Shape<LAYOUT, BWS...> {
+	static constexpr int kNF   = NF;
+	static constexpr int kAggA = AGG_A;
+	static constexpr int kAggB = AGG_B;
+	static_assert(NF >= 0 && NF <= FLS_MAX_FILTERS, "0..4 filters");
 	static_assert(AGG_B < 0 || AGG_A >= 0, "sum(a*b) needs a");
+};
+
+// KINDS bit q: probe q is PHT_2; SMEM bit q: probe q's table is in shared
+// memory (PHT_1 as a presence bitmap, PHT_2 verbatim).
+template <int LAYOUT, int NP, int AGG, int KEY_A, int KEY_B, int KINDS, int SMEM, int... BWS>
+struct ProbeQuery : Shape<LAYOUT, BWS...> {
+	static constexpr int kNP  = NP;
+	static constexpr int kAgg = AGG;
+	static constexpr int kKeyA = KEY_A;
+	static constexpr int kKeyB = KEY_B;
+	__host__ __device__ static constexpr bool pht2(int q) { return (KINDS >> q) & 1; }
+	__host__ __device__ static constexpr bool in_smem(int q) { return (SMEM >> q) & 1; }
+	static_assert(NP >= 1 && NP <= FLS_MAX_PROBES, "1..4 probes");
 };
 
 // Row r of this lane's stream at compile-time bit width (runtime row).
@@ -94,8 +136,16 @@ struct Vec {
 	}
 };
 
+__device__ __forceinline__ uint32_t valid_rows(const StageParams& S, int layout, uint64_t v, uint32_t lane) {
+	const uint64_t start = v * 1024u;
+	if (start + 1024u <= S.n_values) { return 0xffffffffu; }
+	return dev::tail_rows(static_cast<uint32_t>(layout), lane, static_cast<uint32_t>(S.n_values - start));
+}
+
+// ------------------------------------------------------------ filter-aggregate
+
 template <class Q, int F>
-__device__ __forceinline__ void dense_filter(const FixedParams& P, const Vec<Q>& V, uint32_t lane, uint32_t& mask) {
+__device__ __forceinline__ void dense_filter(const FilterParams& P, const Vec<Q>& V, uint32_t lane, uint32_t& mask) {
 	const uint32_t lo = P.lo[F] - P.base[F], range = P.range[F];
 	uint32_t       m[4] = {0, 0, 0, 0};
 	dev::unpack_rows<Q::bw(F)>(V.template col<F>(), lane,
@@ -106,7 +156,7 @@ __device__ __forceinline__ void dense_filter(const FixedParams& P, const Vec<Q>&
 // Dense filters F, F+1, ... while some lane keeps more than sparse_rows rows;
 // f0 receives the first filter left to the row loop (NF if none).
 template <class Q, int F>
-__device__ __forceinline__ void dense_filters(const FixedParams& P, const Vec<Q>& V, uint32_t lane, uint32_t& mask,
+__device__ __forceinline__ void dense_filters(const FilterParams& P, const Vec<Q>& V, uint32_t lane, uint32_t& mask,
                                               int& f0) {
 	if constexpr (F < Q::kNF) {
 		if (max_rows(mask) <= P.sparse_rows) {
@@ -120,39 +170,40 @@ __device__ __forceinline__ void dense_filters(const FixedParams& P, const Vec<Q>
 	}
 }
 
-template <class Q, int F, int F0>
-__device__ __forceinline__ bool row_pass(const FixedParams& P, const Vec<Q>& V, uint32_t lane, uint32_t r) {
+template <class Q, int F>
+__device__ __forceinline__ bool row_pass(const FilterParams& P, const Vec<Q>& V, uint32_t lane, uint32_t r) {
 	if constexpr (F < Q::kNF) {
 		const bool ok = (row_field<Q::bw(F)>(V.template col<F>(), lane, r) - (P.lo[F] - P.base[F])) <= P.range[F];
-		return ok & row_pass<Q, F + 1, F0>(P, V, lane, r);
+		return ok & row_pass<Q, F + 1>(P, V, lane, r);
 	} else {
 		return true;
 	}
 }
 
 template <class Q, int C>
-__device__ __forceinline__ long long row_value(const FixedParams& P, const Vec<Q>& V, uint32_t lane, uint32_t r) {
-	return static_cast<int32_t>(row_field<Q::bw(C)>(V.template col<C>(), lane, r) + P.base[C]);
+__device__ __forceinline__ int32_t row_value(const uint32_t* base, const Vec<Q>& V, uint32_t lane, uint32_t r) {
+	return static_cast<int32_t>(row_field<Q::bw(C)>(V.template col<C>(), lane, r) + base[C]);
 }
 
 // Filters F0.. and the aggregate, one selected row at a time (warp-uniform
 // trip count, branch-free body).
 template <class Q, int F0>
-__device__ __forceinline__ long long row_loop(const FixedParams& P, const Vec<Q>& V, uint32_t lane, uint32_t mask) {
+__device__ __forceinline__ long long row_loop(const FilterParams& P, const Vec<Q>& V, uint32_t lane, uint32_t mask) {
 	const int n_it = max_rows(mask);
 	long long acc  = 0;
 	for (int it = 0; it < n_it; ++it) {
 		const bool     have = mask != 0u;
 		const uint32_t r    = have ? static_cast<uint32_t>(__ffs(mask)) - 1u : 0u;
 		mask &= mask - 1u;
-		const bool pass = have & row_pass<Q, F0, F0>(P, V, lane, r);
+		const bool pass = have & row_pass<Q, F0>(P, V, lane, r);
 		long long  x;
 		if constexpr (Q::kAggA < 0) {
 			x = 1;
 		} else if constexpr (Q::kAggB < 0) {
-			x = row_value<Q, Q::kAggA>(P, V, lane, r);
+			x = row_value<Q, Q::kAggA>(P.base, V, lane, r);
 		} else {
-			x = row_value<Q, Q::kAggA>(P, V, lane, r) * row_value<Q, Q::kAggB>(P, V, lane, r);
+			x = static_cast<long long>(row_value<Q, Q::kAggA>(P.base, V, lane, r)) *
+			    row_value<Q, Q::kAggB>(P.base, V, lane, r);
 		}
 		acc += pass ? x : 0ll;
 	}
@@ -160,7 +211,7 @@ __device__ __forceinline__ long long row_loop(const FixedParams& P, const Vec<Q>
 }
 
 template <class Q, int F0>
-__device__ __forceinline__ long long row_loop_from(const FixedParams& P, const Vec<Q>& V, uint32_t lane,
+__device__ __forceinline__ long long row_loop_from(const FilterParams& P, const Vec<Q>& V, uint32_t lane,
                                                    uint32_t mask, int f0) {
 	if constexpr (F0 <= Q::kNF) {
 		if (f0 == F0) { return row_loop<Q, F0>(P, V, lane, mask); }
@@ -171,13 +222,13 @@ __device__ __forceinline__ long long row_loop_from(const FixedParams& P, const V
 }
 
 template <class Q>
-__device__ __forceinline__ long long dense_agg(const FixedParams& P, const Vec<Q>& V, uint32_t lane, uint32_t mask) {
+__device__ __forceinline__ long long dense_agg(const FilterParams& P, const Vec<Q>& V, uint32_t lane, uint32_t mask) {
 	if constexpr (Q::kAggA < 0) {
 		return __popc(mask);
 	} else {
-		constexpr int A = Q::kAggA;
-		long long     p[4] = {0, 0, 0, 0};
-		const uint32_t ba = P.base[A];
+		constexpr int  A  = Q::kAggA;
+		long long      p[4] = {0, 0, 0, 0};
+		const uint32_t ba   = P.base[A];
 		if constexpr (Q::kAggB < 0) {
 			dev::unpack_rows<Q::bw(A)>(V.template col<A>(), lane, [&](int r, uint32_t x) {
 				p[r & 3] += ((mask >> r) & 1u) ? static_cast<long long>(static_cast<int32_t>(x + ba)) : 0ll;
@@ -198,19 +249,241 @@ __device__ __forceinline__ long long dense_agg(const FixedParams& P, const Vec<Q
 }
 
 template <class Q>
-__device__ __forceinline__ long long process(const FixedParams& P, const Vec<Q>& V, uint64_t v, uint32_t lane) {
-	uint32_t       mask  = 0xffffffffu;
-	const uint64_t start = v * 1024u;
-	if (start + 1024u > P.n_values) { mask = dev::tail_rows(Q::kLayout, lane, static_cast<uint32_t>(P.n_values - start)); }
-	int f0 = Q::kNF;
-	dense_filters<Q, 0>(P, V, lane, mask, f0);
-	if (!__any_sync(0xffffffffu, mask)) { return 0; }
-	if (f0 < Q::kNF) { return row_loop_from<Q, 0>(P, V, lane, mask, f0); }
-	// Every filter ran dense: the aggregate reads the selected rows one at a
-	// time unless most rows are selected.
-	if (Q::kAggA < 0 || max_rows(mask) > kDenseAggRows) { return dense_agg<Q>(P, V, lane, mask); }
-	return row_loop<Q, Q::kNF>(P, V, lane, mask);
+struct FilterBody {
+	static constexpr bool kCtaSetup = false;
+	const FilterParams&   P;
+	long long             acc = 0;
+
+	__device__ __forceinline__ void cta_setup(uint32_t*) {}
+
+	__device__ __forceinline__ void operator()(const Vec<Q>& V, uint64_t v, uint32_t lane) {
+		uint32_t mask = valid_rows(P.S, Q::kLayout, v, lane);
+		int      f0   = Q::kNF;
+		dense_filters<Q, 0>(P, V, lane, mask, f0);
+		if (!__any_sync(0xffffffffu, mask)) { return; }
+		if (f0 < Q::kNF) {
+			acc += row_loop_from<Q, 0>(P, V, lane, mask, f0);
+		} else if (Q::kAggA < 0 || max_rows(mask) > kDenseAggRows) {
+			// Every filter ran dense: the aggregate reads the selected rows one
+			// at a time unless most rows are selected.
+			acc += dense_agg<Q>(P, V, lane, mask);
+		} else {
+			acc += row_loop<Q, Q::kNF>(P, V, lane, mask);
+		}
+	}
+
+	__device__ __forceinline__ void finish(uint32_t lane) {
+		unsigned long long s = static_cast<unsigned long long>(acc);
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1) { s += __shfl_xor_sync(0xffffffffu, s, o); }
+		if (lane == 0 && s) { atomicAdd(P.result, s); }
+	}
+};
+
+// -------------------------------------------------------- probe + group-by
+
+// HASH(X,Y,Z) = (X-Z) % Y (crystal-opt/join.cuh:26) of d = key - keys_min:
+// in-range keys skip the division; a negative remainder is flagged and misses.
+__device__ __forceinline__ bool hash_slot(uint32_t d, int32_t len, uint32_t& h, uint32_t* err) {
+	h = d;
+	if (d >= static_cast<uint32_t>(len)) {
+		const int32_t m = static_cast<int32_t>(d) % len;
+		if (m < 0) {
+			atomicOr(err, kErrHashBit);
+			h = 0;
+			return false;
+		}
+		h = static_cast<uint32_t>(m);
+	}
+	return true;
 }
+
+// One probe's result for a row: hit, and the PHT_2 payload.
+template <class Q, int q>
+__device__ __forceinline__ uint2 table_entry(const ProbeParams& P, const uint32_t* tables, uint32_t h) {
+	if constexpr (Q::pht2(q)) {
+		if constexpr (Q::in_smem(q)) { return reinterpret_cast<const uint2*>(tables + P.smem_off[q])[h]; }
+		return __ldg(reinterpret_cast<const uint2*>(P.ht[q]) + h);
+	} else {
+		if constexpr (Q::in_smem(q)) { return make_uint2((tables[P.smem_off[q] + (h >> 5)] >> (h & 31u)) & 1u, 0u); }
+		return make_uint2(static_cast<uint32_t>(__ldg(P.ht[q] + h)), 0u);
+	}
+}
+
+// Dense PHT_1 probes Q, Q+1, ... over the whole vector while some lane keeps
+// more than sparse_rows rows; f0 receives the first probe left to the row
+// phase.
+template <class Q, int q>
+__device__ __forceinline__ void dense_probes(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
+                                             uint32_t lane, uint32_t& mask, int& f0) {
+	if constexpr (q < Q::kNP && !Q::pht2(q)) {
+		if (max_rows(mask) <= P.sparse_rows) {
+			f0 = q;
+			return;
+		}
+		const uint32_t kb  = P.base[q] - static_cast<uint32_t>(P.kmin[q]);
+		const int32_t  len = P.len[q];
+		uint32_t       hit[4] = {0, 0, 0, 0};
+		dev::unpack_rows<Q::bw(q)>(V.template col<q>(), lane, [&](int r, uint32_t x) {
+			uint32_t   h;
+			const bool ok = hash_slot(x + kb, len, h, P.S.err);
+			const bool b  = ok & (table_entry<Q, q>(P, tables, h).x != 0u);
+			hit[r & 3] |= (b ? 1u : 0u) << r;
+		});
+		mask &= (hit[0] | hit[1]) | (hit[2] | hit[3]);
+		dense_probes<Q, q + 1>(P, tables, V, lane, mask, f0);
+	} else {
+		f0 = q;
+	}
+}
+
+// Probes q.. of a batch of selected rows; the table reads of all rows of the
+// batch are issued before any is consumed.
+template <class Q, int q>
+__device__ __forceinline__ void probe_rows(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
+                                           uint32_t lane, const uint32_t (&rows)[kRowBatch], bool (&pass)[kRowBatch],
+                                           int32_t (&va)[kRowBatch], int32_t (&vb)[kRowBatch], int rem) {
+	if constexpr (q < Q::kNP) {
+		const uint32_t kb  = P.base[q] - static_cast<uint32_t>(P.kmin[q]);
+		const int32_t  len = P.len[q];
+		uint2          e[kRowBatch];
+#pragma unroll
+		for (int j = 0; j < kRowBatch; ++j) {
+			e[j] = make_uint2(0u, 0u);
+			if (j < rem) {
+				const uint32_t d = row_field<Q::bw(q)>(V.template col<q>(), lane, rows[j]) + kb;
+				uint32_t       h;
+				if (pass[j] && hash_slot(d, len, h, P.S.err)) {
+					e[j] = table_entry<Q, q>(P, tables, h);
+				}
+			}
+		}
+#pragma unroll
+		for (int j = 0; j < kRowBatch; ++j) {
+			pass[j] = pass[j] & ((e[j].x | e[j].y) != 0u);
+			if constexpr (q == Q::kKeyA) { va[j] = static_cast<int32_t>(e[j].y); }
+			if constexpr (q == Q::kKeyB) { vb[j] = static_cast<int32_t>(e[j].y); }
+		}
+		probe_rows<Q, q + 1>(P, tables, V, lane, rows, pass, va, vb, rem);
+	}
+}
+
+// Group-by epilogue of one selected row (fls_q21.cu:67-77): group
+// (a*mul + (b - sub)) % n_groups in wrapping 32-bit arithmetic.
+__device__ __forceinline__ void emit(const ProbeParams& P, int32_t a, int32_t b, int32_t measure) {
+	const int32_t key = static_cast<int32_t>(static_cast<uint32_t>(a) * static_cast<uint32_t>(P.mul) +
+	                                         (static_cast<uint32_t>(b) - static_cast<uint32_t>(P.sub)));
+	const int32_t g   = static_cast<uint32_t>(key) < static_cast<uint32_t>(P.n_groups) ? key : key % P.n_groups;
+	if (g < 0) {
+		atomicOr(P.S.err, kErrHashBit);
+		return;
+	}
+	P.res[4 * g]     = b;
+	P.res[4 * g + 1] = a;
+	atomicAdd(reinterpret_cast<unsigned long long*>(P.res + 4 * g + 2),
+	          static_cast<unsigned long long>(static_cast<long long>(measure)));
+}
+
+template <class Q, int F0>
+__device__ __forceinline__ void row_phase(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
+                                          uint32_t lane, uint32_t mask) {
+	const int n_it = max_rows(mask);
+	for (int it0 = 0; it0 < n_it; it0 += kRowBatch) {
+		const int rem = n_it - it0; // warp-uniform
+		uint32_t  rows[kRowBatch];
+		bool      pass[kRowBatch];
+		int32_t   va[kRowBatch], vb[kRowBatch];
+#pragma unroll
+		for (int j = 0; j < kRowBatch; ++j) {
+			pass[j] = mask != 0u;
+			rows[j] = pass[j] ? static_cast<uint32_t>(__ffs(mask)) - 1u : 0u;
+			mask &= mask - 1u;
+			va[j] = vb[j] = 0;
+		}
+		probe_rows<Q, F0>(P, tables, V, lane, rows, pass, va, vb, rem);
+#pragma unroll
+		for (int j = 0; j < kRowBatch; ++j) {
+			if (j < rem && pass[j]) { emit(P, va[j], vb[j], row_value<Q, Q::kAgg>(P.base, V, lane, rows[j])); }
+		}
+	}
+}
+
+template <class Q, int F0>
+__device__ __forceinline__ void row_phase_from(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
+                                               uint32_t lane, uint32_t mask, int f0) {
+	if constexpr (F0 <= Q::kNP) {
+		if (f0 == F0) {
+			row_phase<Q, F0>(P, tables, V, lane, mask);
+			return;
+		}
+		row_phase_from<Q, F0 + 1>(P, tables, V, lane, mask, f0);
+	}
+}
+
+template <class Q>
+struct ProbeBody {
+	static constexpr bool kCtaSetup = true;
+	const ProbeParams&    P;
+	const uint32_t*       tables = nullptr;
+
+	// Shared-memory tables, staged once per CTA by all its warps: PHT_1 as a
+	// presence bitmap (the probe only tests slot != 0, crystal-opt/
+	// join.cuh:42-47), PHT_2 verbatim.
+	__device__ void cta_setup(uint32_t* cta) {
+		tables              = cta;
+		const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll 1
+		for (int q = 0; q < Q::kNP; ++q) {
+			if (!Q::in_smem(q)) { continue; }
+			uint32_t*      dst = cta + P.smem_off[q];
+			const int32_t* ht  = P.ht[q];
+			const uint32_t len = static_cast<uint32_t>(P.len[q]);
+			if (!Q::pht2(q)) {
+				const uint32_t n_words = (len + 31u) / 32u;
+				for (uint32_t w0 = warp * 8u; w0 < n_words; w0 += nw * 8u) {
+					int32_t x[8];
+#pragma unroll
+					for (uint32_t j = 0; j < 8; ++j) {
+						const uint32_t idx = 32u * (w0 + j) + lane;
+						x[j]               = (w0 + j < n_words && idx < len) ? __ldg(ht + idx) : 0;
+					}
+#pragma unroll
+					for (uint32_t j = 0; j < 8; ++j) {
+						const uint32_t b = __ballot_sync(0xffffffffu, x[j] != 0);
+						if (lane == 0 && w0 + j < n_words) { dst[w0 + j] = b; }
+					}
+				}
+			} else {
+				const uint32_t n = 2u * len;
+				for (uint32_t i0 = threadIdx.x; i0 < n; i0 += 4u * blockDim.x) {
+					int32_t x[4];
+#pragma unroll
+					for (uint32_t j = 0; j < 4; ++j) {
+						const uint32_t idx = i0 + j * blockDim.x;
+						x[j]               = idx < n ? __ldg(ht + idx) : 0;
+					}
+#pragma unroll
+					for (uint32_t j = 0; j < 4; ++j) {
+						const uint32_t idx = i0 + j * blockDim.x;
+						if (idx < n) { dst[idx] = static_cast<uint32_t>(x[j]); }
+					}
+				}
+			}
+		}
+	}
+
+	__device__ __forceinline__ void operator()(const Vec<Q>& V, uint64_t v, uint32_t lane) {
+		uint32_t mask = valid_rows(P.S, Q::kLayout, v, lane);
+		int      f0   = Q::kNP;
+		dense_probes<Q, 0>(P, tables, V, lane, mask, f0);
+		if (!__any_sync(0xffffffffu, mask)) { return; }
+		row_phase_from<Q, 0>(P, tables, V, lane, mask, f0);
+	}
+
+	__device__ __forceinline__ void finish(uint32_t) {}
+};
+
+// ---------------------------------------------------------------- pipeline
 
 // Words per vector and stage offset (in vectors' words) of column `lane`.
 template <class Q, int C>
@@ -225,19 +498,19 @@ __device__ __forceinline__ void lane_column(uint32_t lane, uint32_t& vw, uint32_
 	}
 }
 
-// Issue tile t into stage st: lane c copies column c (k vectors, contiguous).
+// Issue tile t into a stage: lane c copies column c (k vectors, contiguous).
 template <class Q>
-__device__ __forceinline__ void issue(const FixedParams& P, uint32_t* stage, uint64_t* bar, uint64_t t, uint32_t lane,
+__device__ __forceinline__ void issue(const StageParams& S, uint32_t* stage, uint64_t* bar, uint64_t t, uint32_t lane,
                                       uint64_t pol) {
-	const uint64_t v0 = t * P.tile;
-	const uint64_t kk = P.n_vec - v0 < P.tile ? P.n_vec - v0 : P.tile;
+	const uint64_t v0 = t * S.tile;
+	const uint64_t kk = S.n_vec - v0 < S.tile ? S.n_vec - v0 : S.tile;
 	if (lane < static_cast<uint32_t>(Q::NC)) {
 		uint32_t vw = 0, pre = 0;
 		lane_column<Q, 0>(lane, vw, pre);
 		const uint32_t bytes = static_cast<uint32_t>(kk) * vw * 4u;
 		if (bytes) {
 			dev::mbar_expect_tx(bar, bytes);
-			dev::bulk_g2s(stage + P.tile * pre, P.data[lane] + v0 * vw, bytes, bar, pol);
+			dev::bulk_g2s(stage + S.tile * pre, S.data[lane] + v0 * vw, bytes, bar, pol);
 		}
 	}
 	__syncwarp();
@@ -245,58 +518,69 @@ __device__ __forceinline__ void issue(const FixedParams& P, uint32_t* stage, uin
 	__syncwarp();
 }
 
-template <class Q>
-__device__ __forceinline__ void run(const FixedParams& P) {
+// Persistent loop: each warp stages its tiles (tile t = first + j*total) into
+// its own ring of S stages and hands every vector to body(V, v, lane).
+template <class Q, class Body>
+__device__ __forceinline__ void run(const StageParams& S, Body& body) {
 	extern __shared__ __align__(128) uint32_t smem[];
 	const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-	uint32_t*      base = smem + warp * P.warp_smem_words;
-	uint64_t*      bars = reinterpret_cast<uint64_t*>(base + P.bar_off);
+	uint32_t*      base = smem + warp * S.warp_smem_words;
+	uint64_t*      bars = reinterpret_cast<uint64_t*>(base + S.bar_off);
 	if (lane == 0) {
-		for (uint32_t s = 0; s < P.stages; ++s) { dev::mbar_init(bars + s, 1); }
+		for (uint32_t s = 0; s < S.stages; ++s) { dev::mbar_init(bars + s, 1); }
 		dev::fence_mbar_init();
 	}
 	__syncwarp();
 	const uint64_t pol   = dev::l2_evict_first_policy();
-	const uint64_t total = static_cast<uint64_t>(gridDim.x) * P.warps;
-	const uint64_t first = static_cast<uint64_t>(blockIdx.x) * P.warps + warp;
-	for (uint32_t s = 0; s < P.stages; ++s) {
+	const uint64_t total = static_cast<uint64_t>(gridDim.x) * S.warps;
+	const uint64_t first = static_cast<uint64_t>(blockIdx.x) * S.warps + warp;
+	for (uint32_t s = 0; s < S.stages; ++s) {
 		const uint64_t t = first + s * total;
-		if (t >= P.n_tiles) { break; }
-		issue<Q>(P, base + s * P.stage_words, bars + s, t, lane, pol);
+		if (t >= S.n_tiles) { break; }
+		issue<Q>(S, base + s * S.stage_words, bars + s, t, lane, pol);
 	}
-	uint64_t  next  = first + static_cast<uint64_t>(P.stages) * total;
-	uint32_t  st = 0, phase = 0;
-	long long acc = 0;
-	for (uint64_t t = first; t < P.n_tiles; t += total) {
+	if constexpr (Body::kCtaSetup) {
+		body.cta_setup(smem + S.cta_off); // overlaps the first stages' copies
+		__syncthreads();
+	}
+	uint64_t next = first + static_cast<uint64_t>(S.stages) * total;
+	uint32_t st = 0, phase = 0;
+	for (uint64_t t = first; t < S.n_tiles; t += total) {
 		if (!dev::mbar_wait_bounded(bars + st, phase, kWaitPolls)) {
-			atomicOr(P.err, kErrTimeoutBit);
-			for (uint32_t s = 0; s < P.stages; ++s) {
+			atomicOr(S.err, kErrTimeoutBit);
+			for (uint32_t s = 0; s < S.stages; ++s) {
 				dev::mbar_wait_bounded(bars + s, phase, 1u << 10);
 				dev::mbar_wait_bounded(bars + s, phase ^ 1u, 1u << 10);
 			}
 			return;
 		}
-		const uint64_t v0 = t * P.tile;
-		const uint32_t kk = static_cast<uint32_t>(P.n_vec - v0 < P.tile ? P.n_vec - v0 : P.tile);
-		for (uint32_t i = 0; i < kk; ++i) {
-			const Vec<Q> V {base + st * P.stage_words, P.tile, i};
-			acc += process<Q>(P, V, v0 + i, lane);
-		}
+		const uint64_t v0 = t * S.tile;
+		const uint32_t kk = static_cast<uint32_t>(S.n_vec - v0 < S.tile ? S.n_vec - v0 : S.tile);
+		for (uint32_t i = 0; i < kk; ++i) { body(Vec<Q> {base + st * S.stage_words, S.tile, i}, v0 + i, lane); }
 		__syncwarp();
-		if (next < P.n_tiles) {
+		if (next < S.n_tiles) {
 			dev::fence_proxy_async_smem();
-			issue<Q>(P, base + st * P.stage_words, bars + st, next, lane, pol);
+			issue<Q>(S, base + st * S.stage_words, bars + st, next, lane, pol);
 			next += total;
 		}
-		if (++st == P.stages) {
-			st = 0;
+		if (++st == S.stages) {
+			st    = 0;
 			phase ^= 1u;
 		}
 	}
-	unsigned long long s = static_cast<unsigned long long>(acc);
-#pragma unroll
-	for (int o = 16; o > 0; o >>= 1) { s += __shfl_xor_sync(0xffffffffu, s, o); }
-	if (lane == 0 && s) { atomicAdd(P.result, s); }
+	body.finish(lane);
+}
+
+template <class Q>
+__device__ __forceinline__ void filter_kernel(const FilterParams& P) {
+	FilterBody<Q> body {P};
+	run<Q>(P.S, body);
+}
+
+template <class Q>
+__device__ __forceinline__ void probe_kernel(const ProbeParams& P) {
+	ProbeBody<Q> body {P};
+	run<Q>(P.S, body);
 }
 
 } // namespace fixed

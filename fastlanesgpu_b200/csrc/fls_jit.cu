@@ -11,8 +11,10 @@
 #include <dlfcn.h>
 #include <nvrtc.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
+#include <cstring>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -82,16 +84,21 @@ const char* const kStdint =
 const char* const kStddef = "#pragma once\ntypedef decltype(sizeof(0)) size_t;\n";
 const char* const kEmpty  = "#pragma once\n";
 
-std::string shape_source(const std::string& args) {
-	return "#include \"fls_fixed.cuh\"\n"
-	       "extern \"C\" __global__ void __launch_bounds__(512, 1)\n"
-	       "fls_fixed_kernel(const __grid_constant__ fls::fixed::FixedParams P) {\n"
-	       "\tfls::fixed::run<fls::fixed::Query<" +
+// Kernel keys are "<op>:<warps>:<template arguments>"; op F = filter-aggregate,
+// P = probe + group-by.  The warp count fixes __launch_bounds__ so that the
+// compiler may use every register the launch leaves.
+std::string shape_source(const std::string& key) {
+	const size_t a = key.find(':'), b = key.find(':', a + 1);
+	const std::string op = key.substr(0, a), warps = key.substr(a + 1, b - a - 1), args = key.substr(b + 1);
+	const bool filter = op == "F";
+	return std::string("#include \"fls_fixed.cuh\"\n") + "extern \"C\" __global__ void __launch_bounds__(32 * " + warps +
+	       ", 1)\nfls_fixed_kernel(const __grid_constant__ fls::fixed::" + (filter ? "FilterParams" : "ProbeParams") +
+	       " P) {\n\tfls::fixed::" + (filter ? "filter_kernel<fls::fixed::FilterQuery<" : "probe_kernel<fls::fixed::ProbeQuery<") +
 	       args + ">>(P);\n}\n";
 }
 
 // NVRTC compile of one shape into e.cubin; false (log kept) on failure.
-bool compile_shape(const std::string& args, Entry& e) {
+bool compile_shape(const std::string& key, Entry& e) {
 	const Nvrtc& n = nvrtc();
 	if (!n.ok) {
 		g_last_log = "NVRTC library not found";
@@ -108,7 +115,7 @@ bool compile_shape(const std::string& args, Entry& e) {
 	texts.push_back(kStddef);
 	names.push_back("cuda_runtime.h");
 	texts.push_back(kEmpty);
-	const std::string src = shape_source(args);
+	const std::string src = shape_source(key);
 	nvrtcProgram      prog;
 	if (n.create(&prog, src.c_str(), "fls_fixed_query.cu", static_cast<int>(names.size()), texts.data(),
 	             names.data()) != NVRTC_SUCCESS) {
@@ -125,7 +132,7 @@ bool compile_shape(const std::string& args, Entry& e) {
 	std::string log(ls, '\0');
 	if (ls) { n.log(prog, &log[0]); }
 	if (rc != NVRTC_SUCCESS) {
-		g_last_log = "Query<" + args + ">: " + log;
+		g_last_log = key + ": " + log;
 		n.destroy(&prog);
 		return false;
 	}
@@ -162,6 +169,119 @@ Entry& compiled_entry(const std::string& key) {
 	return it->second;
 }
 
+// Stage plan of a specialised kernel: tiles of k vectors, S stages per warp,
+// as many warps (up to the launch configuration's) as shared memory holds
+// next to cta_words of CTA-wide tables.
+fls_status plan_fixed(const DeviceInfo& di, const fls_column* sc, uint32_t n, uint32_t cta_words,
+                      fixed::StageParams& S, uint32_t& grid, size_t& smem) {
+	fls_status st       = FLS_OK;
+	uint32_t   W0 = 0, S0 = 0, ctas = 0, tile_bytes = 0;
+	fls_get_launch_config(&W0, &S0, &ctas, &tile_bytes);
+	std::memset(&S, 0, sizeof(S));
+	uint32_t sum_vec = 0;
+	for (uint32_t c = 0; c < n; ++c) {
+		DevCol d;
+		if ((st = make_devcol(sc[c], d)) != FLS_OK) { return st; }
+		if (sc[c].n_values != sc[0].n_values) { return set_error(FLS_ERR_INVALID_ARG, "columns differ in length"); }
+		S.data[c] = sc[c].data;
+		sum_vec += 32u * sc[c].bw;
+	}
+	S.n_values = sc[0].n_values;
+	S.n_vec    = (S.n_values + 1023u) / 1024u;
+	const uint64_t total_warps = static_cast<uint64_t>(di.sms) * ctas * W0;
+	uint32_t       k = sum_vec ? std::max<uint32_t>(1u, tile_bytes / (4u * sum_vec)) : kMaxTile;
+	k                = std::min<uint32_t>(k, kMaxTile);
+	while (k > 1 && (S.n_vec + k - 1) / k < 4 * total_warps) { k /= 2; }
+	const uint32_t avail = static_cast<uint32_t>(di.max_smem) / 4u;
+	uint32_t       stages = S0, W = 0, per = 0;
+	for (;;) {
+		per = (stages * k * sum_vec + fixed::kSlack + 2u * stages + 3u) & ~3u;
+		W   = avail > cta_words ? std::min<uint32_t>(W0, (avail - cta_words) / per) : 0u;
+		if (W >= std::min<uint32_t>(W0, 8u) || (k == 1 && stages == 2)) { break; }
+		if (k > 1) {
+			k /= 2;
+		} else {
+			--stages;
+		}
+	}
+	if (W == 0) { return set_error(FLS_ERR_CAPACITY, "vectors and tables too large for shared memory"); }
+	S.tile            = k;
+	S.n_tiles         = (S.n_vec + k - 1) / k;
+	S.stages          = stages;
+	S.warps           = W;
+	S.stage_words     = k * sum_vec;
+	S.bar_off         = stages * S.stage_words + fixed::kSlack;
+	S.warp_smem_words = per;
+	S.cta_off         = W * per;
+	smem              = 4ull * (static_cast<size_t>(S.cta_off) + cta_words);
+	grid = static_cast<uint32_t>(std::min<uint64_t>((S.n_tiles + W - 1) / W, static_cast<uint64_t>(di.sms) * ctas));
+	return FLS_OK;
+}
+
+// Loads (first use) and launches the kernel of `key`; used = false if the
+// shape could not be compiled or loaded.
+fls_status launch_fixed(const std::string& key, void* params, uint32_t grid, uint32_t threads, size_t smem,
+                        cudaStream_t stream, bool& used) {
+	used    = false;
+	int dev = 0;
+	fls_status s = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+	if (s != FLS_OK) { return s; }
+	cudaKernel_t kernel {};
+	{
+		std::lock_guard<std::mutex> lk(g_mu);
+		Entry&                      e = compiled_entry(key);
+		if (e.state == 1) {
+			e.state = load_shape(e) ? 2 : -1;
+			if (e.state < 0) { g_failures.fetch_add(1); }
+		}
+		if (e.state != 2) { return FLS_OK; }
+		if (e.smem_set.size() <= static_cast<size_t>(dev)) { e.smem_set.resize(dev + 1, 0); }
+		if (smem > 48u * 1024u && e.smem_set[dev] < smem) {
+			s = cuda_check(cudaKernelSetAttributeForDevice(e.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			                                               static_cast<int>(smem), dev),
+			               "cudaKernelSetAttributeForDevice");
+			if (s != FLS_OK) { return s; }
+			e.smem_set[dev] = smem;
+		}
+		kernel = e.kernel;
+	}
+	void* argv[] = {params};
+	s = cuda_check(cudaLaunchKernel(reinterpret_cast<const void*>(kernel), dim3(grid), dim3(threads), argv, smem, stream),
+	               "cudaLaunchKernel (specialised kernel)");
+	if (s != FLS_OK) { return s; }
+	count_launch();
+	g_launches.fetch_add(1);
+	used = true;
+	return FLS_OK;
+}
+
+std::string key_args(const fls_column* sc, uint32_t n, const char* head) {
+	std::string k = head;
+	for (uint32_t i = 0; i < n; ++i) { k += ", " + std::to_string(static_cast<unsigned>(sc[i].bw)); }
+	return k;
+}
+
+std::string make_key(char op, uint32_t warps, const std::string& args) {
+	return std::string(1, op) + ":" + std::to_string(warps) + ":" + args;
+}
+
+// The device a plan is made for: the current one, or (compiling ahead without
+// a device) an sm_100 B200: 148 SMs, 227 KB of shared memory per CTA.
+DeviceInfo plan_device(bool& have_device) {
+	DeviceInfo di;
+	have_device = device_info(di) == FLS_OK;
+	if (!have_device) {
+		di.sms      = 148;
+		di.max_smem = 232448;
+		di.major    = 10;
+	}
+	return di;
+}
+
+bool uniform_for(const fls_column& c, uint32_t layout) {
+	return c.meta == nullptr && c.scheme == FLS_SCHEME_FOR && c.bw <= 32 && c.layout == layout;
+}
+
 } // namespace
 
 bool jit_shape(const fls_column* cols, const fls_filter* filters, uint32_t n_filters, int32_t agg_a, int32_t agg_b,
@@ -184,25 +304,29 @@ bool jit_shape(const fls_column* cols, const fls_filter* filters, uint32_t n_fil
 	sh.agg_a = slot_of(agg_a);
 	sh.agg_b = slot_of(agg_b);
 	if (sh.n_staged == 0) { return false; }
+	fls_column sc[FLS_MAX_QUERY_COLS];
 	for (uint32_t i = 0; i < sh.n_staged; ++i) {
-		const fls_column& c = cols[sh.staged[i]];
-		if (c.meta != nullptr || c.scheme != FLS_SCHEME_FOR || c.bw > 32 || c.layout != cols[sh.staged[0]].layout) {
-			return false;
-		}
+		sc[i] = cols[sh.staged[i]];
+		if (!uniform_for(sc[i], sc[0].layout)) { return false; }
 	}
-	char key[160];
-	int  len = std::snprintf(key, sizeof(key), "%u, %u, %d, %d", static_cast<unsigned>(cols[sh.staged[0]].layout),
-	                         n_filters, sh.agg_a, sh.agg_b);
-	for (uint32_t i = 0; i < sh.n_staged; ++i) {
-		len += std::snprintf(key + len, sizeof(key) - len, ", %u", static_cast<unsigned>(cols[sh.staged[i]].bw));
-	}
-	sh.key = key;
+	char head[96];
+	std::snprintf(head, sizeof(head), "%u, %u, %d, %d", static_cast<unsigned>(sc[0].layout), n_filters, sh.agg_a,
+	              sh.agg_b);
+	sh.key = key_args(sc, sh.n_staged, head);
 	return true;
 }
 
-bool jit_compile(const JitShape& sh) {
+bool jit_compile(const fls_column* cols, const JitShape& sh) {
+	fls_column sc[FLS_MAX_QUERY_COLS];
+	for (uint32_t i = 0; i < sh.n_staged; ++i) { sc[i] = cols[sh.staged[i]]; }
+	bool                have;
+	const DeviceInfo    di = plan_device(have);
+	fixed::StageParams  S;
+	uint32_t            grid;
+	size_t              smem;
+	if (plan_fixed(di, sc, sh.n_staged, 0u, S, grid, smem) != FLS_OK) { return false; }
 	std::lock_guard<std::mutex> lk(g_mu);
-	return compiled_entry(sh.key).state > 0;
+	return compiled_entry(make_key('F', S.warps, sh.key)).state > 0;
 }
 
 fls_status jit_filter_agg(const fls_column* cols, const fls_filter* filters, uint32_t n_filters, int32_t agg_a,
@@ -212,65 +336,108 @@ fls_status jit_filter_agg(const fls_column* cols, const fls_filter* filters, uin
 	if (!jit_shape(cols, filters, n_filters, agg_a, agg_b, sh)) { return FLS_OK; }
 	fls_column sc[FLS_MAX_QUERY_COLS];
 	for (uint32_t i = 0; i < sh.n_staged; ++i) { sc[i] = cols[sh.staged[i]]; }
-	StageCfg   cfg;
-	uint32_t   grid, threads;
-	size_t     smem;
-	fls_status s = plan_stages(sc, sh.n_staged, 0u, 0u, cfg, grid, threads, smem);
+	fixed::FilterParams P {};
+	uint32_t            grid;
+	size_t              smem;
+	DeviceInfo          di;
+	fls_status          s = device_info(di);
 	if (s != FLS_OK) { return s; }
-	int dev = 0;
-	if ((s = cuda_check(cudaGetDevice(&dev), "cudaGetDevice")) != FLS_OK) { return s; }
-
-	fixed::FixedParams P {};
-	for (uint32_t i = 0; i < sh.n_staged; ++i) {
-		P.data[i] = sc[i].data;
-		P.base[i] = static_cast<uint32_t>(sc[i].base);
-	}
+	if ((s = plan_fixed(di, sc, sh.n_staged, 0u, P.S, grid, smem)) != FLS_OK) { return s; }
+	P.S.err = device_error_word();
+	for (uint32_t i = 0; i < sh.n_staged; ++i) { P.base[i] = static_cast<uint32_t>(sc[i].base); }
 	for (uint32_t f = 0; f < n_filters; ++f) {
 		P.lo[f]    = static_cast<uint32_t>(filters[f].lo);
 		P.range[f] = static_cast<uint32_t>(filters[f].hi) - static_cast<uint32_t>(filters[f].lo);
 	}
-	P.n_values        = cfg.n_values;
-	P.n_vec           = cfg.n_vec;
-	P.n_tiles         = cfg.n_tiles;
-	P.tile            = cfg.tile;
-	P.stages          = cfg.stages;
-	P.warps           = cfg.warps;
-	P.stage_words     = cfg.stage_words;
-	P.bar_off         = cfg.stages * cfg.stage_words + fixed::kSlack;
-	P.warp_smem_words = (P.bar_off + 2u * cfg.stages + 3u) & ~3u;
-	P.sparse_rows     = sparse_rows;
-	P.result          = reinterpret_cast<unsigned long long*>(d_result);
-	P.err             = cfg.err;
-	const size_t fsmem = 4ull * P.warp_smem_words * cfg.warps;
+	P.sparse_rows = sparse_rows;
+	P.result      = reinterpret_cast<unsigned long long*>(d_result);
+	return launch_fixed(make_key('F', P.S.warps, sh.key), &P, grid, 32u * P.S.warps, smem, stream, used);
+}
 
-	cudaKernel_t kernel {};
-	{
-		std::lock_guard<std::mutex> lk(g_mu);
-		Entry&                      e = compiled_entry(sh.key);
-		if (e.state == 1) {
-			e.state = load_shape(e) ? 2 : -1;
-			if (e.state < 0) { g_failures.fetch_add(1); }
+bool jit_probe_shape(const fls_join_agg_desc* d, JitProbeShape& sh) {
+	sh.n_staged = 0;
+	for (uint32_t q = 0; q < d->n_probes; ++q) {
+		for (uint32_t g = 0; g < q; ++g) {
+			if (d->probes[g].col == d->probes[q].col) { return false; } // one column probed twice
 		}
-		if (e.state != 2) { return FLS_OK; }
-		if (e.smem_set.size() <= static_cast<size_t>(dev)) { e.smem_set.resize(dev + 1, 0); }
-		if (fsmem > 48u * 1024u && e.smem_set[dev] < fsmem) {
-			s = cuda_check(cudaKernelSetAttributeForDevice(e.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			                                               static_cast<int>(fsmem), dev),
-			               "cudaKernelSetAttributeForDevice");
-			if (s != FLS_OK) { return s; }
-			e.smem_set[dev] = fsmem;
-		}
-		kernel = e.kernel;
+		sh.staged[sh.n_staged++] = d->probes[q].col;
 	}
-	void* argv[] = {&P};
-	s = cuda_check(cudaLaunchKernel(reinterpret_cast<const void*>(kernel), dim3(grid), dim3(threads), argv, fsmem,
-	                                stream),
-	               "cudaLaunchKernel (specialised filter-aggregate)");
+	sh.agg = -1;
+	for (uint32_t i = 0; i < sh.n_staged; ++i) {
+		if (sh.staged[i] == d->agg_col) { sh.agg = static_cast<int>(i); }
+	}
+	if (sh.agg < 0) {
+		sh.agg                   = static_cast<int>(sh.n_staged);
+		sh.staged[sh.n_staged++] = d->agg_col;
+	}
+	for (uint32_t i = 0; i < sh.n_staged; ++i) {
+		if (!uniform_for(d->cols[sh.staged[i]], d->cols[sh.staged[0]].layout)) { return false; }
+	}
+	// Tables go to shared memory in probe order while they fit the budget.
+	uint32_t kinds = 0, in_smem = 0;
+	sh.cta_words   = 0;
+	for (uint32_t q = 0; q < d->n_probes; ++q) {
+		const fls_probe& p     = d->probes[q];
+		const uint64_t   words = p.kind == 1 ? (static_cast<uint64_t>(p.ht_len) + 31u) / 32u
+		                                     : 2ull * static_cast<uint64_t>(p.ht_len);
+		if (p.kind == 2) { kinds |= 1u << q; }
+		sh.smem_off[q] = 0;
+		if (sh.cta_words + words <= kJitTableWords) {
+			in_smem |= 1u << q;
+			sh.smem_off[q] = sh.cta_words;
+			sh.cta_words += static_cast<uint32_t>((words + 3u) & ~3ull);
+		}
+	}
+	fls_column sc[FLS_MAX_QUERY_COLS];
+	for (uint32_t i = 0; i < sh.n_staged; ++i) { sc[i] = d->cols[sh.staged[i]]; }
+	char head[128];
+	std::snprintf(head, sizeof(head), "%u, %u, %d, %d, %d, %u, %u", static_cast<unsigned>(sc[0].layout), d->n_probes,
+	              sh.agg, d->key_a, d->key_b, kinds, in_smem);
+	sh.key = key_args(sc, sh.n_staged, head);
+	return true;
+}
+
+bool jit_compile(const fls_join_agg_desc* d, const JitProbeShape& sh) {
+	fls_column sc[FLS_MAX_QUERY_COLS];
+	for (uint32_t i = 0; i < sh.n_staged; ++i) { sc[i] = d->cols[sh.staged[i]]; }
+	bool               have;
+	const DeviceInfo   di = plan_device(have);
+	fixed::StageParams S;
+	uint32_t           grid;
+	size_t             smem;
+	if (plan_fixed(di, sc, sh.n_staged, sh.cta_words, S, grid, smem) != FLS_OK) { return false; }
+	std::lock_guard<std::mutex> lk(g_mu);
+	return compiled_entry(make_key('P', S.warps, sh.key)).state > 0;
+}
+
+fls_status jit_probe_groupby(const fls_join_agg_desc* d, int32_t* d_res, int32_t sparse_rows, cudaStream_t stream,
+                             bool& used) {
+	used = false;
+	JitProbeShape sh;
+	if (!jit_probe_shape(d, sh)) { return FLS_OK; }
+	fls_column sc[FLS_MAX_QUERY_COLS];
+	for (uint32_t i = 0; i < sh.n_staged; ++i) { sc[i] = d->cols[sh.staged[i]]; }
+	fixed::ProbeParams P {};
+	uint32_t           grid;
+	size_t             smem;
+	DeviceInfo         di;
+	fls_status         s = device_info(di);
 	if (s != FLS_OK) { return s; }
-	count_launch();
-	g_launches.fetch_add(1);
-	used = true;
-	return FLS_OK;
+	if ((s = plan_fixed(di, sc, sh.n_staged, sh.cta_words, P.S, grid, smem)) != FLS_OK) { return s; }
+	P.S.err = device_error_word();
+	for (uint32_t i = 0; i < sh.n_staged; ++i) { P.base[i] = static_cast<uint32_t>(sc[i].base); }
+	for (uint32_t q = 0; q < d->n_probes; ++q) {
+		P.ht[q]       = d->probes[q].ht;
+		P.len[q]      = d->probes[q].ht_len;
+		P.kmin[q]     = d->probes[q].keys_min;
+		P.smem_off[q] = sh.smem_off[q];
+	}
+	P.mul         = d->group_mul;
+	P.sub         = d->group_sub;
+	P.n_groups    = d->n_groups;
+	P.sparse_rows = sparse_rows;
+	P.res         = d_res;
+	return launch_fixed(make_key('P', P.S.warps, sh.key), &P, grid, 32u * P.S.warps, smem, stream, used);
 }
 
 } // namespace fls

@@ -309,13 +309,32 @@ struct JitShape {
 // two ranges on one column, no column read).
 bool jit_shape(const fls_column* cols, const fls_filter* filters, uint32_t n_filters, int32_t agg_a, int32_t agg_b,
                JitShape& sh);
-// NVRTC compile of a shape (cached; no device needed).  False on failure.
-bool jit_compile(const JitShape& sh);
+// NVRTC compile of a shape as the current device (or, with none, a B200)
+// would launch it (cached; no device needed).  False on failure.
+bool jit_compile(const fls_column* cols, const JitShape& sh);
 // Filter-aggregate through the specialised kernel (filters in evaluation
 // order).  used = false, with FLS_OK, when the shape does not qualify or its
 // specialisation is unavailable: run the general kernel then.
 fls_status jit_filter_agg(const fls_column* cols, const fls_filter* filters, uint32_t n_filters, int32_t agg_a,
                           int32_t agg_b, int64_t* d_result, int32_t sparse_rows, cudaStream_t stream, bool& used);
+
+// Probe + group-by shapes: staged columns (probe keys in probe order, then the
+// measure column if no probe reads it), which tables live in shared memory.
+constexpr uint32_t kJitTableWords = 64u * 1024u / 4u; // shared-memory budget for hash tables
+struct JitProbeShape {
+	uint32_t    staged[FLS_MAX_QUERY_COLS];
+	uint32_t    n_staged = 0;
+	int         agg      = -1;
+	uint32_t    smem_off[FLS_MAX_PROBES];
+	uint32_t    cta_words = 0;
+	std::string key;
+};
+// False when a staged column is not uniform FOR or one column is probed twice
+// (the descriptor must already be validated).
+bool       jit_probe_shape(const fls_join_agg_desc* desc, JitProbeShape& sh);
+bool       jit_compile(const fls_join_agg_desc* desc, const JitProbeShape& sh);
+fls_status jit_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res, int32_t sparse_rows, cudaStream_t stream,
+                             bool& used);
 
 // Lays out shared memory for a set of columns; extra_words per warp and
 // cta_words per CTA are operator-specific scratch.

@@ -517,6 +517,30 @@ fls_status order_filters(const fls_filter_agg_desc* desc, fls_filter (&order)[FL
 	return FLS_OK;
 }
 
+// Validates a probe + group-by descriptor.
+fls_status check_join_desc(const fls_join_agg_desc* desc) {
+	if (!desc || !desc->cols) { return set_error(FLS_ERR_INVALID_ARG, "fls_query_probe_groupby: null pointer"); }
+	if (desc->n_probes == 0 || desc->n_probes > FLS_MAX_PROBES) { return set_error(FLS_ERR_INVALID_ARG, "1..4 probes"); }
+	if (desc->agg_col >= desc->n_cols || desc->n_groups <= 0) {
+		return set_error(FLS_ERR_INVALID_ARG, "bad aggregate column or group count");
+	}
+	const int32_t np = static_cast<int32_t>(desc->n_probes);
+	if (desc->key_a < 0 || desc->key_b < 0 || desc->key_a >= np || desc->key_b >= np ||
+	    desc->probes[desc->key_a].kind != 2 || desc->probes[desc->key_b].kind != 2) {
+		return set_error(FLS_ERR_INVALID_ARG, "group keys must name PHT_2 probes");
+	}
+	for (uint32_t p = 0; p < desc->n_probes; ++p) {
+		const fls_probe& pr = desc->probes[p];
+		if (pr.col >= desc->n_cols || !pr.ht || pr.ht_len <= 0 || (pr.kind != 1 && pr.kind != 2)) {
+			return set_error(FLS_ERR_INVALID_ARG, "bad probe");
+		}
+		if (pr.kind == 2 && (reinterpret_cast<uintptr_t>(pr.ht) & 7u)) {
+			return set_error(FLS_ERR_ALIGNMENT, "PHT_2 tables must be 8-byte aligned");
+		}
+	}
+	return FLS_OK;
+}
+
 } // namespace
 
 extern "C" {
@@ -564,7 +588,20 @@ fls_status fls_jit_precompile(const fls_filter_agg_desc* desc) {
 	if (!jit_shape(desc->cols, order, desc->n_filters, desc->agg_a, desc->agg_b, sh)) {
 		return set_error(FLS_ERR_UNSUPPORTED, "query does not qualify for specialisation (uniform FOR columns only)");
 	}
-	if (!jit_compile(sh)) {
+	if (!jit_compile(desc->cols, sh)) {
+		return set_error(FLS_ERR_UNSUPPORTED, std::string("specialisation failed: ") + fls_jit_last_log());
+	}
+	return FLS_OK;
+}
+
+fls_status fls_jit_precompile_probe(const fls_join_agg_desc* desc) {
+	fls_status s = check_join_desc(desc);
+	if (s != FLS_OK) { return s; }
+	JitProbeShape sh;
+	if (!jit_probe_shape(desc, sh)) {
+		return set_error(FLS_ERR_UNSUPPORTED, "query does not qualify for specialisation (uniform FOR columns only)");
+	}
+	if (!jit_compile(desc, sh)) {
 		return set_error(FLS_ERR_UNSUPPORTED, std::string("specialisation failed: ") + fls_jit_last_log());
 	}
 	return FLS_OK;
@@ -587,19 +624,10 @@ fls_status fls_pht_build(const int32_t* d_filter, int32_t filter_eq, const int32
 }
 
 fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res, fls_stream_t stream) {
-	if (!desc || !d_res || !desc->cols) {
-		return set_error(FLS_ERR_INVALID_ARG, "fls_query_probe_groupby: null pointer");
-	}
-	if (desc->n_probes == 0 || desc->n_probes > FLS_MAX_PROBES) { return set_error(FLS_ERR_INVALID_ARG, "1..4 probes"); }
-	if (desc->agg_col >= desc->n_cols || desc->n_groups <= 0) {
-		return set_error(FLS_ERR_INVALID_ARG, "bad aggregate column or group count");
-	}
+	if (!d_res) { return set_error(FLS_ERR_INVALID_ARG, "fls_query_probe_groupby: null pointer"); }
 	if (reinterpret_cast<uintptr_t>(d_res) & 7u) { return set_error(FLS_ERR_ALIGNMENT, "result must be 8-byte aligned"); }
-	const int32_t np = static_cast<int32_t>(desc->n_probes);
-	if (desc->key_a < 0 || desc->key_b < 0 || desc->key_a >= np || desc->key_b >= np ||
-	    desc->probes[desc->key_a].kind != 2 || desc->probes[desc->key_b].kind != 2) {
-		return set_error(FLS_ERR_INVALID_ARG, "group keys must name PHT_2 probes");
-	}
+	fls_status s = check_join_desc(desc);
+	if (s != FLS_OK) { return s; }
 	ProbeParams op {};
 	op.n_probes = desc->n_probes;
 	// Small tables go to shared memory, first come first served.
@@ -607,12 +635,6 @@ fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res
 	const uint32_t budget    = 48u * 1024u / 4u;
 	for (uint32_t p = 0; p < desc->n_probes; ++p) {
 		const fls_probe& pr = desc->probes[p];
-		if (pr.col >= desc->n_cols || !pr.ht || pr.ht_len <= 0 || (pr.kind != 1 && pr.kind != 2)) {
-			return set_error(FLS_ERR_INVALID_ARG, "bad probe");
-		}
-		if (pr.kind == 2 && (reinterpret_cast<uintptr_t>(pr.ht) & 7u)) {
-			return set_error(FLS_ERR_ALIGNMENT, "PHT_2 tables must be 8-byte aligned");
-		}
 		op.p_col[p]          = pr.col;
 		op.p_ht[p]           = pr.ht;
 		op.p_len[p]          = pr.ht_len;
@@ -643,15 +665,20 @@ fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res
 		const uint32_t    mask = col.meta ? col.scheme_mask : (1u << col.scheme);
 		rnd                   = rnd && !(mask & seq_schemes);
 	}
-	StageCfg   cfg;
-	uint32_t   grid, threads;
-	size_t     smem;
-	fls_status s = plan_stages(desc->cols, desc->n_cols, 0u, cta_words, cfg, grid, threads, smem);
+	StageCfg cfg;
+	uint32_t grid, threads;
+	size_t   smem;
+	s = plan_stages(desc->cols, desc->n_cols, 0u, cta_words, cfg, grid, threads, smem);
 	if (s != FLS_OK) { return s; }
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
 	s = cuda_check(cudaMemsetAsync(d_res, 0, sizeof(int32_t) * 4u * static_cast<size_t>(desc->n_groups), st),
 	               "cudaMemsetAsync");
 	if (s != FLS_OK) { return s; }
+	if (tuning_jit()) {
+		bool used = false;
+		s         = jit_probe_groupby(desc, d_res, op.sparse_rows, st, used);
+		if (s != FLS_OK || used) { return s; }
+	}
 	if (rnd) {
 		ProbeGroupByRowOp rop;
 		static_cast<ProbeParams&>(rop) = op;

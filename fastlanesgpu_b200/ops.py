@@ -182,22 +182,38 @@ def probe_groupby(cols, probes, agg_col: int, key_a: int, key_b: int, group_mul:
     reference's result array int32[4*n_groups]: [key_b value, key_a value,
     int64 sum (2 words)] per group."""
     import torch
-    if len(probes) > MAX_PROBES:
-        raise ValueError("at most 4 probes")
-    arr = columns_array(cols)
-    d = JoinAggDesc()
-    d.cols = arr
-    d.n_cols = len(cols)
-    for i, (c, ht, ln, kmin, kind) in enumerate(probes):
-        d.probes[i].col, d.probes[i].ht, d.probes[i].ht_len = c, ht.data_ptr(), ln
-        d.probes[i].keys_min, d.probes[i].kind = kmin, kind
-    d.n_probes = len(probes)
-    d.agg_col, d.key_a, d.key_b = agg_col, key_a, key_b
-    d.group_mul, d.group_sub, d.n_groups = group_mul, group_sub, n_groups
+    d, _keep = _join_desc(columns_array(cols), len(cols), probes, agg_col, key_a, key_b, group_mul, group_sub,
+                          n_groups)
     if out is None:
         out = torch.empty(4 * n_groups, dtype=torch.int32, device=cols[0].data.device)
     check(lib().fls_query_probe_groupby(ctypes.byref(d), out.data_ptr(), _stream()), "fls_query_probe_groupby")
     return out
+
+
+def _join_desc(arr, n_cols: int, probes, agg_col, key_a, key_b, group_mul, group_sub, n_groups):
+    if len(probes) > MAX_PROBES:
+        raise ValueError("at most 4 probes")
+    d = JoinAggDesc()
+    d.cols = arr
+    d.n_cols = n_cols
+    for i, (c, ht, ln, kmin, kind) in enumerate(probes):
+        d.probes[i].col, d.probes[i].ht_len = c, ln
+        d.probes[i].ht = ht if isinstance(ht, int) else ht.data_ptr()
+        d.probes[i].keys_min, d.probes[i].kind = kmin, kind
+    d.n_probes = len(probes)
+    d.agg_col, d.key_a, d.key_b = agg_col, key_a, key_b
+    d.group_mul, d.group_sub, d.n_groups = group_mul, group_sub, n_groups
+    return d, arr
+
+
+def jit_precompile_probe(col_descs, probes, agg_col: int, key_a: int, key_b: int, group_mul: int, group_sub: int,
+                         n_groups: int) -> None:
+    """Compiles the specialised probe + group-by kernel for this query shape
+    (probe tables may be given as integer addresses).  Needs no GPU."""
+    descs = [c.desc if hasattr(c, "desc") else c for c in col_descs]
+    arr = (Column * len(descs))(*descs)
+    d, _keep = _join_desc(arr, len(descs), probes, agg_col, key_a, key_b, group_mul, group_sub, n_groups)
+    check(lib().fls_jit_precompile_probe(ctypes.byref(d)), "fls_jit_precompile_probe")
 
 
 def crystal_q11(cols, n_rows: int, date_gt: int, date_lt: int, qty_lt: int, disc_ge: int, disc_le: int, out=None):

@@ -338,10 +338,11 @@ typedef enum fls_tune_param {
 	 * loop over the selected rows that reads only their fields.  Default 4;
 	 * 0 restores the default. */
 	FLS_TUNE_SPARSE_ROWS = 0,
-	/* 1 (default): fls_query_filter_agg on uniform FOR columns runs a kernel
-	 * compiled at first use (NVRTC) for the query's exact bit widths, filter
-	 * count and aggregate, cached per shape in the process; any compile or
-	 * load failure falls back to the general kernel.  0: always the general
+	/* 1 (default): fls_query_filter_agg and fls_query_probe_groupby on
+	 * uniform FOR columns run a kernel compiled at first use (NVRTC) for the
+	 * query's exact shape (bit widths, filter or probe count and kinds,
+	 * aggregate, warps per CTA), cached per shape in the process; any compile
+	 * or load failure falls back to the general kernel.  0: always the general
 	 * kernel.  Results are identical either way. */
 	FLS_TUNE_JIT = 1
 } fls_tune_param;
@@ -364,6 +365,8 @@ const char* fls_jit_last_log(void);
  * the query does not qualify or the compile failed (fls_last_error has the
  * log). */
 fls_status fls_jit_precompile(const fls_filter_agg_desc* desc);
+/* The same for the kernel fls_query_probe_groupby would run. */
+fls_status fls_jit_precompile_probe(const fls_join_agg_desc* desc);
 
 /* Number of kernels this library has launched in this process (all threads). */
 uint64_t fls_kernel_launch_count(void);

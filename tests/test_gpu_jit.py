@@ -148,3 +148,134 @@ def test_jit_unused_columns_are_not_read(jit_on):
             EncodedColumn.uniform(a, bw=12).to_device()]
     got, used = _run(cols, [(2, 10, 2000)], 1, -1, jit=True)
     assert used == 1 and got == _numpy([a, c, a], [(2, 10, 2000)], 1, -1)
+
+
+# ------------------------------------------------------------ probe + group-by
+
+def _q21_tables(n, seed, part_ids, supp_ids):
+    import torch
+    t = datagen.q21_tables(n, seed=seed, part_ids=part_ids, supp_ids=supp_ids)
+    dev = {k: torch.from_numpy(v).cuda() for k, v in t.items()}
+    ht_s = ops.build_pht(dev["s_suppkey"], supp_ids, filt=dev["s_region"], filter_eq=1)
+    ht_p = ops.build_pht(dev["p_partkey"], part_ids, vals=dev["p_brand1"], filt=dev["p_category"], filter_eq=1)
+    ht_d = ops.build_pht(dev["d_datekey"], datagen.N_DAYS, vals=dev["d_year"])
+    return t, ht_s, ht_p, ht_d
+
+
+def _probe_run(cols, probes, agg, ka, kb, mul, sub, ng, jit):
+    ops.set_tuning(TUNE_JIT, 1 if jit else 0)
+    before = _launches()
+    res = ops.probe_groupby(cols, probes, agg, ka, kb, mul, sub, ng).cpu().numpy()
+    ops.check_device_error()
+    return res, _launches() - before
+
+
+@pytest.mark.parametrize("n,part_ids,supp_ids", [(1, 1 << 10, 1 << 8), (5000, 1 << 12, 1 << 10),
+                                                 ((1 << 20) + 77, 1 << 19, 1 << 17), (1 << 23, 1 << 19, 1 << 17)])
+def test_jit_q21_against_oracle(jit_on, oracle, n, part_ids, supp_ids):
+    t, ht_s, ht_p, ht_d = _q21_tables(n, 31, part_ids, supp_ids)
+    names = ["lo_suppkey", "lo_partkey", "lo_orderdate", "lo_revenue"]
+    cols = [EncodedColumn.uniform(t[k], bw=datagen.Q21_BITS[k]).to_device() for k in names]
+    probes = [(0, ht_s, ht_s.numel(), 0, 1), (1, ht_p, ht_p.numel() // 2, 0, 2), (2, ht_d, ht_d.numel() // 2, 0, 2)]
+    got, used = _probe_run(cols, probes, 3, 1, 2, 7, 1992, datagen.N_GROUPS, jit=True)
+    assert used == 1
+    want = oracle.probe_groupby(t["lo_suppkey"], t["lo_partkey"], t["lo_orderdate"], t["lo_revenue"],
+                                ht_s.cpu().numpy(), ht_p.cpu().numpy(), ht_d.cpu().numpy())
+    assert np.array_equal(got, want)
+    assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
+
+
+def _numpy_probe(keys, measure, probes_np, agg_vals, ka, kb, mul, sub, ng):
+    """Probe + group-by semantics of fls_q21.cu probe_v1 with crystal-opt/join.cuh
+    hashing, restated over numpy arrays (tables as int32 numpy arrays)."""
+    n = measure.size
+    sel = np.ones(n, bool)
+    vals = {}
+    for q, (col, ht, ln, kmin, kind) in enumerate(probes_np):
+        d = (keys[col].astype(np.int64) - kmin).astype(np.int32).astype(np.int64)
+        h = np.where((d >= 0) & (d < ln), d, np.fmod(d, ln))
+        ok = h >= 0
+        hc = np.where(ok, h, 0)
+        if kind == 1:
+            hit = ok & (ht[hc] != 0)
+            v = np.zeros(n, np.int64)
+        else:
+            x, y = ht[2 * hc], ht[2 * hc + 1]
+            hit = ok & ((x != 0) | (y != 0))
+            v = y.astype(np.int64)
+        sel &= hit
+        vals[q] = v
+    a, b = vals[ka][sel], vals[kb][sel]
+    key = ((a * mul + (b - sub)) & 0xFFFFFFFF).astype(np.uint32).astype(np.int32).astype(np.int64)
+    g = np.where((key >= 0) & (key < ng), key, np.fmod(key, ng))
+    assert (g >= 0).all()
+    res = np.zeros((ng, 2), np.int64)
+    res32 = np.zeros(4 * ng, np.int32)
+    m = measure[sel].astype(np.int64)
+    np.add.at(res[:, 1], g, m)
+    res32[4 * g] = b
+    res32[4 * g + 1] = a
+    sums = res[:, 1].astype(np.uint64).view(np.uint32).reshape(ng, 2)
+    res32[2::4] = sums[:, 0].view(np.int32)
+    res32[3::4] = sums[:, 1].view(np.int32)
+    return res32
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_jit_probe_random_shapes(jit_on, seed):
+    import torch
+    g = np.random.default_rng(500 + seed)
+    n = int(g.choice([17, 1024, 3000, 50 * 1024 + 9, 200 * 1024]))
+    n_probes = int(g.integers(1, 5))
+    layout = LAYOUT_TRANSPOSED if g.random() < 0.3 else LAYOUT_NORMAL
+    keys, cols, probes_np, probes = [], [], [], []
+    ka = kb = None
+    for q in range(n_probes):
+        kind = 2 if (q == n_probes - 1 and ka is None) or g.random() < 0.5 else 1
+        ln = int(g.choice([7, 300, 2556, 40000, 1 << 17, 1 << 20]))  # the largest go to global memory
+        kmin = int(g.integers(0, 50))
+        bw = int(max(1, int(np.ceil(np.log2(ln + kmin + 64)))))
+        k = g.integers(kmin, min(kmin + ln + 40, 1 << bw), n).astype(np.int32)  # some keys wrap (modulo path)
+        keys.append(k)
+        cols.append(EncodedColumn.uniform(k, bw=bw, layout=layout).to_device())
+        ht = np.zeros(ln if kind == 1 else 2 * ln, np.int32)
+        present = g.random(ln) < g.choice([0.05, 0.3, 0.9])
+        if kind == 1:
+            ht[present] = 1 + np.nonzero(present)[0]
+        else:
+            ht[0::2][present] = 1 + np.nonzero(present)[0]
+            ht[1::2][present] = g.integers(0, 6, int(present.sum()))
+            ka = q if ka is None else ka
+            kb = q
+        probes_np.append((q, ht, ln, kmin, kind))
+        probes.append((q, torch.from_numpy(ht).cuda(), ln, kmin, kind))
+    measure = g.integers(-2**20, 2**20, n).astype(np.int32)
+    keys.append(measure)
+    cols.append(EncodedColumn.uniform(measure, bw=21, base=-2**20, layout=layout).to_device())
+    agg = n_probes
+    ng = 36
+    want = _numpy_probe(keys, measure, probes_np, None, ka, kb, 6, 0, ng)
+    got_jit, used = _probe_run(cols, probes, agg, ka, kb, 6, 0, ng, jit=True)
+    got_gen, used_gen = _probe_run(cols, probes, agg, ka, kb, 6, 0, ng, jit=False)
+    assert used == 1 and used_gen == 0
+    assert np.array_equal(got_gen, want)
+    assert np.array_equal(got_jit, want)
+    assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
+
+
+def test_jit_probe_out_of_range_keys_flagged(jit_on):
+    """Keys below keys_min hash to a negative slot: the row is dropped and the
+    device error word is set, in the specialised kernel as in the general one."""
+    import torch
+    from fastlanesgpu_b200 import FlsError
+    n = 8 * 1024
+    t, ht_s, ht_p, ht_d = _q21_tables(n, 24, 1 << 12, 1 << 10)
+    names = ["lo_suppkey", "lo_partkey", "lo_orderdate", "lo_revenue"]
+    cols = [EncodedColumn.uniform(t[k], bw=datagen.Q21_BITS[k]).to_device() for k in names]
+    probes = [(0, ht_s, ht_s.numel(), 5, 1), (1, ht_p, ht_p.numel() // 2, 0, 2), (2, ht_d, ht_d.numel() // 2, 0, 2)]
+    before = _launches()
+    ops.probe_groupby(cols, probes, 3, 1, 2, 7, 1992, datagen.N_GROUPS)
+    assert _launches() - before == 1
+    with pytest.raises(FlsError):
+        ops.check_device_error()
+    torch.cuda.synchronize()

@@ -46,3 +46,23 @@ def test_precompile_refuses_unqualified_queries():
     assert e.value.status == 7
     with pytest.raises(FlsError):
         ops.jit_precompile([_col(8)], [(3, 1, 2)], 0, -1)  # filter column out of range
+
+
+def test_precompile_q21_probe_shape():
+    bits = datagen.Q21_BITS
+    cols = [_col(bits[k]) for k in ("lo_suppkey", "lo_partkey", "lo_orderdate", "lo_revenue")]
+    probes = [(0, 0x200000, 1 << 17, 0, 1), (1, 0x400000, 1 << 19, 0, 2), (2, 0x800000, datagen.N_DAYS, 0, 2)]
+    ops.jit_precompile_probe(cols, probes, 3, 1, 2, 7, 1992, datagen.N_GROUPS)
+    assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
+
+
+@pytest.mark.parametrize("probes,agg", [
+    ([(0, 0x200000, 1000, 5, 2)], 0),                                   # measure = probed column
+    ([(1, 0x200000, 70000, 0, 1), (0, 0x400000, 3000, 0, 2)], 2),       # global bitmap probe, smem PHT_2
+    ([(0, 0x200000, 10, 0, 2), (1, 0x400000, 20, 1, 2), (2, 0x800000, 30, 2, 1), (3, 0xA00000, 40, 3, 2)], 4),
+])
+def test_precompile_probe_edge_shapes(probes, agg):
+    cols = [_col(bw) for bw in (17, 3, 32, 0, 9)]
+    ka = next(i for i, p in enumerate(probes) if p[4] == 2)
+    ops.jit_precompile_probe(cols, probes, agg, ka, ka, 3, 1, 100)
+    assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
