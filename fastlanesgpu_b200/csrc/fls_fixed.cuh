@@ -94,8 +94,10 @@ struct FilterQuery : Shape<LAYOUT, BWS...> {
 };
 
 // KINDS bit q: probe q is PHT_2; SMEM bit q: probe q's table is in shared
-// memory (PHT_1 as a presence bitmap, PHT_2 verbatim).
-template <int LAYOUT, int NP, int AGG, int KEY_A, int KEY_B, int KINDS, int SMEM, int... BWS>
+// memory (PHT_1 as a presence bitmap, PHT_2 verbatim); DIRECT bit q: the host
+// proved every key of probe q's column lands in [keys_min, keys_min + len)
+// (from the column's base and bit width), so its slot is key - keys_min.
+template <int LAYOUT, int NP, int AGG, int KEY_A, int KEY_B, int KINDS, int SMEM, int DIRECT, int... BWS>
 struct ProbeQuery : Shape<LAYOUT, BWS...> {
 	static constexpr int kNP  = NP;
 	static constexpr int kAgg = AGG;
@@ -103,6 +105,7 @@ struct ProbeQuery : Shape<LAYOUT, BWS...> {
 	static constexpr int kKeyB = KEY_B;
 	__host__ __device__ static constexpr bool pht2(int q) { return (KINDS >> q) & 1; }
 	__host__ __device__ static constexpr bool in_smem(int q) { return (SMEM >> q) & 1; }
+	__host__ __device__ static constexpr bool direct(int q) { return (DIRECT >> q) & 1; }
 	static_assert(NP >= 1 && NP <= FLS_MAX_PROBES, "1..4 probes");
 };
 
@@ -282,18 +285,26 @@ struct FilterBody {
 
 // -------------------------------------------------------- probe + group-by
 
+// Signed remainder, kept out of line: it runs only for keys outside the
+// table's range, and inlined copies at every row would crowd the
+// instruction cache.
+__device__ __noinline__ int32_t rem_slow(int32_t x, int32_t n) { return x % n; }
+
 // HASH(X,Y,Z) = (X-Z) % Y (crystal-opt/join.cuh:26) of d = key - keys_min:
 // in-range keys skip the division; a negative remainder is flagged and misses.
+template <bool DIRECT>
 __device__ __forceinline__ bool hash_slot(uint32_t d, int32_t len, uint32_t& h, uint32_t* err) {
 	h = d;
-	if (d >= static_cast<uint32_t>(len)) {
-		const int32_t m = static_cast<int32_t>(d) % len;
-		if (m < 0) {
-			atomicOr(err, kErrHashBit);
-			h = 0;
-			return false;
+	if constexpr (!DIRECT) {
+		if (d >= static_cast<uint32_t>(len)) {
+			const int32_t m = rem_slow(static_cast<int32_t>(d), len);
+			if (m < 0) {
+				atomicOr(err, kErrHashBit);
+				h = 0;
+				return false;
+			}
+			h = static_cast<uint32_t>(m);
 		}
-		h = static_cast<uint32_t>(m);
 	}
 	return true;
 }
@@ -326,7 +337,7 @@ __device__ __forceinline__ void dense_probes(const ProbeParams& P, const uint32_
 		uint32_t       hit[4] = {0, 0, 0, 0};
 		dev::unpack_rows<Q::bw(q)>(V.template col<q>(), lane, [&](int r, uint32_t x) {
 			uint32_t   h;
-			const bool ok = hash_slot(x + kb, len, h, P.S.err);
+			const bool ok = hash_slot<Q::direct(q)>(x + kb, len, h, P.S.err);
 			const bool b  = ok & (table_entry<Q, q>(P, tables, h).x != 0u);
 			hit[r & 3] |= (b ? 1u : 0u) << r;
 		});
@@ -353,7 +364,7 @@ __device__ __forceinline__ void probe_rows(const ProbeParams& P, const uint32_t*
 			if (j < rem) {
 				const uint32_t d = row_field<Q::bw(q)>(V.template col<q>(), lane, rows[j]) + kb;
 				uint32_t       h;
-				if (pass[j] && hash_slot(d, len, h, P.S.err)) {
+				if (pass[j] && hash_slot<Q::direct(q)>(d, len, h, P.S.err)) {
 					e[j] = table_entry<Q, q>(P, tables, h);
 				}
 			}
@@ -373,7 +384,7 @@ __device__ __forceinline__ void probe_rows(const ProbeParams& P, const uint32_t*
 __device__ __forceinline__ void emit(const ProbeParams& P, int32_t a, int32_t b, int32_t measure) {
 	const int32_t key = static_cast<int32_t>(static_cast<uint32_t>(a) * static_cast<uint32_t>(P.mul) +
 	                                         (static_cast<uint32_t>(b) - static_cast<uint32_t>(P.sub)));
-	const int32_t g   = static_cast<uint32_t>(key) < static_cast<uint32_t>(P.n_groups) ? key : key % P.n_groups;
+	const int32_t g   = static_cast<uint32_t>(key) < static_cast<uint32_t>(P.n_groups) ? key : rem_slow(key, P.n_groups);
 	if (g < 0) {
 		atomicOr(P.S.err, kErrHashBit);
 		return;

@@ -193,16 +193,28 @@ fls_status plan_fixed(const DeviceInfo& di, const fls_column* sc, uint32_t n, ui
 	k                = std::min<uint32_t>(k, kMaxTile);
 	while (k > 1 && (S.n_vec + k - 1) / k < 4 * total_warps) { k /= 2; }
 	const uint32_t avail = static_cast<uint32_t>(di.max_smem) / 4u;
-	uint32_t       stages = S0, W = 0, per = 0;
+	auto warp_words = [&](uint32_t stages_) { return (stages_ * k * sum_vec + fixed::kSlack + 2u * stages_ + 3u) & ~3u; };
+	auto warps_for  = [&](uint32_t per_) {
+		return avail > cta_words ? std::min<uint32_t>(W0, (avail - cta_words) / per_) : 0u;
+	};
+	uint32_t stages = S0, W = 0, per = 0;
 	for (;;) {
-		per = (stages * k * sum_vec + fixed::kSlack + 2u * stages + 3u) & ~3u;
-		W   = avail > cta_words ? std::min<uint32_t>(W0, (avail - cta_words) / per) : 0u;
-		if (W >= std::min<uint32_t>(W0, 8u) || (k == 1 && stages == 2)) { break; }
+		per = warp_words(stages);
+		W   = warps_for(per);
+		if (W >= std::min<uint32_t>(W0, 8u) || (k == 1 && stages <= 2)) { break; }
 		if (k > 1) {
 			k /= 2;
 		} else {
 			--stages;
 		}
+	}
+	// Wide rows (joins next to their tables): one stage per warp when that
+	// holds more warps.  Warps hide the copy latency of each other's stages,
+	// and the measured joins run faster with more warps than with more stages.
+	if (W < W0 && k == 1 && stages > 1 && warps_for(warp_words(1)) > W) {
+		stages = 1;
+		per    = warp_words(1);
+		W      = warps_for(per);
 	}
 	if (W == 0) { return set_error(FLS_ERR_CAPACITY, "vectors and tables too large for shared memory"); }
 	S.tile            = k;
@@ -374,10 +386,15 @@ bool jit_probe_shape(const fls_join_agg_desc* d, JitProbeShape& sh) {
 		if (!uniform_for(d->cols[sh.staged[i]], d->cols[sh.staged[0]].layout)) { return false; }
 	}
 	// Tables go to shared memory in probe order while they fit the budget.
-	uint32_t kinds = 0, in_smem = 0;
+	// A probe is direct when base + [0, 2^bw) - keys_min lies in [0, len).
+	uint32_t kinds = 0, in_smem = 0, direct = 0;
 	sh.cta_words   = 0;
 	for (uint32_t q = 0; q < d->n_probes; ++q) {
-		const fls_probe& p     = d->probes[q];
+		const fls_probe&  p  = d->probes[q];
+		const fls_column& kc = d->cols[p.col];
+		const int64_t     lo = static_cast<int64_t>(kc.base) - p.keys_min;
+		const int64_t     hi = lo + (kc.bw >= 32 ? (int64_t {1} << 32) : (int64_t {1} << kc.bw)) - 1;
+		if (kc.bw < 32 && lo >= 0 && hi < p.ht_len) { direct |= 1u << q; }
 		const uint64_t   words = p.kind == 1 ? (static_cast<uint64_t>(p.ht_len) + 31u) / 32u
 		                                     : 2ull * static_cast<uint64_t>(p.ht_len);
 		if (p.kind == 2) { kinds |= 1u << q; }
@@ -391,8 +408,8 @@ bool jit_probe_shape(const fls_join_agg_desc* d, JitProbeShape& sh) {
 	fls_column sc[FLS_MAX_QUERY_COLS];
 	for (uint32_t i = 0; i < sh.n_staged; ++i) { sc[i] = d->cols[sh.staged[i]]; }
 	char head[128];
-	std::snprintf(head, sizeof(head), "%u, %u, %d, %d, %d, %u, %u", static_cast<unsigned>(sc[0].layout), d->n_probes,
-	              sh.agg, d->key_a, d->key_b, kinds, in_smem);
+	std::snprintf(head, sizeof(head), "%u, %u, %d, %d, %d, %u, %u, %u", static_cast<unsigned>(sc[0].layout),
+	              d->n_probes, sh.agg, d->key_a, d->key_b, kinds, in_smem, direct);
 	sh.key = key_args(sc, sh.n_staged, head);
 	return true;
 }

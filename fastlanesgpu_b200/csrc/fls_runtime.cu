@@ -249,10 +249,9 @@ fls_status fls_check_device_error(fls_stream_t stream) {
 }
 
 fls_status fls_set_launch_config(uint32_t warps_per_cta, uint32_t stages, uint32_t ctas_per_sm, uint32_t tile_bytes) {
-	if (warps_per_cta > kMaxWarps || stages > 8 || ctas_per_sm > 4 || (stages != 0 && stages < 2) ||
-	    tile_bytes > 65536) {
+	if (warps_per_cta > kMaxWarps || stages > 8 || ctas_per_sm > 4 || tile_bytes > 65536) {
 		return set_error(FLS_ERR_INVALID_ARG,
-		                 "launch config out of range (warps <= 16, 2 <= stages <= 8, ctas <= 4, tile_bytes <= 64K)");
+		                 "launch config out of range (warps <= 16, stages <= 8, ctas <= 4, tile_bytes <= 64K)");
 	}
 	const LaunchCfg d;
 	std::lock_guard<std::mutex> lk(g_cfg_mu);
