@@ -39,8 +39,13 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["q11", "q21", "decode"], default="q11")
-    ap.add_argument("--rows", type=int, default=1 << 27)
-    ap.add_argument("--decode-bw", type=int, default=16, help="bit width of the decode workload")
+    ap.add_argument("--rows", type=int, default=0, help="rows per GPU (0 = 2^27 for queries, 2^28 for decode)")
+    ap.add_argument("--decode-bw", type=int, default=16, help="bit width of the FOR decode workload")
+    ap.add_argument("--decode-scheme", choices=["for", "delta", "rle"], default="for",
+                    help="decode input: uniform FOR bit-packing, delta over sorted keys (geometric gaps p=0.3), "
+                         "RLE (geometric runs of mean 16, values in [0,2^16))")
+    ap.add_argument("--decode-out", choices=["sum", "hbm"], default="sum",
+                    help="decode fused with a uint64 sum, or decode to HBM")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -48,7 +53,10 @@ def parse_args():
     ap.add_argument("--sparse-rows", type=int, default=0, help="FLS_TUNE_SPARSE_ROWS (0 = default)")
     ap.add_argument("--jit", type=int, choices=[0, 1], default=1,
                     help="FLS_TUNE_JIT: 1 = kernel specialised to the query's shape, 0 = general kernel")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if not a.rows:
+        a.rows = (1 << 28) if a.workload == "decode" else (1 << 27)
+    return a
 
 
 # ------------------------------------------------------------------ helpers
@@ -181,6 +189,7 @@ def build_q21(rows: int, seed: int):
 
 
 def run_ours(a, dist: Dist):
+    import numpy as np
     import torch
 
     from fastlanesgpu_b200 import EncodedColumn, datagen, ops
@@ -227,17 +236,39 @@ def run_ours(a, dist: Dist):
                     "filters": "part category 1/5, supplier region 1/25"}
         metric_key = "q21"
     else:
-        vals = datagen.uniform_bits(a.rows, a.decode_bw, seed=seed)
-        hcols = [EncodedColumn.uniform(vals, bw=a.decode_bw)]
+        from fastlanesgpu_b200 import LAYOUT_TRANSPOSED, SCHEME_DELTA, SCHEME_RLE
+        if a.decode_scheme == "for":
+            vals = datagen.uniform_bits(a.rows, a.decode_bw, seed=seed)
+            hcols = [EncodedColumn.uniform(vals, bw=a.decode_bw)]
+            what, key = f"bit-pack + FOR, bw {a.decode_bw} (uniform column)", f"for_bw{a.decode_bw}"
+        elif a.decode_scheme == "delta":
+            vals = datagen.sorted_geometric(a.rows, p=0.3, seed=seed)
+            hcols = [EncodedColumn.encode(vals, SCHEME_DELTA, layout=LAYOUT_TRANSPOSED)]
+            what, key = "delta over sorted keys with geometric gaps (p=0.3), per-vector bw", "delta"
+        else:
+            vals = datagen.geometric_runs(a.rows, mean_run=16.0, value_bits=16, seed=seed)
+            hcols = [EncodedColumn.encode(vals, SCHEME_RLE, layout=LAYOUT_TRANSPOSED)]
+            what, key = "RLE, geometric runs (mean 16) of values in [0,2^16)", "rle"
+        del vals
         dcols = [c.to_device(dev) for c in hcols]
-        res = torch.zeros(1, dtype=torch.int64, device=dev)
+        if a.decode_out == "sum":
+            res = torch.zeros(1, dtype=torch.int64, device=dev)
 
-        def step():
-            ops.query_aggregate(dcols[0], out=res)
-            return res
-        workload = {"workload": f"decode fused with sum, bit-pack bw {a.decode_bw}", "rows_per_gpu": a.rows}
-        metric_key = f"decode_sum_bw{a.decode_bw}"
+            def step():
+                ops.query_aggregate(dcols[0], out=res)
+                return res
+        else:
+            res = torch.empty(dcols[0].n_vec * 1024, dtype=torch.int32, device=dev)
+
+            def step():
+                ops.unpack_global(dcols[0], out=res)
+                return res
+        out_bytes = 4 * dcols[0].n_vec * 1024 if a.decode_out == "hbm" else 0
+        workload = {"workload": f"decode {'to HBM' if a.decode_out == 'hbm' else 'fused with uint64 sum'}: {what}",
+                    "rows_per_gpu": a.rows}
+        metric_key = f"decode_{a.decode_out}_{key}"
     comp_bytes = sum(c.nbytes for c in hcols)
+    algo_bytes = comp_bytes + (out_bytes if a.workload == "decode" else 0)
 
     def collective():
         # the one exchange of the sharded query: combine the ranks' partial aggregates
@@ -281,8 +312,14 @@ def run_ours(a, dist: Dist):
     ops.check_device_error()
 
     # ------------------------------------------- end-to-end through the C ABI
-    pinned = [torch.from_numpy(c.words.view("int32")).pin_memory() for c in hcols]
-    h2d = sum(p.numel() * 4 for p in pinned)
+    # every encoded buffer of every column: packed words and, for per-vector
+    # columns, the vector metadata
+    copies = []
+    for c, dc in zip(hcols, dcols):
+        copies.append((dc.data, torch.from_numpy(c.words.view("int32")).pin_memory()))
+        if c.meta is not None:
+            copies.append((dc.meta, torch.from_numpy(c.meta.view(np.uint8)).pin_memory()))
+    h2d = sum(hp.numel() * hp.element_size() for _, hp in copies)
     d2h = res.numel() * res.element_size()
     host_res = torch.empty_like(res, device="cpu").pin_memory()
     n_e2e = max(3, min(a.e2e_steps, a.steps))
@@ -291,8 +328,8 @@ def run_ours(a, dist: Dist):
     x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     x0.record(stream)
     for _ in range(n_e2e):
-        for dc, hp in zip(dcols, pinned):
-            dc.data.copy_(hp, non_blocking=True)
+        for dst, hp in copies:
+            dst.copy_(hp.view(dst.dtype).view(dst.shape), non_blocking=True)
         step()
         collective()
         host_res.copy_(res, non_blocking=True)
@@ -305,7 +342,7 @@ def run_ours(a, dist: Dist):
     value = rows_total * a.steps / (ms / 1e3)
     ms_step = ms / a.steps
     peak, peak_src = measured_peak_gbs()
-    achieved = comp_bytes / (ms_local / a.steps / 1e3) / 1e9
+    achieved = algo_bytes / (ms_local / a.steps / 1e3) / 1e9
     traffic = profiled_traffic(metric_key)
     out = {
         "metric": "fused decode+query rows/s", "value": value, "unit": "rows/s", "n_gpus": dist.world,
@@ -321,7 +358,7 @@ def run_ours(a, dist: Dist):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
                      else "fallback 6650 GB/s",
-                     "traffic": traffic, "algorithmic_bytes_per_launch": comp_bytes},
+                     "traffic": traffic, "algorithmic_bytes_per_launch": algo_bytes},
         "gpu_launches": int(launches),
         "launch_config": dict(zip(["warps", "stages", "ctas_per_sm", "tile_bytes"], ops.get_launch_config()),
                               sparse_rows=ops.get_tuning(0), jit=ops.get_tuning(1),

@@ -89,10 +89,16 @@ fls_status fls_decode_u32(const fls_column* col, uint32_t* d_out, uint32_t order
 	const bool orig = order == FLS_ORDER_ORIGINAL && col->layout == FLS_LAYOUT_TRANSPOSED;
 	fls_status s    = plan_stages(col, 1, orig ? kTBufWords : 0u, 0u, cfg, grid, threads, smem);
 	if (s != FLS_OK) { return s; }
+	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+	if (tuning_jit() && !orig) {
+		bool used = false;
+		s         = jit_decode(col, 1, d_out, nullptr, st, used);
+		if (s != FLS_OK || used) { return s; }
+	}
 	DecodeOp op {};
 	op.out      = d_out;
 	op.original = orig ? 1u : 0u;
-	return launch_staged(cfg, op, grid, threads, smem, reinterpret_cast<cudaStream_t>(stream));
+	return launch_staged(cfg, op, grid, threads, smem, st);
 }
 
 fls_status fls_decode_sum_u32(const fls_column* col, uint64_t* d_sum, fls_stream_t stream) {
@@ -104,6 +110,11 @@ fls_status fls_decode_sum_u32(const fls_column* col, uint64_t* d_sum, fls_stream
 	if (s != FLS_OK) { return s; }
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
 	if ((s = cuda_check(cudaMemsetAsync(d_sum, 0, sizeof(uint64_t), st), "cudaMemsetAsync")) != FLS_OK) { return s; }
+	if (tuning_jit()) {
+		bool used = false;
+		s         = jit_decode(col, 0, nullptr, d_sum, st, used);
+		if (s != FLS_OK || used) { return s; }
+	}
 	DecodeSumOp op {};
 	op.sum = reinterpret_cast<unsigned long long*>(d_sum);
 	return launch_staged(cfg, op, grid, threads, smem, st);

@@ -12,7 +12,8 @@
 //  * filter-aggregate (FilterQuery): columns staged in filter order (column f
 //    holds filter f), then aggregate columns no filter reads;
 //  * probe + group-by (ProbeQuery): columns staged in probe order (column q
-//    holds the key of probe q), then the measure column if no probe reads it.
+//    holds the key of probe q), then the measure column if no probe reads it;
+//  * decode fused with a sum, and decode to HBM (DecodeQuery): one column.
 #pragma once
 
 #include "fls_device.cuh"
@@ -58,12 +59,21 @@ struct ProbeParams {
 	int32_t*       res;
 };
 
+struct DecodeParams {
+	StageParams         S;
+	uint32_t            base; // FOR base of the column
+	uint32_t            pad_;
+	unsigned long long* sum;  // decode-sum: uint64 total
+	uint32_t*           out;  // decode to HBM: n_vec * 1024 values
+};
+
 // The host (nvcc + host compiler) and NVRTC must agree on the parameter
 // blocks.  Every field is naturally aligned and padded explicitly, so equal
 // sizes mean equal offsets.
 static_assert(sizeof(StageParams) == 128 && alignof(StageParams) == 8, "StageParams layout");
 static_assert(sizeof(FilterParams) == 208, "FilterParams layout");
 static_assert(sizeof(ProbeParams) == 264, "ProbeParams layout");
+static_assert(sizeof(DecodeParams) == 152, "DecodeParams layout");
 
 // Bit widths of the staged columns and where they sit in a stage.
 template <int LAYOUT, int... BWS>
@@ -107,6 +117,16 @@ struct ProbeQuery : Shape<LAYOUT, BWS...> {
 	__host__ __device__ static constexpr bool in_smem(int q) { return (SMEM >> q) & 1; }
 	__host__ __device__ static constexpr bool direct(int q) { return (DIRECT >> q) & 1; }
 	static_assert(NP >= 1 && NP <= FLS_MAX_PROBES, "1..4 probes");
+};
+
+// MODE 0: decode fused with a uint64 sum; MODE 1: decode to HBM in stored
+// order.  NOWRAP: the host proved base + (2^BW - 1) < 2^32, so no decoded
+// value wraps and the base can be added once per vector (sum of x + base =
+// sum of x + count * base).
+template <int LAYOUT, int BW, int MODE, bool NOWRAP>
+struct DecodeQuery : Shape<LAYOUT, BW> {
+	static constexpr int  kMode   = MODE;
+	static constexpr bool kNoWrap = NOWRAP;
 };
 
 // Row r of this lane's stream at compile-time bit width (runtime row).
@@ -494,6 +514,55 @@ struct ProbeBody {
 	__device__ __forceinline__ void finish(uint32_t) {}
 };
 
+// ------------------------------------------------------------------ decode
+
+template <class Q>
+struct DecodeBody {
+	static constexpr bool kCtaSetup = false;
+	const DecodeParams&   P;
+	unsigned long long    acc = 0;
+
+	__device__ __forceinline__ void cta_setup(uint32_t*) {}
+
+	__device__ __forceinline__ void operator()(const Vec<Q>& V, uint64_t v, uint32_t lane) {
+		constexpr int  BW   = Q::bw(0);
+		const uint32_t base = P.base;
+		if constexpr (Q::kMode == 1) {
+			uint32_t* dst = P.out + v * 1024u + lane;
+			dev::unpack_rows<BW>(V.template col<0>(), lane, [&](int r, uint32_t x) { __stcs(dst + 32 * r, x + base); });
+		} else {
+			const uint32_t m = valid_rows(P.S, Q::kLayout, v, lane);
+			if constexpr (Q::kNoWrap && BW <= 27) {
+				// 32 values of at most 27 bits: the lane's sum fits 32 bits.
+				uint32_t s = 0;
+				if (m == 0xffffffffu) {
+					dev::unpack_rows<BW>(V.template col<0>(), lane, [&](int, uint32_t x) { s += x; });
+				} else {
+					dev::unpack_rows<BW>(V.template col<0>(), lane,
+					                     [&](int r, uint32_t x) { s += ((m >> r) & 1u) ? x : 0u; });
+				}
+				acc += static_cast<unsigned long long>(s) +
+				       static_cast<unsigned long long>(__popc(m)) * static_cast<unsigned long long>(base);
+			} else {
+				unsigned long long p[4] = {0, 0, 0, 0};
+				dev::unpack_rows<BW>(V.template col<0>(), lane, [&](int r, uint32_t x) {
+					p[r & 3] += ((m >> r) & 1u) ? static_cast<unsigned long long>(x + base) : 0ull;
+				});
+				acc += (p[0] + p[1]) + (p[2] + p[3]);
+			}
+		}
+	}
+
+	__device__ __forceinline__ void finish(uint32_t lane) {
+		if constexpr (Q::kMode == 0) {
+			unsigned long long s = acc;
+#pragma unroll
+			for (int o = 16; o > 0; o >>= 1) { s += __shfl_xor_sync(0xffffffffu, s, o); }
+			if (lane == 0 && s) { atomicAdd(P.sum, s); }
+		}
+	}
+};
+
 // ---------------------------------------------------------------- pipeline
 
 // Words per vector and stage offset (in vectors' words) of column `lane`.
@@ -591,6 +660,12 @@ __device__ __forceinline__ void filter_kernel(const FilterParams& P) {
 template <class Q>
 __device__ __forceinline__ void probe_kernel(const ProbeParams& P) {
 	ProbeBody<Q> body {P};
+	run<Q>(P.S, body);
+}
+
+template <class Q>
+__device__ __forceinline__ void decode_kernel(const DecodeParams& P) {
+	DecodeBody<Q> body {P};
 	run<Q>(P.S, body);
 }
 

@@ -85,15 +85,17 @@ const char* const kStddef = "#pragma once\ntypedef decltype(sizeof(0)) size_t;\n
 const char* const kEmpty  = "#pragma once\n";
 
 // Kernel keys are "<op>:<warps>:<template arguments>"; op F = filter-aggregate,
-// P = probe + group-by.  The warp count fixes __launch_bounds__ so that the
+// P = probe + group-by, D = decode.  The warp count fixes __launch_bounds__ so that the
 // compiler may use every register the launch leaves.
 std::string shape_source(const std::string& key) {
 	const size_t a = key.find(':'), b = key.find(':', a + 1);
 	const std::string op = key.substr(0, a), warps = key.substr(a + 1, b - a - 1), args = key.substr(b + 1);
-	const bool filter = op == "F";
+	const char* params = op == "F" ? "FilterParams" : op == "P" ? "ProbeParams" : "DecodeParams";
+	const char* body   = op == "F"   ? "filter_kernel<fls::fixed::FilterQuery<"
+	                     : op == "P" ? "probe_kernel<fls::fixed::ProbeQuery<"
+	                                 : "decode_kernel<fls::fixed::DecodeQuery<";
 	return std::string("#include \"fls_fixed.cuh\"\n") + "extern \"C\" __global__ void __launch_bounds__(32 * " + warps +
-	       ", 1)\nfls_fixed_kernel(const __grid_constant__ fls::fixed::" + (filter ? "FilterParams" : "ProbeParams") +
-	       " P) {\n\tfls::fixed::" + (filter ? "filter_kernel<fls::fixed::FilterQuery<" : "probe_kernel<fls::fixed::ProbeQuery<") +
+	       ", 1)\nfls_fixed_kernel(const __grid_constant__ fls::fixed::" + params + " P) {\n\tfls::fixed::" + body +
 	       args + ">>(P);\n}\n";
 }
 
@@ -455,6 +457,30 @@ fls_status jit_probe_groupby(const fls_join_agg_desc* d, int32_t* d_res, int32_t
 	P.sparse_rows = sparse_rows;
 	P.res         = d_res;
 	return launch_fixed(make_key('P', P.S.warps, sh.key), &P, grid, 32u * P.S.warps, smem, stream, used);
+}
+
+fls_status jit_decode(const fls_column* col, int mode, uint32_t* d_out, uint64_t* d_sum, cudaStream_t stream,
+                      bool& used) {
+	used = false;
+	if (!uniform_for(*col, col->layout)) { return FLS_OK; }
+	const bool no_wrap =
+	    col->bw < 32 && static_cast<uint64_t>(static_cast<uint32_t>(col->base)) + (uint64_t {1} << col->bw) - 1u <
+	                        (uint64_t {1} << 32);
+	fixed::DecodeParams P {};
+	uint32_t            grid;
+	size_t              smem;
+	DeviceInfo          di;
+	fls_status          s = device_info(di);
+	if (s != FLS_OK) { return s; }
+	if ((s = plan_fixed(di, col, 1, 0u, P.S, grid, smem)) != FLS_OK) { return s; }
+	P.S.err = device_error_word();
+	P.base  = static_cast<uint32_t>(col->base);
+	P.sum   = reinterpret_cast<unsigned long long*>(d_sum);
+	P.out   = d_out;
+	const std::string args = std::to_string(static_cast<unsigned>(col->layout)) + ", " +
+	                         std::to_string(static_cast<unsigned>(col->bw)) + ", " + std::to_string(mode) + ", " +
+	                         (no_wrap ? "true" : "false");
+	return launch_fixed(make_key('D', P.S.warps, args), &P, grid, 32u * P.S.warps, smem, stream, used);
 }
 
 } // namespace fls

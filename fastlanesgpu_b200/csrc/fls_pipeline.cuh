@@ -335,6 +335,10 @@ bool       jit_probe_shape(const fls_join_agg_desc* desc, JitProbeShape& sh);
 bool       jit_compile(const fls_join_agg_desc* desc, const JitProbeShape& sh);
 fls_status jit_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res, int32_t sparse_rows, cudaStream_t stream,
                              bool& used);
+// Decode of a uniform FOR column: mode 0 = fused uint64 sum into d_sum, mode 1
+// = to HBM (stored order) into d_out.
+fls_status jit_decode(const fls_column* col, int mode, uint32_t* d_out, uint64_t* d_sum, cudaStream_t stream,
+                      bool& used);
 
 // Lays out shared memory for a set of columns; extra_words per warp and
 // cta_words per CTA are operator-specific scratch.

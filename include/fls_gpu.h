@@ -338,12 +338,13 @@ typedef enum fls_tune_param {
 	 * loop over the selected rows that reads only their fields.  Default 4;
 	 * 0 restores the default. */
 	FLS_TUNE_SPARSE_ROWS = 0,
-	/* 1 (default): fls_query_filter_agg and fls_query_probe_groupby on
-	 * uniform FOR columns run a kernel compiled at first use (NVRTC) for the
-	 * query's exact shape (bit widths, filter or probe count and kinds,
-	 * aggregate, warps per CTA), cached per shape in the process; any compile
-	 * or load failure falls back to the general kernel.  0: always the general
-	 * kernel.  Results are identical either way. */
+	/* 1 (default): fls_query_filter_agg, fls_query_probe_groupby,
+	 * fls_decode_sum_u32 and fls_decode_u32 (stored order) on uniform FOR
+	 * columns run a kernel compiled at first use (NVRTC) for the exact shape
+	 * (bit widths, filter or probe count and kinds, aggregate, warps per CTA),
+	 * cached per shape in the process; any compile or load failure falls back
+	 * to the general kernel.  0: always the general kernel.  Results are
+	 * identical either way. */
 	FLS_TUNE_JIT = 1
 } fls_tune_param;
 fls_status fls_set_tuning(uint32_t param, int64_t value);

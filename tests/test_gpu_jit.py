@@ -279,3 +279,47 @@ def test_jit_probe_out_of_range_keys_flagged(jit_on):
     with pytest.raises(FlsError):
         ops.check_device_error()
     torch.cuda.synchronize()
+
+
+# ------------------------------------------------------------------ decode
+
+@pytest.mark.parametrize("bw", [0, 1, 3, 8, 13, 16, 24, 27, 28, 31, 32])
+@pytest.mark.parametrize("base", [0, -7, 2**31 - 5])
+def test_jit_decode_sum_and_hbm(jit_on, oracle, bw, base):
+    """Specialised decode-sum (32-bit partial sums with the base added once per
+    vector when no value can wrap; per-value uint64 adds otherwise) and decode to
+    HBM equal the general kernel and the oracle, on full and partial vectors."""
+    n = 70 * 1024 + 333
+    g = np.random.default_rng(bw * 7 + (base & 0xFF))
+    packed = (g.integers(0, 1 << 32, n, dtype=np.uint64) & ((1 << bw) - 1)).astype(np.uint32)
+    vals = (packed + np.uint32(base & 0xFFFFFFFF)).view(np.int32)  # wraps like the decoder does
+    col = EncodedColumn.uniform(vals, bw=bw, base=base).to_device()
+    want_sum = int(vals.view(np.uint32).astype(np.uint64).sum())
+    for jit in (1, 0):
+        ops.set_tuning(TUNE_JIT, jit)
+        before = _launches()
+        s = int(ops.query_aggregate(col).cpu()[0]) & 0xFFFFFFFFFFFFFFFF
+        out = ops.unpack_global(col).cpu().numpy()[:n]
+        ops.check_device_error()
+        assert _launches() - before == (2 if jit else 0)
+        assert s == want_sum, (jit, bw, base)
+        assert np.array_equal(out, vals), (jit, bw, base)
+    assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
+
+
+def test_jit_decode_transposed_orders(jit_on):
+    """Transposed uniform columns: stored order runs specialised, original order
+    takes the general kernel; both agree with the host's untransposed values."""
+    from fastlanesgpu_b200._lib import ORDER_ORIGINAL
+    n = 9 * 1024 + 100
+    vals = datagen.uniform_bits(n, 9, seed=77)
+    col = EncodedColumn.uniform(vals, bw=9, layout=LAYOUT_TRANSPOSED).to_device()
+    before = _launches()
+    stored = ops.unpack_global(col).cpu().numpy()
+    assert _launches() - before == 1
+    orig = ops.unpack_global(col, order=ORDER_ORIGINAL).cpu().numpy()[:n]
+    assert _launches() - before == 1
+    assert np.array_equal(orig, vals)
+    for v in range(n // 1024):
+        assert np.array_equal(ops.untranspose(stored[v * 1024:(v + 1) * 1024].view(np.uint32)).view(np.int32),
+                              vals[v * 1024:(v + 1) * 1024])
