@@ -38,7 +38,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["q11", "q21", "decode"], default="q11")
+    ap.add_argument("--workload", choices=["q11", "q21", "decode", "mixed"], default="q11")
     ap.add_argument("--rows", type=int, default=0, help="rows per GPU (0 = 2^27 for queries, 2^28 for decode)")
     ap.add_argument("--decode-bw", type=int, default=16, help="bit width of the FOR decode workload")
     ap.add_argument("--decode-scheme", choices=["for", "delta", "rle"], default="for",
@@ -53,6 +53,13 @@ def parse_args():
     ap.add_argument("--sparse-rows", type=int, default=0, help="FLS_TUNE_SPARSE_ROWS (0 = default)")
     ap.add_argument("--jit", type=int, choices=[0, 1], default=1,
                     help="FLS_TUNE_JIT: 1 = kernel specialised to the query's shape, 0 = general kernel")
+    ap.add_argument("--mixed-columns", type=int, default=64, help="mixed workload: number of columns")
+    ap.add_argument("--mixed-max-log", type=int, default=26, help="mixed workload: longest column is 2^this rows")
+    ap.add_argument("--train-vectors", type=int, default=1 << 20, help="mixed workload: MLP training vectors")
+    ap.add_argument("--train-epochs", type=int, default=6)
+    ap.add_argument("--queries", type=int, default=256, help="mixed workload: batched filter-aggregate queries")
+    ap.add_argument("--threshold", type=float, default=0.9, help="selector confidence below which the "
+                                                                    "exhaustive encoder decides")
     a = ap.parse_args()
     if not a.rows:
         a.rows = (1 << 28) if a.workload == "decode" else (1 << 27)
@@ -397,6 +404,187 @@ def cpu_baseline_q11(a, hcols, budget_s: float):
                       f"(unpack_fused.cuh host-compiled) + fls_q11.cu loop, OpenMP {threads} threads"}
 
 
+def _pad_vectors(v):
+    """A column padded to whole vectors with its last value (as the encoder pads)."""
+    import numpy as np
+    r = (-v.size) % 1024
+    return v if r == 0 else np.concatenate([v, np.full(r, v[-1], v.dtype)])
+
+
+def run_mixed(a, dist: Dist):
+    """Learned encoding + batched mixed workload: the MLP is trained on the GPU
+    on exhaustively labelled vectors; 64 columns of uneven length and
+    distribution are encoded with the learned picks and with the exhaustive
+    encoder; 256 seeded filter-aggregate queries run as one CUDA-graph replay of
+    the batch executor and as one launch per query."""
+    import numpy as np
+    import torch
+
+    from fastlanesgpu_b200 import LAYOUT_TRANSPOSED, ORDER_ORIGINAL, EncodedColumn, datagen, ops
+    from fastlanesgpu_b200.batch import Batch, graph_of
+    from fastlanesgpu_b200.selector import LearnedSelector, corpus_device, gpu_features
+    dev = torch.device("cuda", dist.local)
+    stream = torch.cuda.current_stream()
+    ops.set_tuning(1, a.jit)
+    threads = os.cpu_count() or 1
+
+    def now():
+        torch.cuda.synchronize()
+        return time.perf_counter()
+
+    # ------------------------------------------------ train the selector
+    t0 = now()
+    train_dev = corpus_device(a.train_vectors, seed=7, device=dev)
+    train_host = train_dev.cpu().numpy()
+    t1 = now()
+    _, labels = ops.encode_exhaustive(train_host)
+    t2 = now()
+    sel = LearnedSelector(device=dev, seed=1)
+    feats = gpu_features(train_dev)
+    losses = sel.train(feats, torch.from_numpy(labels).to(dev), epochs=a.train_epochs, batch=4096, lr=3e-3)
+    t3 = now()
+    del train_dev, train_host, feats
+    training = {"vectors": a.train_vectors, "epochs": a.train_epochs, "batch": 4096,
+                "corpus_gen_s": t1 - t0, "exhaustive_label_s": t2 - t1, "gpu_train_s": t3 - t2,
+                "loss_first_epoch": losses[0], "loss_last_epoch": losses[-1]}
+
+    # --------------------------------------------------- the 64 columns
+    cols = datagen.mixed_columns(a.mixed_columns, 16, a.mixed_max_log, seed=64, device=dev)
+    host = [_pad_vectors(v.cpu().numpy()) for _, v in cols]
+    lens = [int(v.numel()) for _, v in cols]
+    n_vec = [h.size // 1024 for h in host]
+    rows_all = sum(lens)
+    # exhaustive: exact size of every scheme of every vector, argmin, encode
+    t0 = time.perf_counter()
+    ex = [ops.encode_exhaustive(h, threads) for h in host]
+    t1 = time.perf_counter()
+    enc_ex = [EncodedColumn.encode(h[:n], best, layout=LAYOUT_TRANSPOSED) for h, n, (_, best) in zip(host, lens, ex)]
+    t2 = time.perf_counter()
+    ex_select_s, ex_encode_s = t1 - t0, t2 - t1
+    # learned: upload, GPU statistics + MLP, exhaustive only below the threshold
+    cat = np.concatenate(host)
+    t0 = time.perf_counter()
+    schemes, info = sel.select(cat, threshold=a.threshold)
+    t1 = time.perf_counter()
+    splits = np.cumsum(n_vec)[:-1]
+    enc_ln = [EncodedColumn.encode(h[:n], sc, layout=LAYOUT_TRANSPOSED)
+              for h, n, sc in zip(host, lens, np.split(schemes, splits))]
+    t2 = time.perf_counter()
+    ln_select_s, ln_encode_s = t1 - t0, t2 - t1
+    size_ex = sum(c.nbytes for c in enc_ex)
+    size_ln = sum(c.nbytes for c in enc_ln)
+    size_for = sum(int(sz[:, 0].astype(np.int64).sum()) for sz, _ in ex)  # bit-packing only
+    del cat
+
+    # lossless: decode every learned column on the GPU and compare
+    dcols = [c.to_device(dev) for c in enc_ln]
+    lossless = all(torch.equal(ops.unpack_global(dc, order=ORDER_ORIGINAL)[:n], v)
+                   for dc, n, (_, v) in zip(dcols, lens, cols))
+
+    # ----------------------------------------------- 256 seeded queries
+    g = np.random.default_rng(256)
+    queries = []
+    for q in range(a.queries):
+        c = q % len(cols)
+        smp = host[c][: lens[c]: 97] if lens[c] > 97 * 64 else host[c][: lens[c]]
+        lo_q, hi_q = np.sort(g.random(2))
+        lo, hi = (int(x) for x in np.quantile(smp, [lo_q, hi_q]))
+        queries.append((c, lo, hi, c))
+    want = []
+    for c, lo, hi, _ in queries:  # plain torch on the raw columns
+        v = cols[c][1].to(torch.int64)
+        m = (v >= lo) & (v <= hi)
+        want.append((int(v[m].sum()), int(m.sum())))
+    batch = Batch(dcols, queries)
+    graph = graph_of(batch.run)
+    res = batch.results.view(-1, 2)
+
+    def per_query():
+        return [ops.query_filter_agg([dcols[c]], [(0, lo, hi)], agg_a=0) for c, lo, hi, _ in queries]
+
+    pq = [int(x.cpu()[0]) for x in per_query()]
+    graph.replay()
+    torch.cuda.synchronize()
+    got = [(int(s_), int(n_)) for s_, n_ in res.cpu().tolist()]
+    exact = got == want and pq == [w[0] for w in want]
+
+    def timed(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    # kernels per batch: what one fls_batch_run enqueues (the graph replays it)
+    l0 = ops.kernel_launch_count()
+    batch.run()
+    per_run = ops.kernel_launch_count() - l0
+    clocks = ClockSampler(dist.local)
+    clocks.start()
+    w0 = time.time()
+    batch_ms = timed(graph.replay, a.steps)
+    w1 = time.time()
+    launches = per_run * a.steps
+    clocks.mark(w0, w1)
+    per_query_ms = timed(per_query, max(3, a.steps // 10))
+    # end to end: encoded columns H2D, the batch, results D2H
+    copies = []
+    for c, dc in zip(enc_ln, dcols):
+        copies.append((dc.data, torch.from_numpy(c.words.view("int32")).pin_memory()))
+        copies.append((dc.meta, torch.from_numpy(c.meta.view(np.uint8)).pin_memory()))
+    host_res = torch.empty(res.numel(), dtype=torch.int64).pin_memory()
+
+    def e2e():
+        for dst, hp in copies:
+            dst.copy_(hp.view(dst.dtype).view(dst.shape), non_blocking=True)
+        graph.replay()
+        host_res.copy_(batch.results, non_blocking=True)
+    e2e_ms = timed(e2e, 3)
+    clk = clocks.stop()
+
+    q_rows = sum(lens[c] for c, _, _, _ in queries)
+    q_bytes = sum(enc_ln[c].nbytes for c, _, _, _ in queries)
+    peak, peak_src = measured_peak_gbs()
+    achieved = q_bytes / (batch_ms / 1e3) / 1e9
+    return {
+        "metric": "fused decode+query rows/s", "value": q_rows / (batch_ms / 1e3), "unit": "rows/s",
+        "n_gpus": dist.world, "steps": a.steps, "warmup": 3, "ms_per_step": batch_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32->int64", "data": "synthetic (seeded)",
+        "config": {"workload": f"mixed: {len(cols)} columns (lengths 2^16..2^{a.mixed_max_log}; uniform, Zipf 1.1, "
+                               f"sorted gaps, geometric runs), learned encoding, {len(queries)} filter-aggregate "
+                               "queries in one CUDA-graph batch launch",
+                   "rows_in_columns": rows_all, "rows_scanned_per_step": q_rows,
+                   "l2": "columns larger than L2 (126 MB) in total, no flush", "parallelism": "1 GPU"},
+        "learned_encoding": {
+            "bytes_exhaustive": size_ex, "bytes_learned": size_ln, "bytes_bitpack_only": size_for,
+            "regret": size_ln / size_ex - 1.0,
+            "select_s_exhaustive": ex_select_s, "select_s_learned": ln_select_s,
+            "encode_s_exhaustive": ex_select_s + ex_encode_s, "encode_s_learned": ln_select_s + ln_encode_s,
+            "select_speedup": ex_select_s / ln_select_s,
+            "encode_speedup": (ex_select_s + ex_encode_s) / (ln_select_s + ln_encode_s),
+            "fallback_vectors": info["fallback_vectors"], "vectors": info["vectors"], "threshold": a.threshold,
+            "host_threads": threads, "learned_parts_s": {k: v for k, v in info.items() if k.endswith("_s")},
+            "lossless": bool(lossless), "training": training},
+        "batched": {"ms_batch_graph": batch_ms, "ms_per_query_launches": per_query_ms,
+                    "speedup": per_query_ms / batch_ms, "queries": len(queries), "work_items": batch.n_items,
+                    "results_equal": bool(exact)},
+        "e2e": {"value": q_rows / (e2e_ms / 1e3), "unit": "rows/s",
+                "h2d_bytes_per_step": sum(hp.numel() * hp.element_size() for _, hp in copies),
+                "d2h_bytes_per_step": host_res.numel() * 8, "ms_per_step": e2e_ms,
+                "path": "pinned host encoded columns -> H2D -> batch graph (C ABI) -> D2H results"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
+                     else "fallback 6650 GB/s", "traffic": None, "algorithmic_bytes_per_launch": q_bytes},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+
+
 def run_reference(a, dist: Dist):
     """--impl reference: the reference's own CPU implementation of the path."""
     import numpy as np
@@ -446,6 +634,11 @@ def main():
         return
     dist.init()
     try:
+        if a.workload == "mixed":
+            if dist.world > 1:
+                raise SystemExit("--workload mixed runs on one GPU")
+            print(json.dumps(run_mixed(a, dist)), flush=True)
+            return
         out, _, hcols = run_ours(a, dist)
         if dist.rank == 0:
             if dist.world == 1 and a.workload == "q11" and not a.no_cpu_baseline:

@@ -106,3 +106,45 @@ def q21_tables(n: int, seed: int = 21, part_ids: int = 1 << 19, supp_ids: int = 
 
 Q21_BITS = {"lo_suppkey": 17, "lo_partkey": 19, "lo_orderdate": 12, "lo_revenue": 24}
 N_GROUPS = (1998 - 1992 + 1) * (5 * 5 * 40)
+
+
+MIXED_FAMILIES = ("uniform", "zipf", "sorted_gaps", "geometric_runs")
+
+
+def mixed_columns(n_cols: int = 64, lo_log: int = 16, hi_log: int = 26, seed: int = 64, device="cpu"):
+    """Columns of the mixed workload, generated with torch on `device`:
+    lengths log-uniform in [2^lo_log, 2^hi_log]; family i % 4 of
+    MIXED_FAMILIES: uniform in [0, 2^w) with w in {8, 12, 16, 20}; Zipf s=1.1
+    over [0, 2^20) (ranks truncated to 2^20, rank 1 -> 0); sorted keys with
+    geometric gaps (p=0.3); runs of geometric length (mean 16) of values in
+    [0, 2^16).  Returns [(family, int32 tensor)]."""
+    import torch
+    dev = torch.device(device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    lens = rng(seed)
+    k = torch.arange(1, (1 << 20) + 1, dtype=torch.float64, device=dev) ** -1.1
+    zcdf = torch.cumsum(k, 0)
+    zcdf /= zcdf[-1].clone()
+    cols = []
+    for i in range(n_cols):
+        n = int(2 ** lens.uniform(lo_log, hi_log))
+        fam = MIXED_FAMILIES[i % 4]
+        if fam == "uniform":
+            w = int(lens.choice([8, 12, 16, 20]))
+            v = torch.randint(0, 1 << w, (n,), generator=g, device=dev, dtype=torch.int64)
+        elif fam == "zipf":
+            v = torch.searchsorted(zcdf, torch.rand(n, generator=g, device=dev, dtype=torch.float64))
+            v = torch.clamp(v, max=(1 << 20) - 1)
+        elif fam == "sorted_gaps":
+            u = torch.rand(n, generator=g, device=dev, dtype=torch.float64)
+            gaps = torch.floor(torch.log1p(-u) / torch.log1p(torch.tensor(-0.3, dtype=torch.float64))) + 1
+            v = torch.cumsum(gaps.to(torch.int64), 0)
+        else:
+            starts = torch.rand(n, generator=g, device=dev) < 1.0 / 16.0
+            starts[0] = True
+            run = torch.cumsum(starts.to(torch.int64), 0) - 1
+            vals = torch.randint(0, 1 << 16, (int(run[-1]) + 1,), generator=g, device=dev, dtype=torch.int64)
+            v = vals[run]
+        cols.append((fam, v.to(torch.int32)))
+    return cols

@@ -67,6 +67,72 @@ def training_corpus(n_vectors: int, seed: int = 0) -> np.ndarray:
     return np.concatenate(parts)[: n_vectors * 1024]
 
 
+def _zipf_cdf(s_values, n_ranks: int, device):
+    """float64 CDFs of Zipf(s) truncated to ranks 1..n_ranks, one row per s."""
+    import torch
+    k = torch.arange(1, n_ranks + 1, dtype=torch.float64, device=device)
+    w = k[None, :] ** (-torch.as_tensor(s_values, dtype=torch.float64, device=device)[:, None])
+    c = torch.cumsum(w, dim=1)
+    return c / c[:, -1:]
+
+
+def corpus_device(n_vectors: int, seed: int = 0, device="cuda"):
+    """Training vectors of the mixed workload's four families plus constant
+    vectors, generated on `device` (int32 tensor of n_vectors * 1024 values,
+    vectors shuffled): uniform values in [base, base + 2^w) with w in [1, 31];
+    Zipf(s in [1.05, 2.5], truncated to 2^20 ranks) folded into [0, 2^[6, 24));
+    sorted keys with geometric gaps (p in [0.02, 0.95]) from a random start;
+    runs of geometric length (mean in [2, 96]) of values in [0, 2^[2, 25))."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    dev = torch.device(device)
+
+    def rnd(*shape):
+        return torch.rand(*shape, generator=g, device=dev, dtype=torch.float64)
+
+    def ints(lo, hi, *shape):
+        return torch.randint(lo, hi, shape, generator=g, device=dev, dtype=torch.int64)
+
+    fam = ints(0, 20, n_vectors)
+    fam = torch.where(fam < 19, fam % 4, torch.full_like(fam, 4))  # 1 in 20 vectors constant
+    out = torch.empty((n_vectors, 1024), dtype=torch.int32, device=dev)
+    s_grid = torch.linspace(1.05, 2.5, 16, dtype=torch.float64)
+    cdf = _zipf_cdf(s_grid, 1 << 20, dev)
+    for f in range(5):
+        idx = torch.nonzero(fam == f).flatten()
+        k = int(idx.numel())
+        if k == 0:
+            continue
+        if f == 0:
+            w = ints(1, 32, k, 1)
+            v = (ints(0, 1 << 32, k, 1024) & ((1 << w) - 1)) + ints(-(1 << 20), 1 << 20, k, 1)
+        elif f == 1:
+            which = ints(0, 16, k)
+            u = rnd(k, 1024)
+            v = torch.empty((k, 1024), dtype=torch.int64, device=dev)
+            for j in range(16):
+                rows = torch.nonzero(which == j).flatten()
+                if rows.numel():
+                    v[rows] = torch.searchsorted(cdf[j], u[rows].contiguous())
+            v = v % (1 << ints(6, 24, k, 1))
+        elif f == 2:
+            p = 0.02 + 0.93 * rnd(k, 1)
+            gaps = torch.floor(torch.log1p(-rnd(k, 1024)) / torch.log1p(-p)).to(torch.int64) + 1
+            v = torch.cumsum(gaps, dim=1) + ints(-(1 << 20), 1 << 20, k, 1)
+        elif f == 3:
+            mean = 2.0 + 94.0 * rnd(k, 1)
+            starts = rnd(k, 1024) < 1.0 / mean
+            starts[:, 0] = True
+            run = torch.cumsum(starts.to(torch.int64), dim=1) - 1
+            vals = ints(0, 1 << 32, k, 1024) & ((1 << ints(2, 25, k, 1)) - 1)
+            v = torch.gather(vals, 1, run)
+        else:
+            v = ints(-1000, 1000, k, 1).expand(k, 1024)
+        out[idx] = torch.clamp(v, -2**31, 2**31 - 1).to(torch.int32)
+    return out.reshape(-1)
+
+
 class LearnedSelector:
     """The MLP parameters on a device plus training / selection."""
 
