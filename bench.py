@@ -422,6 +422,7 @@ def run_mixed(a, dist: Dist):
 
     from fastlanesgpu_b200 import LAYOUT_TRANSPOSED, ORDER_ORIGINAL, EncodedColumn, datagen, ops
     from fastlanesgpu_b200.batch import Batch, graph_of
+    from fastlanesgpu_b200.column import encode_column_gpu
     from fastlanesgpu_b200.selector import LearnedSelector, corpus_device, gpu_features
     dev = torch.device("cuda", dist.local)
     stream = torch.cuda.current_stream()
@@ -461,23 +462,43 @@ def run_mixed(a, dist: Dist):
     enc_ex = [EncodedColumn.encode(h[:n], best, layout=LAYOUT_TRANSPOSED) for h, n, (_, best) in zip(host, lens, ex)]
     t2 = time.perf_counter()
     ex_select_s, ex_encode_s = t1 - t0, t2 - t1
-    # learned: upload, GPU statistics + MLP, exhaustive only below the threshold
-    cat = np.concatenate(host)
+    # learned, on the GPU: upload the raw columns, statistics + MLP, the
+    # exhaustive encoder only for low-confidence vectors, GPU encode.  Both
+    # arms start from the raw columns in pinned host memory.
+    cat_t = torch.empty(sum(h.size for h in host), dtype=torch.int32, pin_memory=True)
+    cat = cat_t.numpy()
+    np.concatenate(host, out=cat)
+    vstart = np.concatenate([[0], np.cumsum(n_vec)])
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
-    schemes, info = sel.select(cat, threshold=a.threshold)
+    cat_dev = cat_t.to(dev, non_blocking=True)
+    torch.cuda.synchronize()
     t1 = time.perf_counter()
-    splits = np.cumsum(n_vec)[:-1]
-    enc_ln = [EncodedColumn.encode(h[:n], sc, layout=LAYOUT_TRANSPOSED)
-              for h, n, sc in zip(host, lens, np.split(schemes, splits))]
+    schemes_dev, info = sel.select_device(cat_dev, cat, threshold=a.threshold)
     t2 = time.perf_counter()
-    ln_select_s, ln_encode_s = t1 - t0, t2 - t1
+    dcols = [encode_column_gpu(cat_dev[vstart[i] * 1024: vstart[i] * 1024 + lens[i]],
+                               schemes_dev[vstart[i]: vstart[i + 1]].contiguous(), layout=LAYOUT_TRANSPOSED)
+             for i in range(len(cols))]
+    torch.cuda.synchronize()
+    t3 = time.perf_counter()
+    ln_upload_s, ln_select_s, ln_encode_s = t1 - t0, t2 - t1, t3 - t2
+    # the exhaustive picks encoded on the GPU as well (selection is then the
+    # only difference between the arms)
+    t0 = time.perf_counter()
+    best_dev = torch.from_numpy(np.concatenate([b for _, b in ex])).to(dev)
+    ex_gpu = [encode_column_gpu(cat_dev[vstart[i] * 1024: vstart[i] * 1024 + lens[i]],
+                                best_dev[vstart[i]: vstart[i + 1]].contiguous(), layout=LAYOUT_TRANSPOSED)
+              for i in range(len(cols))]
+    torch.cuda.synchronize()
+    ex_gpu_encode_s = time.perf_counter() - t0 + ln_upload_s
     size_ex = sum(c.nbytes for c in enc_ex)
-    size_ln = sum(c.nbytes for c in enc_ln)
+    size_ex_gpu = sum(c.nbytes for c in ex_gpu)
+    size_ln = sum(c.nbytes for c in dcols)
     size_for = sum(int(sz[:, 0].astype(np.int64).sum()) for sz, _ in ex)  # bit-packing only
-    del cat
+    schemes_ln = schemes_dev.cpu().numpy()
+    del cat, cat_t, cat_dev, ex_gpu, best_dev
 
     # lossless: decode every learned column on the GPU and compare
-    dcols = [c.to_device(dev) for c in enc_ln]
     lossless = all(torch.equal(ops.unpack_global(dc, order=ORDER_ORIGINAL)[:n], v)
                    for dc, n, (_, v) in zip(dcols, lens, cols))
 
@@ -534,9 +555,9 @@ def run_mixed(a, dist: Dist):
     per_query_ms = timed(per_query, max(3, a.steps // 10))
     # end to end: encoded columns H2D, the batch, results D2H
     copies = []
-    for c, dc in zip(enc_ln, dcols):
-        copies.append((dc.data, torch.from_numpy(c.words.view("int32")).pin_memory()))
-        copies.append((dc.meta, torch.from_numpy(c.meta.view(np.uint8)).pin_memory()))
+    for dc in dcols:
+        copies.append((dc.data, dc.data.cpu().pin_memory()))
+        copies.append((dc.meta, dc.meta.cpu().pin_memory()))
     host_res = torch.empty(res.numel(), dtype=torch.int64).pin_memory()
 
     def e2e():
@@ -548,7 +569,7 @@ def run_mixed(a, dist: Dist):
     clk = clocks.stop()
 
     q_rows = sum(lens[c] for c, _, _, _ in queries)
-    q_bytes = sum(enc_ln[c].nbytes for c, _, _, _ in queries)
+    q_bytes = sum(dcols[c].nbytes for c, _, _, _ in queries)
     peak, peak_src = measured_peak_gbs()
     achieved = q_bytes / (batch_ms / 1e3) / 1e9
     return {
@@ -562,13 +583,20 @@ def run_mixed(a, dist: Dist):
                    "l2": "columns larger than L2 (126 MB) in total, no flush", "parallelism": "1 GPU"},
         "learned_encoding": {
             "bytes_exhaustive": size_ex, "bytes_learned": size_ln, "bytes_bitpack_only": size_for,
+            "bytes_exhaustive_gpu_encoder": size_ex_gpu,
             "regret": size_ln / size_ex - 1.0,
-            "select_s_exhaustive": ex_select_s, "select_s_learned": ln_select_s,
-            "encode_s_exhaustive": ex_select_s + ex_encode_s, "encode_s_learned": ln_select_s + ln_encode_s,
-            "select_speedup": ex_select_s / ln_select_s,
-            "encode_speedup": (ex_select_s + ex_encode_s) / (ln_select_s + ln_encode_s),
+            "scheme_counts_learned": np.bincount(schemes_ln, minlength=5).tolist(),
+            "scheme_counts_exhaustive": np.bincount(np.concatenate([b for _, b in ex]), minlength=5).tolist(),
+            "exhaustive": {"where": f"host, {threads} threads", "select_s": ex_select_s, "encode_s": ex_encode_s,
+                           "total_s": ex_select_s + ex_encode_s},
+            "learned": {"where": "GPU (upload, statistics, MLP, encode) + host exhaustive fallback",
+                        "upload_s": ln_upload_s, "select_s": ln_select_s, "encode_s": ln_encode_s,
+                        "total_s": ln_upload_s + ln_select_s + ln_encode_s,
+                        "parts_s": {k: v for k, v in info.items() if k.endswith("_s")}},
+            "exhaustive_select_then_gpu_encode_s": ex_select_s + ex_gpu_encode_s,
+            "encode_speedup": (ex_select_s + ex_encode_s) / (ln_upload_s + ln_select_s + ln_encode_s),
+            "select_speedup": ex_select_s / (ln_upload_s + ln_select_s),
             "fallback_vectors": info["fallback_vectors"], "vectors": info["vectors"], "threshold": a.threshold,
-            "host_threads": threads, "learned_parts_s": {k: v for k, v in info.items() if k.endswith("_s")},
             "lossless": bool(lossless), "training": training},
         "batched": {"ms_batch_graph": batch_ms, "ms_per_query_launches": per_query_ms,
                     "speedup": per_query_ms / batch_ms, "queries": len(queries), "work_items": batch.n_items,

@@ -124,6 +124,69 @@ class DeviceColumn:
         return self.host.nbytes
 
 
+class DeviceEncodedColumn:
+    """A per-vector encoded column produced on the GPU (fls_encode_column_gpu):
+    the device words and metadata with their C descriptor; same interface as
+    DeviceColumn."""
+
+    def __init__(self, data, meta, n_values: int, layout: int, payload_words: int, max_vec_words: int,
+                 scheme_mask: int):
+        self.host = None
+        self.data, self.meta = data, meta
+        self._n_values, self.layout, self.payload_words = n_values, layout, payload_words
+        self.desc = Column(data=data.data_ptr(), meta=meta.data_ptr(), n_values=n_values, n_words=int(data.numel()),
+                           layout=layout, scheme=0, bw=0, base=0, max_vec_words=max_vec_words,
+                           scheme_mask=scheme_mask)
+
+    @property
+    def n_values(self) -> int:
+        return self._n_values
+
+    @property
+    def n_vec(self) -> int:
+        return n_vectors(self._n_values)
+
+    @property
+    def nbytes(self) -> int:
+        return self.payload_words * 4 + self.n_vec * 16
+
+    def to_host(self) -> EncodedColumn:
+        """The same column as a host EncodedColumn (words and metadata copied back)."""
+        words = self.data.cpu().numpy().view(np.uint32).copy()
+        meta = self.meta.cpu().numpy().view(META_DTYPE).copy()
+        return EncodedColumn(words=words, meta=meta, n_values=self._n_values, layout=self.layout,
+                             max_vec_words=self.desc.max_vec_words, scheme_mask=self.desc.scheme_mask,
+                             payload_words=self.payload_words)
+
+
+def encode_column_gpu(values, schemes=0, layout: int = LAYOUT_TRANSPOSED, round4: bool = False,
+                      compact: bool = True) -> DeviceEncodedColumn:
+    """Encodes a device int32 column on the GPU: `schemes` is one scheme for
+    every vector or a device uint8 tensor with one per vector (for example the
+    learned selector's picks).  compact=True trims the output to the payload."""
+    import torch
+    n = int(values.numel())
+    nv = n_vectors(n)
+    dev = values.device
+    bound = int(lib().fls_encode_bound_words(n))
+    out = torch.empty(bound + 4, dtype=torch.int32, device=dev)
+    meta = torch.empty(nv * 4, dtype=torch.int32, device=dev)
+    info = torch.zeros(3, dtype=torch.int64, device=dev)
+    ws_bytes = int(lib().fls_encode_gpu_workspace_bytes(n))
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    per_vec = not isinstance(schemes, (int, np.integer))
+    if per_vec:
+        assert schemes.dtype == torch.uint8 and schemes.numel() == nv and schemes.device == dev
+    check(lib().fls_encode_column_gpu(values.data_ptr(), n, schemes.data_ptr() if per_vec else None,
+                                      0 if per_vec else int(schemes), layout, int(round4), out.data_ptr(), bound + 4,
+                                      meta.data_ptr(), info.data_ptr(), ws.data_ptr(), ws_bytes,
+                                      torch.cuda.current_stream().cuda_stream), "fls_encode_column_gpu")
+    total, mx, mask = (int(x) for x in info.cpu())
+    if compact:
+        out = out[:max(total, 4)].clone()
+    return DeviceEncodedColumn(out, meta, n, layout, total, mx, mask)
+
+
 def columns_array(cols) -> ctypes.Array:
     arr = (Column * len(cols))()
     for i, c in enumerate(cols):
@@ -131,5 +194,6 @@ def columns_array(cols) -> ctypes.Array:
     return arr
 
 
-__all__ = ["EncodedColumn", "DeviceColumn", "META_DTYPE", "columns_array", "n_vectors", "_lib",
+__all__ = ["EncodedColumn", "DeviceColumn", "DeviceEncodedColumn", "encode_column_gpu", "META_DTYPE", "columns_array",
+           "n_vectors", "_lib",
            "SCHEME_DELTA", "LAYOUT_TRANSPOSED"]

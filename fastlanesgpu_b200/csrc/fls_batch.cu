@@ -1,14 +1,16 @@
 // fls_batch.cu -- batched persistent execution of many filter-aggregate queries
 // over many columns of uneven length and bit width in one launch.
 //
-// The host cuts every query (filter lo <= x <= hi on one column, sum of
-// another column of the same length) into work items of `chunk` consecutive
+// The host groups queries (filter lo <= x <= hi on one column, sum of another
+// column of the same length) that read the same pair of columns, up to four
+// per group, and cuts every group into work items of `chunk` consecutive
 // vectors.  One persistent kernel runs all items: each warp pulls the next item
 // from a global counter (dynamic load balancing across columns of very
-// different lengths), streams the item's vectors through its own two-slot
-// bulk-copy pipeline, and adds the item's sum and count into the query's
-// result with one atomic each.  fls_batch_run only resets the counter and
-// launches, so it can be captured into a CUDA graph and replayed.
+// different lengths), streams the item's vectors through its own bulk-copy
+// pipeline, decodes each vector once into registers, evaluates every query of
+// the group on those values, and adds each query's sum and count into its
+// result with one atomic each per item.  fls_batch_run only resets the counter
+// and launches, so it can be captured into a CUDA graph and replayed.
 //
 // No reference counterpart: the reference launches one grid per query
 // (fls_q11.cu:150-160).
@@ -20,10 +22,20 @@
 
 #include "fls_pipeline.cuh"
 
+namespace fls {
+// Queries sharing one (filter column, aggregated column) pair.
+constexpr uint32_t kGroupQueries = 4;
+struct BatchGroup {
+	uint32_t col, agg_col, n_q, pad;
+	uint32_t q[kGroupQueries];
+};
+} // namespace fls
+
 struct fls_batch {
-	std::vector<fls::DevCol>    cols;
+	std::vector<fls::DevCol>     cols;
 	std::vector<fls_batch_query> queries;
-	std::vector<uint4>           items; // {query, first vector, end vector, 0}
+	std::vector<fls::BatchGroup> groups;
+	std::vector<uint4>           items; // {group, first vector, end vector, 0}
 	uint32_t                     slot_words = 0;
 	uint32_t                     has_dict   = 0;
 	void*                        ws         = nullptr; // device workspace after upload
@@ -38,6 +50,7 @@ constexpr uint32_t kBatchStages = 3;
 struct BatchParams {
 	const DevCol*          cols;
 	const fls_batch_query* queries;
+	const BatchGroup*      groups;
 	const uint4*           items;
 	uint32_t               n_items;
 	uint32_t*              counter;
@@ -106,22 +119,30 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) batch_kernel(const __grid_c
 		if (lane == 0) { item = atomicAdd(P.counter, 1u); }
 		item = __shfl_sync(0xffffffffu, item, 0);
 		if (item >= P.n_items) { break; }
-		const uint4            it = P.items[item];
-		const fls_batch_query& q  = P.queries[it.x];
-		const DevCol&          cf = P.cols[q.col];
-		const DevCol&          ca = P.cols[q.agg_col];
-		const uint64_t         v0 = it.y, v1 = it.z;
-		const uint32_t         lo = static_cast<uint32_t>(q.lo), range = static_cast<uint32_t>(q.hi) - lo;
-		const bool             empty = q.lo > q.hi;
-		const bool             same  = q.col == q.agg_col;
+		const uint4       it = P.items[item];
+		const BatchGroup  gr = P.groups[it.x];
+		const DevCol&     cf = P.cols[gr.col];
+		const DevCol&     ca = P.cols[gr.agg_col];
+		const uint64_t    v0 = it.y, v1 = it.z;
+		const bool        same = gr.col == gr.agg_col;
+		const uint64_t    rows = P.queries[gr.q[0]].n_values;
+		uint32_t          lo[kGroupQueries], range[kGroupQueries];
+		bool              live[kGroupQueries];
+#pragma unroll
+		for (uint32_t j = 0; j < kGroupQueries; ++j) {
+			const fls_batch_query& q = P.queries[gr.q[j < gr.n_q ? j : 0]];
+			lo[j]    = static_cast<uint32_t>(q.lo);
+			range[j] = static_cast<uint32_t>(q.hi) - lo[j];
+			live[j]  = j < gr.n_q && q.lo <= q.hi;
+		}
 		// prologue
 		uint32_t s_issue = st;
 		for (uint32_t k = 0; k < kBatchStages && v0 + k < v1; ++k) {
 			batch_issue(P, base, L, s_issue, cf, ca, same, v0 + k, lane, pol);
 			s_issue = (s_issue + 1u == kBatchStages) ? 0u : s_issue + 1u;
 		}
-		long long          sum = 0;
-		unsigned long long cnt = 0;
+		long long          sum[kGroupQueries] = {0, 0, 0, 0};
+		uint32_t           cnt[kGroupQueries] = {0, 0, 0, 0}; // at most 32 * chunk per lane
 		for (uint64_t v = v0; v < v1; ++v) {
 			if (!dev::mbar_wait_bounded(bars + st, phase, kWaitPolls)) {
 				raise_err(P.err, kErrTimeout);
@@ -133,7 +154,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) batch_kernel(const __grid_c
 			}
 			const uint4* info = reinterpret_cast<const uint4*>(base + L.info) + st * 2u;
 			const uint4  fi = info[0], ai = same ? info[0] : info[1];
-			if ((fi.y & 0xffu) != kBadScheme && (ai.y & 0xffu) != kBadScheme && !empty) {
+			if ((fi.y & 0xffu) != kBadScheme && (ai.y & 0xffu) != kBadScheme) {
 				VecInfo vf {}, va {};
 				vf.base = static_cast<int32_t>(fi.x), vf.scheme = fi.y & 0xffu, vf.bw = (fi.y >> 8) & 0xffu;
 				vf.aux  = fi.y >> 16;
@@ -142,36 +163,41 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) batch_kernel(const __grid_c
 				const uint32_t* sf = base + L.slots + (st * 2u) * P.slot_words;
 				const uint32_t* sa = same ? sf : sf + P.slot_words;
 				// rows of a partial last vector
-				const uint64_t rows  = q.n_values;
-				uint32_t       mask  = 0xffffffffu;
+				uint32_t valid = 0xffffffffu;
 				if ((v + 1) * 1024u > rows) {
-					mask = dev::tail_rows(cf.layout, lane, static_cast<uint32_t>(rows - v * 1024u));
+					valid = dev::tail_rows(cf.layout, lane, static_cast<uint32_t>(rows - v * 1024u));
 				}
-				const uint32_t flo = lo - dev::value_offset(vf);
-				uint32_t       m[4] = {0, 0, 0, 0};
-				dev::decode_each<false>(sf, vf, base + L.dict, lane,
-				                        [&](int r, uint32_t x) { m[r & 3] |= (x - flo <= range ? 1u : 0u) << r; });
-				mask &= (m[0] | m[1]) | (m[2] | m[3]);
-				cnt += static_cast<unsigned>(__popc(mask));
-				if (__reduce_max_sync(0xffffffffu, __popc(mask)) <= 4 && va.scheme == FLS_SCHEME_FOR) {
-					dev::ForRows ra;
-					ra.init(sa, va, lane);
-					const int n_it = __reduce_max_sync(0xffffffffu, __popc(mask));
-					uint32_t  mm   = mask;
-					for (int k = 0; k < n_it; ++k) {
-						const bool     have = mm != 0u;
-						const uint32_t r    = have ? static_cast<uint32_t>(__ffs(mm)) - 1u : 0u;
-						mm &= mm - 1u;
-						const long long x = static_cast<int32_t>(ra.get(r));
-						sum += have ? x : 0ll;
+				// Decode once; every query of the group reads the registers:
+				// row masks first, then the sums (over the same values, or over
+				// the aggregated column decoded row by row into the sums).
+				uint32_t x[32];
+				dev::decode_vals(sf, vf, base + L.dict, lane, x);
+				uint32_t m[kGroupQueries];
+#pragma unroll
+				for (uint32_t j = 0; j < kGroupQueries; ++j) {
+					uint32_t mj = 0;
+#pragma unroll
+					for (int r = 0; r < 32; ++r) { mj |= (x[r] - lo[j] <= range[j] ? 1u : 0u) << r; }
+					m[j] = live[j] ? (mj & valid) : 0u;
+					cnt[j] += static_cast<unsigned>(__popc(m[j]));
+				}
+				long long p[kGroupQueries] = {0, 0, 0, 0};
+				if (same) {
+#pragma unroll
+					for (int r = 0; r < 32; ++r) {
+						const long long a = static_cast<int32_t>(x[r]);
+#pragma unroll
+						for (uint32_t j = 0; j < kGroupQueries; ++j) { p[j] += ((m[j] >> r) & 1u) ? a : 0ll; }
 					}
-				} else if (__any_sync(0xffffffffu, mask)) {
-					long long p[4] = {0, 0, 0, 0};
-					dev::decode_each<true>(sa, va, base + L.dict, lane, [&](int r, uint32_t x) {
-						p[r & 3] += ((mask >> r) & 1u) ? static_cast<long long>(static_cast<int32_t>(x)) : 0ll;
+				} else {
+					dev::decode_each<true>(sa, va, base + L.dict, lane, [&](int r, uint32_t y) {
+						const long long a = static_cast<int32_t>(y);
+#pragma unroll
+						for (uint32_t j = 0; j < kGroupQueries; ++j) { p[j] += ((m[j] >> r) & 1u) ? a : 0ll; }
 					});
-					sum += (p[0] + p[1]) + (p[2] + p[3]);
 				}
+#pragma unroll
+				for (uint32_t j = 0; j < kGroupQueries; ++j) { sum[j] += p[j]; }
 			}
 			__syncwarp();
 			if (v + kBatchStages < v1) {
@@ -183,11 +209,15 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) batch_kernel(const __grid_c
 				phase ^= 1u;
 			}
 		}
-		const unsigned long long s = warp_sum_u64(static_cast<unsigned long long>(sum));
-		const unsigned long long c = warp_sum_u64(cnt);
-		if (lane == 0) {
-			if (s) { atomicAdd(reinterpret_cast<unsigned long long*>(P.results + 2u * it.x), s); }
-			if (c) { atomicAdd(reinterpret_cast<unsigned long long*>(P.results + 2u * it.x + 1u), c); }
+#pragma unroll
+		for (uint32_t j = 0; j < kGroupQueries; ++j) {
+			if (j >= gr.n_q) { break; }
+			const unsigned long long s = warp_sum_u64(static_cast<unsigned long long>(sum[j]));
+			const unsigned long long c = warp_sum_u64(cnt[j]);  // widened before the warp sum
+			if (lane == 0) {
+				if (s) { atomicAdd(reinterpret_cast<unsigned long long*>(P.results + 2u * gr.q[j]), s); }
+				if (c) { atomicAdd(reinterpret_cast<unsigned long long*>(P.results + 2u * gr.q[j] + 1u), c); }
+			}
 		}
 	}
 }
@@ -195,11 +225,12 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) batch_kernel(const __grid_c
 size_t ws_align(size_t x) { return (x + 255u) & ~static_cast<size_t>(255u); }
 
 struct WsLayout {
-	size_t cols, queries, items, counter, total;
+	size_t cols, queries, groups, items, counter, total;
 	explicit WsLayout(const fls_batch& b) {
 		cols    = 0;
 		queries = cols + ws_align(b.cols.size() * sizeof(DevCol));
-		items   = queries + ws_align(b.queries.size() * sizeof(fls_batch_query));
+		groups  = queries + ws_align(b.queries.size() * sizeof(fls_batch_query));
+		items   = groups + ws_align(b.groups.size() * sizeof(BatchGroup));
 		counter = items + ws_align(b.items.size() * sizeof(uint4));
 		total   = counter + 256;
 	}
@@ -208,8 +239,9 @@ struct WsLayout {
 } // namespace
 
 // Shared by fls_batch_run and its static-scratch variant.
-fls_status batch_launch(const fls_batch* b, const DevCol* cols, const fls_batch_query* queries, const uint4* items,
-                        uint32_t* counter, int64_t* d_results, cudaStream_t st) {
+fls_status batch_launch(const fls_batch* b, const DevCol* cols, const fls_batch_query* queries,
+                        const BatchGroup* groups, const uint4* items, uint32_t* counter, int64_t* d_results,
+                        cudaStream_t st) {
 	DeviceInfo di;
 	fls_status s = device_info(di);
 	if (s != FLS_OK) { return s; }
@@ -243,6 +275,7 @@ fls_status batch_launch(const fls_batch* b, const DevCol* cols, const fls_batch_
 	BatchParams P;
 	P.cols       = cols;
 	P.queries    = queries;
+	P.groups     = groups;
 	P.items      = items;
 	P.n_items    = static_cast<uint32_t>(b->items.size());
 	P.counter    = counter;
@@ -266,8 +299,8 @@ extern "C" {
 
 fls_status fls_batch_create(const fls_column* cols, uint32_t n_cols, const fls_batch_query* queries,
                             uint32_t n_queries, uint32_t chunk_vectors, fls_batch** out) {
-	if (!cols || !queries || !out || n_cols == 0 || chunk_vectors == 0) {
-		return set_error(FLS_ERR_INVALID_ARG, "fls_batch_create: bad arguments");
+	if (!cols || !queries || !out || n_cols == 0 || chunk_vectors == 0 || chunk_vectors > (1u << 20)) {
+		return set_error(FLS_ERR_INVALID_ARG, "fls_batch_create: bad arguments (chunk_vectors in [1, 2^20])");
 	}
 	fls_batch* b = new (std::nothrow) fls_batch;
 	if (!b) { return set_error(FLS_ERR_CAPACITY, "out of host memory"); }
@@ -286,6 +319,7 @@ fls_status fls_batch_create(const fls_column* cols, uint32_t n_cols, const fls_b
 	}
 	b->slot_words = (slot + 3u) & ~3u;
 	b->queries.assign(queries, queries + n_queries);
+	std::vector<int64_t> open_group(static_cast<size_t>(n_cols) * n_cols, -1); // (col, agg) -> group being filled
 	for (uint32_t q = 0; q < n_queries; ++q) {
 		fls_batch_query& bq = b->queries[q];
 		if (bq.col >= n_cols || bq.agg_col >= n_cols || cols[bq.col].n_values != cols[bq.agg_col].n_values ||
@@ -293,10 +327,19 @@ fls_status fls_batch_create(const fls_column* cols, uint32_t n_cols, const fls_b
 			delete b;
 			return set_error(FLS_ERR_INVALID_ARG, "batch query names missing or mismatched columns");
 		}
-		bq.n_values          = cols[bq.col].n_values;
-		const uint64_t n_vec = (bq.n_values + 1023u) / 1024u;
+		bq.n_values    = cols[bq.col].n_values;
+		int64_t& slot_g = open_group[static_cast<size_t>(bq.col) * n_cols + bq.agg_col];
+		if (slot_g < 0 || b->groups[static_cast<size_t>(slot_g)].n_q == kGroupQueries) {
+			slot_g = static_cast<int64_t>(b->groups.size());
+			b->groups.push_back(BatchGroup {bq.col, bq.agg_col, 0u, 0u, {0u, 0u, 0u, 0u}});
+		}
+		BatchGroup& g    = b->groups[static_cast<size_t>(slot_g)];
+		g.q[g.n_q++] = q;
+	}
+	for (uint32_t gi = 0; gi < b->groups.size(); ++gi) {
+		const uint64_t n_vec = (cols[b->groups[gi].col].n_values + 1023u) / 1024u;
 		for (uint64_t v = 0; v < n_vec; v += chunk_vectors) {
-			b->items.push_back(make_uint4(q, static_cast<uint32_t>(v),
+			b->items.push_back(make_uint4(gi, static_cast<uint32_t>(v),
 			                              static_cast<uint32_t>(std::min<uint64_t>(n_vec, v + chunk_vectors)), 0u));
 		}
 	}
@@ -320,6 +363,10 @@ fls_status fls_batch_upload(fls_batch* b, void* d_workspace, uint64_t workspace_
 		s = cuda_check(cudaMemcpyAsync(w + L.queries, b->queries.data(), b->queries.size() * sizeof(fls_batch_query),
 		                               cudaMemcpyHostToDevice, st), "upload queries");
 	}
+	if (s == FLS_OK && !b->groups.empty()) {
+		s = cuda_check(cudaMemcpyAsync(w + L.groups, b->groups.data(), b->groups.size() * sizeof(BatchGroup),
+		                               cudaMemcpyHostToDevice, st), "upload groups");
+	}
 	if (s == FLS_OK && !b->items.empty()) {
 		s = cuda_check(cudaMemcpyAsync(w + L.items, b->items.data(), b->items.size() * sizeof(uint4),
 		                               cudaMemcpyHostToDevice, st), "upload items");
@@ -336,9 +383,10 @@ fls_status fls_batch_run(const fls_batch* b, int64_t* d_results, fls_stream_t st
 	if (!b || !d_results || !b->ws) { return set_error(FLS_ERR_INVALID_ARG, "fls_batch_run: not uploaded"); }
 	const WsLayout L(*b);
 	char*          w = static_cast<char*>(b->ws);
-	return batch_launch(b, reinterpret_cast<const DevCol*>(w + L.cols), reinterpret_cast<const fls_batch_query*>(w + L.queries),
-	                    reinterpret_cast<const uint4*>(w + L.items), reinterpret_cast<uint32_t*>(w + L.counter), d_results,
-	                    reinterpret_cast<cudaStream_t>(stream));
+	return batch_launch(b, reinterpret_cast<const DevCol*>(w + L.cols),
+	                    reinterpret_cast<const fls_batch_query*>(w + L.queries),
+	                    reinterpret_cast<const BatchGroup*>(w + L.groups), reinterpret_cast<const uint4*>(w + L.items),
+	                    reinterpret_cast<uint32_t*>(w + L.counter), d_results, reinterpret_cast<cudaStream_t>(stream));
 }
 
 void fls_batch_destroy(fls_batch* b) { delete b; }

@@ -201,14 +201,17 @@ class LearnedSelector:
                                   _stream()), "fls_mlp_infer")
         return best, conf
 
-    def select(self, values: np.ndarray, threshold: float = 0.9, values_dev=None):
+    def select(self, values: np.ndarray, threshold: float = 0.9, values_dev=None, values_pinned=None):
         """Scheme per vector of a host column: the MLP's pick, or the exhaustive
-        choice where the MLP's confidence is below `threshold`.  Returns
-        (schemes, info) with the timing of each part."""
+        choice where the MLP's confidence is below `threshold`.  The column is
+        uploaded from `values_pinned` (a pinned host tensor holding `values`)
+        when given.  Returns (schemes, info) with the timing of each part."""
         import torch
         t0 = time.perf_counter()
         if values_dev is None:
-            values_dev = torch.from_numpy(np.ascontiguousarray(values, dtype=np.int32)).to(self.device)
+            src = values_pinned if values_pinned is not None else torch.from_numpy(
+                np.ascontiguousarray(values, dtype=np.int32))
+            values_dev = src.to(self.device, non_blocking=values_pinned is not None)
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         feats = gpu_features(values_dev)
@@ -224,6 +227,26 @@ class LearnedSelector:
         t3 = time.perf_counter()
         return schemes, {"upload_s": t1 - t0, "gpu_select_s": t2 - t1, "fallback_s": t3 - t2,
                          "fallback_vectors": int(low.size), "vectors": int(schemes.size)}
+
+    def select_device(self, values_dev, values_host: np.ndarray, threshold: float = 0.9):
+        """Scheme per vector of a device column without leaving the device:
+        the MLP's picks (device uint8), replaced by the exhaustive encoder's
+        choice (computed on `values_host`, the same values) where the
+        confidence is below `threshold`.  Returns (schemes_dev, info)."""
+        import torch
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        best, conf = self.predict(gpu_features(values_dev))
+        low = torch.nonzero(conf < threshold).flatten().cpu().numpy()
+        t1 = time.perf_counter()
+        if low.size:
+            sub = np.concatenate([_vector(values_host, int(v)) for v in low])
+            _, sub_best = encode_exhaustive(sub)
+            best[torch.from_numpy(low).to(best.device)] = torch.from_numpy(sub_best).to(best.device)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        return best, {"gpu_select_s": t1 - t0, "fallback_s": t2 - t1, "fallback_vectors": int(low.size),
+                      "vectors": int(best.numel())}
 
     def state(self) -> np.ndarray:
         return self.params.cpu().numpy()

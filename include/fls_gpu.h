@@ -135,6 +135,21 @@ fls_status fls_encode_column(const int32_t* values, uint64_t n, const uint8_t* s
                              uint32_t layout, int round4, uint32_t* out, uint64_t* out_words, fls_vec_meta* meta,
                              uint32_t* max_vec_words, uint32_t* scheme_mask);
 
+/* The same encoder on the GPU, for a column already in device memory:
+ * identical words and metadata to fls_encode_column.  d_schemes (device, one
+ * per vector) may be NULL to use `scheme` for every vector; an out-of-range
+ * per-vector scheme is encoded as FOR and flagged in the device error word.
+ * d_out holds at least fls_encode_bound_words(n) words; d_meta n_vec entries
+ * (both 16-byte aligned); d_info (device uint64[3]) receives the payload words
+ * written, the largest vector's words and the scheme mask.  d_workspace holds
+ * fls_encode_gpu_workspace_bytes(n) bytes.  Stream-ordered; no reference
+ * counterpart (the reference encodes on the host, pack.cpp:29607). */
+uint64_t   fls_encode_gpu_workspace_bytes(uint64_t n);
+fls_status fls_encode_column_gpu(const int32_t* d_values, uint64_t n, const uint8_t* d_schemes, uint32_t scheme,
+                                 uint32_t layout, int round4, uint32_t* d_out, uint64_t out_capacity_words,
+                                 fls_vec_meta* d_meta, uint64_t* d_info, void* d_workspace, uint64_t workspace_bytes,
+                                 fls_stream_t stream);
+
 /* Exhaustive per-vector encoder (the selector's judge): exact encoded size in
  * bytes (payload + 16 B metadata) of every scheme for every vector
  * (sizes: n_vec*5, UINT32_MAX = not representable) and the argmin scheme, ties
