@@ -41,9 +41,9 @@ def parse_args():
     ap.add_argument("--workload", choices=["q11", "q21", "decode", "mixed"], default="q11")
     ap.add_argument("--rows", type=int, default=0, help="rows per GPU (0 = 2^27 for queries, 2^28 for decode)")
     ap.add_argument("--decode-bw", type=int, default=16, help="bit width of the FOR decode workload")
-    ap.add_argument("--decode-scheme", choices=["for", "delta", "rle"], default="for",
+    ap.add_argument("--decode-scheme", choices=["for", "delta", "rle", "dict"], default="for",
                     help="decode input: uniform FOR bit-packing, delta over sorted keys (geometric gaps p=0.3), "
-                         "RLE (geometric runs of mean 16, values in [0,2^16))")
+                         "RLE (geometric runs of mean 16, values in [0,2^16)), dictionary (Zipf 1.1 over 2^20)")
     ap.add_argument("--decode-out", choices=["sum", "hbm"], default="sum",
                     help="decode fused with a uint64 sum, or decode to HBM")
     ap.add_argument("--e2e-steps", type=int, default=10)
@@ -60,6 +60,8 @@ def parse_args():
     ap.add_argument("--queries", type=int, default=256, help="mixed workload: batched filter-aggregate queries")
     ap.add_argument("--threshold", type=float, default=0.9, help="selector confidence below which the "
                                                                     "exhaustive encoder decides")
+    ap.add_argument("--decode-kappa", type=float, default=0.03,
+                    help="training labels: argmin size * (1 + kappa * (decode cost - 1))")
     a = ap.parse_args()
     if not a.rows:
         a.rows = (1 << 28) if a.workload == "decode" else (1 << 27)
@@ -252,10 +254,15 @@ def run_ours(a, dist: Dist):
             vals = datagen.sorted_geometric(a.rows, p=0.3, seed=seed)
             hcols = [EncodedColumn.encode(vals, SCHEME_DELTA, layout=LAYOUT_TRANSPOSED)]
             what, key = "delta over sorted keys with geometric gaps (p=0.3), per-vector bw", "delta"
-        else:
+        elif a.decode_scheme == "rle":
             vals = datagen.geometric_runs(a.rows, mean_run=16.0, value_bits=16, seed=seed)
             hcols = [EncodedColumn.encode(vals, SCHEME_RLE, layout=LAYOUT_TRANSPOSED)]
             what, key = "RLE, geometric runs (mean 16) of values in [0,2^16)", "rle"
+        else:
+            from fastlanesgpu_b200 import SCHEME_DICT
+            vals = datagen.zipf_device(a.rows, s=1.1, domain=1 << 20, seed=seed, device=dev).cpu().numpy()
+            hcols = [EncodedColumn.encode(vals, SCHEME_DICT, layout=LAYOUT_TRANSPOSED)]
+            what, key = "dictionary, Zipf 1.1 over [0,2^20)", "dict"
         del vals
         dcols = [c.to_device(dev) for c in hcols]
         if a.decode_out == "sum":
@@ -423,7 +430,7 @@ def run_mixed(a, dist: Dist):
     from fastlanesgpu_b200 import LAYOUT_TRANSPOSED, ORDER_ORIGINAL, EncodedColumn, datagen, ops
     from fastlanesgpu_b200.batch import Batch, graph_of
     from fastlanesgpu_b200.column import encode_column_gpu
-    from fastlanesgpu_b200.selector import LearnedSelector, corpus_device, gpu_features
+    from fastlanesgpu_b200.selector import LearnedSelector, corpus_device, decode_aware_labels, gpu_features
     dev = torch.device("cuda", dist.local)
     stream = torch.cuda.current_stream()
     ops.set_tuning(1, a.jit)
@@ -438,14 +445,15 @@ def run_mixed(a, dist: Dist):
     train_dev = corpus_device(a.train_vectors, seed=7, device=dev)
     train_host = train_dev.cpu().numpy()
     t1 = now()
-    _, labels = ops.encode_exhaustive(train_host)
+    tr_sizes, _ = ops.encode_exhaustive(train_host)
+    labels = decode_aware_labels(tr_sizes, a.decode_kappa)
     t2 = now()
     sel = LearnedSelector(device=dev, seed=1)
     feats = gpu_features(train_dev)
     losses = sel.train(feats, torch.from_numpy(labels).to(dev), epochs=a.train_epochs, batch=4096, lr=3e-3)
     t3 = now()
     del train_dev, train_host, feats
-    training = {"vectors": a.train_vectors, "epochs": a.train_epochs, "batch": 4096,
+    training = {"vectors": a.train_vectors, "epochs": a.train_epochs, "batch": 4096, "decode_kappa": a.decode_kappa,
                 "corpus_gen_s": t1 - t0, "exhaustive_label_s": t2 - t1, "gpu_train_s": t3 - t2,
                 "loss_first_epoch": losses[0], "loss_last_epoch": losses[-1]}
 
@@ -474,7 +482,7 @@ def run_mixed(a, dist: Dist):
     cat_dev = cat_t.to(dev, non_blocking=True)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
-    schemes_dev, info = sel.select_device(cat_dev, cat, threshold=a.threshold)
+    schemes_dev, info = sel.select_device(cat_dev, cat, threshold=a.threshold, kappa=a.decode_kappa)
     t2 = time.perf_counter()
     dcols = [encode_column_gpu(cat_dev[vstart[i] * 1024: vstart[i] * 1024 + lens[i]],
                                schemes_dev[vstart[i]: vstart[i + 1]].contiguous(), layout=LAYOUT_TRANSPOSED)
@@ -496,7 +504,7 @@ def run_mixed(a, dist: Dist):
     size_ln = sum(c.nbytes for c in dcols)
     size_for = sum(int(sz[:, 0].astype(np.int64).sum()) for sz, _ in ex)  # bit-packing only
     schemes_ln = schemes_dev.cpu().numpy()
-    del cat, cat_t, cat_dev, ex_gpu, best_dev
+    del cat, cat_t, cat_dev, best_dev
 
     # lossless: decode every learned column on the GPU and compare
     lossless = all(torch.equal(ops.unpack_global(dc, order=ORDER_ORIGINAL)[:n], v)
@@ -553,6 +561,15 @@ def run_mixed(a, dist: Dist):
     launches = per_run * a.steps
     clocks.mark(w0, w1)
     per_query_ms = timed(per_query, max(3, a.steps // 10))
+    # the same queries over the exhaustive encoder's columns (decode cost of
+    # the two encodings)
+    batch_ex = Batch(ex_gpu, queries)
+    graph_ex = graph_of(batch_ex.run)
+    graph_ex.replay()
+    torch.cuda.synchronize()
+    exact = exact and [(int(s_), int(n_)) for s_, n_ in batch_ex.results.view(-1, 2).cpu().tolist()] == want
+    batch_ex_ms = timed(graph_ex.replay, max(3, a.steps // 5))
+    del graph_ex, batch_ex
     # end to end: encoded columns H2D, the batch, results D2H
     copies = []
     for dc in dcols:
@@ -599,6 +616,7 @@ def run_mixed(a, dist: Dist):
             "fallback_vectors": info["fallback_vectors"], "vectors": info["vectors"], "threshold": a.threshold,
             "lossless": bool(lossless), "training": training},
         "batched": {"ms_batch_graph": batch_ms, "ms_per_query_launches": per_query_ms,
+                    "ms_batch_graph_exhaustive_encoding": batch_ex_ms,
                     "speedup": per_query_ms / batch_ms, "queries": len(queries), "work_items": batch.n_items,
                     "results_equal": bool(exact)},
         "e2e": {"value": q_rows / (e2e_ms / 1e3), "unit": "rows/s",

@@ -38,6 +38,7 @@ struct fls_batch {
 	std::vector<uint4>           items; // {group, first vector, end vector, 0}
 	uint32_t                     slot_words = 0;
 	uint32_t                     has_dict   = 0;
+	bool                         any_pair   = false; // some query aggregates another column than it filters
 	void*                        ws         = nullptr; // device workspace after upload
 	uint64_t                     ws_bytes   = 0;
 };
@@ -56,6 +57,7 @@ struct BatchParams {
 	uint32_t*              counter;
 	long long*             results; // 2 per query: sum, count
 	uint32_t               slot_words;
+	uint32_t               n_slots; // staged columns per stage: 1 (filter = aggregate everywhere) or 2
 	uint32_t               has_dict;
 	uint32_t               warps;
 	uint32_t*              err;
@@ -65,9 +67,10 @@ struct BatchParams {
 // slack, dictionary scratch, stage infos and barriers.
 struct BatchLayout {
 	uint32_t slots, dict, info, bars, total;
-	__host__ __device__ BatchLayout(uint32_t slot_words) {
+	// n_slots = 1 when every query aggregates its own filter column.
+	__host__ __device__ BatchLayout(uint32_t slot_words, uint32_t n_slots) {
 		slots = 0;
-		dict  = slots + kBatchStages * 2u * slot_words + kSlotSlackWords;
+		dict  = slots + kBatchStages * n_slots * slot_words + kSlotSlackWords;
 		info  = dict + kDictWords;
 		bars  = info + kBatchStages * 2u * 4u;
 		total = (bars + 2u * kBatchStages + 3u) & ~3u;
@@ -92,7 +95,8 @@ __device__ __forceinline__ bool batch_issue(const BatchParams& P, uint32_t* base
 		if (!ok) { raise_err(P.err, kErrBadMeta); }
 		if (ok && vi.words) {
 			dev::mbar_expect_tx(bar, vi.words * 4u);
-			dev::bulk_g2s(base + L.slots + (st * 2u + lane) * P.slot_words, c.data + vi.offset, vi.words * 4u, bar, pol);
+			dev::bulk_g2s(base + L.slots + (st * P.n_slots + lane) * P.slot_words, c.data + vi.offset, vi.words * 4u,
+			              bar, pol);
 		}
 	}
 	__syncwarp();
@@ -104,7 +108,7 @@ __device__ __forceinline__ bool batch_issue(const BatchParams& P, uint32_t* base
 __global__ void __launch_bounds__(kMaxWarps * 32, 1) batch_kernel(const __grid_constant__ BatchParams P) {
 	extern __shared__ __align__(128) uint32_t smem[];
 	const uint32_t    lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-	const BatchLayout L(P.slot_words);
+	const BatchLayout L(P.slot_words, P.n_slots);
 	uint32_t*         base = smem + warp * L.total;
 	uint64_t*         bars = reinterpret_cast<uint64_t*>(base + L.bars);
 	if (lane == 0) {
@@ -160,7 +164,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) batch_kernel(const __grid_c
 				vf.aux  = fi.y >> 16;
 				va.base = static_cast<int32_t>(ai.x), va.scheme = ai.y & 0xffu, va.bw = (ai.y >> 8) & 0xffu;
 				va.aux  = ai.y >> 16;
-				const uint32_t* sf = base + L.slots + (st * 2u) * P.slot_words;
+				const uint32_t* sf = base + L.slots + (st * P.n_slots) * P.slot_words;
 				const uint32_t* sa = same ? sf : sf + P.slot_words;
 				// rows of a partial last vector
 				uint32_t valid = 0xffffffffu;
@@ -253,9 +257,10 @@ fls_status batch_launch(const fls_batch* b, const DevCol* cols, const fls_batch_
 	if (b->items.empty()) { return FLS_OK; }
 	uint32_t          warps, stages, ctas, tile;
 	fls_get_launch_config(&warps, &stages, &ctas, &tile);
-	const BatchLayout L(b->slot_words);
-	while (warps > 1 && 4ull * L.total * warps > static_cast<uint64_t>(di.max_smem)) { warps /= 2; }
-	if (4ull * L.total * warps > static_cast<uint64_t>(di.max_smem)) {
+	const uint32_t    n_slots = b->any_pair ? 2u : 1u;
+	const BatchLayout L(b->slot_words, n_slots);
+	warps = std::min<uint32_t>(warps, static_cast<uint32_t>(di.max_smem) / (4u * L.total));
+	if (warps == 0) {
 		return set_error(FLS_ERR_CAPACITY, "batch vectors too large for shared-memory staging");
 	}
 	{
@@ -281,6 +286,7 @@ fls_status batch_launch(const fls_batch* b, const DevCol* cols, const fls_batch_
 	P.counter    = counter;
 	P.results    = reinterpret_cast<long long*>(d_results);
 	P.slot_words = b->slot_words;
+	P.n_slots    = n_slots;
 	P.has_dict   = b->has_dict;
 	P.warps      = warps;
 	P.err        = device_error_word();
@@ -328,6 +334,7 @@ fls_status fls_batch_create(const fls_column* cols, uint32_t n_cols, const fls_b
 			return set_error(FLS_ERR_INVALID_ARG, "batch query names missing or mismatched columns");
 		}
 		bq.n_values    = cols[bq.col].n_values;
+		b->any_pair    = b->any_pair || bq.col != bq.agg_col;
 		int64_t& slot_g = open_group[static_cast<size_t>(bq.col) * n_cols + bq.agg_col];
 		if (slot_g < 0 || b->groups[static_cast<size_t>(slot_g)].n_q == kGroupQueries) {
 			slot_g = static_cast<int64_t>(b->groups.size());

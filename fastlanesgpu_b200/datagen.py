@@ -111,6 +111,19 @@ N_GROUPS = (1998 - 1992 + 1) * (5 * 5 * 40)
 MIXED_FAMILIES = ("uniform", "zipf", "sorted_gaps", "geometric_runs")
 
 
+def zipf_device(n: int, s: float = 1.1, domain: int = 1 << 20, seed: int = 5, device="cpu"):
+    """Zipf(s) ranks truncated to [1, domain], minus 1 (values in [0, domain)),
+    drawn by inverse CDF with torch on `device` (int32 tensor)."""
+    import torch
+    dev = torch.device(device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    cdf = torch.cumsum(torch.arange(1, domain + 1, dtype=torch.float64, device=dev) ** -s, 0)
+    cdf /= cdf[-1].clone()
+    v = torch.searchsorted(cdf, torch.rand(n, generator=g, device=dev, dtype=torch.float64))
+    return torch.clamp(v, max=domain - 1).to(torch.int32)
+
+
 def mixed_columns(n_cols: int = 64, lo_log: int = 16, hi_log: int = 26, seed: int = 64, device="cpu"):
     """Columns of the mixed workload, generated with torch on `device`:
     lengths log-uniform in [2^lo_log, 2^hi_log]; family i % 4 of

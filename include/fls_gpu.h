@@ -153,7 +153,7 @@ fls_status fls_encode_column_gpu(const int32_t* d_values, uint64_t n, const uint
 /* Exhaustive per-vector encoder (the selector's judge): exact encoded size in
  * bytes (payload + 16 B metadata) of every scheme for every vector
  * (sizes: n_vec*5, UINT32_MAX = not representable) and the argmin scheme, ties
- * broken by the decode-cost order CONST < FOR < DICT < RLE < DELTA. */
+ * broken by the measured decode-cost order CONST < FOR < DELTA < RLE < DICT. */
 fls_status fls_encode_exhaustive(const int32_t* values, uint64_t n, uint32_t* sizes, uint8_t* best, int n_threads);
 
 /* The 16 per-vector statistics the learned selector reads (n_vec*16 floats). */
