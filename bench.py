@@ -632,29 +632,53 @@ def run_mixed(a, dist: Dist):
 
 
 def run_reference(a, dist: Dist):
-    """--impl reference: the reference's own CPU implementation of the path."""
+    """--impl reference: the reference's own CPU implementation of the path (its
+    unpack compiled from its sources, the fls_q11.cu / fls_q21.cu scalar loops),
+    all host threads, on a bounded sample of the same workload."""
     import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
     from fastlanesgpu_b200 import datagen
     R = orc.Reference()
     threads = os.cpu_count() or 1
+    if a.workload == "mixed" or (a.workload == "decode" and a.decode_scheme != "for"):
+        return {"impl": "reference", "unavailable": "the reference has no CPU implementation of this workload "
+                "(learned selection, batching, or per-vector DELTA/RLE/DICT columns)"}
     sample = min(a.rows, 1 << 24)
-    if a.workload != "q11":
-        raise SystemExit("--impl reference supports the q11 workload")
-    t = datagen.lineorder_q11(sample, seed=1000)
-    names = ["date", "discount", "quantity", "price"]
-    words = [R.pack_column(t[k], datagen.Q11_BITS[k], threads) for k in names]
-    bws = [datagen.Q11_BITS[k] for k in names]
-    f = datagen.Q11_FILTER
-    args = (words, bws, sample, *f["date"], *f["discount"], f["quantity"][1] + 1, threads)
+    if a.workload == "q11":
+        t = datagen.lineorder_q11(sample, seed=1000)
+        names = ["date", "discount", "quantity", "price"]
+        words = [R.pack_column(t[k], datagen.Q11_BITS[k], threads) for k in names]
+        bws = [datagen.Q11_BITS[k] for k in names]
+        f = datagen.Q11_FILTER
+        args = (words, bws, sample, *f["date"], *f["discount"], f["quantity"][1] + 1, threads)
+        fn, what = R.q11_sum, "fused decode + filter-aggregate (Q1.1 shape)"
+        how = "the reference's unpack (host-compiled from its sources) + fls_q11.cu loop"
+    elif a.workload == "q21":
+        t = datagen.q21_tables(sample, seed=1000)
+        O = orc.Oracle()
+        ht_s = O.pht1_build(t["s_region"], 1, t["s_suppkey"], t["s_suppkey"].size)
+        ht_p = O.pht2_build(t["p_category"], 1, t["p_partkey"], t["p_brand1"], t["p_partkey"].size)
+        ht_d = O.pht2_build(None, 0, t["d_datekey"], t["d_year"], datagen.N_DAYS)
+        names = ["lo_suppkey", "lo_partkey", "lo_orderdate", "lo_revenue"]
+        words = [R.pack_column(t[k], datagen.Q21_BITS[k], threads) for k in names]
+        bws = [datagen.Q21_BITS[k] for k in names]
+        args = (words, bws, sample, ht_s, ht_p, ht_d, 0, threads)
+        fn, what = R.q21_groupby, "fused decode + 3-way perfect-hash probe + 7000-group int64 group-by (Q2.1 shape)"
+        how = "the reference's unpack (host-compiled from its sources) + fls_q21.cu probe_v1 loop"
+    else:
+        vals = datagen.uniform_bits(sample, a.decode_bw, seed=1000)
+        packed = R.pack_column(vals, a.decode_bw, threads)
+        args = (packed, a.decode_bw, sample // 1024, threads)
+        fn, what = R.decode_sum, f"decode fused with uint64 sum: bit-pack + FOR, bw {a.decode_bw}"
+        how = "the reference's unpack (host-compiled from its sources) + uint64 sum"
     for _ in range(max(1, min(a.warmup, 3))):
-        R.q11_sum(*args)
+        fn(*args)
     steps = max(1, min(a.steps, 10))
     times = []
     for _ in range(steps):
         t0 = time.perf_counter()
-        R.q11_sum(*args)
+        fn(*args)
         times.append(time.perf_counter() - t0)
     value = sample * len(times) / sum(times)
     return {
@@ -662,11 +686,9 @@ def run_reference(a, dist: Dist):
         "n_gpus": a.gpus, "steps": steps, "warmup": max(1, min(a.warmup, 3)),
         "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32->int64", "data": "synthetic (seeded)",
-        "config": {"workload": "fused decode + filter-aggregate (Q1.1 shape)", "rows_per_gpu": a.rows,
-                   "sample_rows_per_step": sample},
+        "config": {"workload": what, "rows_per_gpu": a.rows, "sample_rows_per_step": sample},
         "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "reference",
-                         "sample": f"{sample} rows per step of the same table shape; the reference's unpack "
-                                   f"(host-compiled from its sources) + fls_q11.cu loop, OpenMP {threads} threads"},
+                         "sample": f"{sample} rows per step of the same table shape; {how}, OpenMP {threads} threads"},
         "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
