@@ -43,6 +43,8 @@ struct FilterParams {
 	uint32_t            base[FLS_MAX_QUERY_COLS]; // FOR base of each staged column
 	uint32_t            lo[FLS_MAX_FILTERS];      // filter lower bound (unsigned wrap)
 	uint32_t            range[FLS_MAX_FILTERS];   // hi - lo
+	uint32_t            field_lo[FLS_MAX_FILTERS]; // SWAR filters: bounds on the packed field, in [0, 2^bw]
+	uint32_t            field_hi[FLS_MAX_FILTERS]; //   (an empty range is (1, 0))
 	int32_t             sparse_rows;
 	uint32_t            pad_;
 	unsigned long long* result;
@@ -71,7 +73,7 @@ struct DecodeParams {
 // blocks.  Every field is naturally aligned and padded explicitly, so equal
 // sizes mean equal offsets.
 static_assert(sizeof(StageParams) == 128 && alignof(StageParams) == 8, "StageParams layout");
-static_assert(sizeof(FilterParams) == 208, "FilterParams layout");
+static_assert(sizeof(FilterParams) == 240, "FilterParams layout");
 static_assert(sizeof(ProbeParams) == 264, "ProbeParams layout");
 static_assert(sizeof(DecodeParams) == 152, "DecodeParams layout");
 
@@ -94,11 +96,16 @@ struct Shape {
 	static_assert(NC >= 1 && NC <= FLS_MAX_QUERY_COLS, "1..8 staged columns");
 };
 
-template <int LAYOUT, int NF, int AGG_A, int AGG_B, int... BWS>
+// SWAR bit f: filter f may test packed fields several at a time against
+// field_lo/field_hi (the host proved base + 2^bw - 1 <= INT32_MAX, so the
+// decoded values do not wrap and value in [lo, hi] <=> field in
+// [lo - base, hi - base] clamped to the field's domain).
+template <int LAYOUT, int NF, int AGG_A, int AGG_B, int SWAR, int... BWS>
 struct FilterQuery : Shape<LAYOUT, BWS...> {
 	static constexpr int kNF   = NF;
 	static constexpr int kAggA = AGG_A;
 	static constexpr int kAggB = AGG_B;
+	__host__ __device__ static constexpr bool swar(int f) { return (SWAR >> f) & 1; }
 	static_assert(NF >= 0 && NF <= FLS_MAX_FILTERS, "0..4 filters");
 	static_assert(AGG_B < 0 || AGG_A >= 0, "sum(a*b) needs a");
 };
@@ -167,13 +174,66 @@ __device__ __forceinline__ uint32_t valid_rows(const StageParams& S, int layout,
 
 // ------------------------------------------------------------ filter-aggregate
 
+// Row r's field of a lane stream, unmasked above the field (one shift).
+template <int BW>
+__device__ __forceinline__ uint32_t field_raw(const dev::LaneWords<BW>& lw, int r) {
+	const int bit = r * BW, k = bit >> 5, sh = bit & 31;
+	if (sh + BW <= 32) { return lw.w[k] >> sh; }
+	return __funnelshift_r(lw.w[k], lw.w[k + 1], sh);
+}
+
+// In-range row mask of a 4-bit column, eight rows per word: even and odd
+// nibbles go to bytes below a guard bit 0x80, so (x + 0x80 - lo) and
+// (hi + 0x80 - x) keep the guard exactly when lo <= x and x <= hi, with no
+// borrow across bytes; a multiply gathers the eight flags of a word.
+__device__ __forceinline__ uint32_t swar_mask_bw4(const dev::LaneWords<4>& lw, uint32_t L, uint32_t H) {
+	const uint32_t c1 = 0x80808080u - L * 0x01010101u, c2 = (H | 0x80u) * 0x01010101u;
+	uint32_t       y[4];
+#pragma unroll
+	for (int k = 0; k < 4; ++k) {
+		const uint32_t e  = lw.w[k] & 0x0F0F0F0Fu, o = (lw.w[k] >> 4) & 0x0F0F0F0Fu;
+		const uint32_t re = (e + c1) & (c2 - e) & 0x80808080u;
+		const uint32_t ro = (o + c1) & (c2 - o) & 0x80808080u;
+		// bits 8j, 8j+1 = rows 8k+2j, 8k+2j+1; the multiply packs them into byte 3
+		y[k] = ((re >> 7) | (ro >> 6)) * 0x01041040u;
+	}
+	return __byte_perm(__byte_perm(y[0], y[1], 0x0073), __byte_perm(y[2], y[3], 0x0073), 0x5410);
+}
+
+// In-range row mask of an even width <= 14: rows p and p + 16 share their bit
+// offset, so both fields are tested at once in two 16-bit halves below guard
+// bits 0x8000.
+template <int BW>
+__device__ __forceinline__ uint32_t swar_mask_pairs(const dev::LaneWords<BW>& lw, uint32_t L, uint32_t H) {
+	constexpr uint32_t M2 = ((1u << BW) - 1u) * 0x00010001u, G = 0x80008000u;
+	const uint32_t     c1 = G - L * 0x00010001u, c2 = (H | 0x8000u) * 0x00010001u;
+	uint32_t           acc = 0;
+#pragma unroll
+	for (int p = 15; p >= 0; --p) {
+		const uint32_t f = __byte_perm(field_raw<BW>(lw, p), field_raw<BW>(lw, p + 16), 0x5410) & M2;
+		acc              = acc * 2u + (((f + c1) & (c2 - f) & G) >> 15); // bits p and 16 + p after the loop
+	}
+	return acc;
+}
+
 template <class Q, int F>
 __device__ __forceinline__ void dense_filter(const FilterParams& P, const Vec<Q>& V, uint32_t lane, uint32_t& mask) {
-	const uint32_t lo = P.lo[F] - P.base[F], range = P.range[F];
-	uint32_t       m[4] = {0, 0, 0, 0};
-	dev::unpack_rows<Q::bw(F)>(V.template col<F>(), lane,
-	                           [&](int r, uint32_t p) { m[r & 3] |= (p - lo <= range ? 1u : 0u) << r; });
-	mask &= (m[0] | m[1]) | (m[2] | m[3]);
+	constexpr int BW = Q::bw(F);
+	if constexpr (Q::swar(F) && BW == 4) {
+		dev::LaneWords<4> lw;
+		dev::load_words<4>(V.template col<F>(), lane, lw);
+		mask &= swar_mask_bw4(lw, P.field_lo[F], P.field_hi[F]);
+	} else if constexpr (Q::swar(F) && BW % 2 == 0 && BW >= 2 && BW <= 14) {
+		dev::LaneWords<BW> lw;
+		dev::load_words<BW>(V.template col<F>(), lane, lw);
+		mask &= swar_mask_pairs<BW>(lw, P.field_lo[F], P.field_hi[F]);
+	} else {
+		const uint32_t lo = P.lo[F] - P.base[F], range = P.range[F];
+		uint32_t       m[4] = {0, 0, 0, 0};
+		dev::unpack_rows<BW>(V.template col<F>(), lane,
+		                     [&](int r, uint32_t p) { m[r & 3] |= (p - lo <= range ? 1u : 0u) << r; });
+		mask &= (m[0] | m[1]) | (m[2] | m[3]);
+	}
 }
 
 // Dense filters F, F+1, ... while some lane keeps more than sparse_rows rows;

@@ -323,9 +323,18 @@ bool jit_shape(const fls_column* cols, const fls_filter* filters, uint32_t n_fil
 		sc[i] = cols[sh.staged[i]];
 		if (!uniform_for(sc[i], sc[0].layout)) { return false; }
 	}
+	// Filters that may test several packed fields at once: widths with a SWAR
+	// form (4, or even up to 14) on columns whose decoded values cannot wrap.
+	uint32_t swar = 0;
+	for (uint32_t f = 0; f < n_filters; ++f) {
+		const uint32_t bw = sc[f].bw;
+		const bool     form = bw == 4 || (bw % 2 == 0 && bw >= 2 && bw <= 14);
+		if (form && static_cast<int64_t>(sc[f].base) + (int64_t {1} << bw) - 1 <= INT32_MAX) { swar |= 1u << f; }
+	}
+	sh.swar = swar;
 	char head[96];
-	std::snprintf(head, sizeof(head), "%u, %u, %d, %d", static_cast<unsigned>(sc[0].layout), n_filters, sh.agg_a,
-	              sh.agg_b);
+	std::snprintf(head, sizeof(head), "%u, %u, %d, %d, %u", static_cast<unsigned>(sc[0].layout), n_filters, sh.agg_a,
+	              sh.agg_b, swar);
 	sh.key = key_args(sc, sh.n_staged, head);
 	return true;
 }
@@ -362,6 +371,15 @@ fls_status jit_filter_agg(const fls_column* cols, const fls_filter* filters, uin
 	for (uint32_t f = 0; f < n_filters; ++f) {
 		P.lo[f]    = static_cast<uint32_t>(filters[f].lo);
 		P.range[f] = static_cast<uint32_t>(filters[f].hi) - static_cast<uint32_t>(filters[f].lo);
+		if ((sh.swar >> f) & 1u) {
+			// value = base + field exactly, so value in [lo, hi] <=> field in
+			// [lo - base, hi - base] within the field's domain [0, 2^bw).
+			const int64_t top = (int64_t {1} << sc[f].bw) - 1;
+			const int64_t L   = std::max<int64_t>(0, static_cast<int64_t>(filters[f].lo) - sc[f].base);
+			const int64_t H   = std::min<int64_t>(top, static_cast<int64_t>(filters[f].hi) - sc[f].base);
+			P.field_lo[f]     = L <= H ? static_cast<uint32_t>(L) : 1u;
+			P.field_hi[f]     = L <= H ? static_cast<uint32_t>(H) : 0u;
+		}
 	}
 	P.sparse_rows = sparse_rows;
 	P.result      = reinterpret_cast<unsigned long long*>(d_result);

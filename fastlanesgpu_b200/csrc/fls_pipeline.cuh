@@ -303,6 +303,7 @@ struct JitShape {
 	uint32_t    staged[FLS_MAX_QUERY_COLS];
 	uint32_t    n_staged = 0;
 	int         agg_a = -1, agg_b = -1;
+	uint32_t    swar = 0; // filters tested several packed fields at a time
 	std::string key;
 };
 // False when the query does not qualify (a non-FOR or non-uniform column,

@@ -62,7 +62,7 @@ def _random_case(g, n):
     layout = LAYOUT_TRANSPOSED if g.random() < 0.3 else LAYOUT_NORMAL
     vals, cols = [], []
     for _ in range(n_cols):
-        bw = int(g.choice([0, 1, 3, 4, 7, 8, 12, 16, 17, 24, 31, 32]))
+        bw = int(g.choice([0, 1, 2, 3, 4, 6, 7, 8, 10, 12, 14, 16, 17, 24, 31, 32]))
         if bw == 32:
             v = g.integers(-2**31, 2**31, n, dtype=np.int64).astype(np.int32)
             base = 0
@@ -102,6 +102,39 @@ def test_jit_random_shapes(jit_on, seed):
     assert got_gen == want
     assert got_jit == want, (filters, a, b, [c.desc.bw for c in cols])
     assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
+
+
+@pytest.mark.parametrize("bw", [2, 4, 6, 8, 10, 12, 14])
+def test_jit_swar_filter_edges(jit_on, bw):
+    """Filters that test several packed fields at once (4-bit and even widths
+    up to 14): ranges below, across and above the column's domain, empty after
+    clamping, single values, negative bases and a base so large that decoded
+    values could wrap (then the per-row form runs); sparse_rows 32 forces the
+    dense form on every filter."""
+    g = np.random.default_rng(bw)
+    n = 20 * 1024 + 77
+    top = (1 << bw) - 1
+    ops.set_tuning(TUNE_SPARSE_ROWS, 32)
+    for base in (0, -123456, 2**31 - 1 - top, 2**31 - top // 2):
+        f = g.integers(0, top + 1, n)
+        vals = (f + base).astype(np.int64)
+        vals = ((vals + 2**31) % 2**32 - 2**31).astype(np.int32)  # the decoder's wrap for the last base
+        a = g.integers(-1000, 1000, n).astype(np.int32)
+        cols = [EncodedColumn.uniform(vals, bw=bw, base=base).to_device(), EncodedColumn.uniform(a, bw=11, base=-1000)
+                .to_device()]
+        lo_v, hi_v = int(vals.min()), int(vals.max())
+        ranges = [(lo_v, hi_v), (lo_v - 50, lo_v), (hi_v, hi_v + 50), (lo_v - 100, lo_v - 1), (hi_v + 1, hi_v + 9),
+                  (lo_v + top // 3, lo_v + top // 2), (-2**31, 2**31 - 1), (int(vals[5]), int(vals[5]))]
+        for lo, hi in ranges:
+            lo, hi = min(max(lo, -2**31), 2**31 - 1), min(max(hi, -2**31), 2**31 - 1)
+            for filters in ([(0, lo, hi)], [(0, lo, hi), (1, -500, 400)]):
+                got, used = _run(cols, filters, 1, -1, jit=True)
+                assert used == (1 if lo <= hi else 0), (bw, base, lo, hi)  # an empty range launches nothing
+                sel = np.ones(n, bool)
+                for c, l, h in filters:
+                    v = [vals, a][c]
+                    sel &= (v >= l) & (v <= h)
+                assert got == int(a[sel].astype(np.int64).sum()), (bw, base, lo, hi)
 
 
 @pytest.mark.parametrize("sparse_rows", [1, 4, 12, 32])
