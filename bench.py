@@ -38,7 +38,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["q11", "q21", "decode", "mixed"], default="q11")
+    ap.add_argument("--workload", choices=["q11", "q21", "q31", "q41", "decode", "mixed"], default="q11")
     ap.add_argument("--rows", type=int, default=0, help="rows per GPU (0 = 2^27 for queries, 2^28 for decode)")
     ap.add_argument("--decode-bw", type=int, default=16, help="bit width of the FOR decode workload")
     ap.add_argument("--decode-scheme", choices=["for", "delta", "rle", "dict"], default="for",
@@ -244,6 +244,24 @@ def run_ours(a, dist: Dist):
                     "rows_per_gpu": a.rows, "columns": "supp 17b, part 19b, date 12b, revenue 24b",
                     "filters": "part category 1/5, supplier region 1/25"}
         metric_key = "q21"
+    elif a.workload in ("q31", "q41"):
+        t, tables, hcols, dcols, probes, jkw = datagen.ssb_join(a.workload, a.rows, seed, device=dev)
+        res = torch.zeros(jkw["res_stride"] * jkw["n_groups"], dtype=torch.int32, device=dev)
+
+        def step():
+            ops.join_groupby(dcols, probes, out=res, **jkw)
+            return res
+        if a.workload == "q31":
+            workload = {"workload": "fused decode + 3 perfect-hash probes + 4375-group int64 group-by (Q3.1 shape, "
+                                    "fls_q31.cu)", "rows_per_gpu": a.rows,
+                        "columns": "supp 17b, cust 18b, date 12b, revenue 24b",
+                        "filters": "supplier region 1/5, customer region 1/5, years 1992-1997"}
+        else:
+            workload = {"workload": "fused decode + 4 perfect-hash probes + 175-group int64 sum(revenue - supplycost) "
+                                    "(Q4.1 shape, fls_q41.cu)", "rows_per_gpu": a.rows,
+                        "columns": "supp 17b, cust 18b, part 19b, date 12b, revenue 24b, supplycost 18b",
+                        "filters": "supplier region 1/5, customer region 1/5, part manufacturer 2/5"}
+        metric_key = a.workload
     else:
         from fastlanesgpu_b200 import LAYOUT_TRANSPOSED, SCHEME_DELTA, SCHEME_RLE
         if a.decode_scheme == "for":
@@ -288,14 +306,19 @@ def run_ours(a, dist: Dist):
         # the one exchange of the sharded query: combine the ranks' partial aggregates
         if not dist.pg:
             return
-        if a.workload == "q21":
-            # reference layout per group: (year, brand) int32 pair + uint64 sum
-            r64 = res.view(torch.int64).view(-1, 2)
-            keys, sums = r64[:, 0].contiguous(), r64[:, 1].contiguous()
+        if a.workload in ("q21", "q31", "q41"):
+            # reference layout per group: key words (equal on every rank that
+            # saw the group, 0 elsewhere) + a uint64 sum
+            stride, sum_slot = (4, 2) if a.workload == "q21" else (jkw["res_stride"], jkw["sum_slot"])
+            r64 = res.view(torch.int64).view(-1, stride // 2)
+            sc = sum_slot // 2
+            keys = torch.cat([r64[:, :sc], r64[:, sc + 1:]], dim=1).contiguous()
+            sums = r64[:, sc].contiguous()
             dist.pg.all_reduce(keys, op=dist.pg.ReduceOp.MAX)
             allreduce_sum(sums)
-            r64[:, 0].copy_(keys)
-            r64[:, 1].copy_(sums)
+            r64[:, :sc].copy_(keys[:, :sc])
+            r64[:, sc + 1:].copy_(keys[:, sc:])
+            r64[:, sc].copy_(sums)
         else:
             allreduce_sum(res)
 
@@ -654,6 +677,27 @@ def run_reference(a, dist: Dist):
         args = (words, bws, sample, *f["date"], *f["discount"], f["quantity"][1] + 1, threads)
         fn, what = R.q11_sum, "fused decode + filter-aggregate (Q1.1 shape)"
         how = "the reference's unpack (host-compiled from its sources) + fls_q11.cu loop"
+    elif a.workload in ("q31", "q41"):
+        O = orc.Oracle()
+        if a.workload == "q31":
+            t = datagen.q31_tables(sample, seed=1000)
+            hs = O.pht2_build(t["s_region"], 1, t["s_suppkey"], t["s_nation"], t["s_suppkey"].size)
+            hc = O.pht2_build(t["c_region"], 1, t["c_custkey"], t["c_nation"], t["c_custkey"].size)
+            hd = O.pht2_build(t["d_in_range"], 1, t["d_datekey"], t["d_year"], datagen.N_DAYS)
+            names, bits = ["lo_suppkey", "lo_custkey", "lo_orderdate", "lo_revenue"], datagen.Q31_BITS
+            tabs, fn, shape = (hs, hc, hd), R.q31_groupby, "Q3.1"
+        else:
+            t = datagen.q41_tables(sample, seed=1000)
+            hs = O.pht1_build(t["s_region"], 1, t["s_suppkey"], t["s_suppkey"].size)
+            hc = O.pht2_build(t["c_region"], 1, t["c_custkey"], t["c_nation"], t["c_custkey"].size)
+            hp = O.pht1_build(t["p_mfgr_low"], 1, t["p_partkey"], t["p_partkey"].size)
+            hd = O.pht2_build(None, 0, t["d_datekey"], t["d_year"], datagen.N_DAYS)
+            names = ["lo_suppkey", "lo_custkey", "lo_partkey", "lo_orderdate", "lo_revenue", "lo_supplycost"]
+            bits, tabs, fn, shape = datagen.Q41_BITS, (hs, hc, hp, hd), R.q41_groupby, "Q4.1"
+        words = [R.pack_column(t[k], bits[k], threads) for k in names]
+        args = (words, [bits[k] for k in names], sample, *tabs, 0, threads)
+        what = f"fused decode + perfect-hash probes + int64 group-by ({shape} shape)"
+        how = f"the reference's unpack (host-compiled from its sources) + fls_{a.workload}.cu probe_v1 loop"
     elif a.workload == "q21":
         t = datagen.q21_tables(sample, seed=1000)
         O = orc.Oracle()

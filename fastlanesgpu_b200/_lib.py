@@ -74,6 +74,18 @@ class JoinAggDesc(ctypes.Structure):
                 ("group_sub", ctypes.c_int32), ("n_groups", ctypes.c_int32)]
 
 
+MAX_GROUP_KEYS = 3
+
+
+class JoinGroupbyDesc(ctypes.Structure):
+    _fields_ = [("cols", ctypes.POINTER(Column)), ("n_cols", ctypes.c_uint32),
+                ("probes", Probe * MAX_PROBES), ("n_probes", ctypes.c_uint32), ("agg_col", ctypes.c_uint32),
+                ("agg_sub_col", ctypes.c_int32), ("n_keys", ctypes.c_uint32),
+                ("key_probe", ctypes.c_int32 * MAX_GROUP_KEYS), ("key_mul", ctypes.c_int32 * MAX_GROUP_KEYS),
+                ("key_slot", ctypes.c_int32 * MAX_GROUP_KEYS), ("group_sub", ctypes.c_int32),
+                ("n_groups", ctypes.c_int32), ("res_stride", ctypes.c_uint32), ("sum_slot", ctypes.c_uint32)]
+
+
 class JitStats(ctypes.Structure):
     _fields_ = [("compiled", ctypes.c_uint64), ("launches", ctypes.c_uint64), ("failures", ctypes.c_uint64),
                 ("cached", ctypes.c_uint64)]
@@ -136,6 +148,8 @@ _SIGS = {
     "fls_jit_last_log": (ctypes.c_char_p, []),
     "fls_jit_precompile": (ctypes.c_int, [ctypes.POINTER(FilterAggDesc)]),
     "fls_jit_precompile_probe": (ctypes.c_int, [ctypes.POINTER(JoinAggDesc)]),
+    "fls_jit_precompile_join": (ctypes.c_int, [ctypes.POINTER(JoinGroupbyDesc)]),
+    "fls_query_join_groupby": (ctypes.c_int, [ctypes.POINTER(JoinGroupbyDesc), _VP, _VP]),
 }
 
 _LIB = None

@@ -57,7 +57,11 @@ struct ProbeParams {
 	int32_t        len[FLS_MAX_PROBES];
 	int32_t        kmin[FLS_MAX_PROBES];
 	uint32_t       smem_off[FLS_MAX_PROBES]; // words into the CTA scratch (tables flagged as shared)
-	int32_t        mul, sub, n_groups, sparse_rows;
+	int32_t        key_mul[FLS_MAX_GROUP_KEYS];
+	int32_t        key_slot[FLS_MAX_GROUP_KEYS]; // word of each key in the group record, -1 = not written
+	int32_t        sub, n_groups, sparse_rows;
+	uint32_t       stride, sum_slot; // group record: int32 words, word of the int64 sum
+	uint32_t       pad_;
 	int32_t*       res;
 };
 
@@ -74,7 +78,7 @@ struct DecodeParams {
 // sizes mean equal offsets.
 static_assert(sizeof(StageParams) == 128 && alignof(StageParams) == 8, "StageParams layout");
 static_assert(sizeof(FilterParams) == 240, "FilterParams layout");
-static_assert(sizeof(ProbeParams) == 264, "ProbeParams layout");
+static_assert(sizeof(ProbeParams) == 296, "ProbeParams layout");
 static_assert(sizeof(DecodeParams) == 152, "DecodeParams layout");
 
 // Bit widths of the staged columns and where they sit in a stage.
@@ -110,16 +114,20 @@ struct FilterQuery : Shape<LAYOUT, BWS...> {
 	static_assert(AGG_B < 0 || AGG_A >= 0, "sum(a*b) needs a");
 };
 
-// KINDS bit q: probe q is PHT_2; SMEM bit q: probe q's table is in shared
-// memory (PHT_1 as a presence bitmap, PHT_2 verbatim); DIRECT bit q: the host
-// proved every key of probe q's column lands in [keys_min, keys_min + len)
-// (from the column's base and bit width), so its slot is key - keys_min.
-template <int LAYOUT, int NP, int AGG, int KEY_A, int KEY_B, int KINDS, int SMEM, int DIRECT, int... BWS>
+// AGG / SUB: staged columns of the measure and of the column subtracted from
+// it (-1: none).  NK group keys, the payloads of probes K0, K1, K2.  KINDS bit
+// q: probe q is PHT_2; SMEM bit q: probe q's table is in shared memory (PHT_1
+// as a presence bitmap, PHT_2 verbatim); DIRECT bit q: the host proved every
+// key of probe q's column lands in [keys_min, keys_min + len) (from the
+// column's base and bit width), so its slot is key - keys_min.
+template <int LAYOUT, int NP, int AGG, int SUB, int NK, int K0, int K1, int K2, int KINDS, int SMEM, int DIRECT,
+          int... BWS>
 struct ProbeQuery : Shape<LAYOUT, BWS...> {
 	static constexpr int kNP  = NP;
 	static constexpr int kAgg = AGG;
-	static constexpr int kKeyA = KEY_A;
-	static constexpr int kKeyB = KEY_B;
+	static constexpr int kSub = SUB;
+	static constexpr int kNK  = NK;
+	__host__ __device__ static constexpr int key_probe(int k) { return k == 0 ? K0 : k == 1 ? K1 : K2; }
 	__host__ __device__ static constexpr bool pht2(int q) { return (KINDS >> q) & 1; }
 	__host__ __device__ static constexpr bool in_smem(int q) { return (SMEM >> q) & 1; }
 	__host__ __device__ static constexpr bool direct(int q) { return (DIRECT >> q) & 1; }
@@ -433,7 +441,7 @@ __device__ __forceinline__ void dense_probes(const ProbeParams& P, const uint32_
 template <class Q, int q>
 __device__ __forceinline__ void probe_rows(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
                                            uint32_t lane, const uint32_t (&rows)[kRowBatch], bool (&pass)[kRowBatch],
-                                           int32_t (&va)[kRowBatch], int32_t (&vb)[kRowBatch], int rem) {
+                                           int32_t (&kv)[FLS_MAX_GROUP_KEYS][kRowBatch], int rem) {
 	if constexpr (q < Q::kNP) {
 		const uint32_t kb  = P.base[q] - static_cast<uint32_t>(P.kmin[q]);
 		const int32_t  len = P.len[q];
@@ -452,26 +460,37 @@ __device__ __forceinline__ void probe_rows(const ProbeParams& P, const uint32_t*
 #pragma unroll
 		for (int j = 0; j < kRowBatch; ++j) {
 			pass[j] = pass[j] & ((e[j].x | e[j].y) != 0u);
-			if constexpr (q == Q::kKeyA) { va[j] = static_cast<int32_t>(e[j].y); }
-			if constexpr (q == Q::kKeyB) { vb[j] = static_cast<int32_t>(e[j].y); }
+#pragma unroll
+			for (int k = 0; k < Q::kNK; ++k) {
+				if (Q::key_probe(k) == q) { kv[k][j] = static_cast<int32_t>(e[j].y); }
+			}
 		}
-		probe_rows<Q, q + 1>(P, tables, V, lane, rows, pass, va, vb, rem);
+		probe_rows<Q, q + 1>(P, tables, V, lane, rows, pass, kv, rem);
 	}
 }
 
-// Group-by epilogue of one selected row (fls_q21.cu:67-77): group
-// (a*mul + (b - sub)) % n_groups in wrapping 32-bit arithmetic.
-__device__ __forceinline__ void emit(const ProbeParams& P, int32_t a, int32_t b, int32_t measure) {
-	const int32_t key = static_cast<int32_t>(static_cast<uint32_t>(a) * static_cast<uint32_t>(P.mul) +
-	                                         (static_cast<uint32_t>(b) - static_cast<uint32_t>(P.sub)));
-	const int32_t g   = static_cast<uint32_t>(key) < static_cast<uint32_t>(P.n_groups) ? key : rem_slow(key, P.n_groups);
+// Group-by epilogue of one selected row (fls_q21.cu:67-77, fls_q31.cu:82-91,
+// fls_q41.cu:96-104): the group of the keys in wrapping 32-bit arithmetic,
+// the key values into their words of the group record, the measure into its
+// int64 sum.
+template <class Q>
+__device__ __forceinline__ void emit(const ProbeParams& P, const int32_t (&kv)[FLS_MAX_GROUP_KEYS][kRowBatch], int j,
+                                     int32_t measure) {
+	uint32_t key = 0u - static_cast<uint32_t>(P.sub);
+#pragma unroll
+	for (int k = 0; k < Q::kNK; ++k) { key += static_cast<uint32_t>(kv[k][j]) * static_cast<uint32_t>(P.key_mul[k]); }
+	const int32_t g = key < static_cast<uint32_t>(P.n_groups) ? static_cast<int32_t>(key)
+	                                                          : rem_slow(static_cast<int32_t>(key), P.n_groups);
 	if (g < 0) {
 		atomicOr(P.S.err, kErrHashBit);
 		return;
 	}
-	P.res[4 * g]     = b;
-	P.res[4 * g + 1] = a;
-	atomicAdd(reinterpret_cast<unsigned long long*>(P.res + 4 * g + 2),
+	int32_t* rec = P.res + static_cast<int64_t>(g) * P.stride;
+#pragma unroll
+	for (int k = 0; k < Q::kNK; ++k) {
+		if (P.key_slot[k] >= 0) { rec[P.key_slot[k]] = kv[k][j]; }
+	}
+	atomicAdd(reinterpret_cast<unsigned long long*>(rec + P.sum_slot),
 	          static_cast<unsigned long long>(static_cast<long long>(measure)));
 }
 
@@ -483,18 +502,23 @@ __device__ __forceinline__ void row_phase(const ProbeParams& P, const uint32_t* 
 		const int rem = n_it - it0; // warp-uniform
 		uint32_t  rows[kRowBatch];
 		bool      pass[kRowBatch];
-		int32_t   va[kRowBatch], vb[kRowBatch];
+		int32_t   kv[FLS_MAX_GROUP_KEYS][kRowBatch];
 #pragma unroll
 		for (int j = 0; j < kRowBatch; ++j) {
 			pass[j] = mask != 0u;
 			rows[j] = pass[j] ? static_cast<uint32_t>(__ffs(mask)) - 1u : 0u;
 			mask &= mask - 1u;
-			va[j] = vb[j] = 0;
+#pragma unroll
+			for (int k = 0; k < FLS_MAX_GROUP_KEYS; ++k) { kv[k][j] = 0; }
 		}
-		probe_rows<Q, F0>(P, tables, V, lane, rows, pass, va, vb, rem);
+		probe_rows<Q, F0>(P, tables, V, lane, rows, pass, kv, rem);
 #pragma unroll
 		for (int j = 0; j < kRowBatch; ++j) {
-			if (j < rem && pass[j]) { emit(P, va[j], vb[j], row_value<Q, Q::kAgg>(P.base, V, lane, rows[j])); }
+			if (j < rem && pass[j]) {
+				uint32_t m = static_cast<uint32_t>(row_value<Q, Q::kAgg>(P.base, V, lane, rows[j]));
+				if constexpr (Q::kSub >= 0) { m -= static_cast<uint32_t>(row_value<Q, Q::kSub>(P.base, V, lane, rows[j])); }
+				emit<Q>(P, kv, j, static_cast<int32_t>(m));
+			}
 		}
 	}
 }

@@ -386,7 +386,7 @@ fls_status jit_filter_agg(const fls_column* cols, const fls_filter* filters, uin
 	return launch_fixed(make_key('F', P.S.warps, sh.key), &P, grid, 32u * P.S.warps, smem, stream, used);
 }
 
-bool jit_probe_shape(const fls_join_agg_desc* d, JitProbeShape& sh) {
+bool jit_probe_shape(const fls_join_groupby_desc* d, JitProbeShape& sh) {
 	sh.n_staged = 0;
 	for (uint32_t q = 0; q < d->n_probes; ++q) {
 		for (uint32_t g = 0; g < q; ++g) {
@@ -394,14 +394,16 @@ bool jit_probe_shape(const fls_join_agg_desc* d, JitProbeShape& sh) {
 		}
 		sh.staged[sh.n_staged++] = d->probes[q].col;
 	}
-	sh.agg = -1;
-	for (uint32_t i = 0; i < sh.n_staged; ++i) {
-		if (sh.staged[i] == d->agg_col) { sh.agg = static_cast<int>(i); }
-	}
-	if (sh.agg < 0) {
-		sh.agg                   = static_cast<int>(sh.n_staged);
-		sh.staged[sh.n_staged++] = d->agg_col;
-	}
+	auto slot_of = [&](int32_t c) -> int {
+		if (c < 0) { return -1; }
+		for (uint32_t i = 0; i < sh.n_staged; ++i) {
+			if (sh.staged[i] == static_cast<uint32_t>(c)) { return static_cast<int>(i); }
+		}
+		sh.staged[sh.n_staged] = static_cast<uint32_t>(c);
+		return static_cast<int>(sh.n_staged++);
+	};
+	sh.agg = slot_of(static_cast<int32_t>(d->agg_col));
+	sh.sub = slot_of(d->agg_sub_col);
 	for (uint32_t i = 0; i < sh.n_staged; ++i) {
 		if (!uniform_for(d->cols[sh.staged[i]], d->cols[sh.staged[0]].layout)) { return false; }
 	}
@@ -415,8 +417,8 @@ bool jit_probe_shape(const fls_join_agg_desc* d, JitProbeShape& sh) {
 		const int64_t     lo = static_cast<int64_t>(kc.base) - p.keys_min;
 		const int64_t     hi = lo + (kc.bw >= 32 ? (int64_t {1} << 32) : (int64_t {1} << kc.bw)) - 1;
 		if (kc.bw < 32 && lo >= 0 && hi < p.ht_len) { direct |= 1u << q; }
-		const uint64_t   words = p.kind == 1 ? (static_cast<uint64_t>(p.ht_len) + 31u) / 32u
-		                                     : 2ull * static_cast<uint64_t>(p.ht_len);
+		const uint64_t words = p.kind == 1 ? (static_cast<uint64_t>(p.ht_len) + 31u) / 32u
+		                                   : 2ull * static_cast<uint64_t>(p.ht_len);
 		if (p.kind == 2) { kinds |= 1u << q; }
 		sh.smem_off[q] = 0;
 		if (sh.cta_words + words <= kJitTableWords) {
@@ -427,14 +429,16 @@ bool jit_probe_shape(const fls_join_agg_desc* d, JitProbeShape& sh) {
 	}
 	fls_column sc[FLS_MAX_QUERY_COLS];
 	for (uint32_t i = 0; i < sh.n_staged; ++i) { sc[i] = d->cols[sh.staged[i]]; }
-	char head[128];
-	std::snprintf(head, sizeof(head), "%u, %u, %d, %d, %d, %u, %u, %u", static_cast<unsigned>(sc[0].layout),
-	              d->n_probes, sh.agg, d->key_a, d->key_b, kinds, in_smem, direct);
+	int kp[FLS_MAX_GROUP_KEYS] = {-1, -1, -1};
+	for (uint32_t k = 0; k < d->n_keys; ++k) { kp[k] = d->key_probe[k]; }
+	char head[160];
+	std::snprintf(head, sizeof(head), "%u, %u, %d, %d, %u, %d, %d, %d, %u, %u, %u", static_cast<unsigned>(sc[0].layout),
+	              d->n_probes, sh.agg, sh.sub, d->n_keys, kp[0], kp[1], kp[2], kinds, in_smem, direct);
 	sh.key = key_args(sc, sh.n_staged, head);
 	return true;
 }
 
-bool jit_compile(const fls_join_agg_desc* d, const JitProbeShape& sh) {
+bool jit_compile(const fls_join_groupby_desc* d, const JitProbeShape& sh) {
 	fls_column sc[FLS_MAX_QUERY_COLS];
 	for (uint32_t i = 0; i < sh.n_staged; ++i) { sc[i] = d->cols[sh.staged[i]]; }
 	bool               have;
@@ -447,7 +451,7 @@ bool jit_compile(const fls_join_agg_desc* d, const JitProbeShape& sh) {
 	return compiled_entry(make_key('P', S.warps, sh.key)).state > 0;
 }
 
-fls_status jit_probe_groupby(const fls_join_agg_desc* d, int32_t* d_res, int32_t sparse_rows, cudaStream_t stream,
+fls_status jit_probe_groupby(const fls_join_groupby_desc* d, int32_t* d_res, int32_t sparse_rows, cudaStream_t stream,
                              bool& used) {
 	used = false;
 	JitProbeShape sh;
@@ -469,9 +473,14 @@ fls_status jit_probe_groupby(const fls_join_agg_desc* d, int32_t* d_res, int32_t
 		P.kmin[q]     = d->probes[q].keys_min;
 		P.smem_off[q] = sh.smem_off[q];
 	}
-	P.mul         = d->group_mul;
+	for (uint32_t k = 0; k < FLS_MAX_GROUP_KEYS; ++k) {
+		P.key_mul[k]  = k < d->n_keys ? d->key_mul[k] : 0;
+		P.key_slot[k] = k < d->n_keys ? d->key_slot[k] : -1;
+	}
 	P.sub         = d->group_sub;
 	P.n_groups    = d->n_groups;
+	P.stride      = d->res_stride;
+	P.sum_slot    = d->sum_slot;
 	P.sparse_rows = sparse_rows;
 	P.res         = d_res;
 	return launch_fixed(make_key('P', P.S.warps, sh.key), &P, grid, 32u * P.S.warps, smem, stream, used);

@@ -326,16 +326,17 @@ struct JitProbeShape {
 	uint32_t    staged[FLS_MAX_QUERY_COLS];
 	uint32_t    n_staged = 0;
 	int         agg      = -1;
+	int         sub      = -1; // staged column subtracted from the measure
 	uint32_t    smem_off[FLS_MAX_PROBES];
 	uint32_t    cta_words = 0;
 	std::string key;
 };
 // False when a staged column is not uniform FOR or one column is probed twice
 // (the descriptor must already be validated).
-bool       jit_probe_shape(const fls_join_agg_desc* desc, JitProbeShape& sh);
-bool       jit_compile(const fls_join_agg_desc* desc, const JitProbeShape& sh);
-fls_status jit_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res, int32_t sparse_rows, cudaStream_t stream,
-                             bool& used);
+bool       jit_probe_shape(const fls_join_groupby_desc* desc, JitProbeShape& sh);
+bool       jit_compile(const fls_join_groupby_desc* desc, const JitProbeShape& sh);
+fls_status jit_probe_groupby(const fls_join_groupby_desc* desc, int32_t* d_res, int32_t sparse_rows,
+                             cudaStream_t stream, bool& used);
 // Decode of a uniform FOR column: mode 0 = fused uint64 sum into d_sum, mode 1
 // = to HBM (stored order) into d_out.
 fls_status jit_decode(const fls_column* col, int mode, uint32_t* d_out, uint64_t* d_sum, cudaStream_t stream,

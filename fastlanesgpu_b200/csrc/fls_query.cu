@@ -217,7 +217,8 @@ struct TableState {
 	const uint32_t* tables;
 };
 
-// Shared parameters of the probe + group-by operators (fls_q21.cu probe_v1).
+// Shared parameters of the probe + group-by operators (fls_q21.cu,
+// fls_q31.cu, fls_q41.cu probe_v1).
 struct ProbeParams {
 	uint32_t       n_probes;
 	uint32_t       p_col[FLS_MAX_PROBES];
@@ -226,10 +227,22 @@ struct ProbeParams {
 	int32_t        p_min[FLS_MAX_PROBES];
 	int32_t        p_kind[FLS_MAX_PROBES];
 	uint32_t       p_smem_off[FLS_MAX_PROBES]; // words into the CTA scratch, ~0u = probe global memory
-	int32_t        key_a, key_b, mul, sub, n_groups;
+	int32_t        n_keys;
+	int32_t        key_probe[FLS_MAX_GROUP_KEYS], key_mul[FLS_MAX_GROUP_KEYS], key_slot[FLS_MAX_GROUP_KEYS];
+	int32_t        sub, n_groups;
+	uint32_t       stride, sum_slot; // group record: int32 words, word of the int64 sum
 	uint32_t       agg_col;
+	int32_t        agg_sub; // column subtracted from the measure, or -1
 	int32_t*       res;
 	int32_t        sparse_rows; // see FilterAggOp
+
+	// Payload of probe q becomes the value of every key that names it.
+	__device__ __forceinline__ void take_key(uint32_t q, int32_t val, int32_t (&kv)[FLS_MAX_GROUP_KEYS]) const {
+#pragma unroll
+		for (int k = 0; k < FLS_MAX_GROUP_KEYS; ++k) {
+			if (k < n_keys && key_probe[k] == static_cast<int32_t>(q)) { kv[k] = val; }
+		}
+	}
 
 	// Small hash tables are staged into shared memory once per CTA: PHT_1 tables
 	// as a presence bitmap (the probe only tests slot != 0, crystal-opt/
@@ -307,19 +320,28 @@ struct ProbeParams {
 		return (s.x | s.y) != 0u;
 	}
 
-	// Group-by epilogue of one selected row (fls_q21.cu:67-77).
-	__device__ __forceinline__ void emit(int32_t a, int32_t b, uint32_t measure, uint32_t* err) const {
-		// (a*mul + (b - sub)) % n_groups in wrapping 32-bit arithmetic.
-		const int32_t key = static_cast<int32_t>(static_cast<uint32_t>(a) * static_cast<uint32_t>(mul) +
-		                                         (static_cast<uint32_t>(b) - static_cast<uint32_t>(sub)));
-		const int32_t g   = static_cast<uint32_t>(key) < static_cast<uint32_t>(n_groups) ? key : key % n_groups;
+	// Group-by epilogue of one selected row (fls_q21.cu:67-77, fls_q31.cu:82-91,
+	// fls_q41.cu:96-104): the group of the key values in wrapping 32-bit
+	// arithmetic, the key values into their words of the group record, the
+	// measure (an int32, widened) into its int64 sum.
+	__device__ __forceinline__ void emit(const int32_t (&kv)[FLS_MAX_GROUP_KEYS], uint32_t measure, uint32_t* err) const {
+		uint32_t key = 0u - static_cast<uint32_t>(sub);
+#pragma unroll
+		for (int k = 0; k < FLS_MAX_GROUP_KEYS; ++k) {
+			if (k < n_keys) { key += static_cast<uint32_t>(kv[k]) * static_cast<uint32_t>(key_mul[k]); }
+		}
+		const int32_t g = key < static_cast<uint32_t>(n_groups) ? static_cast<int32_t>(key)
+		                                                         : static_cast<int32_t>(key) % n_groups;
 		if (g < 0) {
 			raise_err(err, kErrHash);
 			return;
 		}
-		res[4 * g]     = b;
-		res[4 * g + 1] = a;
-		atomicAdd(reinterpret_cast<unsigned long long*>(res + 4 * g + 2),
+		int32_t* rec = res + static_cast<int64_t>(g) * stride;
+#pragma unroll
+		for (int k = 0; k < FLS_MAX_GROUP_KEYS; ++k) {
+			if (k < n_keys && key_slot[k] >= 0) { rec[key_slot[k]] = kv[k]; }
+		}
+		atomicAdd(reinterpret_cast<unsigned long long*>(rec + sum_slot),
 		          static_cast<unsigned long long>(static_cast<long long>(static_cast<int32_t>(measure))));
 	}
 };
@@ -353,6 +375,7 @@ struct ProbeGroupByRowOp : ProbeParams {
 		}
 		// Row-at-a-time rest; FOR vectors use the hoisted fast field reader.
 		bool fast = staged(ws, st, i, agg_col).vi.scheme == FLS_SCHEME_FOR;
+		if (agg_sub >= 0) { fast = fast && staged(ws, st, i, static_cast<uint32_t>(agg_sub)).vi.scheme == FLS_SCHEME_FOR; }
 		for (uint32_t q = p; q < n_probes; ++q) { fast = fast && staged(ws, st, i, p_col[q]).vi.scheme == FLS_SCHEME_FOR; }
 		if (fast) {
 			dev::ForRows kr[FLS_MAX_PROBES], mr;
@@ -367,12 +390,17 @@ struct ProbeGroupByRowOp : ProbeParams {
 				const StagedVec sv = staged(ws, st, i, agg_col);
 				mr.init(sv.s, sv.vi, lane);
 			}
+			dev::ForRows sr {};
+			if (agg_sub >= 0) {
+				const StagedVec sv = staged(ws, st, i, static_cast<uint32_t>(agg_sub));
+				sr.init(sv.s, sv.vi, lane);
+			}
 			const int n_it = max_rows(mask);
 			for (int it = 0; it < n_it; ++it) {
 				const bool     have = mask != 0u;
 				const uint32_t r    = have ? static_cast<uint32_t>(__ffs(mask)) - 1u : 0u;
 				mask &= mask - 1u;
-				int32_t a = 0, b = 0;
+				int32_t kv[FLS_MAX_GROUP_KEYS] = {0, 0, 0};
 				bool    pass = have;
 #pragma unroll
 				for (uint32_t q = 0; q < FLS_MAX_PROBES; ++q) {
@@ -380,31 +408,35 @@ struct ProbeGroupByRowOp : ProbeParams {
 						int32_t val = 0;
 						const uint32_t key = kr[q].get(r);
 						if (pass) { pass = probe(S, q, key, &val, cfg.err); }
-						if (static_cast<int32_t>(q) == key_a) { a = val; }
-						if (static_cast<int32_t>(q) == key_b) { b = val; }
+						take_key(q, val, kv);
 					}
 				}
-				const uint32_t m = mr.get(r);
-				if (pass) { emit(a, b, m, cfg.err); }
+				const uint32_t m = mr.get(r) - (agg_sub >= 0 ? sr.get(r) : 0u);
+				if (pass) { emit(kv, m, cfg.err); }
 			}
 			return;
 		}
 		while (mask) {
 			const uint32_t r = static_cast<uint32_t>(__ffs(mask)) - 1u;
 			mask &= mask - 1u;
-			int32_t a = 0, b = 0;
+			int32_t kv[FLS_MAX_GROUP_KEYS] = {0, 0, 0};
 			bool    pass = true;
 			for (uint32_t q = p; q < n_probes && pass; ++q) {
 				const StagedVec sv = staged(ws, st, i, p_col[q]);
 				int32_t         val = 0;
 				pass = !sv.bad() && probe(S, q, dev::value_at(sv.s, sv.vi, lane, r), &val, cfg.err);
-				if (static_cast<int32_t>(q) == key_a) { a = val; }
-				if (static_cast<int32_t>(q) == key_b) { b = val; }
+				take_key(q, val, kv);
 			}
 			if (!pass) { continue; }
 			const StagedVec sm = staged(ws, st, i, agg_col);
 			if (sm.bad()) { continue; }
-			emit(a, b, dev::value_at(sm.s, sm.vi, lane, r), cfg.err);
+			uint32_t m = dev::value_at(sm.s, sm.vi, lane, r);
+			if (agg_sub >= 0) {
+				const StagedVec sb = staged(ws, st, i, static_cast<uint32_t>(agg_sub));
+				if (sb.bad()) { continue; }
+				m -= dev::value_at(sb.s, sb.vi, lane, r);
+			}
+			emit(kv, m, cfg.err);
 		}
 	}
 	__device__ void finish(State&, uint32_t, const StageCfg&) const {}
@@ -417,37 +449,83 @@ struct ProbeGroupByDenseOp : ProbeParams {
 
 	__device__ void cta_setup(State& S, uint32_t* cta_smem, const StageCfg&) const { stage_tables(S, cta_smem); }
 
+	// Decodes probe column q and, for the selected rows, looks up its payload.
+	__device__ __forceinline__ void payloads(const State& S, uint32_t q, uint32_t mask, const WarpStage& ws, uint32_t st,
+	                                         uint32_t i, uint32_t lane, uint32_t (&vals)[32], uint32_t* err) const {
+		const StagedVec sv = staged(ws, st, i, p_col[q]);
+		dev::decode_vals(sv.s, sv.vi, ws.dict(), lane, vals);
+#pragma unroll
+		for (uint32_t r = 0; r < 32; ++r) {
+			int32_t val = 0;
+			if ((mask >> r) & 1u) { probe(S, q, vals[r], &val, err); }
+			vals[r] = static_cast<uint32_t>(val);
+		}
+	}
+
 	__device__ void process(State& S, uint64_t v, const WarpStage& ws, uint32_t st, uint32_t i, uint32_t lane,
 	                        const StageCfg& cfg) const {
 		uint32_t mask = valid_rows(cfg, v, lane);
 		uint32_t vals[32];
-		int32_t  pa[32], pb[32];
+		// 1. the selection: every probe over the whole vector
 		for (uint32_t p = 0; p < n_probes; ++p) {
 			const StagedVec sv = staged(ws, st, i, p_col[p]);
 			if (sv.bad()) { return; }
 			dev::decode_vals(sv.s, sv.vi, ws.dict(), lane, vals);
-			const bool wa = static_cast<int32_t>(p) == key_a, wb = static_cast<int32_t>(p) == key_b;
-			uint32_t   hit = 0;
+			uint32_t hit = 0;
 #pragma unroll
 			for (uint32_t r = 0; r < 32; ++r) {
 				if ((mask >> r) & 1u) {
 					int32_t val = 0;
-					if (probe(S, p, vals[r], &val, cfg.err)) {
-						hit |= 1u << r;
-						if (wa) { pa[r] = val; }
-						if (wb) { pb[r] = val; }
-					}
+					if (probe(S, p, vals[r], &val, cfg.err)) { hit |= 1u << r; }
 				}
 			}
 			mask &= hit;
 			if (!__any_sync(0xffffffffu, mask)) { return; }
 		}
-		const StagedVec sm = staged(ws, st, i, agg_col);
-		if (sm.bad()) { return; }
-		dev::decode_vals(sm.s, sm.vi, ws.dict(), lane, vals);
+		if (staged(ws, st, i, agg_col).bad() || (agg_sub >= 0 && staged(ws, st, i, static_cast<uint32_t>(agg_sub)).bad())) {
+			return;
+		}
+		// 2. group ids: the key payloads re-read for the selected rows
+		uint32_t grp[32];
+#pragma unroll
+		for (uint32_t r = 0; r < 32; ++r) { grp[r] = 0u - static_cast<uint32_t>(sub); }
+		for (int k = 0; k < n_keys; ++k) {
+			payloads(S, static_cast<uint32_t>(key_probe[k]), mask, ws, st, i, lane, vals, cfg.err);
+#pragma unroll
+			for (uint32_t r = 0; r < 32; ++r) { grp[r] += vals[r] * static_cast<uint32_t>(key_mul[k]); }
+		}
 #pragma unroll
 		for (uint32_t r = 0; r < 32; ++r) {
-			if ((mask >> r) & 1u) { emit(pa[r], pb[r], vals[r], cfg.err); }
+			const int32_t key = static_cast<int32_t>(grp[r]);
+			const int32_t g   = grp[r] < static_cast<uint32_t>(n_groups) ? key : key % n_groups;
+			if (((mask >> r) & 1u) && g < 0) {
+				raise_err(cfg.err, kErrHash);
+				mask &= ~(1u << r);
+			}
+			grp[r] = static_cast<uint32_t>(g);
+		}
+		// 3. key words of the group records
+		for (int k = 0; k < n_keys; ++k) {
+			if (key_slot[k] < 0) { continue; }
+			payloads(S, static_cast<uint32_t>(key_probe[k]), mask, ws, st, i, lane, vals, cfg.err);
+#pragma unroll
+			for (uint32_t r = 0; r < 32; ++r) {
+				if ((mask >> r) & 1u) { res[static_cast<int64_t>(grp[r]) * stride + key_slot[k]] = static_cast<int32_t>(vals[r]); }
+			}
+		}
+		// 4. the measure (minus the subtracted column) into the sums
+		const StagedVec sm = staged(ws, st, i, agg_col);
+		dev::decode_vals(sm.s, sm.vi, ws.dict(), lane, vals);
+		if (agg_sub >= 0) {
+			const StagedVec sb = staged(ws, st, i, static_cast<uint32_t>(agg_sub));
+			dev::decode_each<true>(sb.s, sb.vi, ws.dict(), lane, [&](int r, uint32_t y) { vals[r] -= y; });
+		}
+#pragma unroll
+		for (uint32_t r = 0; r < 32; ++r) {
+			if ((mask >> r) & 1u) {
+				atomicAdd(reinterpret_cast<unsigned long long*>(res + static_cast<int64_t>(grp[r]) * stride + sum_slot),
+				          static_cast<unsigned long long>(static_cast<long long>(static_cast<int32_t>(vals[r]))));
+			}
 		}
 	}
 	__device__ void finish(State&, uint32_t, const StageCfg&) const {}
@@ -541,6 +619,67 @@ fls_status check_join_desc(const fls_join_agg_desc* desc) {
 	return FLS_OK;
 }
 
+// fls_q21.cu's group-by as the general form: keys (payload of key_a) x mul and
+// (payload of key_b) x 1, record {b, a, int64 sum}.
+fls_join_groupby_desc groupby_of(const fls_join_agg_desc& d) {
+	fls_join_groupby_desc g {};
+	g.cols   = d.cols;
+	g.n_cols = d.n_cols;
+	for (uint32_t p = 0; p < FLS_MAX_PROBES; ++p) { g.probes[p] = d.probes[p]; }
+	g.n_probes     = d.n_probes;
+	g.agg_col      = d.agg_col;
+	g.agg_sub_col  = -1;
+	g.n_keys       = 2;
+	g.key_probe[0] = d.key_a;
+	g.key_probe[1] = d.key_b;
+	g.key_probe[2] = -1;
+	g.key_mul[0]   = d.group_mul;
+	g.key_mul[1]   = 1;
+	g.key_mul[2]   = 0;
+	g.key_slot[0]  = 1;
+	g.key_slot[1]  = 0;
+	g.key_slot[2]  = -1;
+	g.group_sub    = d.group_sub;
+	g.n_groups     = d.n_groups;
+	g.res_stride   = 4;
+	g.sum_slot     = 2;
+	return g;
+}
+
+// Validates a general join + group-by descriptor.
+fls_status check_groupby_desc(const fls_join_groupby_desc* d) {
+	if (!d || !d->cols) { return set_error(FLS_ERR_INVALID_ARG, "fls_query_join_groupby: null pointer"); }
+	if (d->n_probes == 0 || d->n_probes > FLS_MAX_PROBES) { return set_error(FLS_ERR_INVALID_ARG, "1..4 probes"); }
+	if (d->agg_col >= d->n_cols || d->agg_sub_col >= static_cast<int32_t>(d->n_cols) || d->agg_sub_col < -1 ||
+	    d->n_groups <= 0) {
+		return set_error(FLS_ERR_INVALID_ARG, "bad measure column or group count");
+	}
+	if (d->res_stride < 2 || (d->res_stride & 1u) || (d->sum_slot & 1u) || d->sum_slot + 1u >= d->res_stride) {
+		return set_error(FLS_ERR_INVALID_ARG, "group record: even stride, even sum word inside the record");
+	}
+	if (d->n_keys == 0 || d->n_keys > FLS_MAX_GROUP_KEYS) { return set_error(FLS_ERR_INVALID_ARG, "1..3 group keys"); }
+	for (uint32_t k = 0; k < d->n_keys; ++k) {
+		const int32_t q = d->key_probe[k], w = d->key_slot[k];
+		if (q < 0 || q >= static_cast<int32_t>(d->n_probes) || d->probes[q].kind != 2) {
+			return set_error(FLS_ERR_INVALID_ARG, "group keys must name PHT_2 probes");
+		}
+		if (w < -1 || w >= static_cast<int32_t>(d->res_stride) || w == static_cast<int32_t>(d->sum_slot) ||
+		    w == static_cast<int32_t>(d->sum_slot) + 1) {
+			return set_error(FLS_ERR_INVALID_ARG, "key word outside the group record or on the sum");
+		}
+	}
+	for (uint32_t p = 0; p < d->n_probes; ++p) {
+		const fls_probe& pr = d->probes[p];
+		if (pr.col >= d->n_cols || !pr.ht || pr.ht_len <= 0 || (pr.kind != 1 && pr.kind != 2)) {
+			return set_error(FLS_ERR_INVALID_ARG, "bad probe");
+		}
+		if (pr.kind == 2 && (reinterpret_cast<uintptr_t>(pr.ht) & 7u)) {
+			return set_error(FLS_ERR_ALIGNMENT, "PHT_2 tables must be 8-byte aligned");
+		}
+	}
+	return FLS_OK;
+}
+
 } // namespace
 
 extern "C" {
@@ -597,6 +736,13 @@ fls_status fls_jit_precompile(const fls_filter_agg_desc* desc) {
 fls_status fls_jit_precompile_probe(const fls_join_agg_desc* desc) {
 	fls_status s = check_join_desc(desc);
 	if (s != FLS_OK) { return s; }
+	const fls_join_groupby_desc g = groupby_of(*desc);
+	return fls_jit_precompile_join(&g);
+}
+
+fls_status fls_jit_precompile_join(const fls_join_groupby_desc* desc) {
+	fls_status s = check_groupby_desc(desc);
+	if (s != FLS_OK) { return s; }
 	JitProbeShape sh;
 	if (!jit_probe_shape(desc, sh)) {
 		return set_error(FLS_ERR_UNSUPPORTED, "query does not qualify for specialisation (uniform FOR columns only)");
@@ -623,10 +769,10 @@ fls_status fls_pht_build(const int32_t* d_filter, int32_t filter_eq, const int32
 	return cuda_check(cudaGetLastError(), "pht_build_kernel launch");
 }
 
-fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res, fls_stream_t stream) {
-	if (!d_res) { return set_error(FLS_ERR_INVALID_ARG, "fls_query_probe_groupby: null pointer"); }
+fls_status fls_query_join_groupby(const fls_join_groupby_desc* desc, int32_t* d_res, fls_stream_t stream) {
+	if (!d_res) { return set_error(FLS_ERR_INVALID_ARG, "fls_query_join_groupby: null pointer"); }
 	if (reinterpret_cast<uintptr_t>(d_res) & 7u) { return set_error(FLS_ERR_ALIGNMENT, "result must be 8-byte aligned"); }
-	fls_status s = check_join_desc(desc);
+	fls_status s = check_groupby_desc(desc);
 	if (s != FLS_OK) { return s; }
 	ProbeParams op {};
 	op.n_probes = desc->n_probes;
@@ -649,12 +795,18 @@ fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res
 			op.p_smem_off[p] = ~0u;
 		}
 	}
-	op.key_a    = desc->key_a;
-	op.key_b    = desc->key_b;
-	op.mul      = desc->group_mul;
-	op.sub      = desc->group_sub;
-	op.n_groups = desc->n_groups;
+	op.n_keys = static_cast<int32_t>(desc->n_keys);
+	for (uint32_t k = 0; k < FLS_MAX_GROUP_KEYS; ++k) {
+		op.key_probe[k] = k < desc->n_keys ? desc->key_probe[k] : -1;
+		op.key_mul[k]   = k < desc->n_keys ? desc->key_mul[k] : 0;
+		op.key_slot[k]  = k < desc->n_keys ? desc->key_slot[k] : -1;
+	}
+	op.sub         = desc->group_sub;
+	op.n_groups    = desc->n_groups;
+	op.stride      = desc->res_stride;
+	op.sum_slot    = desc->sum_slot;
 	op.agg_col     = desc->agg_col;
+	op.agg_sub     = desc->agg_sub_col;
 	op.res         = d_res;
 	op.sparse_rows = tuning_sparse_rows();
 	// The row-at-a-time form needs random access to every column it reads.
@@ -671,7 +823,10 @@ fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res
 	s = plan_stages(desc->cols, desc->n_cols, 0u, cta_words, cfg, grid, threads, smem);
 	if (s != FLS_OK) { return s; }
 	cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-	s = cuda_check(cudaMemsetAsync(d_res, 0, sizeof(int32_t) * 4u * static_cast<size_t>(desc->n_groups), st),
+	s = cuda_check(cudaMemsetAsync(d_res, 0,
+	                               sizeof(int32_t) * static_cast<size_t>(desc->res_stride) *
+	                                   static_cast<size_t>(desc->n_groups),
+	                               st),
 	               "cudaMemsetAsync");
 	if (s != FLS_OK) { return s; }
 	if (tuning_jit()) {
@@ -689,4 +844,11 @@ fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res
 	return launch_staged(cfg, dop, grid, threads, smem, st);
 }
 
+fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res, fls_stream_t stream) {
+	if (!d_res) { return set_error(FLS_ERR_INVALID_ARG, "fls_query_probe_groupby: null pointer"); }
+	fls_status s = check_join_desc(desc);
+	if (s != FLS_OK) { return s; }
+	const fls_join_groupby_desc g = groupby_of(*desc);
+	return fls_query_join_groupby(&g, d_res, stream);
+}
 } // extern "C"

@@ -105,6 +105,63 @@ def q21_tables(n: int, seed: int = 21, part_ids: int = 1 << 19, supp_ids: int = 
 
 
 Q21_BITS = {"lo_suppkey": 17, "lo_partkey": 19, "lo_orderdate": 12, "lo_revenue": 24}
+
+
+def q31_tables(n: int, seed: int = 31, cust_ids: int = 1 << 18, supp_ids: int = 1 << 17) -> dict:
+    """Q3.1-shape join workload: fact foreign keys customer (18 bit), supplier
+    (17 bit), date (12 bit) and revenue (24 bit); dimension nations U[0,25)
+    with region = nation // 5; customer and supplier filtered on region 1
+    (1/5 each), dates on years 1992..1997."""
+    g = rng(seed)
+    c_nation = g.integers(0, 25, size=cust_ids).astype(np.int32)
+    s_nation = g.integers(0, 25, size=supp_ids).astype(np.int32)
+    d_year = year_of_day(np.arange(N_DAYS))
+    return {
+        "lo_custkey": g.integers(0, cust_ids, size=n).astype(np.int32),
+        "lo_suppkey": g.integers(0, supp_ids, size=n).astype(np.int32),
+        "lo_orderdate": g.integers(0, N_DAYS, size=n).astype(np.int32),
+        "lo_revenue": g.integers(90000, 10_500_001, size=n).astype(np.int32),
+        "c_custkey": np.arange(cust_ids, dtype=np.int32), "c_nation": c_nation,
+        "c_region": (c_nation // 5).astype(np.int32),
+        "s_suppkey": np.arange(supp_ids, dtype=np.int32), "s_nation": s_nation,
+        "s_region": (s_nation // 5).astype(np.int32),
+        "d_datekey": np.arange(N_DAYS, dtype=np.int32), "d_year": d_year,
+        "d_in_range": ((d_year >= 1992) & (d_year <= 1997)).astype(np.int32),
+    }
+
+
+Q31_BITS = {"lo_suppkey": 17, "lo_custkey": 18, "lo_orderdate": 12, "lo_revenue": 24}
+Q31_GROUPS = 7 * 25 * 25
+
+
+def q41_tables(n: int, seed: int = 41, cust_ids: int = 1 << 18, supp_ids: int = 1 << 17,
+               part_ids: int = 1 << 19) -> dict:
+    """Q4.1-shape join workload: fact foreign keys supplier, customer, part
+    (19 bit), date; revenue (24 bit) and supply cost U[50000, 150000) (18 bit);
+    supplier and customer on region 1, part manufacturer in {0, 1} of 5 (2/5),
+    every date."""
+    g = rng(seed)
+    c_nation = g.integers(0, 25, size=cust_ids).astype(np.int32)
+    s_nation = g.integers(0, 25, size=supp_ids).astype(np.int32)
+    p_mfgr = g.integers(0, 5, size=part_ids).astype(np.int32)
+    return {
+        "lo_suppkey": g.integers(0, supp_ids, size=n).astype(np.int32),
+        "lo_custkey": g.integers(0, cust_ids, size=n).astype(np.int32),
+        "lo_partkey": g.integers(0, part_ids, size=n).astype(np.int32),
+        "lo_orderdate": g.integers(0, N_DAYS, size=n).astype(np.int32),
+        "lo_revenue": g.integers(90000, 10_500_001, size=n).astype(np.int32),
+        "lo_supplycost": g.integers(50000, 150000, size=n).astype(np.int32),
+        "c_custkey": np.arange(cust_ids, dtype=np.int32), "c_nation": c_nation,
+        "c_region": (c_nation // 5).astype(np.int32),
+        "s_suppkey": np.arange(supp_ids, dtype=np.int32), "s_region": (s_nation // 5).astype(np.int32),
+        "p_partkey": np.arange(part_ids, dtype=np.int32), "p_mfgr_low": (p_mfgr < 2).astype(np.int32),
+        "d_datekey": np.arange(N_DAYS, dtype=np.int32), "d_year": year_of_day(np.arange(N_DAYS)),
+    }
+
+
+Q41_BITS = {"lo_suppkey": 17, "lo_custkey": 18, "lo_partkey": 19, "lo_orderdate": 12, "lo_revenue": 24,
+            "lo_supplycost": 18}
+Q41_GROUPS = 7 * 25
 N_GROUPS = (1998 - 1992 + 1) * (5 * 5 * 40)
 
 
@@ -161,3 +218,43 @@ def mixed_columns(n_cols: int = 64, lo_log: int = 16, hi_log: int = 26, seed: in
             v = vals[run]
         cols.append((fam, v.to(torch.int32)))
     return cols
+
+
+def ssb_join(query: str, n: int, seed: int, device="cuda"):
+    """Device columns, hash tables and the join + group-by arguments of the
+    Q3.1 / Q4.1 shapes (fls_q31.cu / fls_q41.cu): (tables, hash tables, host
+    encoded columns, device columns, probes, join_groupby keyword arguments)."""
+    import torch
+
+    from . import ops
+    from .column import EncodedColumn
+    if query == "q31":
+        t = q31_tables(n, seed=seed)
+        names, bits = ["lo_suppkey", "lo_custkey", "lo_orderdate", "lo_revenue"], Q31_BITS
+    else:
+        t = q41_tables(n, seed=seed)
+        names = ["lo_suppkey", "lo_custkey", "lo_partkey", "lo_orderdate", "lo_revenue", "lo_supplycost"]
+        bits = Q41_BITS
+    dev = {k: torch.from_numpy(v).to(device) for k, v in t.items() if not k.startswith("lo_")}
+    hcols = [EncodedColumn.uniform(t[k], bw=bits[k]) for k in names]
+    dcols = [c.to_device(device) for c in hcols]
+    if query == "q31":
+        ht_s = ops.build_pht(dev["s_suppkey"], dev["s_suppkey"].numel(), vals=dev["s_nation"], filt=dev["s_region"])
+        ht_c = ops.build_pht(dev["c_custkey"], dev["c_custkey"].numel(), vals=dev["c_nation"], filt=dev["c_region"])
+        ht_d = ops.build_pht(dev["d_datekey"], N_DAYS, vals=dev["d_year"], filt=dev["d_in_range"])
+        tables = {"ht_s": ht_s, "ht_c": ht_c, "ht_d": ht_d}
+        probes = [(0, ht_s, ht_s.numel() // 2, 0, 2), (1, ht_c, ht_c.numel() // 2, 0, 2),
+                  (2, ht_d, ht_d.numel() // 2, 0, 2)]
+        kw = dict(agg_col=3, keys=[(0, 175, 2), (1, 7, 1), (2, 1, 0)], group_sub=1992, n_groups=Q31_GROUPS,
+                  res_stride=6, sum_slot=4)
+    else:
+        ht_s = ops.build_pht(dev["s_suppkey"], dev["s_suppkey"].numel(), filt=dev["s_region"])
+        ht_c = ops.build_pht(dev["c_custkey"], dev["c_custkey"].numel(), vals=dev["c_nation"], filt=dev["c_region"])
+        ht_p = ops.build_pht(dev["p_partkey"], dev["p_partkey"].numel(), filt=dev["p_mfgr_low"])
+        ht_d = ops.build_pht(dev["d_datekey"], N_DAYS, vals=dev["d_year"])
+        tables = {"ht_s": ht_s, "ht_c": ht_c, "ht_p": ht_p, "ht_d": ht_d}
+        probes = [(0, ht_s, ht_s.numel(), 0, 1), (1, ht_c, ht_c.numel() // 2, 0, 2), (2, ht_p, ht_p.numel(), 0, 1),
+                  (3, ht_d, ht_d.numel() // 2, 0, 2)]
+        kw = dict(agg_col=4, keys=[(1, 7, 1), (3, 1, 0)], group_sub=1992, n_groups=Q41_GROUPS, res_stride=4,
+                  sum_slot=2, agg_sub_col=5)
+    return t, tables, hcols, dcols, probes, kw

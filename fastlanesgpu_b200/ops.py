@@ -23,7 +23,8 @@ import ctypes
 
 import numpy as np
 
-from ._lib import (MAX_FILTERS, MAX_PROBES, ORDER_STORED, Column, FilterAggDesc, JitStats, JoinAggDesc, check, lib)
+from ._lib import (MAX_FILTERS, MAX_GROUP_KEYS, MAX_PROBES, ORDER_STORED, Column, FilterAggDesc, JitStats, JoinAggDesc,
+                   JoinGroupbyDesc, check, lib)
 from .column import DeviceColumn, columns_array
 
 
@@ -204,6 +205,51 @@ def _join_desc(arr, n_cols: int, probes, agg_col, key_a, key_b, group_mul, group
     d.agg_col, d.key_a, d.key_b = agg_col, key_a, key_b
     d.group_mul, d.group_sub, d.n_groups = group_mul, group_sub, n_groups
     return d, arr
+
+
+def _groupby_desc(arr, n_cols: int, probes, agg_col, keys, group_sub, n_groups, res_stride, sum_slot, agg_sub_col):
+    if len(probes) > MAX_PROBES or not 1 <= len(keys) <= MAX_GROUP_KEYS:
+        raise ValueError("1..4 probes and 1..3 group keys")
+    d = JoinGroupbyDesc()
+    d.cols = arr
+    d.n_cols = n_cols
+    for i, (c, ht, ln, kmin, kind) in enumerate(probes):
+        d.probes[i].col, d.probes[i].ht_len = c, ln
+        d.probes[i].ht = ht if isinstance(ht, int) else ht.data_ptr()
+        d.probes[i].keys_min, d.probes[i].kind = kmin, kind
+    d.n_probes = len(probes)
+    d.agg_col, d.agg_sub_col = agg_col, agg_sub_col
+    d.n_keys = len(keys)
+    for k, (probe, mul, slot) in enumerate(keys):
+        d.key_probe[k], d.key_mul[k], d.key_slot[k] = probe, mul, slot
+    d.group_sub, d.n_groups, d.res_stride, d.sum_slot = group_sub, n_groups, res_stride, sum_slot
+    return d, arr
+
+
+def join_groupby(cols, probes, agg_col: int, keys, group_sub: int, n_groups: int, res_stride: int, sum_slot: int,
+                 agg_sub_col: int = -1, out=None):
+    """The general probe + group-by (fls_q21/q31/q41.cu probe_v1): probes
+    [(col, ht, ht_len, keys_min, kind)]; keys [(probe, multiplier, record word
+    or -1)]; group = (sum of payload * multiplier - group_sub) % n_groups;
+    records of res_stride int32 words with the int64 sum of cols[agg_col]
+    (minus cols[agg_sub_col]) at word sum_slot.  Returns the device int32 array."""
+    import torch
+    d, _keep = _groupby_desc(columns_array(cols), len(cols), probes, agg_col, keys, group_sub, n_groups, res_stride,
+                             sum_slot, agg_sub_col)
+    if out is None:
+        out = torch.empty(res_stride * n_groups, dtype=torch.int32, device=cols[0].data.device)
+    check(lib().fls_query_join_groupby(ctypes.byref(d), out.data_ptr(), _stream()), "fls_query_join_groupby")
+    return out
+
+
+def jit_precompile_join(col_descs, probes, agg_col, keys, group_sub, n_groups, res_stride, sum_slot,
+                        agg_sub_col: int = -1) -> None:
+    """Compiles the specialised join + group-by kernel for this query shape."""
+    descs = [c.desc if hasattr(c, "desc") else c for c in col_descs]
+    arr = (Column * len(descs))(*descs)
+    d, _keep = _groupby_desc(arr, len(descs), probes, agg_col, keys, group_sub, n_groups, res_stride, sum_slot,
+                             agg_sub_col)
+    check(lib().fls_jit_precompile_join(ctypes.byref(d)), "fls_jit_precompile_join")
 
 
 def jit_precompile_probe(col_descs, probes, agg_col: int, key_a: int, key_b: int, group_mul: int, group_sub: int,

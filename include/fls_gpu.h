@@ -235,6 +235,37 @@ typedef struct fls_join_agg_desc {
 
 fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res, fls_stream_t stream);
 
+/* The general form of the join + group-by kernels (fls_q21.cu probe_v1,
+ * fls_q31.cu:28-93 probe_v1, fls_q41.cu:27-112 probe_v1): probes in order,
+ * then group g = (sum over keys of payload[key_probe[k]] * key_mul[k] -
+ * group_sub) % n_groups (wrapping 32-bit arithmetic) over 1..3 PHT_2 payloads,
+ * and a record of res_stride int32 words per group: payload k at word
+ * key_slot[k] (-1: not written) and the int64 sum of the measure at word
+ * sum_slot.  The measure is cols[agg_col], or cols[agg_col] - cols[agg_sub_col]
+ * as an int32 difference (fls_q41.cu:101) when agg_sub_col >= 0.  Examples:
+ * Q2.1 keys (brand x7, year x1), sub 1992, stride 4, slots (1, 0), sum 2;
+ * Q3.1 keys (s_nation x175, c_nation x7, year x1), 4375 groups, stride 6,
+ * slots (2, 1, 0), sum 4; Q4.1 keys (c_nation x7, year x1), 175 groups,
+ * stride 4, slots (1, 0), sum 2, measure revenue - supplycost.  d_res
+ * (device, n_groups * res_stride int32, 8-byte aligned) is zeroed by the call. */
+#define FLS_MAX_GROUP_KEYS 3
+typedef struct fls_join_groupby_desc {
+	const fls_column* cols;
+	uint32_t          n_cols;
+	fls_probe         probes[FLS_MAX_PROBES];
+	uint32_t          n_probes;
+	uint32_t          agg_col;
+	int32_t           agg_sub_col;
+	uint32_t          n_keys;
+	int32_t           key_probe[FLS_MAX_GROUP_KEYS];
+	int32_t           key_mul[FLS_MAX_GROUP_KEYS];
+	int32_t           key_slot[FLS_MAX_GROUP_KEYS];
+	int32_t           group_sub, n_groups;
+	uint32_t          res_stride, sum_slot;
+} fls_join_groupby_desc;
+
+fls_status fls_query_join_groupby(const fls_join_groupby_desc* desc, int32_t* d_res, fls_stream_t stream);
+
 /* ------------------------------------ batched persistent execution (device) */
 
 /* One filter-aggregate query of a batch: rows with lo <= cols[col] <= hi,
@@ -381,8 +412,10 @@ const char* fls_jit_last_log(void);
  * the query does not qualify or the compile failed (fls_last_error has the
  * log). */
 fls_status fls_jit_precompile(const fls_filter_agg_desc* desc);
-/* The same for the kernel fls_query_probe_groupby would run. */
+/* The same for the kernel fls_query_probe_groupby / fls_query_join_groupby
+ * would run. */
 fls_status fls_jit_precompile_probe(const fls_join_agg_desc* desc);
+fls_status fls_jit_precompile_join(const fls_join_groupby_desc* desc);
 
 /* Number of kernels this library has launched in this process (all threads). */
 uint64_t fls_kernel_launch_count(void);

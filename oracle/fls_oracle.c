@@ -448,6 +448,68 @@ void orc_probe_groupby(const int32_t* supp, const int32_t* part, const int32_t* 
 	}
 }
 
+/* PHT_2 lookup: hit, and the payload (the u64 slot's high word). */
+static int pht2_get(const int32_t* ht, int32_t len, int32_t keys_min, int32_t key, int32_t* val) {
+	int32_t  h;
+	uint64_t slot;
+	if (!pht_hash(key, len, keys_min, &h)) { return 0; }
+	memcpy(&slot, &ht[2 * (int64_t)h], 8);
+	if (slot == 0) { return 0; }
+	*val = (int32_t)(slot >> 32);
+	return 1;
+}
+
+static void add_i64(int32_t* p, int64_t x) {
+	uint64_t acc;
+	memcpy(&acc, p, 8);
+	acc += (uint64_t)x;
+	memcpy(p, &acc, 8);
+}
+
+void orc_q31_groupby(const int32_t* supp, const int32_t* cust, const int32_t* date, const int32_t* rev, uint64_t n,
+                     const int32_t* ht_s, int32_t s_len, const int32_t* ht_c, int32_t c_len, const int32_t* ht_d,
+                     int32_t d_len, int32_t d_keys_min, int32_t* res) {
+	/* fls_q31.cu:57-93 probe_v1: supplier -> s_nation, customer -> c_nation,
+	 * date -> year (all PHT_2); group (s_nation*175 + c_nation*7 + year-1992)
+	 * % 4375 into records of 6 words {year, c_nation, s_nation, -, sum}. */
+	const int32_t n_grp = (1998 - 1992 + 1) * 25 * 25;
+	for (uint64_t t = 0; t < n; ++t) {
+		int32_t s_nation, c_nation, year;
+		if (!pht2_get(ht_s, s_len, 0, supp[t], &s_nation)) { continue; }
+		if (!pht2_get(ht_c, c_len, 0, cust[t], &c_nation)) { continue; }
+		if (!pht2_get(ht_d, d_len, d_keys_min, date[t], &year)) { continue; }
+		const int32_t g = (int32_t)((uint32_t)s_nation * 175u + (uint32_t)c_nation * 7u + ((uint32_t)year - 1992u)) % n_grp;
+		if (g < 0) { continue; }
+		res[6 * g]     = year;
+		res[6 * g + 1] = c_nation;
+		res[6 * g + 2] = s_nation;
+		add_i64(&res[6 * g + 4], (int64_t)rev[t]);
+	}
+}
+
+void orc_q41_groupby(const int32_t* supp, const int32_t* cust, const int32_t* part, const int32_t* date,
+                     const int32_t* rev, const int32_t* cost, uint64_t n, const int32_t* ht_s, int32_t s_len,
+                     const int32_t* ht_c, int32_t c_len, const int32_t* ht_p, int32_t p_len, const int32_t* ht_d,
+                     int32_t d_len, int32_t d_keys_min, int32_t* res) {
+	/* fls_q41.cu:61-112 probe_v1: supplier (PHT_1), customer -> c_nation,
+	 * part (PHT_1), date -> year; group (c_nation*7 + year-1992) % 175 into
+	 * records of 4 words {year, c_nation, sum}; measure revenue - supplycost as
+	 * an int32 difference. */
+	const int32_t n_grp = (1998 - 1992 + 1) * 25;
+	for (uint64_t t = 0; t < n; ++t) {
+		int32_t h, c_nation, year;
+		if (!pht_hash(supp[t], s_len, 0, &h) || ht_s[h] == 0) { continue; }
+		if (!pht2_get(ht_c, c_len, 0, cust[t], &c_nation)) { continue; }
+		if (!pht_hash(part[t], p_len, 0, &h) || ht_p[h] == 0) { continue; }
+		if (!pht2_get(ht_d, d_len, d_keys_min, date[t], &year)) { continue; }
+		const int32_t g = (int32_t)((uint32_t)c_nation * 7u + ((uint32_t)year - 1992u)) % n_grp;
+		if (g < 0) { continue; }
+		res[4 * g]     = year;
+		res[4 * g + 1] = c_nation;
+		add_i64(&res[4 * g + 2], (int64_t)(int32_t)((uint32_t)rev[t] - (uint32_t)cost[t]));
+	}
+}
+
 /* ---- learned selector ------------------------------------------------------ */
 
 double orc_mlp_loss_grad(const float* P, const float* x, const uint8_t* y, uint32_t B, double* g) {

@@ -87,6 +87,13 @@ void orc_pht2_build(const int32_t* filter, int32_t filter_eq, const int32_t* key
                     int32_t* ht, int32_t len, int32_t keys_min);
 /* Probe + group-by of fls_q21.cu probe_v1: res is int32[4*7000]; group g gets
  * res[4g]=year, res[4g+1]=brand and a uint64 revenue sum at res[4g+2]. */
+void orc_q31_groupby(const int32_t* supp, const int32_t* cust, const int32_t* date, const int32_t* rev, uint64_t n,
+                     const int32_t* ht_s, int32_t s_len, const int32_t* ht_c, int32_t c_len, const int32_t* ht_d,
+                     int32_t d_len, int32_t d_keys_min, int32_t* res);
+void orc_q41_groupby(const int32_t* supp, const int32_t* cust, const int32_t* part, const int32_t* date,
+                     const int32_t* rev, const int32_t* cost, uint64_t n, const int32_t* ht_s, int32_t s_len,
+                     const int32_t* ht_c, int32_t c_len, const int32_t* ht_p, int32_t p_len, const int32_t* ht_d,
+                     int32_t d_len, int32_t d_keys_min, int32_t* res);
 void orc_probe_groupby(const int32_t* supp, const int32_t* part, const int32_t* date, const int32_t* rev, uint64_t n,
                        const int32_t* ht_s, int32_t s_len, const int32_t* ht_p, int32_t p_len, const int32_t* ht_d,
                        int32_t d_len, int32_t d_keys_min, int32_t* res);

@@ -63,6 +63,10 @@ class Oracle:
                                      ctypes.c_int32]
         L.orc_probe_groupby.argtypes = [_i32p, _i32p, _i32p, _i32p, ctypes.c_uint64, _i32p, ctypes.c_int32, _i32p,
                                         ctypes.c_int32, _i32p, ctypes.c_int32, ctypes.c_int32, _i32p]
+        L.orc_q31_groupby.argtypes = ([_i32p] * 4 + [ctypes.c_uint64] + [_i32p, ctypes.c_int32] * 3
+                                      + [ctypes.c_int32, _i32p])
+        L.orc_q41_groupby.argtypes = ([_i32p] * 6 + [ctypes.c_uint64] + [_i32p, ctypes.c_int32] * 4
+                                      + [ctypes.c_int32, _i32p])
 
     # -- layout / packing -------------------------------------------------
     def tpos(self) -> np.ndarray:
@@ -192,6 +196,26 @@ class Oracle:
         return res
 
 
+    def q31_groupby(self, supp, cust, date, rev, ht_s, ht_c, ht_d, d_keys_min=0):
+        """fls_q31.cu probe_v1 restated: int32[6 * 4375] group records."""
+        cols = [np.ascontiguousarray(c, dtype=np.int32) for c in (supp, cust, date, rev)]
+        res = np.zeros(6 * 4375, np.int32)
+        self.L.orc_q31_groupby(*[_p(c, _i32p) for c in cols], ctypes.c_uint64(cols[0].size),
+                               _p(ht_s, _i32p), ht_s.size // 2, _p(ht_c, _i32p), ht_c.size // 2,
+                               _p(ht_d, _i32p), ht_d.size // 2, d_keys_min, _p(res, _i32p))
+        return res
+
+    def q41_groupby(self, supp, cust, part, date, rev, cost, ht_s, ht_c, ht_p, ht_d, d_keys_min=0):
+        """fls_q41.cu probe_v1 restated: int32[4 * 175] group records."""
+        cols = [np.ascontiguousarray(c, dtype=np.int32) for c in (supp, cust, part, date, rev, cost)]
+        res = np.zeros(4 * 175, np.int32)
+        self.L.orc_q41_groupby(*[_p(c, _i32p) for c in cols], ctypes.c_uint64(cols[0].size),
+                               _p(ht_s, _i32p), ht_s.size, _p(ht_c, _i32p), ht_c.size // 2,
+                               _p(ht_p, _i32p), ht_p.size, _p(ht_d, _i32p), ht_d.size // 2, d_keys_min,
+                               _p(res, _i32p))
+        return res
+
+
 class Reference:
     """The reference's own FastLanes code, compiled from its sources."""
 
@@ -211,6 +235,12 @@ class Reference:
         L.ref_q21_groupby.restype = None
         L.ref_q21_groupby.argtypes = ([_u32p, ctypes.c_uint] * 4 + [ctypes.c_uint64]
                                       + [_i32p, ctypes.c_int32] * 3 + [ctypes.c_int32, _i32p, ctypes.c_int])
+        L.ref_q31_groupby.restype = None
+        L.ref_q31_groupby.argtypes = ([_u32p, ctypes.c_uint] * 4 + [ctypes.c_uint64]
+                                      + [_i32p, ctypes.c_int32] * 3 + [ctypes.c_int32, _i32p, ctypes.c_int])
+        L.ref_q41_groupby.restype = None
+        L.ref_q41_groupby.argtypes = ([_u32p, ctypes.c_uint] * 6 + [ctypes.c_uint64]
+                                      + [_i32p, ctypes.c_int32] * 4 + [ctypes.c_int32, _i32p, ctypes.c_int])
         L.ref_decode_sum.restype = ctypes.c_uint64
         L.ref_decode_sum.argtypes = [_u32p, ctypes.c_uint, ctypes.c_uint64, ctypes.c_int]
         L.ref_pack_column.restype = None
@@ -293,6 +323,25 @@ class Reference:
         res = np.zeros(4 * N_GROUPS, np.int32)
         self.L.ref_q21_groupby(*args, n_rows, _p(ht_s, _i32p), ht_s.size, _p(ht_p, _i32p), ht_p.size // 2,
                                _p(ht_d, _i32p), ht_d.size // 2, d_keys_min, _p(res, _i32p), threads)
+        return res
+
+    def q31_groupby(self, cols, bws, n_rows, ht_s, ht_c, ht_d, d_keys_min, threads):
+        args = []
+        for c, b in zip(cols, bws):
+            args += [_p(c, _u32p), b]
+        res = np.zeros(6 * 4375, np.int32)
+        self.L.ref_q31_groupby(*args, n_rows, _p(ht_s, _i32p), ht_s.size // 2, _p(ht_c, _i32p), ht_c.size // 2,
+                               _p(ht_d, _i32p), ht_d.size // 2, d_keys_min, _p(res, _i32p), threads)
+        return res
+
+    def q41_groupby(self, cols, bws, n_rows, ht_s, ht_c, ht_p, ht_d, d_keys_min, threads):
+        args = []
+        for c, b in zip(cols, bws):
+            args += [_p(c, _u32p), b]
+        res = np.zeros(4 * 175, np.int32)
+        self.L.ref_q41_groupby(*args, n_rows, _p(ht_s, _i32p), ht_s.size, _p(ht_c, _i32p), ht_c.size // 2,
+                               _p(ht_p, _i32p), ht_p.size, _p(ht_d, _i32p), ht_d.size // 2, d_keys_min,
+                               _p(res, _i32p), threads)
         return res
 
     def pack_column(self, values, bw, threads):

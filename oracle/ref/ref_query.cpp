@@ -140,3 +140,118 @@ extern "C" void ref_pack_column(const uint32_t* values, uint64_t n, unsigned bw,
 		ref_pack_u32(buf, out + v * 32ull * bw, bw);
 	}
 }
+
+// The reference's decoders + the loops of fls_q31.cu:57-93 (probe_v1): PHT_2
+// supplier / customer / date payloads, group (s_nation*175 + c_nation*7 +
+// year-1992) % 4375, records of 6 words {year, c_nation, s_nation, -, sum}.
+static bool pht2_payload(const int32_t* ht, int32_t len, int32_t keys_min, int32_t key, int32_t* val) {
+	int32_t h;
+	if (!pht_slot(key, len, keys_min, &h)) { return false; }
+	uint64_t slot;
+	std::memcpy(&slot, &ht[2 * (int64_t)h], 8);
+	if (slot == 0) { return false; }
+	*val = (int32_t)(slot >> 32);
+	return true;
+}
+
+static void merge_groups(int32_t* res, const int32_t* words, const long long* sums, const char* seen, int n_grp,
+                         int stride, int n_words, int sum_slot) {
+	for (int g = 0; g < n_grp; ++g) {
+		if (!seen[g]) { continue; }
+		for (int w = 0; w < n_words; ++w) { res[stride * g + w] = words[n_words * g + w]; }
+		uint64_t acc;
+		std::memcpy(&acc, &res[stride * g + sum_slot], 8);
+		acc += (uint64_t)sums[g];
+		std::memcpy(&res[stride * g + sum_slot], &acc, 8);
+	}
+}
+
+extern "C" void ref_q31_groupby(const uint32_t* supp_p, unsigned supp_bw, const uint32_t* cust_p, unsigned cust_bw,
+                                const uint32_t* date_p, unsigned date_bw, const uint32_t* rev_p, unsigned rev_bw,
+                                uint64_t n_rows, const int32_t* ht_s, int32_t s_len, const int32_t* ht_c,
+                                int32_t c_len, const int32_t* ht_d, int32_t d_len, int32_t d_keys_min, int32_t* res,
+                                int n_threads) {
+	const uint64_t n_vec = (n_rows + 1023) / 1024;
+	const int      n_grp = (1998 - 1992 + 1) * 25 * 25;
+#pragma omp parallel num_threads(n_threads)
+	{
+		long long* local = new long long[n_grp]();
+		char*      seen  = new char[n_grp]();
+		int32_t*   words = new int32_t[3 * n_grp]();
+#pragma omp for schedule(static)
+		for (uint64_t v = 0; v < n_vec; ++v) {
+			uint32_t s[1024], c[1024], d[1024], r[1024];
+			decode_vec(supp_p, supp_bw, v, s);
+			decode_vec(cust_p, cust_bw, v, c);
+			decode_vec(date_p, date_bw, v, d);
+			decode_vec(rev_p, rev_bw, v, r);
+			const uint64_t n = (v + 1 == n_vec) ? n_rows - v * 1024 : 1024;
+			for (uint64_t t = 0; t < n; ++t) {
+				int32_t s_nation, c_nation, year;
+				if (!pht2_payload(ht_s, s_len, 0, (int32_t)s[t], &s_nation)) { continue; }
+				if (!pht2_payload(ht_c, c_len, 0, (int32_t)c[t], &c_nation)) { continue; }
+				if (!pht2_payload(ht_d, d_len, d_keys_min, (int32_t)d[t], &year)) { continue; }
+				const int g = (s_nation * 25 * 7 + c_nation * 7 + (year - 1992)) % n_grp;
+				if (g < 0) { continue; }
+				words[3 * g]     = year;
+				words[3 * g + 1] = c_nation;
+				words[3 * g + 2] = s_nation;
+				seen[g]          = 1;
+				local[g] += (long long)(int32_t)r[t];
+			}
+		}
+#pragma omp critical
+		merge_groups(res, words, local, seen, n_grp, 6, 3, 4);
+		delete[] local;
+		delete[] seen;
+		delete[] words;
+	}
+}
+
+// The reference's decoders + the loops of fls_q41.cu:61-112 (probe_v1):
+// supplier and part PHT_1, customer -> c_nation and date -> year PHT_2, group
+// (c_nation*7 + year-1992) % 175, measure revenue - supplycost (int32).
+extern "C" void ref_q41_groupby(const uint32_t* supp_p, unsigned supp_bw, const uint32_t* cust_p, unsigned cust_bw,
+                                const uint32_t* part_p, unsigned part_bw, const uint32_t* date_p, unsigned date_bw,
+                                const uint32_t* rev_p, unsigned rev_bw, const uint32_t* cost_p, unsigned cost_bw,
+                                uint64_t n_rows, const int32_t* ht_s, int32_t s_len, const int32_t* ht_c,
+                                int32_t c_len, const int32_t* ht_p, int32_t p_len, const int32_t* ht_d, int32_t d_len,
+                                int32_t d_keys_min, int32_t* res, int n_threads) {
+	const uint64_t n_vec = (n_rows + 1023) / 1024;
+	const int      n_grp = (1998 - 1992 + 1) * 25;
+#pragma omp parallel num_threads(n_threads)
+	{
+		long long* local = new long long[n_grp]();
+		char*      seen  = new char[n_grp]();
+		int32_t*   words = new int32_t[2 * n_grp]();
+#pragma omp for schedule(static)
+		for (uint64_t v = 0; v < n_vec; ++v) {
+			uint32_t s[1024], c[1024], p[1024], d[1024], r[1024], k[1024];
+			decode_vec(supp_p, supp_bw, v, s);
+			decode_vec(cust_p, cust_bw, v, c);
+			decode_vec(part_p, part_bw, v, p);
+			decode_vec(date_p, date_bw, v, d);
+			decode_vec(rev_p, rev_bw, v, r);
+			decode_vec(cost_p, cost_bw, v, k);
+			const uint64_t n = (v + 1 == n_vec) ? n_rows - v * 1024 : 1024;
+			for (uint64_t t = 0; t < n; ++t) {
+				int32_t h, c_nation, year;
+				if (!pht_slot((int32_t)s[t], s_len, 0, &h) || ht_s[h] == 0) { continue; }
+				if (!pht2_payload(ht_c, c_len, 0, (int32_t)c[t], &c_nation)) { continue; }
+				if (!pht_slot((int32_t)p[t], p_len, 0, &h) || ht_p[h] == 0) { continue; }
+				if (!pht2_payload(ht_d, d_len, d_keys_min, (int32_t)d[t], &year)) { continue; }
+				const int g = (c_nation * 7 + (year - 1992)) % n_grp;
+				if (g < 0) { continue; }
+				words[2 * g]     = year;
+				words[2 * g + 1] = c_nation;
+				seen[g]          = 1;
+				local[g] += (long long)(int32_t)(r[t] - k[t]);
+			}
+		}
+#pragma omp critical
+		merge_groups(res, words, local, seen, n_grp, 4, 2, 2);
+		delete[] local;
+		delete[] seen;
+		delete[] words;
+	}
+}

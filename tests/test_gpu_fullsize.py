@@ -85,3 +85,21 @@ def test_decode_delta_rle_2p27(cuda, scheme):
     assert int(ops.query_aggregate(col).cpu()[0]) & 0xFFFFFFFFFFFFFFFF == want
     assert torch.equal(ops.unpack_global(col, order=ORDER_ORIGINAL)[:n], raw)
     ops.check_device_error()
+
+
+@pytest.mark.parametrize("query", ["q31", "q41"])
+def test_ssb_joins_full_size(both_paths, oracle, query):
+    n = 1 << 27
+    t, tables, hcols, dcols, probes, kw = datagen.ssb_join(query, n, seed=3141)
+    ht = {k: v.cpu().numpy() for k, v in tables.items()}
+    if query == "q31":
+        want = oracle.q31_groupby(t["lo_suppkey"], t["lo_custkey"], t["lo_orderdate"], t["lo_revenue"], ht["ht_s"],
+                                  ht["ht_c"], ht["ht_d"])
+    else:
+        want = oracle.q41_groupby(t["lo_suppkey"], t["lo_custkey"], t["lo_partkey"], t["lo_orderdate"],
+                                  t["lo_revenue"], t["lo_supplycost"], ht["ht_s"], ht["ht_c"], ht["ht_p"], ht["ht_d"])
+    for jit in both_paths:
+        ops.set_tuning(TUNE_JIT, jit)
+        got = ops.join_groupby(dcols, probes, **kw).cpu().numpy()
+        ops.check_device_error()
+        assert np.array_equal(got, want), (query, jit)

@@ -66,3 +66,23 @@ def test_precompile_probe_edge_shapes(probes, agg):
     ka = next(i for i, p in enumerate(probes) if p[4] == 2)
     ops.jit_precompile_probe(cols, probes, agg, ka, ka, 3, 1, 100)
     assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
+
+
+@pytest.mark.parametrize("query", ["q31", "q41"])
+def test_precompile_ssb_join_shapes(query):
+    if query == "q31":
+        bits = datagen.Q31_BITS
+        cols = [_col(bits[k]) for k in ("lo_suppkey", "lo_custkey", "lo_orderdate", "lo_revenue")]
+        probes = [(0, 0x200000, 1 << 17, 0, 2), (1, 0x400000, 1 << 18, 0, 2), (2, 0x800000, datagen.N_DAYS, 0, 2)]
+        kw = dict(agg_col=3, keys=[(0, 175, 2), (1, 7, 1), (2, 1, 0)], group_sub=1992, n_groups=4375, res_stride=6,
+                  sum_slot=4)
+    else:
+        bits = datagen.Q41_BITS
+        cols = [_col(bits[k]) for k in ("lo_suppkey", "lo_custkey", "lo_partkey", "lo_orderdate", "lo_revenue",
+                                        "lo_supplycost")]
+        probes = [(0, 0x200000, 1 << 17, 0, 1), (1, 0x400000, 1 << 18, 0, 2), (2, 0x600000, 1 << 19, 0, 1),
+                  (3, 0x800000, datagen.N_DAYS, 0, 2)]
+        kw = dict(agg_col=4, keys=[(1, 7, 1), (3, 1, 0)], group_sub=1992, n_groups=175, res_stride=4, sum_slot=2,
+                  agg_sub_col=5)
+    ops.jit_precompile_join(cols, probes, **kw)
+    assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()

@@ -123,3 +123,42 @@ def test_scheme_roundtrip(oracle, scheme, kind):
             continue
         assert m.n_words % 4 == 0
         assert np.array_equal(oracle.decode_vec(p, m, transposed=transposed), v)
+
+
+@pytest.mark.parametrize("query", ["q21", "q31", "q41"])
+def test_join_loops_match_reference(oracle, reference, query):
+    """The oracle's restated join + group-by loops (fls_q21/q31/q41.cu) equal the
+    reference's CPU arm (its own decoders of the packed columns)."""
+    from fastlanesgpu_b200 import datagen
+    n = 200_000 + 17
+    if query == "q21":
+        t = datagen.q21_tables(n, seed=9, part_ids=1 << 14, supp_ids=1 << 12)
+        hs = oracle.pht1_build(t["s_region"], 1, t["s_suppkey"], 1 << 12)
+        hp = oracle.pht2_build(t["p_category"], 1, t["p_partkey"], t["p_brand1"], 1 << 14)
+        hd = oracle.pht2_build(None, 0, t["d_datekey"], t["d_year"], datagen.N_DAYS)
+        names, bits = ["lo_suppkey", "lo_partkey", "lo_orderdate", "lo_revenue"], datagen.Q21_BITS
+        want = oracle.probe_groupby(*[t[k] for k in names], hs, hp, hd)
+        words = [reference.pack_column(t[k], bits[k], 4) for k in names]
+        got = reference.q21_groupby(words, [bits[k] for k in names], n, hs, hp, hd, 0, 4)
+    elif query == "q31":
+        t = datagen.q31_tables(n, seed=9, cust_ids=1 << 14, supp_ids=1 << 12)
+        hs = oracle.pht2_build(t["s_region"], 1, t["s_suppkey"], t["s_nation"], 1 << 12)
+        hc = oracle.pht2_build(t["c_region"], 1, t["c_custkey"], t["c_nation"], 1 << 14)
+        hd = oracle.pht2_build(t["d_in_range"], 1, t["d_datekey"], t["d_year"], datagen.N_DAYS)
+        names, bits = ["lo_suppkey", "lo_custkey", "lo_orderdate", "lo_revenue"], datagen.Q31_BITS
+        want = oracle.q31_groupby(*[t[k] for k in names], hs, hc, hd)
+        words = [reference.pack_column(t[k], bits[k], 4) for k in names]
+        got = reference.q31_groupby(words, [bits[k] for k in names], n, hs, hc, hd, 0, 4)
+    else:
+        t = datagen.q41_tables(n, seed=9, cust_ids=1 << 14, supp_ids=1 << 12, part_ids=1 << 15)
+        hs = oracle.pht1_build(t["s_region"], 1, t["s_suppkey"], 1 << 12)
+        hc = oracle.pht2_build(t["c_region"], 1, t["c_custkey"], t["c_nation"], 1 << 14)
+        hp = oracle.pht1_build(t["p_mfgr_low"], 1, t["p_partkey"], 1 << 15)
+        hd = oracle.pht2_build(None, 0, t["d_datekey"], t["d_year"], datagen.N_DAYS)
+        names = ["lo_suppkey", "lo_custkey", "lo_partkey", "lo_orderdate", "lo_revenue", "lo_supplycost"]
+        bits = datagen.Q41_BITS
+        want = oracle.q41_groupby(*[t[k] for k in names], hs, hc, hp, hd)
+        words = [reference.pack_column(t[k], bits[k], 4) for k in names]
+        got = reference.q41_groupby(words, [bits[k] for k in names], n, hs, hc, hp, hd, 0, 4)
+    assert (want != 0).sum() > 10
+    assert np.array_equal(got, want)
