@@ -117,11 +117,13 @@ struct FilterQuery : Shape<LAYOUT, BWS...> {
 // AGG / SUB: staged columns of the measure and of the column subtracted from
 // it (-1: none).  NK group keys, the payloads of probes K0, K1, K2.  KINDS bit
 // q: probe q is PHT_2; SMEM bit q: probe q's table is in shared memory (PHT_1
-// as a presence bitmap, PHT_2 verbatim); DIRECT bit q: the host proved every
-// key of probe q's column lands in [keys_min, keys_min + len) (from the
-// column's base and bit width), so its slot is key - keys_min.
-template <int LAYOUT, int NP, int AGG, int SUB, int NK, int K0, int K1, int K2, int KINDS, int SMEM, int DIRECT,
-          int... BWS>
+// as a presence bitmap, PHT_2 verbatim); PBIT bit q: a PHT_2 table too large
+// for shared memory has its presence bitmap there (a slot hits when its 64-bit
+// entry is not zero), its payloads stay in global memory; DIRECT bit q: the
+// host proved every key of probe q's column lands in [keys_min, keys_min +
+// len) (from the column's base and bit width), so its slot is key - keys_min.
+template <int LAYOUT, int NP, int AGG, int SUB, int NK, int K0, int K1, int K2, int KINDS, int SMEM, int PBIT,
+          int DIRECT, int... BWS>
 struct ProbeQuery : Shape<LAYOUT, BWS...> {
 	static constexpr int kNP  = NP;
 	static constexpr int kAgg = AGG;
@@ -130,6 +132,9 @@ struct ProbeQuery : Shape<LAYOUT, BWS...> {
 	__host__ __device__ static constexpr int key_probe(int k) { return k == 0 ? K0 : k == 1 ? K1 : K2; }
 	__host__ __device__ static constexpr bool pht2(int q) { return (KINDS >> q) & 1; }
 	__host__ __device__ static constexpr bool in_smem(int q) { return (SMEM >> q) & 1; }
+	__host__ __device__ static constexpr bool pbit(int q) { return (PBIT >> q) & 1; }
+	// Probes whose hit test reads shared memory only (or a PHT_1 array).
+	__host__ __device__ static constexpr bool dense_ok(int q) { return !pht2(q) || in_smem(q) || pbit(q); }
 	__host__ __device__ static constexpr bool direct(int q) { return (DIRECT >> q) & 1; }
 	static_assert(NP >= 1 && NP <= FLS_MAX_PROBES, "1..4 probes");
 };
@@ -409,13 +414,25 @@ __device__ __forceinline__ uint2 table_entry(const ProbeParams& P, const uint32_
 	}
 }
 
-// Dense PHT_1 probes Q, Q+1, ... over the whole vector while some lane keeps
-// more than sparse_rows rows; f0 receives the first probe left to the row
-// phase.
+// Whether slot h of probe q's table hits, from the cheapest copy.
+template <class Q, int q>
+__device__ __forceinline__ bool table_hit(const ProbeParams& P, const uint32_t* tables, uint32_t h) {
+	if constexpr (Q::pht2(q) && Q::pbit(q)) {
+		return ((tables[P.smem_off[q] + (h >> 5)] >> (h & 31u)) & 1u) != 0u;
+	} else {
+		const uint2 e = table_entry<Q, q>(P, tables, h);
+		return (e.x | e.y) != 0u;
+	}
+}
+
+// Dense probes q, q+1, ... over the whole vector (probes whose hit test reads
+// shared memory: PHT_1 bitmaps, PHT_2 tables or their presence bitmaps) while
+// some lane keeps more than sparse_rows rows; f0 receives the first probe left
+// to the row phase.
 template <class Q, int q>
 __device__ __forceinline__ void dense_probes(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
                                              uint32_t lane, uint32_t& mask, int& f0) {
-	if constexpr (q < Q::kNP && !Q::pht2(q)) {
+	if constexpr (q < Q::kNP && Q::dense_ok(q)) {
 		if (max_rows(mask) <= P.sparse_rows) {
 			f0 = q;
 			return;
@@ -426,7 +443,7 @@ __device__ __forceinline__ void dense_probes(const ProbeParams& P, const uint32_
 		dev::unpack_rows<Q::bw(q)>(V.template col<q>(), lane, [&](int r, uint32_t x) {
 			uint32_t   h;
 			const bool ok = hash_slot<Q::direct(q)>(x + kb, len, h, P.S.err);
-			const bool b  = ok & (table_entry<Q, q>(P, tables, h).x != 0u);
+			const bool b  = ok & table_hit<Q, q>(P, tables, h);
 			hit[r & 3] |= (b ? 1u : 0u) << r;
 		});
 		mask &= (hit[0] | hit[1]) | (hit[2] | hit[3]);
@@ -466,6 +483,42 @@ __device__ __forceinline__ void probe_rows(const ProbeParams& P, const uint32_t*
 			}
 		}
 		probe_rows<Q, q + 1>(P, tables, V, lane, rows, pass, kv, rem);
+	}
+}
+
+// Payloads of the key probes q < F0 (their hits were tested densely) for a
+// batch of selected rows; the reads of all rows are issued before any is used.
+template <class Q, int q, int F0>
+__device__ __forceinline__ void key_payloads(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
+                                             uint32_t lane, const uint32_t (&rows)[kRowBatch],
+                                             const bool (&pass)[kRowBatch], int32_t (&kv)[FLS_MAX_GROUP_KEYS][kRowBatch],
+                                             int rem) {
+	if constexpr (q < F0) {
+		constexpr int k = Q::key_probe(0) == q ? 0 : Q::key_probe(1) == q ? 1 : Q::key_probe(2) == q ? 2 : -1;
+		if constexpr (k >= 0 && k < Q::kNK) {
+			const uint32_t kb  = P.base[q] - static_cast<uint32_t>(P.kmin[q]);
+			const int32_t  len = P.len[q];
+			uint2          e[kRowBatch];
+#pragma unroll
+			for (int j = 0; j < kRowBatch; ++j) {
+				e[j] = make_uint2(0u, 0u);
+				if (j < rem && pass[j]) {
+					uint32_t h;
+					if (hash_slot<Q::direct(q)>(row_field<Q::bw(q)>(V.template col<q>(), lane, rows[j]) + kb, len, h,
+					                            P.S.err)) {
+						e[j] = table_entry<Q, q>(P, tables, h);
+					}
+				}
+			}
+#pragma unroll
+			for (int j = 0; j < kRowBatch; ++j) {
+#pragma unroll
+				for (int kk = 0; kk < Q::kNK; ++kk) {
+					if (Q::key_probe(kk) == q) { kv[kk][j] = static_cast<int32_t>(e[j].y); }
+				}
+			}
+		}
+		key_payloads<Q, q + 1, F0>(P, tables, V, lane, rows, pass, kv, rem);
 	}
 }
 
@@ -511,6 +564,7 @@ __device__ __forceinline__ void row_phase(const ProbeParams& P, const uint32_t* 
 #pragma unroll
 			for (int k = 0; k < FLS_MAX_GROUP_KEYS; ++k) { kv[k][j] = 0; }
 		}
+		key_payloads<Q, 0, F0>(P, tables, V, lane, rows, pass, kv, rem);
 		probe_rows<Q, F0>(P, tables, V, lane, rows, pass, kv, rem);
 #pragma unroll
 		for (int j = 0; j < kRowBatch; ++j) {
@@ -543,24 +597,34 @@ struct ProbeBody {
 
 	// Shared-memory tables, staged once per CTA by all its warps: PHT_1 as a
 	// presence bitmap (the probe only tests slot != 0, crystal-opt/
-	// join.cuh:42-47), PHT_2 verbatim.
+	// join.cuh:42-47), PHT_2 verbatim or, for large PHT_2 tables, as a presence
+	// bitmap of the slots whose 64-bit entry is not zero.
 	__device__ void cta_setup(uint32_t* cta) {
 		tables              = cta;
 		const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll 1
 		for (int q = 0; q < Q::kNP; ++q) {
-			if (!Q::in_smem(q)) { continue; }
+			if (!Q::in_smem(q) && !Q::pbit(q)) { continue; }
 			uint32_t*      dst = cta + P.smem_off[q];
 			const int32_t* ht  = P.ht[q];
 			const uint32_t len = static_cast<uint32_t>(P.len[q]);
-			if (!Q::pht2(q)) {
+			if (!Q::pht2(q) || Q::pbit(q)) {
+				const bool     two     = Q::pht2(q);
 				const uint32_t n_words = (len + 31u) / 32u;
 				for (uint32_t w0 = warp * 8u; w0 < n_words; w0 += nw * 8u) {
 					int32_t x[8];
 #pragma unroll
 					for (uint32_t j = 0; j < 8; ++j) {
 						const uint32_t idx = 32u * (w0 + j) + lane;
-						x[j]               = (w0 + j < n_words && idx < len) ? __ldg(ht + idx) : 0;
+						x[j]               = 0;
+						if (w0 + j < n_words && idx < len) {
+							if (two) {
+								const int2 e = __ldg(reinterpret_cast<const int2*>(ht) + idx);
+								x[j]         = e.x | e.y;
+							} else {
+								x[j] = __ldg(ht + idx);
+							}
+						}
 					}
 #pragma unroll
 					for (uint32_t j = 0; j < 8; ++j) {

@@ -407,24 +407,35 @@ bool jit_probe_shape(const fls_join_groupby_desc* d, JitProbeShape& sh) {
 	for (uint32_t i = 0; i < sh.n_staged; ++i) {
 		if (!uniform_for(d->cols[sh.staged[i]], d->cols[sh.staged[0]].layout)) { return false; }
 	}
-	// Tables go to shared memory in probe order while they fit the budget.
-	// A probe is direct when base + [0, 2^bw) - keys_min lies in [0, len).
-	uint32_t kinds = 0, in_smem = 0, direct = 0;
+	// Tables go to shared memory in probe order while they fit the budget:
+	// PHT_1 as bitmaps, PHT_2 verbatim or else as presence bitmaps (payloads
+	// then come from global memory, for the selected rows only).  A probe is
+	// direct when base + [0, 2^bw) - keys_min lies in [0, len).
+	uint32_t kinds = 0, in_smem = 0, pbit = 0, direct = 0;
 	sh.cta_words   = 0;
+	auto place     = [&](uint64_t words, uint32_t q) {
+        if (sh.cta_words + words > kJitTableWords) { return false; }
+        sh.smem_off[q] = sh.cta_words;
+        sh.cta_words += static_cast<uint32_t>((words + 3u) & ~3ull);
+        return true;
+	};
 	for (uint32_t q = 0; q < d->n_probes; ++q) {
 		const fls_probe&  p  = d->probes[q];
 		const fls_column& kc = d->cols[p.col];
 		const int64_t     lo = static_cast<int64_t>(kc.base) - p.keys_min;
 		const int64_t     hi = lo + (kc.bw >= 32 ? (int64_t {1} << 32) : (int64_t {1} << kc.bw)) - 1;
 		if (kc.bw < 32 && lo >= 0 && hi < p.ht_len) { direct |= 1u << q; }
-		const uint64_t words = p.kind == 1 ? (static_cast<uint64_t>(p.ht_len) + 31u) / 32u
-		                                   : 2ull * static_cast<uint64_t>(p.ht_len);
-		if (p.kind == 2) { kinds |= 1u << q; }
-		sh.smem_off[q] = 0;
-		if (sh.cta_words + words <= kJitTableWords) {
-			in_smem |= 1u << q;
-			sh.smem_off[q] = sh.cta_words;
-			sh.cta_words += static_cast<uint32_t>((words + 3u) & ~3ull);
+		const uint64_t bits_words = (static_cast<uint64_t>(p.ht_len) + 31u) / 32u;
+		sh.smem_off[q]            = 0;
+		if (p.kind == 1) {
+			if (place(bits_words, q)) { in_smem |= 1u << q; }
+		} else {
+			kinds |= 1u << q;
+			if (place(2ull * static_cast<uint64_t>(p.ht_len), q)) {
+				in_smem |= 1u << q;
+			} else if (place(bits_words, q)) {
+				pbit |= 1u << q;
+			}
 		}
 	}
 	fls_column sc[FLS_MAX_QUERY_COLS];
@@ -432,8 +443,9 @@ bool jit_probe_shape(const fls_join_groupby_desc* d, JitProbeShape& sh) {
 	int kp[FLS_MAX_GROUP_KEYS] = {-1, -1, -1};
 	for (uint32_t k = 0; k < d->n_keys; ++k) { kp[k] = d->key_probe[k]; }
 	char head[160];
-	std::snprintf(head, sizeof(head), "%u, %u, %d, %d, %u, %d, %d, %d, %u, %u, %u", static_cast<unsigned>(sc[0].layout),
-	              d->n_probes, sh.agg, sh.sub, d->n_keys, kp[0], kp[1], kp[2], kinds, in_smem, direct);
+	std::snprintf(head, sizeof(head), "%u, %u, %d, %d, %u, %d, %d, %d, %u, %u, %u, %u",
+	              static_cast<unsigned>(sc[0].layout), d->n_probes, sh.agg, sh.sub, d->n_keys, kp[0], kp[1], kp[2], kinds,
+	              in_smem, pbit, direct);
 	sh.key = key_args(sc, sh.n_staged, head);
 	return true;
 }

@@ -321,7 +321,7 @@ fls_status jit_filter_agg(const fls_column* cols, const fls_filter* filters, uin
 
 // Probe + group-by shapes: staged columns (probe keys in probe order, then the
 // measure column if no probe reads it), which tables live in shared memory.
-constexpr uint32_t kJitTableWords = 64u * 1024u / 4u; // shared-memory budget for hash tables
+constexpr uint32_t kJitTableWords = 72u * 1024u / 4u; // shared-memory budget for hash tables
 struct JitProbeShape {
 	uint32_t    staged[FLS_MAX_QUERY_COLS];
 	uint32_t    n_staged = 0;
