@@ -53,6 +53,8 @@ def parse_args():
     ap.add_argument("--sparse-rows", type=int, default=0, help="FLS_TUNE_SPARSE_ROWS (0 = default)")
     ap.add_argument("--jit", type=int, choices=[0, 1], default=1,
                     help="FLS_TUNE_JIT: 1 = kernel specialised to the query's shape, 0 = general kernel")
+    ap.add_argument("--group-smem", type=int, choices=[0, 1], default=1,
+                    help="FLS_TUNE_GROUP_SMEM: 1 = per-CTA group sums in shared memory, 0 = a global atomic per row")
     ap.add_argument("--mixed-columns", type=int, default=64, help="mixed workload: number of columns")
     ap.add_argument("--mixed-max-log", type=int, default=26, help="mixed workload: longest column is 2^this rows")
     ap.add_argument("--train-vectors", type=int, default=1 << 20, help="mixed workload: MLP training vectors")
@@ -209,6 +211,7 @@ def run_ours(a, dist: Dist):
     if a.sparse_rows:
         ops.set_tuning(0, a.sparse_rows)
     ops.set_tuning(1, a.jit)
+    ops.set_tuning(2, a.group_smem)
     from fastlanesgpu_b200.shard import allreduce_sum, shard_seed
     seed = shard_seed(1000, dist.rank)
     # ---------------------------------------------------------------- setup
@@ -398,7 +401,7 @@ def run_ours(a, dist: Dist):
                      "traffic": traffic, "algorithmic_bytes_per_launch": algo_bytes},
         "gpu_launches": int(launches),
         "launch_config": dict(zip(["warps", "stages", "ctas_per_sm", "tile_bytes"], ops.get_launch_config()),
-                              sparse_rows=ops.get_tuning(0), jit=ops.get_tuning(1),
+                              sparse_rows=ops.get_tuning(0), jit=ops.get_tuning(1), group_smem=ops.get_tuning(2),
                               jit_launches=int(ops.jit_stats()["launches"])),
         "clocks": clk,
     }

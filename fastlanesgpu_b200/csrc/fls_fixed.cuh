@@ -26,7 +26,9 @@ constexpr uint32_t kWaitPolls     = 1u << 17; // bounded stage waits (each <= ~2
 constexpr uint32_t kErrTimeoutBit = 1u << 2;
 constexpr uint32_t kErrHashBit    = 1u << 3;
 constexpr int      kDenseAggRows  = 16; // above this many rows in some lane, aggregate whole vectors
-constexpr int      kRowBatch      = 8;  // selected rows per lane whose table reads are in flight together
+constexpr int      kRowBatch      = 4;  // selected rows per lane whose table reads are in flight together
+constexpr uint32_t kFreeSlot      = 0xffffffffu; // tag of an unclaimed group-sum slot
+constexpr int      kMaxDenseProbes = 2; // probes compiled for whole-vector evaluation (each unrolls 32 rows)
 
 // The staged pipeline's parameters (shared by both operators).
 struct StageParams {
@@ -61,7 +63,10 @@ struct ProbeParams {
 	int32_t        key_slot[FLS_MAX_GROUP_KEYS]; // word of each key in the group record, -1 = not written
 	int32_t        sub, n_groups, sparse_rows;
 	uint32_t       stride, sum_slot; // group record: int32 words, word of the int64 sum
+	uint32_t       gsum_off;         // GSM: words into the CTA scratch of the group-sum slots
+	uint32_t       gslot_mask;       // GSM: slots - 1 (a power of two)
 	uint32_t       pad_;
+	const uint32_t* bits;            // presence bitmaps at the tables' shared-memory offsets
 	int32_t*       res;
 };
 
@@ -78,7 +83,7 @@ struct DecodeParams {
 // sizes mean equal offsets.
 static_assert(sizeof(StageParams) == 128 && alignof(StageParams) == 8, "StageParams layout");
 static_assert(sizeof(FilterParams) == 240, "FilterParams layout");
-static_assert(sizeof(ProbeParams) == 296, "ProbeParams layout");
+static_assert(sizeof(ProbeParams) == 312, "ProbeParams layout");
 static_assert(sizeof(DecodeParams) == 152, "DecodeParams layout");
 
 // Bit widths of the staged columns and where they sit in a stage.
@@ -122,13 +127,17 @@ struct FilterQuery : Shape<LAYOUT, BWS...> {
 // entry is not zero), its payloads stay in global memory; DIRECT bit q: the
 // host proved every key of probe q's column lands in [keys_min, keys_min +
 // len) (from the column's base and bit width), so its slot is key - keys_min.
+// GSM: each CTA sums its groups in a direct-mapped cache of group-sum slots
+// in shared memory (a group claims its slot, or else adds to its record
+// directly) and adds the slots' non-zero sums to the records once, at its end.
 template <int LAYOUT, int NP, int AGG, int SUB, int NK, int K0, int K1, int K2, int KINDS, int SMEM, int PBIT,
-          int DIRECT, int... BWS>
+          int DIRECT, int GSM, int... BWS>
 struct ProbeQuery : Shape<LAYOUT, BWS...> {
 	static constexpr int kNP  = NP;
 	static constexpr int kAgg = AGG;
 	static constexpr int kSub = SUB;
 	static constexpr int kNK  = NK;
+	static constexpr bool kGroupSmem = GSM != 0;
 	__host__ __device__ static constexpr int key_probe(int k) { return k == 0 ? K0 : k == 1 ? K1 : K2; }
 	__host__ __device__ static constexpr bool pht2(int q) { return (KINDS >> q) & 1; }
 	__host__ __device__ static constexpr bool in_smem(int q) { return (SMEM >> q) & 1; }
@@ -428,11 +437,14 @@ __device__ __forceinline__ bool table_hit(const ProbeParams& P, const uint32_t* 
 // Dense probes q, q+1, ... over the whole vector (probes whose hit test reads
 // shared memory: PHT_1 bitmaps, PHT_2 tables or their presence bitmaps) while
 // some lane keeps more than sparse_rows rows; f0 receives the first probe left
-// to the row phase.
+// to the row phase.  At most kMaxDenseProbes: after two selective probes few
+// rows are left, and each dense probe adds a fully unrolled unpack to the
+// kernel (instruction-cache misses cost more than the rare dense third probe
+// would save).
 template <class Q, int q>
 __device__ __forceinline__ void dense_probes(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
                                              uint32_t lane, uint32_t& mask, int& f0) {
-	if constexpr (q < Q::kNP && Q::dense_ok(q)) {
+	if constexpr (q < Q::kNP && q < kMaxDenseProbes && Q::dense_ok(q)) {
 		if (max_rows(mask) <= P.sparse_rows) {
 			f0 = q;
 			return;
@@ -453,82 +465,69 @@ __device__ __forceinline__ void dense_probes(const ProbeParams& P, const uint32_
 	}
 }
 
-// Probes q.. of a batch of selected rows; the table reads of all rows of the
-// batch are issued before any is consumed.
+// Probe q of a batch of selected rows: hit test and group-key payload.
 template <class Q, int q>
-__device__ __forceinline__ void probe_rows(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
-                                           uint32_t lane, const uint32_t (&rows)[kRowBatch], bool (&pass)[kRowBatch],
-                                           int32_t (&kv)[FLS_MAX_GROUP_KEYS][kRowBatch], int rem) {
-	if constexpr (q < Q::kNP) {
-		const uint32_t kb  = P.base[q] - static_cast<uint32_t>(P.kmin[q]);
-		const int32_t  len = P.len[q];
-		uint2          e[kRowBatch];
+__device__ __forceinline__ void probe_rows_one(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
+                                               uint32_t lane, const uint32_t (&rows)[kRowBatch],
+                                               bool (&pass)[kRowBatch], int32_t (&kv)[FLS_MAX_GROUP_KEYS][kRowBatch],
+                                               int rem) {
+	const uint32_t kb  = P.base[q] - static_cast<uint32_t>(P.kmin[q]);
+	const int32_t  len = P.len[q];
+	uint2          e[kRowBatch];
 #pragma unroll
-		for (int j = 0; j < kRowBatch; ++j) {
-			e[j] = make_uint2(0u, 0u);
-			if (j < rem) {
-				const uint32_t d = row_field<Q::bw(q)>(V.template col<q>(), lane, rows[j]) + kb;
-				uint32_t       h;
-				if (pass[j] && hash_slot<Q::direct(q)>(d, len, h, P.S.err)) {
-					e[j] = table_entry<Q, q>(P, tables, h);
-				}
+	for (int j = 0; j < kRowBatch; ++j) {
+		e[j] = make_uint2(0u, 0u);
+		if (j < rem) {
+			const uint32_t d = row_field<Q::bw(q)>(V.template col<q>(), lane, rows[j]) + kb;
+			uint32_t       h;
+			if (pass[j] && hash_slot<Q::direct(q)>(d, len, h, P.S.err)) {
+				e[j] = table_entry<Q, q>(P, tables, h);
 			}
 		}
+	}
 #pragma unroll
-		for (int j = 0; j < kRowBatch; ++j) {
-			pass[j] = pass[j] & ((e[j].x | e[j].y) != 0u);
+	for (int j = 0; j < kRowBatch; ++j) {
+		pass[j] = pass[j] & ((e[j].x | e[j].y) != 0u);
 #pragma unroll
-			for (int k = 0; k < Q::kNK; ++k) {
-				if (Q::key_probe(k) == q) { kv[k][j] = static_cast<int32_t>(e[j].y); }
-			}
+		for (int k = 0; k < Q::kNK; ++k) {
+			if (Q::key_probe(k) == q) { kv[k][j] = static_cast<int32_t>(e[j].y); }
 		}
-		probe_rows<Q, q + 1>(P, tables, V, lane, rows, pass, kv, rem);
 	}
 }
 
-// Payloads of the key probes q < F0 (their hits were tested densely) for a
-// batch of selected rows; the reads of all rows are issued before any is used.
-template <class Q, int q, int F0>
-__device__ __forceinline__ void key_payloads(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
-                                             uint32_t lane, const uint32_t (&rows)[kRowBatch],
-                                             const bool (&pass)[kRowBatch], int32_t (&kv)[FLS_MAX_GROUP_KEYS][kRowBatch],
-                                             int rem) {
-	if constexpr (q < F0) {
-		constexpr int k = Q::key_probe(0) == q ? 0 : Q::key_probe(1) == q ? 1 : Q::key_probe(2) == q ? 2 : -1;
-		if constexpr (k >= 0 && k < Q::kNK) {
-			const uint32_t kb  = P.base[q] - static_cast<uint32_t>(P.kmin[q]);
-			const int32_t  len = P.len[q];
-			uint2          e[kRowBatch];
-#pragma unroll
-			for (int j = 0; j < kRowBatch; ++j) {
-				e[j] = make_uint2(0u, 0u);
-				if (j < rem && pass[j]) {
-					uint32_t h;
-					if (hash_slot<Q::direct(q)>(row_field<Q::bw(q)>(V.template col<q>(), lane, rows[j]) + kb, len, h,
-					                            P.S.err)) {
-						e[j] = table_entry<Q, q>(P, tables, h);
-					}
-				}
-			}
-#pragma unroll
-			for (int j = 0; j < kRowBatch; ++j) {
-#pragma unroll
-				for (int kk = 0; kk < Q::kNK; ++kk) {
-					if (Q::key_probe(kk) == q) { kv[kk][j] = static_cast<int32_t>(e[j].y); }
-				}
-			}
+// Probes of a batch of selected rows: those from f0 on (warp-uniform), and
+// the group-key probes before f0 for their payloads (a row selected there
+// hits that table already, so testing it again changes nothing).  The table
+// reads of all rows of the batch are issued before any is consumed.  One
+// instance serves every f0, which keeps the kernel small enough for the
+// instruction cache.
+template <class Q, int q>
+__device__ __forceinline__ void probe_rows(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
+                                           uint32_t lane, const uint32_t (&rows)[kRowBatch], bool (&pass)[kRowBatch],
+                                           int32_t (&kv)[FLS_MAX_GROUP_KEYS][kRowBatch], int rem, int f0) {
+	if constexpr (q < Q::kNP) {
+		constexpr bool key = (Q::key_probe(0) == q && Q::kNK > 0) || (Q::key_probe(1) == q && Q::kNK > 1) ||
+		                     (Q::key_probe(2) == q && Q::kNK > 2);
+		if (key || q >= f0) {
+			probe_rows_one<Q, q>(P, tables, V, lane, rows, pass, kv, rem);
 		}
-		key_payloads<Q, q + 1, F0>(P, tables, V, lane, rows, pass, kv, rem);
+		probe_rows<Q, q + 1>(P, tables, V, lane, rows, pass, kv, rem, f0);
 	}
 }
 
 // Group-by epilogue of one selected row (fls_q21.cu:67-77, fls_q31.cu:82-91,
 // fls_q41.cu:96-104): the group of the keys in wrapping 32-bit arithmetic,
 // the key values into their words of the group record, the measure into its
-// int64 sum.
+// int64 sum.  With GSM a group owns slot g & gslot_mask of the CTA's cache
+// once it has claimed the slot's tag (its claimer writes the key words);
+// rows of a group that lost its slot to another group go to the record as
+// without GSM.  A slot sums as two 32-bit words: the low word by atomic add,
+// the high word by the measure's sign extension plus the carry out of that
+// add (the carry follows from the low word's value just before it, so the
+// pair sums modulo 2^64 in any order).
 template <class Q>
-__device__ __forceinline__ void emit(const ProbeParams& P, const int32_t (&kv)[FLS_MAX_GROUP_KEYS][kRowBatch], int j,
-                                     int32_t measure) {
+__device__ __forceinline__ void emit(const ProbeParams& P, uint32_t* tables,
+                                     const int32_t (&kv)[FLS_MAX_GROUP_KEYS][kRowBatch], int j, int32_t measure) {
 	uint32_t key = 0u - static_cast<uint32_t>(P.sub);
 #pragma unroll
 	for (int k = 0; k < Q::kNK; ++k) { key += static_cast<uint32_t>(kv[k][j]) * static_cast<uint32_t>(P.key_mul[k]); }
@@ -539,17 +538,39 @@ __device__ __forceinline__ void emit(const ProbeParams& P, const int32_t (&kv)[F
 		return;
 	}
 	int32_t* rec = P.res + static_cast<int64_t>(g) * P.stride;
-#pragma unroll
-	for (int k = 0; k < Q::kNK; ++k) {
-		if (P.key_slot[k] >= 0) { rec[P.key_slot[k]] = kv[k][j]; }
+	bool cached = false, claimed = false;
+	if constexpr (Q::kGroupSmem) {
+		const uint32_t slot = static_cast<uint32_t>(g) & P.gslot_mask;
+		uint32_t*      tag  = tables + P.gsum_off + 2u * (P.gslot_mask + 1u) + slot;
+		uint32_t       t    = *tag; // a claimed tag never changes
+		if (t == kFreeSlot) {
+			t       = atomicCAS(tag, kFreeSlot, static_cast<uint32_t>(g));
+			claimed = t == kFreeSlot;
+		}
+		cached = claimed || t == static_cast<uint32_t>(g);
+		if (cached) {
+			uint32_t*      sum = tables + P.gsum_off + 2u * slot;
+			const uint32_t lo  = static_cast<uint32_t>(measure);
+			const uint32_t old = atomicAdd(sum, lo);
+			const uint32_t hi  = (measure < 0 ? 0xffffffffu : 0u) + (old + lo < old ? 1u : 0u);
+			if (hi != 0u) { atomicAdd(sum + 1, hi); }
+		}
 	}
-	atomicAdd(reinterpret_cast<unsigned long long*>(rec + P.sum_slot),
-	          static_cast<unsigned long long>(static_cast<long long>(measure)));
+	if (!cached || claimed) {
+#pragma unroll
+		for (int k = 0; k < Q::kNK; ++k) {
+			if (P.key_slot[k] >= 0) { rec[P.key_slot[k]] = kv[k][j]; }
+		}
+	}
+	if (!cached) {
+		atomicAdd(reinterpret_cast<unsigned long long*>(rec + P.sum_slot),
+		          static_cast<unsigned long long>(static_cast<long long>(measure)));
+	}
 }
 
-template <class Q, int F0>
-__device__ __forceinline__ void row_phase(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
-                                          uint32_t lane, uint32_t mask) {
+template <class Q>
+__device__ __forceinline__ void row_phase(const ProbeParams& P, uint32_t* tables, const Vec<Q>& V, uint32_t lane,
+                                          uint32_t mask, int f0) {
 	const int n_it = max_rows(mask);
 	for (int it0 = 0; it0 < n_it; it0 += kRowBatch) {
 		const int rem = n_it - it0; // warp-uniform
@@ -564,28 +585,15 @@ __device__ __forceinline__ void row_phase(const ProbeParams& P, const uint32_t* 
 #pragma unroll
 			for (int k = 0; k < FLS_MAX_GROUP_KEYS; ++k) { kv[k][j] = 0; }
 		}
-		key_payloads<Q, 0, F0>(P, tables, V, lane, rows, pass, kv, rem);
-		probe_rows<Q, F0>(P, tables, V, lane, rows, pass, kv, rem);
+		probe_rows<Q, 0>(P, tables, V, lane, rows, pass, kv, rem, f0);
 #pragma unroll
 		for (int j = 0; j < kRowBatch; ++j) {
 			if (j < rem && pass[j]) {
 				uint32_t m = static_cast<uint32_t>(row_value<Q, Q::kAgg>(P.base, V, lane, rows[j]));
 				if constexpr (Q::kSub >= 0) { m -= static_cast<uint32_t>(row_value<Q, Q::kSub>(P.base, V, lane, rows[j])); }
-				emit<Q>(P, kv, j, static_cast<int32_t>(m));
+				emit<Q>(P, tables, kv, j, static_cast<int32_t>(m));
 			}
 		}
-	}
-}
-
-template <class Q, int F0>
-__device__ __forceinline__ void row_phase_from(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
-                                               uint32_t lane, uint32_t mask, int f0) {
-	if constexpr (F0 <= Q::kNP) {
-		if (f0 == F0) {
-			row_phase<Q, F0>(P, tables, V, lane, mask);
-			return;
-		}
-		row_phase_from<Q, F0 + 1>(P, tables, V, lane, mask, f0);
 	}
 }
 
@@ -593,47 +601,42 @@ template <class Q>
 struct ProbeBody {
 	static constexpr bool kCtaSetup = true;
 	const ProbeParams&    P;
-	const uint32_t*       tables = nullptr;
+	uint32_t*             tables = nullptr;
 
-	// Shared-memory tables, staged once per CTA by all its warps: PHT_1 as a
-	// presence bitmap (the probe only tests slot != 0, crystal-opt/
-	// join.cuh:42-47), PHT_2 verbatim or, for large PHT_2 tables, as a presence
-	// bitmap of the slots whose 64-bit entry is not zero.
+	// Shared-memory tables, staged once per CTA by all its threads: presence
+	// bitmaps (of PHT_1 tables, whose probe only tests slot != 0, crystal-opt/
+	// join.cuh:42-47, and of PHT_2 tables too large to stage, whose slot hits
+	// when its 64-bit entry is not zero) copied from P.bits, where the host
+	// built them once per query at the same offsets; small PHT_2 tables
+	// verbatim.  GSM: every slot of the group-sum cache starts free.
 	__device__ void cta_setup(uint32_t* cta) {
-		tables              = cta;
-		const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+		tables = cta;
 #pragma unroll 1
 		for (int q = 0; q < Q::kNP; ++q) {
 			if (!Q::in_smem(q) && !Q::pbit(q)) { continue; }
-			uint32_t*      dst = cta + P.smem_off[q];
-			const int32_t* ht  = P.ht[q];
 			const uint32_t len = static_cast<uint32_t>(P.len[q]);
 			if (!Q::pht2(q) || Q::pbit(q)) {
-				const bool     two     = Q::pht2(q);
-				const uint32_t n_words = (len + 31u) / 32u;
-				for (uint32_t w0 = warp * 8u; w0 < n_words; w0 += nw * 8u) {
-					int32_t x[8];
+				// 16-byte units: offsets and slot sizes are multiples of 4 words.
+				const uint32_t n4  = ((len + 31u) / 32u + 3u) / 4u;
+				const uint4*   src = reinterpret_cast<const uint4*>(P.bits + P.smem_off[q]);
+				uint4*         dst = reinterpret_cast<uint4*>(cta + P.smem_off[q]);
+				for (uint32_t i0 = threadIdx.x; i0 < n4; i0 += 4u * blockDim.x) {
+					uint4 x[4];
 #pragma unroll
-					for (uint32_t j = 0; j < 8; ++j) {
-						const uint32_t idx = 32u * (w0 + j) + lane;
-						x[j]               = 0;
-						if (w0 + j < n_words && idx < len) {
-							if (two) {
-								const int2 e = __ldg(reinterpret_cast<const int2*>(ht) + idx);
-								x[j]         = e.x | e.y;
-							} else {
-								x[j] = __ldg(ht + idx);
-							}
-						}
+					for (uint32_t j = 0; j < 4; ++j) {
+						const uint32_t i = i0 + j * blockDim.x;
+						x[j]             = i < n4 ? __ldg(src + i) : make_uint4(0u, 0u, 0u, 0u);
 					}
 #pragma unroll
-					for (uint32_t j = 0; j < 8; ++j) {
-						const uint32_t b = __ballot_sync(0xffffffffu, x[j] != 0);
-						if (lane == 0 && w0 + j < n_words) { dst[w0 + j] = b; }
+					for (uint32_t j = 0; j < 4; ++j) {
+						const uint32_t i = i0 + j * blockDim.x;
+						if (i < n4) { dst[i] = x[j]; }
 					}
 				}
 			} else {
-				const uint32_t n = 2u * len;
+				uint32_t*      dst = cta + P.smem_off[q];
+				const int32_t* ht  = P.ht[q];
+				const uint32_t n   = 2u * len;
 				for (uint32_t i0 = threadIdx.x; i0 < n; i0 += 4u * blockDim.x) {
 					int32_t x[4];
 #pragma unroll
@@ -649,6 +652,12 @@ struct ProbeBody {
 				}
 			}
 		}
+		if constexpr (Q::kGroupSmem) {
+			const uint32_t slots = P.gslot_mask + 1u;
+			for (uint32_t i = threadIdx.x; i < 3u * slots; i += blockDim.x) {
+				cta[P.gsum_off + i] = i < 2u * slots ? 0u : kFreeSlot;
+			}
+		}
 	}
 
 	__device__ __forceinline__ void operator()(const Vec<Q>& V, uint64_t v, uint32_t lane) {
@@ -656,10 +665,27 @@ struct ProbeBody {
 		int      f0   = Q::kNP;
 		dense_probes<Q, 0>(P, tables, V, lane, mask, f0);
 		if (!__any_sync(0xffffffffu, mask)) { return; }
-		row_phase_from<Q, 0>(P, tables, V, lane, mask, f0);
+		row_phase<Q>(P, tables, V, lane, mask, f0);
 	}
 
-	__device__ __forceinline__ void finish(uint32_t) {}
+	// GSM: once every warp of the CTA is done, the CTA adds each claimed
+	// slot's non-zero sum to its group's record.
+	__device__ __forceinline__ void finish(uint32_t) {
+		if constexpr (Q::kGroupSmem) {
+			__syncthreads();
+			const uint32_t  slots = P.gslot_mask + 1u;
+			const uint32_t* sum   = tables + P.gsum_off;
+			const uint32_t* tag   = sum + 2u * slots;
+			for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) {
+				const uint32_t           g = tag[i];
+				const unsigned long long v =
+				    static_cast<unsigned long long>(sum[2u * i]) | (static_cast<unsigned long long>(sum[2u * i + 1u]) << 32);
+				if (g != kFreeSlot && v != 0ull) {
+					atomicAdd(reinterpret_cast<unsigned long long*>(P.res + static_cast<int64_t>(g) * P.stride + P.sum_slot), v);
+				}
+			}
+		}
+	}
 };
 
 // ------------------------------------------------------------------ decode
@@ -775,12 +801,15 @@ __device__ __forceinline__ void run(const StageParams& S, Body& body) {
 	uint32_t st = 0, phase = 0;
 	for (uint64_t t = first; t < S.n_tiles; t += total) {
 		if (!dev::mbar_wait_bounded(bars + st, phase, kWaitPolls)) {
+			// Copies that did not land: flag, drain (bounded) and leave the
+			// loop; finish() still runs so that CTA-wide barriers there see
+			// every warp.
 			atomicOr(S.err, kErrTimeoutBit);
 			for (uint32_t s = 0; s < S.stages; ++s) {
 				dev::mbar_wait_bounded(bars + s, phase, 1u << 10);
 				dev::mbar_wait_bounded(bars + s, phase ^ 1u, 1u << 10);
 			}
-			return;
+			break;
 		}
 		const uint64_t v0 = t * S.tile;
 		const uint32_t kk = static_cast<uint32_t>(S.n_vec - v0 < S.tile ? S.n_vec - v0 : S.tile);

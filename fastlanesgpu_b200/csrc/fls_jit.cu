@@ -386,6 +386,65 @@ fls_status jit_filter_agg(const fls_column* cols, const fls_filter* filters, uin
 	return launch_fixed(make_key('F', P.S.warps, sh.key), &P, grid, 32u * P.S.warps, smem, stream, used);
 }
 
+// Presence bitmaps of up to FLS_MAX_PROBES tables: bit i of word w of table j
+// (at out + off[j]) is set when slot 32w + i is not zero (PHT_1) or its
+// 64-bit entry is not zero (PHT_2).  One warp per word, coalesced reads.
+struct PresenceJobs {
+	const int32_t* ht[FLS_MAX_PROBES];
+	uint32_t       len[FLS_MAX_PROBES];
+	uint32_t       off[FLS_MAX_PROBES];
+	uint32_t       two[FLS_MAX_PROBES];
+	uint32_t       n;
+};
+
+__global__ void __launch_bounds__(256) presence_bits_kernel(const __grid_constant__ PresenceJobs J, uint32_t* out) {
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+	for (uint32_t j = 0; j < J.n; ++j) {
+		const uint32_t len = J.len[j], n_words = (len + 31u) / 32u;
+		for (uint32_t w = warp; w < n_words; w += nw) {
+			const uint32_t idx = 32u * w + lane;
+			int32_t        x   = 0;
+			if (idx < len) {
+				if (J.two[j]) {
+					const int2 e = __ldg(reinterpret_cast<const int2*>(J.ht[j]) + idx);
+					x            = e.x | e.y;
+				} else {
+					x = __ldg(J.ht[j] + idx);
+				}
+			}
+			const uint32_t b = __ballot_sync(0xffffffffu, x != 0);
+			if (lane == 0) { out[J.off[j] + w] = b; }
+		}
+	}
+}
+
+// A memory pool per device for the per-query bitmaps that keeps what it
+// holds across synchronisations (the default pool returns memory to the
+// device at every synchronisation and maps it again at the next query).
+cudaMemPool_t bitmap_pool() {
+	static std::mutex                               mu;
+	static std::unordered_map<int, cudaMemPool_t> pools;
+	int                                             dev = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess) { return nullptr; }
+	std::lock_guard<std::mutex> lk(mu);
+	auto                        it = pools.find(dev);
+	if (it != pools.end()) { return it->second; }
+	cudaMemPoolProps props {};
+	props.allocType     = cudaMemAllocationTypePinned;
+	props.location.type = cudaMemLocationTypeDevice;
+	props.location.id   = dev;
+	cudaMemPool_t pool  = nullptr;
+	if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+		cudaGetLastError();
+		return nullptr;
+	}
+	uint64_t keep = 64ull << 20;
+	cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+	pools[dev] = pool;
+	return pool;
+}
+
 bool jit_probe_shape(const fls_join_groupby_desc* d, JitProbeShape& sh) {
 	sh.n_staged = 0;
 	for (uint32_t q = 0; q < d->n_probes; ++q) {
@@ -438,14 +497,25 @@ bool jit_probe_shape(const fls_join_groupby_desc* d, JitProbeShape& sh) {
 			}
 		}
 	}
+	sh.tables_words = sh.cta_words;
+	sh.bitmaps      = pbit | (in_smem & ~kinds);
+	// The group-sum cache after the tables: slots of two sum words and a tag,
+	// as many as the groups rounded up to a power of two, at most
+	// kJitGroupSlots.
+	const uint32_t ng = d->n_groups > 0 ? static_cast<uint32_t>(d->n_groups) : 0u;
+	sh.gsm            = tuning_group_smem() && ng > 0;
+	sh.gslots         = 1u;
+	while (sh.gslots < ng && sh.gslots < kJitGroupSlots) { sh.gslots *= 2u; }
+	sh.gsum_off = sh.cta_words;
+	if (sh.gsm) { sh.cta_words += 3u * sh.gslots + (4u - (3u * sh.gslots) % 4u) % 4u; }
 	fls_column sc[FLS_MAX_QUERY_COLS];
 	for (uint32_t i = 0; i < sh.n_staged; ++i) { sc[i] = d->cols[sh.staged[i]]; }
 	int kp[FLS_MAX_GROUP_KEYS] = {-1, -1, -1};
 	for (uint32_t k = 0; k < d->n_keys; ++k) { kp[k] = d->key_probe[k]; }
 	char head[160];
-	std::snprintf(head, sizeof(head), "%u, %u, %d, %d, %u, %d, %d, %d, %u, %u, %u, %u",
+	std::snprintf(head, sizeof(head), "%u, %u, %d, %d, %u, %d, %d, %d, %u, %u, %u, %u, %d",
 	              static_cast<unsigned>(sc[0].layout), d->n_probes, sh.agg, sh.sub, d->n_keys, kp[0], kp[1], kp[2], kinds,
-	              in_smem, pbit, direct);
+	              in_smem, pbit, direct, sh.gsm ? 1 : 0);
 	sh.key = key_args(sc, sh.n_staged, head);
 	return true;
 }
@@ -494,8 +564,39 @@ fls_status jit_probe_groupby(const fls_join_groupby_desc* d, int32_t* d_res, int
 	P.stride      = d->res_stride;
 	P.sum_slot    = d->sum_slot;
 	P.sparse_rows = sparse_rows;
+	P.gsum_off    = sh.gsum_off;
+	P.gslot_mask  = sh.gslots - 1u;
 	P.res         = d_res;
-	return launch_fixed(make_key('P', P.S.warps, sh.key), &P, grid, 32u * P.S.warps, smem, stream, used);
+	// Presence bitmaps: built once per query into a stream-ordered buffer
+	// that every CTA copies (no allocation: the general kernel runs instead).
+	uint32_t* bits = nullptr;
+	if (sh.bitmaps) {
+		cudaMemPool_t pool = bitmap_pool();
+		if (!pool || cudaMallocFromPoolAsync(reinterpret_cast<void**>(&bits), 4ull * sh.tables_words, pool, stream) !=
+		                 cudaSuccess) {
+			cudaGetLastError();
+			return FLS_OK;
+		}
+		PresenceJobs J {};
+		for (uint32_t q = 0; q < d->n_probes; ++q) {
+			if (!((sh.bitmaps >> q) & 1u)) { continue; }
+			J.ht[J.n]  = d->probes[q].ht;
+			J.len[J.n] = static_cast<uint32_t>(d->probes[q].ht_len);
+			J.off[J.n] = sh.smem_off[q];
+			J.two[J.n] = d->probes[q].kind == 2 ? 1u : 0u;
+			++J.n;
+		}
+		presence_bits_kernel<<<2u * di.sms, 256, 0, stream>>>(J, bits);
+		count_launch(1);
+		if (cudaGetLastError() != cudaSuccess) {
+			cudaFreeAsync(bits, stream);
+			return set_error(FLS_ERR_CUDA, "presence bitmap kernel launch failed");
+		}
+	}
+	P.bits = bits;
+	s      = launch_fixed(make_key('P', P.S.warps, sh.key), &P, grid, 32u * P.S.warps, smem, stream, used);
+	if (bits) { cudaFreeAsync(bits, stream); }
+	return s;
 }
 
 fls_status jit_decode(const fls_column* col, int mode, uint32_t* d_out, uint64_t* d_sum, cudaStream_t stream,

@@ -292,6 +292,7 @@ uint32_t*  device_error_word(); // device address of this device's error word
 void       count_launch(uint64_t n = 1);
 int        tuning_sparse_rows();
 int        tuning_jit();
+int        tuning_group_smem();
 
 // Validates one column descriptor and converts it for a kernel.
 fls_status make_devcol(const fls_column& c, DevCol& d);
@@ -322,6 +323,7 @@ fls_status jit_filter_agg(const fls_column* cols, const fls_filter* filters, uin
 // Probe + group-by shapes: staged columns (probe keys in probe order, then the
 // measure column if no probe reads it), which tables live in shared memory.
 constexpr uint32_t kJitTableWords = 72u * 1024u / 4u; // shared-memory budget for hash tables
+constexpr uint32_t kJitGroupSlots = 2048u;            // most group-sum slots per CTA in shared memory
 struct JitProbeShape {
 	uint32_t    staged[FLS_MAX_QUERY_COLS];
 	uint32_t    n_staged = 0;
@@ -329,6 +331,11 @@ struct JitProbeShape {
 	int         sub      = -1; // staged column subtracted from the measure
 	uint32_t    smem_off[FLS_MAX_PROBES];
 	uint32_t    cta_words = 0;
+	uint32_t    tables_words = 0;  // words of the tables (the presence bitmaps' buffer)
+	uint32_t    bitmaps      = 0;  // probes whose presence bitmap is staged
+	bool        gsm          = false; // group sums in shared memory
+	uint32_t    gslots       = 0;     // their slots (a power of two)
+	uint32_t    gsum_off     = 0;     // their offset (words) in the CTA scratch
 	std::string key;
 };
 // False when a staged column is not uniform FOR or one column is probed twice

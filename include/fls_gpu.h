@@ -391,7 +391,15 @@ typedef enum fls_tune_param {
 	 * cached per shape in the process; any compile or load failure falls back
 	 * to the general kernel.  0: always the general kernel.  Results are
 	 * identical either way. */
-	FLS_TUNE_JIT = 1
+	FLS_TUNE_JIT = 1,
+	/* 1 (default): the specialised join + group-by kernels sum each CTA's rows
+	 * in a direct-mapped cache of group-sum slots in shared memory (the group
+	 * count rounded up to a power of two, at most 2048 slots; a group whose
+	 * slot another group holds adds to its record directly) and add the
+	 * slots to the group records once per CTA, instead of one global int64
+	 * atomic per selected row (few live groups make those atomics contend).
+	 * 0: one global atomic per row.  Results are identical either way. */
+	FLS_TUNE_GROUP_SMEM = 2
 } fls_tune_param;
 fls_status fls_set_tuning(uint32_t param, int64_t value);
 fls_status fls_get_tuning(uint32_t param, int64_t* value);

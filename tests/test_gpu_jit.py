@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from fastlanesgpu_b200 import LAYOUT_NORMAL, LAYOUT_TRANSPOSED, EncodedColumn, datagen, ops
-from fastlanesgpu_b200._lib import TUNE_JIT, TUNE_SPARSE_ROWS
+from fastlanesgpu_b200._lib import TUNE_GROUP_SMEM, TUNE_JIT, TUNE_SPARSE_ROWS
 
 pytestmark = pytest.mark.gpu
 
@@ -293,6 +293,41 @@ def test_jit_probe_random_shapes(jit_on, seed):
     assert used == 1 and used_gen == 0
     assert np.array_equal(got_gen, want)
     assert np.array_equal(got_jit, want)
+    assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
+
+
+@pytest.mark.parametrize("ng,n", [(3, 300 * 1024 + 5), (8192, 1 << 20), (8193, 50 * 1024)])
+def test_jit_probe_group_sums_in_shared_memory(jit_on, ng, n):
+    """Per-CTA group-sum slots in shared memory against one global atomic per
+    row and against numpy: 3 groups in 4 slots; 8192 and 8193 groups in 2048
+    slots, where most groups find their slot held by another and add to
+    their records directly.  Measures near +-2^31 make the slots' 32-bit low
+    words carry and borrow on most rows."""
+    import torch
+    g = np.random.default_rng(ng)
+    ln = 64 if ng == 3 else 16384
+    ht = np.zeros(2 * ln, np.int32)
+    present = g.random(ln) < 0.9
+    ht[0::2][present] = 1 + np.nonzero(present)[0]
+    ht[1::2][present] = g.integers(0, ng, int(present.sum()))
+    k = g.integers(0, ln, n).astype(np.int32)
+    big = g.integers(2**31 - 4096, 2**31, n)
+    measure = np.where(g.random(n) < 0.5, big, -big - 1).astype(np.int64)
+    measure = np.where(g.random(n) < 0.2, g.integers(-100, 100, n), measure).astype(np.int32)
+    cols = [EncodedColumn.uniform(k, bw=int(np.log2(ln))).to_device(),
+            EncodedColumn.uniform(measure, bw=32).to_device()]
+    probes = [(0, torch.from_numpy(ht).cuda(), ln, 0, 2)]
+    want = _numpy_probe([k, measure], measure, [(0, ht, ln, 0, 2)], None, 0, 0, 0, 0, ng)
+    assert np.abs(want.reshape(ng, 4)[:, 2:].copy().view(np.int64)).max() > 2**33
+    try:
+        for gsm in (1, 0):
+            ops.set_tuning(TUNE_GROUP_SMEM, gsm)
+            got, used = _probe_run(cols, probes, 1, 0, 0, 0, 0, ng, jit=True)
+            assert used == 1 and np.array_equal(got, want), gsm
+        got, used = _probe_run(cols, probes, 1, 0, 0, 0, 0, ng, jit=False)
+        assert used == 0 and np.array_equal(got, want)
+    finally:
+        ops.set_tuning(TUNE_GROUP_SMEM, 1)
     assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
 
 

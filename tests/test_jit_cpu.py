@@ -86,3 +86,27 @@ def test_precompile_ssb_join_shapes(query):
                   agg_sub_col=5)
     ops.jit_precompile_join(cols, probes, **kw)
     assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
+
+
+def test_group_smem_tuning_and_shapes():
+    """FLS_TUNE_GROUP_SMEM accepts 0 and 1 only; both settings compile their
+    own specialised Q3.1 kernel (per-CTA group sums in shared memory or one
+    global atomic per row)."""
+    from fastlanesgpu_b200._lib import TUNE_GROUP_SMEM
+    assert ops.get_tuning(TUNE_GROUP_SMEM) == 1
+    with pytest.raises(FlsError):
+        ops.set_tuning(TUNE_GROUP_SMEM, 2)
+    bits = datagen.Q31_BITS
+    cols = [_col(bits[k]) for k in ("lo_suppkey", "lo_custkey", "lo_orderdate", "lo_revenue")]
+    probes = [(0, 0x200000, 1 << 17, 0, 2), (1, 0x400000, 1 << 18, 0, 2), (2, 0x800000, datagen.N_DAYS, 0, 2)]
+    kw = dict(agg_col=3, keys=[(0, 175, 2), (1, 7, 1), (2, 1, 0)], group_sub=1992, n_groups=4375, res_stride=6,
+              sum_slot=4)
+    try:
+        for gsm in (0, 1):
+            ops.set_tuning(TUNE_GROUP_SMEM, gsm)
+            before = ops.jit_stats()["cached"]
+            ops.jit_precompile_join(cols, probes, **kw)
+            assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
+            assert ops.jit_stats()["cached"] >= before
+    finally:
+        ops.set_tuning(TUNE_GROUP_SMEM, 1)
