@@ -117,6 +117,8 @@ _SIGS = {
     "fls_pht_build": (ctypes.c_int, [_VP, ctypes.c_int32, _VP, _VP, ctypes.c_uint64, _VP, ctypes.c_int32,
                                      ctypes.c_int32, _VP]),
     "fls_query_probe_groupby": (ctypes.c_int, [ctypes.POINTER(JoinAggDesc), _VP, _VP]),
+    "fls_query_probe_groupby_ws": (ctypes.c_int, [ctypes.POINTER(JoinAggDesc), _VP, _VP, ctypes.c_uint64, _VP]),
+    "fls_probe_workspace_bytes": (ctypes.c_uint64, [ctypes.POINTER(JoinAggDesc)]),
     "fls_set_launch_config": (ctypes.c_int, [ctypes.c_uint32] * 4),
     "fls_get_launch_config": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
     "fls_kernel_launch_count": (ctypes.c_uint64, []),
@@ -150,6 +152,8 @@ _SIGS = {
     "fls_jit_precompile_probe": (ctypes.c_int, [ctypes.POINTER(JoinAggDesc)]),
     "fls_jit_precompile_join": (ctypes.c_int, [ctypes.POINTER(JoinGroupbyDesc)]),
     "fls_query_join_groupby": (ctypes.c_int, [ctypes.POINTER(JoinGroupbyDesc), _VP, _VP]),
+    "fls_query_join_groupby_ws": (ctypes.c_int, [ctypes.POINTER(JoinGroupbyDesc), _VP, _VP, ctypes.c_uint64, _VP]),
+    "fls_join_workspace_bytes": (ctypes.c_uint64, [ctypes.POINTER(JoinGroupbyDesc)]),
 }
 
 _LIB = None

@@ -606,16 +606,44 @@ struct ProbeBody {
 	// Shared-memory tables, staged once per CTA by all its threads: presence
 	// bitmaps (of PHT_1 tables, whose probe only tests slot != 0, crystal-opt/
 	// join.cuh:42-47, and of PHT_2 tables too large to stage, whose slot hits
-	// when its 64-bit entry is not zero) copied from P.bits, where the host
-	// built them once per query at the same offsets; small PHT_2 tables
-	// verbatim.  GSM: every slot of the group-sum cache starts free.
+	// when its 64-bit entry is not zero) copied from P.bits when a prepass
+	// built them there at the same offsets, else built here from the tables;
+	// small PHT_2 tables verbatim.  GSM: every slot of the group-sum cache
+	// starts free.
 	__device__ void cta_setup(uint32_t* cta) {
 		tables = cta;
 #pragma unroll 1
 		for (int q = 0; q < Q::kNP; ++q) {
 			if (!Q::in_smem(q) && !Q::pbit(q)) { continue; }
 			const uint32_t len = static_cast<uint32_t>(P.len[q]);
-			if (!Q::pht2(q) || Q::pbit(q)) {
+			if ((!Q::pht2(q) || Q::pbit(q)) && P.bits == nullptr) {
+				// No prebuilt bitmaps: one ballot per 32 slots, 8 words per warp
+				// in flight.
+				const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+				const uint32_t n_words = (len + 31u) / 32u;
+				uint32_t*      dst     = cta + P.smem_off[q];
+				for (uint32_t w0 = warp * 8u; w0 < n_words; w0 += nw * 8u) {
+					int32_t x[8];
+#pragma unroll
+					for (uint32_t j = 0; j < 8; ++j) {
+						const uint32_t idx = 32u * (w0 + j) + lane;
+						x[j]               = 0;
+						if (w0 + j < n_words && idx < len) {
+							if (Q::pht2(q)) {
+								const int2 e = __ldg(reinterpret_cast<const int2*>(P.ht[q]) + idx);
+								x[j]         = e.x | e.y;
+							} else {
+								x[j] = __ldg(P.ht[q] + idx);
+							}
+						}
+					}
+#pragma unroll
+					for (uint32_t j = 0; j < 8; ++j) {
+						const uint32_t b = __ballot_sync(0xffffffffu, x[j] != 0);
+						if (lane == 0 && w0 + j < n_words) { dst[w0 + j] = b; }
+					}
+				}
+			} else if (!Q::pht2(q) || Q::pbit(q)) {
 				// 16-byte units: offsets and slot sizes are multiples of 4 words.
 				const uint32_t n4  = ((len + 31u) / 32u + 3u) / 4u;
 				const uint4*   src = reinterpret_cast<const uint4*>(P.bits + P.smem_off[q]);

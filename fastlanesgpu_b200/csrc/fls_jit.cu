@@ -419,32 +419,6 @@ __global__ void __launch_bounds__(256) presence_bits_kernel(const __grid_constan
 	}
 }
 
-// A memory pool per device for the per-query bitmaps that keeps what it
-// holds across synchronisations (the default pool returns memory to the
-// device at every synchronisation and maps it again at the next query).
-cudaMemPool_t bitmap_pool() {
-	static std::mutex                               mu;
-	static std::unordered_map<int, cudaMemPool_t> pools;
-	int                                             dev = 0;
-	if (cudaGetDevice(&dev) != cudaSuccess) { return nullptr; }
-	std::lock_guard<std::mutex> lk(mu);
-	auto                        it = pools.find(dev);
-	if (it != pools.end()) { return it->second; }
-	cudaMemPoolProps props {};
-	props.allocType     = cudaMemAllocationTypePinned;
-	props.location.type = cudaMemLocationTypeDevice;
-	props.location.id   = dev;
-	cudaMemPool_t pool  = nullptr;
-	if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
-		cudaGetLastError();
-		return nullptr;
-	}
-	uint64_t keep = 64ull << 20;
-	cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-	pools[dev] = pool;
-	return pool;
-}
-
 bool jit_probe_shape(const fls_join_groupby_desc* d, JitProbeShape& sh) {
 	sh.n_staged = 0;
 	for (uint32_t q = 0; q < d->n_probes; ++q) {
@@ -533,11 +507,20 @@ bool jit_compile(const fls_join_groupby_desc* d, const JitProbeShape& sh) {
 	return compiled_entry(make_key('P', S.warps, sh.key)).state > 0;
 }
 
-fls_status jit_probe_groupby(const fls_join_groupby_desc* d, int32_t* d_res, int32_t sparse_rows, cudaStream_t stream,
-                             bool& used) {
+uint64_t jit_probe_workspace_bytes(const fls_join_groupby_desc* d) {
+	JitProbeShape sh;
+	if (!tuning_jit() || !jit_probe_shape(d, sh) || !sh.bitmaps) { return 0u; }
+	return 4ull * sh.tables_words;
+}
+
+fls_status jit_probe_groupby(const fls_join_groupby_desc* d, int32_t* d_res, int32_t sparse_rows, void* d_ws,
+                             uint64_t ws_bytes, cudaStream_t stream, bool& used) {
 	used = false;
 	JitProbeShape sh;
 	if (!jit_probe_shape(d, sh)) { return FLS_OK; }
+	if (d_ws && sh.bitmaps && ws_bytes < 4ull * sh.tables_words) {
+		return set_error(FLS_ERR_CAPACITY, "join workspace smaller than fls_join_workspace_bytes");
+	}
 	fls_column sc[FLS_MAX_QUERY_COLS];
 	for (uint32_t i = 0; i < sh.n_staged; ++i) { sc[i] = d->cols[sh.staged[i]]; }
 	fixed::ProbeParams P {};
@@ -567,16 +550,11 @@ fls_status jit_probe_groupby(const fls_join_groupby_desc* d, int32_t* d_res, int
 	P.gsum_off    = sh.gsum_off;
 	P.gslot_mask  = sh.gslots - 1u;
 	P.res         = d_res;
-	// Presence bitmaps: built once per query into a stream-ordered buffer
-	// that every CTA copies (no allocation: the general kernel runs instead).
+	// Presence bitmaps: with a workspace, built once per call for every CTA
+	// to copy; without, each CTA builds its own (P.bits = null).
 	uint32_t* bits = nullptr;
-	if (sh.bitmaps) {
-		cudaMemPool_t pool = bitmap_pool();
-		if (!pool || cudaMallocFromPoolAsync(reinterpret_cast<void**>(&bits), 4ull * sh.tables_words, pool, stream) !=
-		                 cudaSuccess) {
-			cudaGetLastError();
-			return FLS_OK;
-		}
+	if (sh.bitmaps && d_ws) {
+		bits = static_cast<uint32_t*>(d_ws);
 		PresenceJobs J {};
 		for (uint32_t q = 0; q < d->n_probes; ++q) {
 			if (!((sh.bitmaps >> q) & 1u)) { continue; }
@@ -588,15 +566,10 @@ fls_status jit_probe_groupby(const fls_join_groupby_desc* d, int32_t* d_res, int
 		}
 		presence_bits_kernel<<<2u * di.sms, 256, 0, stream>>>(J, bits);
 		count_launch(1);
-		if (cudaGetLastError() != cudaSuccess) {
-			cudaFreeAsync(bits, stream);
-			return set_error(FLS_ERR_CUDA, "presence bitmap kernel launch failed");
-		}
+		if (cudaGetLastError() != cudaSuccess) { return set_error(FLS_ERR_CUDA, "presence bitmap kernel launch failed"); }
 	}
 	P.bits = bits;
-	s      = launch_fixed(make_key('P', P.S.warps, sh.key), &P, grid, 32u * P.S.warps, smem, stream, used);
-	if (bits) { cudaFreeAsync(bits, stream); }
-	return s;
+	return launch_fixed(make_key('P', P.S.warps, sh.key), &P, grid, 32u * P.S.warps, smem, stream, used);
 }
 
 fls_status jit_decode(const fls_column* col, int mode, uint32_t* d_out, uint64_t* d_sum, cudaStream_t stream,

@@ -342,8 +342,12 @@ struct JitProbeShape {
 // (the descriptor must already be validated).
 bool       jit_probe_shape(const fls_join_groupby_desc* desc, JitProbeShape& sh);
 bool       jit_compile(const fls_join_groupby_desc* desc, const JitProbeShape& sh);
-fls_status jit_probe_groupby(const fls_join_groupby_desc* desc, int32_t* d_res, int32_t sparse_rows,
-                             cudaStream_t stream, bool& used);
+// d_ws (optional, 16-byte aligned): room for the presence bitmaps, built
+// once per call by a prepass; without it each CTA builds them.
+fls_status jit_probe_groupby(const fls_join_groupby_desc* desc, int32_t* d_res, int32_t sparse_rows, void* d_ws,
+                             uint64_t ws_bytes, cudaStream_t stream, bool& used);
+// Bytes of workspace the specialised kernel of this query can use (0: none).
+uint64_t jit_probe_workspace_bytes(const fls_join_groupby_desc* desc);
 // Decode of a uniform FOR column: mode 0 = fused uint64 sum into d_sum, mode 1
 // = to HBM (stored order) into d_out.
 fls_status jit_decode(const fls_column* col, int mode, uint32_t* d_out, uint64_t* d_sum, cudaStream_t stream,

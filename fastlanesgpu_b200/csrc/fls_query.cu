@@ -769,8 +769,26 @@ fls_status fls_pht_build(const int32_t* d_filter, int32_t filter_eq, const int32
 	return cuda_check(cudaGetLastError(), "pht_build_kernel launch");
 }
 
+uint64_t fls_join_workspace_bytes(const fls_join_groupby_desc* desc) {
+	return check_groupby_desc(desc) == FLS_OK ? jit_probe_workspace_bytes(desc) : 0u;
+}
+
+uint64_t fls_probe_workspace_bytes(const fls_join_agg_desc* desc) {
+	if (check_join_desc(desc) != FLS_OK) { return 0u; }
+	const fls_join_groupby_desc g = groupby_of(*desc);
+	return fls_join_workspace_bytes(&g);
+}
+
 fls_status fls_query_join_groupby(const fls_join_groupby_desc* desc, int32_t* d_res, fls_stream_t stream) {
+	return fls_query_join_groupby_ws(desc, d_res, nullptr, 0u, stream);
+}
+
+fls_status fls_query_join_groupby_ws(const fls_join_groupby_desc* desc, int32_t* d_res, void* d_workspace,
+                                     uint64_t workspace_bytes, fls_stream_t stream) {
 	if (!d_res) { return set_error(FLS_ERR_INVALID_ARG, "fls_query_join_groupby: null pointer"); }
+	if (reinterpret_cast<uintptr_t>(d_workspace) & 15u) {
+		return set_error(FLS_ERR_ALIGNMENT, "workspace must be 16-byte aligned");
+	}
 	if (reinterpret_cast<uintptr_t>(d_res) & 7u) { return set_error(FLS_ERR_ALIGNMENT, "result must be 8-byte aligned"); }
 	fls_status s = check_groupby_desc(desc);
 	if (s != FLS_OK) { return s; }
@@ -831,7 +849,7 @@ fls_status fls_query_join_groupby(const fls_join_groupby_desc* desc, int32_t* d_
 	if (s != FLS_OK) { return s; }
 	if (tuning_jit()) {
 		bool used = false;
-		s         = jit_probe_groupby(desc, d_res, op.sparse_rows, st, used);
+		s = jit_probe_groupby(desc, d_res, op.sparse_rows, d_workspace, workspace_bytes, st, used);
 		if (s != FLS_OK || used) { return s; }
 	}
 	if (rnd) {
@@ -845,10 +863,15 @@ fls_status fls_query_join_groupby(const fls_join_groupby_desc* desc, int32_t* d_
 }
 
 fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res, fls_stream_t stream) {
+	return fls_query_probe_groupby_ws(desc, d_res, nullptr, 0u, stream);
+}
+
+fls_status fls_query_probe_groupby_ws(const fls_join_agg_desc* desc, int32_t* d_res, void* d_workspace,
+                                      uint64_t workspace_bytes, fls_stream_t stream) {
 	if (!d_res) { return set_error(FLS_ERR_INVALID_ARG, "fls_query_probe_groupby: null pointer"); }
 	fls_status s = check_join_desc(desc);
 	if (s != FLS_OK) { return s; }
 	const fls_join_groupby_desc g = groupby_of(*desc);
-	return fls_query_join_groupby(&g, d_res, stream);
+	return fls_query_join_groupby_ws(&g, d_res, d_workspace, workspace_bytes, stream);
 }
 } // extern "C"

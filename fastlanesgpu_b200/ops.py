@@ -177,8 +177,23 @@ def build_pht(keys, ht_len: int, vals=None, filt=None, filter_eq: int = 1, keys_
     return out
 
 
+def _join_workspace(workspace, n_bytes: int, device):
+    """(pointer, bytes, tensor kept alive) of a join call's workspace:
+    "auto" allocates the bytes the call asks for, None passes none (the
+    kernels then build their shared-memory bitmaps per CTA), a uint8 device
+    tensor is used as given."""
+    import torch
+    if workspace is None or (isinstance(workspace, str) and n_bytes == 0):
+        return None, 0, None
+    if isinstance(workspace, str):
+        if workspace != "auto":
+            raise ValueError("workspace must be 'auto', None or a device tensor")
+        workspace = torch.empty(n_bytes, dtype=torch.uint8, device=device)
+    return workspace.data_ptr(), workspace.numel() * workspace.element_size(), workspace
+
+
 def probe_groupby(cols, probes, agg_col: int, key_a: int, key_b: int, group_mul: int, group_sub: int,
-                  n_groups: int, out=None):
+                  n_groups: int, out=None, workspace="auto"):
     """probes: [(col, ht tensor, ht_len, keys_min, kind)].  Returns the
     reference's result array int32[4*n_groups]: [key_b value, key_a value,
     int64 sum (2 words)] per group."""
@@ -187,7 +202,10 @@ def probe_groupby(cols, probes, agg_col: int, key_a: int, key_b: int, group_mul:
                           n_groups)
     if out is None:
         out = torch.empty(4 * n_groups, dtype=torch.int32, device=cols[0].data.device)
-    check(lib().fls_query_probe_groupby(ctypes.byref(d), out.data_ptr(), _stream()), "fls_query_probe_groupby")
+    n_ws = int(lib().fls_probe_workspace_bytes(ctypes.byref(d))) if workspace is not None else 0
+    ws, ws_bytes, _ws = _join_workspace(workspace, n_ws, out.device)
+    check(lib().fls_query_probe_groupby_ws(ctypes.byref(d), out.data_ptr(), ws, ws_bytes, _stream()),
+          "fls_query_probe_groupby")
     return out
 
 
@@ -227,7 +245,7 @@ def _groupby_desc(arr, n_cols: int, probes, agg_col, keys, group_sub, n_groups, 
 
 
 def join_groupby(cols, probes, agg_col: int, keys, group_sub: int, n_groups: int, res_stride: int, sum_slot: int,
-                 agg_sub_col: int = -1, out=None):
+                 agg_sub_col: int = -1, out=None, workspace="auto"):
     """The general probe + group-by (fls_q21/q31/q41.cu probe_v1): probes
     [(col, ht, ht_len, keys_min, kind)]; keys [(probe, multiplier, record word
     or -1)]; group = (sum of payload * multiplier - group_sub) % n_groups;
@@ -238,7 +256,10 @@ def join_groupby(cols, probes, agg_col: int, keys, group_sub: int, n_groups: int
                              sum_slot, agg_sub_col)
     if out is None:
         out = torch.empty(res_stride * n_groups, dtype=torch.int32, device=cols[0].data.device)
-    check(lib().fls_query_join_groupby(ctypes.byref(d), out.data_ptr(), _stream()), "fls_query_join_groupby")
+    n_ws = int(lib().fls_join_workspace_bytes(ctypes.byref(d))) if workspace is not None else 0
+    ws, ws_bytes, _ws = _join_workspace(workspace, n_ws, out.device)
+    check(lib().fls_query_join_groupby_ws(ctypes.byref(d), out.data_ptr(), ws, ws_bytes, _stream()),
+          "fls_query_join_groupby")
     return out
 
 
@@ -250,6 +271,17 @@ def jit_precompile_join(col_descs, probes, agg_col, keys, group_sub, n_groups, r
     d, _keep = _groupby_desc(arr, len(descs), probes, agg_col, keys, group_sub, n_groups, res_stride, sum_slot,
                              agg_sub_col)
     check(lib().fls_jit_precompile_join(ctypes.byref(d)), "fls_jit_precompile_join")
+
+
+def join_workspace_bytes(col_descs, probes, agg_col, keys, group_sub, n_groups, res_stride, sum_slot,
+                         agg_sub_col: int = -1) -> int:
+    """Bytes of device workspace join_groupby can use for this query (0: none);
+    needs no GPU."""
+    descs = [c.desc if hasattr(c, "desc") else c for c in col_descs]
+    arr = (Column * len(descs))(*descs)
+    d, _keep = _groupby_desc(arr, len(descs), probes, agg_col, keys, group_sub, n_groups, res_stride, sum_slot,
+                             agg_sub_col)
+    return int(lib().fls_join_workspace_bytes(ctypes.byref(d)))
 
 
 def jit_precompile_probe(col_descs, probes, agg_col: int, key_a: int, key_b: int, group_mul: int, group_sub: int,

@@ -266,6 +266,21 @@ typedef struct fls_join_groupby_desc {
 
 fls_status fls_query_join_groupby(const fls_join_groupby_desc* desc, int32_t* d_res, fls_stream_t stream);
 
+/* Optional device workspace of the join + group-by calls.  The specialised
+ * kernels keep the presence bitmaps of large hash tables in shared memory;
+ * with a workspace of fls_join_workspace_bytes(desc) bytes (16-byte aligned)
+ * one small kernel builds them once per call and every CTA copies them,
+ * without one each CTA builds them from the tables (reading every table it
+ * stages whole).  0 when the query stages no bitmap.  Results are identical
+ * either way; the library allocates nothing.  A non-null workspace smaller
+ * than required returns FLS_ERR_CAPACITY. */
+uint64_t   fls_join_workspace_bytes(const fls_join_groupby_desc* desc);
+uint64_t   fls_probe_workspace_bytes(const fls_join_agg_desc* desc);
+fls_status fls_query_join_groupby_ws(const fls_join_groupby_desc* desc, int32_t* d_res, void* d_workspace,
+                                     uint64_t workspace_bytes, fls_stream_t stream);
+fls_status fls_query_probe_groupby_ws(const fls_join_agg_desc* desc, int32_t* d_res, void* d_workspace,
+                                      uint64_t workspace_bytes, fls_stream_t stream);
+
 /* ------------------------------------ batched persistent execution (device) */
 
 /* One filter-aggregate query of a batch: rows with lo <= cols[col] <= hi,

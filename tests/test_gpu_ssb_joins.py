@@ -93,3 +93,45 @@ def test_join_groupby_descriptor_validation(cuda):
     for b in bad:
         with pytest.raises((FlsError, ValueError)):
             ops.join_groupby(dcols, probes, **b)
+
+
+@pytest.mark.parametrize("query", ["q31", "q41"])
+def test_join_groupby_workspace_forms(cuda, oracle, query):
+    """The presence bitmaps built once per call into a workspace, or per CTA
+    without one, give the same result; a workspace smaller than
+    fls_join_workspace_bytes is refused before anything runs."""
+    import torch
+    n = 300 * 1024 + 17
+    t, tables, hcols, dcols, probes, kw = datagen.ssb_join(query, n, seed=n)
+    want = _want(oracle, query, t, tables)
+    need = ops.join_workspace_bytes(dcols, probes, **kw)
+    assert need > 0
+    big = torch.zeros(need + 4096, dtype=torch.uint8, device="cuda")
+    for ws in (None, "auto", big):
+        got = ops.join_groupby(dcols, probes, workspace=ws, **kw).cpu().numpy()
+        ops.check_device_error()
+        assert np.array_equal(got, want), ws if ws is None or isinstance(ws, str) else "tensor"
+    with pytest.raises(FlsError) as e:
+        ops.join_groupby(dcols, probes, workspace=big[:need - 16], **kw)
+    assert e.value.status == 8
+    ops.check_device_error()
+
+
+def test_q21_workspace_forms(cuda, oracle):
+    import torch
+    n = 200 * 1024 + 9
+    t = datagen.q21_tables(n, seed=9)
+    dev = {k: torch.from_numpy(v).cuda() for k, v in t.items() if not k.startswith("lo_")}
+    ht_s = ops.build_pht(dev["s_suppkey"], dev["s_suppkey"].numel(), filt=dev["s_region"], filter_eq=1)
+    ht_p = ops.build_pht(dev["p_partkey"], dev["p_partkey"].numel(), vals=dev["p_brand1"], filt=dev["p_category"],
+                         filter_eq=1)
+    ht_d = ops.build_pht(dev["d_datekey"], datagen.N_DAYS, vals=dev["d_year"])
+    names = ["lo_suppkey", "lo_partkey", "lo_orderdate", "lo_revenue"]
+    cols = [EncodedColumn.uniform(t[k], bw=datagen.Q21_BITS[k]).to_device() for k in names]
+    probes = [(0, ht_s, ht_s.numel(), 0, 1), (1, ht_p, ht_p.numel() // 2, 0, 2), (2, ht_d, ht_d.numel() // 2, 0, 2)]
+    want = oracle.probe_groupby(t["lo_suppkey"], t["lo_partkey"], t["lo_orderdate"], t["lo_revenue"],
+                                ht_s.cpu().numpy(), ht_p.cpu().numpy(), ht_d.cpu().numpy())
+    for ws in (None, "auto"):
+        got = ops.probe_groupby(cols, probes, 3, 1, 2, 7, 1992, datagen.N_GROUPS, workspace=ws).cpu().numpy()
+        ops.check_device_error()
+        assert np.array_equal(got, want), ws

@@ -110,3 +110,24 @@ def test_group_smem_tuning_and_shapes():
             assert ops.jit_stats()["cached"] >= before
     finally:
         ops.set_tuning(TUNE_GROUP_SMEM, 1)
+
+
+def test_join_workspace_bytes():
+    """The join workspace holds the presence bitmaps the specialised kernel
+    stages: Q3.1 stages the supplier (2^17 slots) and customer (2^18) PHT_2
+    bitmaps and the date table verbatim, 17400 words in all; a query whose
+    tables all fit verbatim, or the general kernel (FLS_TUNE_JIT=0), needs none."""
+    from fastlanesgpu_b200._lib import TUNE_JIT
+    bits = datagen.Q31_BITS
+    cols = [_col(bits[k]) for k in ("lo_suppkey", "lo_custkey", "lo_orderdate", "lo_revenue")]
+    probes = [(0, 0x200000, 1 << 17, 0, 2), (1, 0x400000, 1 << 18, 0, 2), (2, 0x800000, datagen.N_DAYS, 0, 2)]
+    kw = dict(agg_col=3, keys=[(0, 175, 2), (1, 7, 1), (2, 1, 0)], group_sub=1992, n_groups=4375, res_stride=6,
+              sum_slot=4)
+    assert ops.join_workspace_bytes(cols, probes, **kw) == 4 * (4096 + 8192 + 5112)
+    small = [(0, 0x200000, 1000, 0, 2), (1, 0x400000, 2000, 0, 2), (2, 0x800000, datagen.N_DAYS, 0, 2)]
+    assert ops.join_workspace_bytes(cols, small, **kw) == 0
+    try:
+        ops.set_tuning(TUNE_JIT, 0)
+        assert ops.join_workspace_bytes(cols, probes, **kw) == 0
+    finally:
+        ops.set_tuning(TUNE_JIT, 1)
