@@ -383,7 +383,11 @@ def run_ours(a, dist: Dist):
     ms_step = ms / a.steps
     peak, peak_src = measured_peak_gbs()
     achieved = algo_bytes / (ms_local / a.steps / 1e3) / 1e9
+    # profiled traffic is per launch at the default size; it grows with the
+    # vectors processed
     traffic = profiled_traffic(metric_key)
+    if traffic is not None:
+        traffic = int(traffic * a.rows / ((1 << 28) if a.workload == "decode" else (1 << 27)))
     out = {
         "metric": "fused decode+query rows/s", "value": value, "unit": "rows/s", "n_gpus": dist.world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
