@@ -83,7 +83,8 @@ class JoinGroupbyDesc(ctypes.Structure):
                 ("agg_sub_col", ctypes.c_int32), ("n_keys", ctypes.c_uint32),
                 ("key_probe", ctypes.c_int32 * MAX_GROUP_KEYS), ("key_mul", ctypes.c_int32 * MAX_GROUP_KEYS),
                 ("key_slot", ctypes.c_int32 * MAX_GROUP_KEYS), ("group_sub", ctypes.c_int32),
-                ("n_groups", ctypes.c_int32), ("res_stride", ctypes.c_uint32), ("sum_slot", ctypes.c_uint32)]
+                ("n_groups", ctypes.c_int32), ("res_stride", ctypes.c_uint32), ("sum_slot", ctypes.c_uint32),
+                ("sum_bits", ctypes.c_uint32)]
 
 
 class JitStats(ctypes.Structure):
@@ -117,6 +118,8 @@ _SIGS = {
     "fls_pht_build": (ctypes.c_int, [_VP, ctypes.c_int32, _VP, _VP, ctypes.c_uint64, _VP, ctypes.c_int32,
                                      ctypes.c_int32, _VP]),
     "fls_query_probe_groupby": (ctypes.c_int, [ctypes.POINTER(JoinAggDesc), _VP, _VP]),
+    "fls_pht_build_ranges": (ctypes.c_int, [_VP] + [ctypes.c_int32] * 4 + [_VP, _VP, ctypes.c_uint64, _VP,
+                                                                            ctypes.c_int32, ctypes.c_int32, _VP]),
     "fls_query_probe_groupby_ws": (ctypes.c_int, [ctypes.POINTER(JoinAggDesc), _VP, _VP, ctypes.c_uint64, _VP]),
     "fls_probe_workspace_bytes": (ctypes.c_uint64, [ctypes.POINTER(JoinAggDesc)]),
     "fls_set_launch_config": (ctypes.c_int, [ctypes.c_uint32] * 4),

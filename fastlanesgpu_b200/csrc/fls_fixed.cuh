@@ -65,7 +65,7 @@ struct ProbeParams {
 	uint32_t       stride, sum_slot; // group record: int32 words, word of the int64 sum
 	uint32_t       gsum_off;         // GSM: words into the CTA scratch of the group-sum slots
 	uint32_t       gslot_mask;       // GSM: slots - 1 (a power of two)
-	uint32_t       pad_;
+	uint32_t       sum32;            // 1: wrapping int32 sum in one record word, 0: int64 in two
 	const uint32_t* bits;            // presence bitmaps at the tables' shared-memory offsets
 	int32_t*       res;
 };
@@ -515,6 +515,16 @@ __device__ __forceinline__ void probe_rows(const ProbeParams& P, const uint32_t*
 	}
 }
 
+// Adds v (an int64 sum, or a measure widened to one) to a group record: the
+// int64 at word sum_slot, or its low 32 bits to the wrapping int32 there.
+__device__ __forceinline__ void add_record_sum(const ProbeParams& P, int32_t* rec, unsigned long long v) {
+	if (P.sum32) {
+		atomicAdd(reinterpret_cast<unsigned int*>(rec + P.sum_slot), static_cast<unsigned int>(v));
+	} else {
+		atomicAdd(reinterpret_cast<unsigned long long*>(rec + P.sum_slot), v);
+	}
+}
+
 // Group-by epilogue of one selected row (fls_q21.cu:67-77, fls_q31.cu:82-91,
 // fls_q41.cu:96-104): the group of the keys in wrapping 32-bit arithmetic,
 // the key values into their words of the group record, the measure into its
@@ -562,10 +572,7 @@ __device__ __forceinline__ void emit(const ProbeParams& P, uint32_t* tables,
 			if (P.key_slot[k] >= 0) { rec[P.key_slot[k]] = kv[k][j]; }
 		}
 	}
-	if (!cached) {
-		atomicAdd(reinterpret_cast<unsigned long long*>(rec + P.sum_slot),
-		          static_cast<unsigned long long>(static_cast<long long>(measure)));
-	}
+	if (!cached) { add_record_sum(P, rec, static_cast<unsigned long long>(static_cast<long long>(measure))); }
 }
 
 template <class Q>
@@ -708,9 +715,7 @@ struct ProbeBody {
 				const uint32_t           g = tag[i];
 				const unsigned long long v =
 				    static_cast<unsigned long long>(sum[2u * i]) | (static_cast<unsigned long long>(sum[2u * i + 1u]) << 32);
-				if (g != kFreeSlot && v != 0ull) {
-					atomicAdd(reinterpret_cast<unsigned long long*>(P.res + static_cast<int64_t>(g) * P.stride + P.sum_slot), v);
-				}
+				if (g != kFreeSlot && v != 0ull) { add_record_sum(P, P.res + static_cast<int64_t>(g) * P.stride, v); }
 			}
 		}
 	}

@@ -549,6 +549,7 @@ fls_status jit_probe_groupby(const fls_join_groupby_desc* d, int32_t* d_res, int
 	P.sparse_rows = sparse_rows;
 	P.gsum_off    = sh.gsum_off;
 	P.gslot_mask  = sh.gslots - 1u;
+	P.sum32       = d->sum_bits == 32 ? 1u : 0u;
 	P.res         = d_res;
 	// Presence bitmaps: with a workspace, built once per call for every CTA
 	// to copy; without, each CTA builds its own (P.bits = null).

@@ -230,7 +230,8 @@ struct ProbeParams {
 	int32_t        n_keys;
 	int32_t        key_probe[FLS_MAX_GROUP_KEYS], key_mul[FLS_MAX_GROUP_KEYS], key_slot[FLS_MAX_GROUP_KEYS];
 	int32_t        sub, n_groups;
-	uint32_t       stride, sum_slot; // group record: int32 words, word of the int64 sum
+	uint32_t       stride, sum_slot; // group record: int32 words, word of the sum
+	uint32_t       sum32;            // 1: wrapping int32 sum in one word, 0: int64 sum in two
 	uint32_t       agg_col;
 	int32_t        agg_sub; // column subtracted from the measure, or -1
 	int32_t*       res;
@@ -323,7 +324,16 @@ struct ProbeParams {
 	// Group-by epilogue of one selected row (fls_q21.cu:67-77, fls_q31.cu:82-91,
 	// fls_q41.cu:96-104): the group of the key values in wrapping 32-bit
 	// arithmetic, the key values into their words of the group record, the
-	// measure (an int32, widened) into its int64 sum.
+	// measure (an int32, widened) into its int64 sum, or into a wrapping int32
+	// sum.
+	__device__ __forceinline__ void add_sum(int32_t* rec, int32_t measure) const {
+		if (sum32) {
+			atomicAdd(reinterpret_cast<unsigned int*>(rec + sum_slot), static_cast<unsigned int>(measure));
+		} else {
+			atomicAdd(reinterpret_cast<unsigned long long*>(rec + sum_slot),
+			          static_cast<unsigned long long>(static_cast<long long>(measure)));
+		}
+	}
 	__device__ __forceinline__ void emit(const int32_t (&kv)[FLS_MAX_GROUP_KEYS], uint32_t measure, uint32_t* err) const {
 		uint32_t key = 0u - static_cast<uint32_t>(sub);
 #pragma unroll
@@ -341,8 +351,7 @@ struct ProbeParams {
 		for (int k = 0; k < FLS_MAX_GROUP_KEYS; ++k) {
 			if (k < n_keys && key_slot[k] >= 0) { rec[key_slot[k]] = kv[k]; }
 		}
-		atomicAdd(reinterpret_cast<unsigned long long*>(rec + sum_slot),
-		          static_cast<unsigned long long>(static_cast<long long>(static_cast<int32_t>(measure))));
+		add_sum(rec, static_cast<int32_t>(measure));
 	}
 };
 
@@ -522,22 +531,23 @@ struct ProbeGroupByDenseOp : ProbeParams {
 		}
 #pragma unroll
 		for (uint32_t r = 0; r < 32; ++r) {
-			if ((mask >> r) & 1u) {
-				atomicAdd(reinterpret_cast<unsigned long long*>(res + static_cast<int64_t>(grp[r]) * stride + sum_slot),
-				          static_cast<unsigned long long>(static_cast<long long>(static_cast<int32_t>(vals[r]))));
-			}
+			if ((mask >> r) & 1u) { add_sum(res + static_cast<int64_t>(grp[r]) * stride, static_cast<int32_t>(vals[r])); }
 		}
 	}
 	__device__ void finish(State&, uint32_t, const StageCfg&) const {}
 };
 
-// Selective perfect-hash build (join.cuh:190-334, fls_q21.cu:197-263).
-__global__ void pht_build_kernel(const int32_t* __restrict__ filter, int32_t filter_eq,
-                                 const int32_t* __restrict__ keys, const int32_t* __restrict__ vals, uint64_t n,
-                                 int32_t* ht, int32_t len, int32_t keys_min, uint32_t* err) {
+// Selective perfect-hash build (join.cuh:190-334, fls_q21.cu:197-263): rows
+// whose filter value lies in [lo0, hi0] or [lo1, hi1].
+__global__ void pht_build_kernel(const int32_t* __restrict__ filter, int32_t lo0, int32_t hi0, int32_t lo1,
+                                 int32_t hi1, const int32_t* __restrict__ keys, const int32_t* __restrict__ vals,
+                                 uint64_t n, int32_t* ht, int32_t len, int32_t keys_min, uint32_t* err) {
 	const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
 	for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
-		if (filter && __ldg(filter + i) != filter_eq) { continue; }
+		if (filter) {
+			const int32_t f = __ldg(filter + i);
+			if (!((f >= lo0 && f <= hi0) || (f >= lo1 && f <= hi1))) { continue; }
+		}
 		const int32_t key = __ldg(keys + i);
 		const int32_t h   = static_cast<int32_t>(static_cast<uint32_t>(key) - static_cast<uint32_t>(keys_min)) % len;
 		if (h < 0) {
@@ -643,6 +653,7 @@ fls_join_groupby_desc groupby_of(const fls_join_agg_desc& d) {
 	g.n_groups     = d.n_groups;
 	g.res_stride   = 4;
 	g.sum_slot     = 2;
+	g.sum_bits     = 64;
 	return g;
 }
 
@@ -654,8 +665,15 @@ fls_status check_groupby_desc(const fls_join_groupby_desc* d) {
 	    d->n_groups <= 0) {
 		return set_error(FLS_ERR_INVALID_ARG, "bad measure column or group count");
 	}
-	if (d->res_stride < 2 || (d->res_stride & 1u) || (d->sum_slot & 1u) || d->sum_slot + 1u >= d->res_stride) {
-		return set_error(FLS_ERR_INVALID_ARG, "group record: even stride, even sum word inside the record");
+	if (d->sum_bits != 0 && d->sum_bits != 32 && d->sum_bits != 64) {
+		return set_error(FLS_ERR_INVALID_ARG, "sum_bits must be 32 or 64");
+	}
+	const bool     sum32     = d->sum_bits == 32;
+	const uint32_t sum_words = sum32 ? 1u : 2u;
+	if (sum32 ? (d->res_stride < 1 || d->sum_slot >= d->res_stride)
+	          : (d->res_stride < 2 || (d->res_stride & 1u) || (d->sum_slot & 1u) || d->sum_slot + 1u >= d->res_stride)) {
+		return set_error(FLS_ERR_INVALID_ARG,
+		                 "group record: sum word inside the record (int64: even stride, even sum word)");
 	}
 	if (d->n_keys == 0 || d->n_keys > FLS_MAX_GROUP_KEYS) { return set_error(FLS_ERR_INVALID_ARG, "1..3 group keys"); }
 	for (uint32_t k = 0; k < d->n_keys; ++k) {
@@ -663,8 +681,8 @@ fls_status check_groupby_desc(const fls_join_groupby_desc* d) {
 		if (q < 0 || q >= static_cast<int32_t>(d->n_probes) || d->probes[q].kind != 2) {
 			return set_error(FLS_ERR_INVALID_ARG, "group keys must name PHT_2 probes");
 		}
-		if (w < -1 || w >= static_cast<int32_t>(d->res_stride) || w == static_cast<int32_t>(d->sum_slot) ||
-		    w == static_cast<int32_t>(d->sum_slot) + 1) {
+		if (w < -1 || w >= static_cast<int32_t>(d->res_stride) ||
+		    (w >= static_cast<int32_t>(d->sum_slot) && w < static_cast<int32_t>(d->sum_slot + sum_words))) {
 			return set_error(FLS_ERR_INVALID_ARG, "key word outside the group record or on the sum");
 		}
 	}
@@ -755,6 +773,13 @@ fls_status fls_jit_precompile_join(const fls_join_groupby_desc* desc) {
 
 fls_status fls_pht_build(const int32_t* d_filter, int32_t filter_eq, const int32_t* d_keys, const int32_t* d_vals,
                          uint64_t n, int32_t* d_ht, int32_t ht_len, int32_t keys_min, fls_stream_t stream) {
+	return fls_pht_build_ranges(d_filter, filter_eq, filter_eq, 1, 0, d_keys, d_vals, n, d_ht, ht_len, keys_min,
+	                            stream);
+}
+
+fls_status fls_pht_build_ranges(const int32_t* d_filter, int32_t lo0, int32_t hi0, int32_t lo1, int32_t hi1,
+                                const int32_t* d_keys, const int32_t* d_vals, uint64_t n, int32_t* d_ht,
+                                int32_t ht_len, int32_t keys_min, fls_stream_t stream) {
 	if (!d_keys || !d_ht || ht_len <= 0) { return set_error(FLS_ERR_INVALID_ARG, "fls_pht_build: bad arguments"); }
 	DeviceInfo di;
 	fls_status s = device_info(di);
@@ -762,8 +787,8 @@ fls_status fls_pht_build(const int32_t* d_filter, int32_t filter_eq, const int32
 	if (n == 0) { return FLS_OK; }
 	const uint64_t want = (n + 255u) / 256u;
 	const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>(want, static_cast<uint64_t>(di.sms) * 8u));
-	pht_build_kernel<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(d_filter, filter_eq, d_keys, d_vals, n,
-	                                                                           d_ht, ht_len, keys_min,
+	pht_build_kernel<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(d_filter, lo0, hi0, lo1, hi1, d_keys,
+	                                                                           d_vals, n, d_ht, ht_len, keys_min,
 	                                                                           device_error_word());
 	count_launch();
 	return cuda_check(cudaGetLastError(), "pht_build_kernel launch");
@@ -823,6 +848,7 @@ fls_status fls_query_join_groupby_ws(const fls_join_groupby_desc* desc, int32_t*
 	op.n_groups    = desc->n_groups;
 	op.stride      = desc->res_stride;
 	op.sum_slot    = desc->sum_slot;
+	op.sum32       = desc->sum_bits == 32 ? 1u : 0u;
 	op.agg_col     = desc->agg_col;
 	op.agg_sub     = desc->agg_sub_col;
 	op.res         = d_res;

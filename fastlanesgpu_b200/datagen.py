@@ -258,3 +258,160 @@ def ssb_join(query: str, n: int, seed: int, device="cuda"):
         kw = dict(agg_col=4, keys=[(1, 7, 1), (3, 1, 0)], group_sub=1992, n_groups=Q41_GROUPS, res_stride=4,
                   sum_slot=2, agg_sub_col=5)
     return t, tables, hcols, dcols, probes, kw
+
+
+# ------------------------------------------------------------- SSB suite
+# All thirteen SSB queries on one seeded SSB-shaped schema (SSB data is not
+# available): cities U[0,250) with nation = city // 10 and region = nation // 5
+# (dbgen's hierarchy), brands U[0,1000) with category = brand // 40 and
+# manufacturer = category // 5, day ids 0..2555 with year and yyyymm.  The
+# predicate constants and group formulas are those of crystal-opt src/ssb
+# (q11.cu .. q43.cu); date keys are day ids instead of yyyymmdd, so date
+# ranges become day-id ranges and the date table is indexed from 0.
+
+SSB_SUPP, SSB_CUST, SSB_PART = 1 << 17, 1 << 18, 1 << 19
+SSB_BITS = {"lo_orderdate": 12, "lo_suppkey": 17, "lo_custkey": 18, "lo_partkey": 19, "lo_quantity": 6,
+            "lo_discount": 4, "lo_extendedprice": 24, "lo_revenue": 24, "lo_supplycost": 18}
+
+
+def day_id(y: int, m: int, d: int) -> int:
+    return int((np.datetime64(f"{y:04d}-{m:02d}-{d:02d}") - np.datetime64("1992-01-01")).astype(int))
+
+
+def ssb_tables(n: int, seed: int = 13) -> dict:
+    """Fact columns of n rows and the four dimension tables."""
+    g = rng(seed)
+    days = np.arange(N_DAYS)
+    dates = np.datetime64("1992-01-01") + days
+    ym = dates.astype("datetime64[M]").astype(int)
+    s_city = g.integers(0, 250, size=SSB_SUPP).astype(np.int32)
+    c_city = g.integers(0, 250, size=SSB_CUST).astype(np.int32)
+    brand = g.integers(0, 1000, size=SSB_PART).astype(np.int32)
+    t = {
+        "lo_orderdate": g.integers(0, N_DAYS, size=n).astype(np.int32),
+        "lo_suppkey": g.integers(0, SSB_SUPP, size=n).astype(np.int32),
+        "lo_custkey": g.integers(0, SSB_CUST, size=n).astype(np.int32),
+        "lo_partkey": g.integers(0, SSB_PART, size=n).astype(np.int32),
+        "lo_quantity": g.integers(1, 51, size=n).astype(np.int32),
+        "lo_discount": g.integers(0, 11, size=n).astype(np.int32),
+        "lo_extendedprice": g.integers(90000, 10_500_001, size=n).astype(np.int32),
+        "lo_revenue": g.integers(90000, 10_500_001, size=n).astype(np.int32),
+        "lo_supplycost": g.integers(50000, 150000, size=n).astype(np.int32),
+        "d_datekey": days.astype(np.int32), "d_year": year_of_day(days),
+        "d_yearmonthnum": ((1970 + ym // 12) * 100 + ym % 12 + 1).astype(np.int32),
+        "s_suppkey": np.arange(SSB_SUPP, dtype=np.int32), "s_city": s_city,
+        "s_nation": (s_city // 10).astype(np.int32), "s_region": (s_city // 50).astype(np.int32),
+        "c_custkey": np.arange(SSB_CUST, dtype=np.int32), "c_city": c_city,
+        "c_nation": (c_city // 10).astype(np.int32), "c_region": (c_city // 50).astype(np.int32),
+        "p_partkey": np.arange(SSB_PART, dtype=np.int32), "p_brand1": brand,
+        "p_category": (brand // 40).astype(np.int32), "p_mfgr": (brand // 200).astype(np.int32),
+    }
+    return t
+
+
+_I32_MIN = -(1 << 31)
+_YEARS_92_97 = [(1992, 1997)]
+_YEARS_97_98 = [(1997, 1998)]
+
+
+def _dim(name):
+    return {"d": ("d_datekey", N_DAYS), "s": ("s_suppkey", SSB_SUPP), "c": ("c_custkey", SSB_CUST),
+            "p": ("p_partkey", SSB_PART)}[name]
+
+
+# filter queries: (fact columns, [(column index, lo, hi)], agg_a, agg_b) with
+# sum(cols[agg_a] * cols[agg_b]); join queries: fact columns, probes
+# [(fact column index, dimension, payload column or None, filter column or
+# None, [(lo, hi)] ranges)], group keys [(probe, multiplier, record word)],
+# group_sub, n_groups, record stride, sum word, sum bits, measure column and
+# subtracted column (or None).
+SSB_QUERIES = {
+    "q11": dict(kind="filter", cols=["lo_orderdate", "lo_discount", "lo_quantity", "lo_extendedprice"],
+                filters=[(0, day_id(1993, 1, 1), day_id(1993, 12, 31)), (1, 1, 3), (2, _I32_MIN, 24)]),
+    "q12": dict(kind="filter", cols=["lo_orderdate", "lo_discount", "lo_quantity", "lo_extendedprice"],
+                filters=[(0, day_id(1994, 1, 1), day_id(1994, 1, 31)), (1, 4, 6), (2, 26, 35)]),
+    "q13": dict(kind="filter", cols=["lo_orderdate", "lo_discount", "lo_quantity", "lo_extendedprice"],
+                filters=[(0, day_id(1994, 2, 4), day_id(1994, 2, 10)), (1, 5, 7), (2, 26, 35)]),
+    "q21": dict(kind="join", cols=["lo_suppkey", "lo_partkey", "lo_orderdate", "lo_revenue"],
+                probes=[(0, "s", None, "s_region", [(1, 1)]), (1, "p", "p_brand1", "p_category", [(1, 1)]),
+                        (2, "d", "d_year", None, None)],
+                keys=[(1, 7, 1), (2, 1, 0)], sub=1992, groups=7 * 1000, stride=4, sum_slot=2, sum_bits=64,
+                agg=3, agg_sub=None),
+    "q22": dict(kind="join", cols=["lo_suppkey", "lo_partkey", "lo_orderdate", "lo_revenue"],
+                probes=[(0, "s", None, "s_region", [(2, 2)]), (1, "p", "p_brand1", "p_brand1", [(260, 267)]),
+                        (2, "d", "d_year", None, None)],
+                keys=[(1, 7, 1), (2, 1, 0)], sub=1992, groups=7 * 1000, stride=4, sum_slot=2, sum_bits=64,
+                agg=3, agg_sub=None),
+    "q23": dict(kind="join", cols=["lo_suppkey", "lo_partkey", "lo_orderdate", "lo_revenue"],
+                probes=[(0, "s", None, "s_region", [(3, 3)]), (1, "p", "p_brand1", "p_brand1", [(260, 260)]),
+                        (2, "d", "d_year", None, None)],
+                keys=[(1, 7, 1), (2, 1, 0)], sub=1992, groups=7 * 1000, stride=4, sum_slot=2, sum_bits=64,
+                agg=3, agg_sub=None),
+    "q31": dict(kind="join", cols=["lo_suppkey", "lo_custkey", "lo_orderdate", "lo_revenue"],
+                probes=[(0, "s", "s_nation", "s_region", [(2, 2)]), (1, "c", "c_nation", "c_region", [(2, 2)]),
+                        (2, "d", "d_year", "d_year", _YEARS_92_97)],
+                keys=[(0, 25 * 7, 2), (1, 7, 1), (2, 1, 0)], sub=1992, groups=7 * 25 * 25, stride=6, sum_slot=4,
+                sum_bits=64, agg=3, agg_sub=None),
+    "q32": dict(kind="join", cols=["lo_suppkey", "lo_custkey", "lo_orderdate", "lo_revenue"],
+                probes=[(0, "s", "s_city", "s_nation", [(24, 24)]), (1, "c", "c_city", "c_nation", [(24, 24)]),
+                        (2, "d", "d_year", "d_year", _YEARS_92_97)],
+                keys=[(0, 250 * 7, 2), (1, 7, 1), (2, 1, 0)], sub=1992, groups=7 * 250 * 250, stride=4, sum_slot=3,
+                sum_bits=32, agg=3, agg_sub=None),
+    "q33": dict(kind="join", cols=["lo_suppkey", "lo_custkey", "lo_orderdate", "lo_revenue"],
+                probes=[(0, "s", "s_city", "s_city", [(231, 231), (235, 235)]),
+                        (1, "c", "c_city", "c_city", [(231, 231), (235, 235)]),
+                        (2, "d", "d_year", "d_year", _YEARS_92_97)],
+                keys=[(0, 250 * 7, 2), (1, 7, 1), (2, 1, 0)], sub=1992, groups=7 * 250 * 250, stride=4, sum_slot=3,
+                sum_bits=32, agg=3, agg_sub=None),
+    "q34": dict(kind="join", cols=["lo_suppkey", "lo_custkey", "lo_orderdate", "lo_revenue"],
+                probes=[(0, "s", "s_city", "s_city", [(231, 231), (235, 235)]),
+                        (1, "c", "c_city", "c_city", [(231, 231), (235, 235)]),
+                        (2, "d", "d_year", "d_yearmonthnum", [(199712, 199712)])],
+                keys=[(0, 250 * 7, 2), (1, 7, 1), (2, 1, 0)], sub=1992, groups=7 * 250 * 250, stride=4, sum_slot=3,
+                sum_bits=32, agg=3, agg_sub=None),
+    "q41": dict(kind="join", cols=["lo_suppkey", "lo_custkey", "lo_partkey", "lo_orderdate", "lo_revenue",
+                                   "lo_supplycost"],
+                probes=[(0, "s", None, "s_region", [(1, 1)]), (1, "c", "c_nation", "c_region", [(1, 1)]),
+                        (2, "p", None, "p_mfgr", [(0, 1)]), (3, "d", "d_year", None, None)],
+                keys=[(1, 7, 1), (3, 1, 0)], sub=1992, groups=7 * 25, stride=4, sum_slot=2, sum_bits=64,
+                agg=4, agg_sub=5),
+    "q42": dict(kind="join", cols=["lo_suppkey", "lo_custkey", "lo_partkey", "lo_orderdate", "lo_revenue",
+                                   "lo_supplycost"],
+                probes=[(0, "s", "s_nation", "s_region", [(1, 1)]), (1, "c", None, "c_region", [(1, 1)]),
+                        (2, "p", "p_category", "p_mfgr", [(0, 0), (1, 1)]),
+                        (3, "d", "d_year", "d_year", _YEARS_97_98)],
+                keys=[(3, 25 * 25, 0), (0, 25, 1), (2, 1, 2)], sub=1992 * 25 * 25, groups=7 * 25 * 25, stride=6,
+                sum_slot=4, sum_bits=64, agg=4, agg_sub=5),
+    "q43": dict(kind="join", cols=["lo_suppkey", "lo_custkey", "lo_partkey", "lo_orderdate", "lo_revenue",
+                                   "lo_supplycost"],
+                probes=[(0, "s", "s_city", "s_nation", [(24, 24)]), (1, "c", None, "c_region", [(1, 1)]),
+                        (2, "p", "p_brand1", "p_category", [(3, 3)]), (3, "d", "d_year", "d_year", _YEARS_97_98)],
+                keys=[(3, 250 * 1000, 0), (0, 1000, 1), (2, 1, 2)], sub=1992 * 250 * 1000, groups=7 * 250 * 1000,
+                stride=4, sum_slot=3, sum_bits=32, agg=4, agg_sub=5),
+}
+
+
+def ssb_device_query(name: str, t: dict, dcols: dict, device="cuda"):
+    """Device hash tables and operator arguments of SSB query `name` over the
+    tables `t` and the device columns `dcols` (fact column name -> device
+    column).  Filter queries: {"kind", "cols", "filters", "agg_a", "agg_b"};
+    join queries: {"kind", "cols", "tables", "probes", "kw"} with probes in the
+    join_groupby form and kw its keyword arguments."""
+    import torch
+
+    from . import ops
+    q = SSB_QUERIES[name]
+    cols = [dcols[c] for c in q["cols"]]
+    if q["kind"] == "filter":
+        return dict(kind="filter", cols=cols, filters=q["filters"], agg_a=3, agg_b=1)
+    tables, probes = [], []
+    for col, dim, payload, filt, ranges in q["probes"]:
+        key_col, length = _dim(dim)
+        to = lambda k: torch.from_numpy(t[k]).to(device)  # noqa: E731
+        ht = ops.build_pht(to(key_col), length, vals=None if payload is None else to(payload),
+                           filt=None if filt is None else to(filt), ranges=ranges)
+        tables.append(ht)
+        probes.append((col, ht, length, 0, 1 if payload is None else 2))
+    kw = dict(agg_col=q["agg"], keys=q["keys"], group_sub=q["sub"], n_groups=q["groups"], res_stride=q["stride"],
+              sum_slot=q["sum_slot"], sum_bits=q["sum_bits"], agg_sub_col=-1 if q["agg_sub"] is None else q["agg_sub"])
+    return dict(kind="join", cols=cols, tables=tables, probes=probes, kw=kw)

@@ -162,18 +162,26 @@ def jit_last_log() -> str:
     return (lib().fls_jit_last_log() or b"").decode(errors="replace")
 
 
-def build_pht(keys, ht_len: int, vals=None, filt=None, filter_eq: int = 1, keys_min: int = 0, out=None):
+def build_pht(keys, ht_len: int, vals=None, filt=None, filter_eq: int = 1, keys_min: int = 0, out=None,
+              ranges=None):
     """Selective perfect-hash table on device int32 columns: PHT_1 (vals None,
-    ht_len slots) or PHT_2 (2*ht_len slots)."""
+    ht_len slots) or PHT_2 (2*ht_len slots).  Rows with filt == filter_eq, or,
+    with ranges=[(lo, hi)] (one or two inclusive ranges), rows whose filt lies
+    in one of them."""
     import torch
     size = ht_len if vals is None else 2 * ht_len
     if out is None:
         out = torch.zeros(size, dtype=torch.int32, device=keys.device)
     else:
         out.zero_()
-    check(lib().fls_pht_build(0 if filt is None else filt.data_ptr(), filter_eq, keys.data_ptr(),
-                              0 if vals is None else vals.data_ptr(), keys.numel(), out.data_ptr(), ht_len,
-                              keys_min, _stream()), "fls_pht_build")
+    if ranges is None:
+        ranges = [(filter_eq, filter_eq)]
+    if not 1 <= len(ranges) <= 2:
+        raise ValueError("one or two filter ranges")
+    (lo0, hi0), (lo1, hi1) = ranges[0], ranges[1] if len(ranges) == 2 else (1, 0)
+    check(lib().fls_pht_build_ranges(0 if filt is None else filt.data_ptr(), lo0, hi0, lo1, hi1, keys.data_ptr(),
+                                     0 if vals is None else vals.data_ptr(), keys.numel(), out.data_ptr(), ht_len,
+                                     keys_min, _stream()), "fls_pht_build_ranges")
     return out
 
 
@@ -225,7 +233,8 @@ def _join_desc(arr, n_cols: int, probes, agg_col, key_a, key_b, group_mul, group
     return d, arr
 
 
-def _groupby_desc(arr, n_cols: int, probes, agg_col, keys, group_sub, n_groups, res_stride, sum_slot, agg_sub_col):
+def _groupby_desc(arr, n_cols: int, probes, agg_col, keys, group_sub, n_groups, res_stride, sum_slot, agg_sub_col,
+                  sum_bits=64):
     if len(probes) > MAX_PROBES or not 1 <= len(keys) <= MAX_GROUP_KEYS:
         raise ValueError("1..4 probes and 1..3 group keys")
     d = JoinGroupbyDesc()
@@ -241,19 +250,21 @@ def _groupby_desc(arr, n_cols: int, probes, agg_col, keys, group_sub, n_groups, 
     for k, (probe, mul, slot) in enumerate(keys):
         d.key_probe[k], d.key_mul[k], d.key_slot[k] = probe, mul, slot
     d.group_sub, d.n_groups, d.res_stride, d.sum_slot = group_sub, n_groups, res_stride, sum_slot
+    d.sum_bits = sum_bits
     return d, arr
 
 
 def join_groupby(cols, probes, agg_col: int, keys, group_sub: int, n_groups: int, res_stride: int, sum_slot: int,
-                 agg_sub_col: int = -1, out=None, workspace="auto"):
+                 agg_sub_col: int = -1, out=None, workspace="auto", sum_bits: int = 64):
     """The general probe + group-by (fls_q21/q31/q41.cu probe_v1): probes
     [(col, ht, ht_len, keys_min, kind)]; keys [(probe, multiplier, record word
     or -1)]; group = (sum of payload * multiplier - group_sub) % n_groups;
     records of res_stride int32 words with the int64 sum of cols[agg_col]
-    (minus cols[agg_sub_col]) at word sum_slot.  Returns the device int32 array."""
+    (minus cols[agg_sub_col]) at word sum_slot (sum_bits 32: a wrapping int32
+    sum in that one word).  Returns the device int32 array."""
     import torch
     d, _keep = _groupby_desc(columns_array(cols), len(cols), probes, agg_col, keys, group_sub, n_groups, res_stride,
-                             sum_slot, agg_sub_col)
+                             sum_slot, agg_sub_col, sum_bits)
     if out is None:
         out = torch.empty(res_stride * n_groups, dtype=torch.int32, device=cols[0].data.device)
     n_ws = int(lib().fls_join_workspace_bytes(ctypes.byref(d))) if workspace is not None else 0
@@ -264,23 +275,23 @@ def join_groupby(cols, probes, agg_col: int, keys, group_sub: int, n_groups: int
 
 
 def jit_precompile_join(col_descs, probes, agg_col, keys, group_sub, n_groups, res_stride, sum_slot,
-                        agg_sub_col: int = -1) -> None:
+                        agg_sub_col: int = -1, sum_bits: int = 64) -> None:
     """Compiles the specialised join + group-by kernel for this query shape."""
     descs = [c.desc if hasattr(c, "desc") else c for c in col_descs]
     arr = (Column * len(descs))(*descs)
     d, _keep = _groupby_desc(arr, len(descs), probes, agg_col, keys, group_sub, n_groups, res_stride, sum_slot,
-                             agg_sub_col)
+                             agg_sub_col, sum_bits)
     check(lib().fls_jit_precompile_join(ctypes.byref(d)), "fls_jit_precompile_join")
 
 
 def join_workspace_bytes(col_descs, probes, agg_col, keys, group_sub, n_groups, res_stride, sum_slot,
-                         agg_sub_col: int = -1) -> int:
+                         agg_sub_col: int = -1, sum_bits: int = 64) -> int:
     """Bytes of device workspace join_groupby can use for this query (0: none);
     needs no GPU."""
     descs = [c.desc if hasattr(c, "desc") else c for c in col_descs]
     arr = (Column * len(descs))(*descs)
     d, _keep = _groupby_desc(arr, len(descs), probes, agg_col, keys, group_sub, n_groups, res_stride, sum_slot,
-                             agg_sub_col)
+                             agg_sub_col, sum_bits)
     return int(lib().fls_join_workspace_bytes(ctypes.byref(d)))
 
 

@@ -208,6 +208,14 @@ fls_status fls_query_filter_agg(const fls_filter_agg_desc* desc, int64_t* d_resu
  * be zeroed by the caller (fls_q21.cu:293-297). */
 fls_status fls_pht_build(const int32_t* d_filter, int32_t filter_eq, const int32_t* d_keys, const int32_t* d_vals,
                          uint64_t n, int32_t* d_ht, int32_t ht_len, int32_t keys_min, fls_stream_t stream);
+/* The same build with the dimension predicates of the other SSB queries
+ * (crystal-opt/pred.cuh BlockPredEQ/GTE/AndLTE/OrEQ as used by the builds of
+ * crystal-opt src/ssb/q22.cu:147-154, q33.cu:102-109, q42.cu:162-171): rows
+ * with lo0 <= d_filter[i] <= hi0 or lo1 <= d_filter[i] <= hi1 (an empty range,
+ * lo > hi, selects nothing; d_filter == NULL selects every row). */
+fls_status fls_pht_build_ranges(const int32_t* d_filter, int32_t lo0, int32_t hi0, int32_t lo1, int32_t hi1,
+                                const int32_t* d_keys, const int32_t* d_vals, uint64_t n, int32_t* d_ht,
+                                int32_t ht_len, int32_t keys_min, fls_stream_t stream);
 
 typedef struct fls_probe {
 	uint32_t       col;      /* probed foreign-key column                        */
@@ -246,8 +254,10 @@ fls_status fls_query_probe_groupby(const fls_join_agg_desc* desc, int32_t* d_res
  * Q2.1 keys (brand x7, year x1), sub 1992, stride 4, slots (1, 0), sum 2;
  * Q3.1 keys (s_nation x175, c_nation x7, year x1), 4375 groups, stride 6,
  * slots (2, 1, 0), sum 4; Q4.1 keys (c_nation x7, year x1), 175 groups,
- * stride 4, slots (1, 0), sum 2, measure revenue - supplycost.  d_res
- * (device, n_groups * res_stride int32, 8-byte aligned) is zeroed by the call. */
+ * stride 4, slots (1, 0), sum 2, measure revenue - supplycost.  sum_bits 32
+ * keeps a wrapping int32 sum in word sum_slot instead (crystal-opt
+ * src/ssb/q32.cu:95-101, q33, q34: stride 4, sum word 3).  d_res (device,
+ * n_groups * res_stride int32, 8-byte aligned) is zeroed by the call. */
 #define FLS_MAX_GROUP_KEYS 3
 typedef struct fls_join_groupby_desc {
 	const fls_column* cols;
@@ -262,6 +272,7 @@ typedef struct fls_join_groupby_desc {
 	int32_t           key_slot[FLS_MAX_GROUP_KEYS];
 	int32_t           group_sub, n_groups;
 	uint32_t          res_stride, sum_slot;
+	uint32_t          sum_bits; /* 64 (or 0): int64 at words sum_slot, +1; 32: int32 at word sum_slot */
 } fls_join_groupby_desc;
 
 fls_status fls_query_join_groupby(const fls_join_groupby_desc* desc, int32_t* d_res, fls_stream_t stream);

@@ -466,6 +466,65 @@ static void add_i64(int32_t* p, int64_t x) {
 	memcpy(p, &acc, 8);
 }
 
+void orc_pht_build_ranges(const int32_t* filter, int32_t lo0, int32_t hi0, int32_t lo1, int32_t hi1,
+                          const int32_t* keys, const int32_t* vals, uint64_t n, int32_t* ht, int32_t len,
+                          int32_t keys_min) {
+	/* crystal-opt src/ssb/q22.cu:118-154 (BlockPredGTE/AndLTE), q33.cu:100-109
+	 * (BlockPredEQ/OrEQ) followed by join.cuh's selective builds. */
+	for (uint64_t t = 0; t < n; ++t) {
+		int32_t h;
+		if (filter && !((filter[t] >= lo0 && filter[t] <= hi0) || (filter[t] >= lo1 && filter[t] <= hi1))) {
+			continue;
+		}
+		if (!pht_hash(keys[t], len, keys_min, &h)) { continue; }
+		if (!vals) {
+			if (ht[h] == 0) { ht[h] = keys[t]; }
+		} else {
+			if (ht[2 * h] == 0) { ht[2 * h] = keys[t]; }
+			ht[2 * h + 1] = vals[t];
+		}
+	}
+}
+
+void orc_join_groupby(uint64_t n, const orc_probe* probes, uint32_t n_probes, const int32_t* agg,
+                      const int32_t* agg_sub, uint32_t n_keys, const int32_t* key_probe, const int32_t* key_mul,
+                      const int32_t* key_slot, int32_t group_sub, int32_t n_groups, uint32_t stride,
+                      uint32_t sum_slot, uint32_t sum_bits, int32_t* res) {
+	/* crystal-opt src/ssb/q32.cu:70-104 and q42.cu:70-116 are this loop with
+	 * their probes, key formulas and records: each probe drops the row on a
+	 * miss (PHT_1: slot == 0; PHT_2: the (key, value) pair read as one u64 is
+	 * 0) or keeps the PHT_2 payload; the selected row writes its key payloads
+	 * into its record and adds its measure to the record's sum. */
+	for (uint64_t t = 0; t < n; ++t) {
+		int32_t  pay[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+		int      keep   = 1;
+		uint32_t key    = 0u - (uint32_t)group_sub;
+		for (uint32_t q = 0; q < n_probes && keep; ++q) {
+			const orc_probe* p = &probes[q];
+			if (p->kind == 1) {
+				int32_t h;
+				keep = pht_hash(p->col[t], p->len, p->keys_min, &h) && p->ht[h] != 0;
+			} else {
+				keep = pht2_get(p->ht, p->len, p->keys_min, p->col[t], &pay[q]);
+			}
+		}
+		if (!keep) { continue; }
+		for (uint32_t k = 0; k < n_keys; ++k) { key += (uint32_t)pay[key_probe[k]] * (uint32_t)key_mul[k]; }
+		const int32_t g = (int32_t)key % n_groups;
+		if (g < 0) { continue; }
+		int32_t* rec = res + (int64_t)g * stride;
+		for (uint32_t k = 0; k < n_keys; ++k) {
+			if (key_slot[k] >= 0) { rec[key_slot[k]] = pay[key_probe[k]]; }
+		}
+		const int32_t m = (int32_t)((uint32_t)agg[t] - (agg_sub ? (uint32_t)agg_sub[t] : 0u));
+		if (sum_bits == 32) {
+			rec[sum_slot] = (int32_t)((uint32_t)rec[sum_slot] + (uint32_t)m);
+		} else {
+			add_i64(&rec[sum_slot], (int64_t)m);
+		}
+	}
+}
+
 void orc_q31_groupby(const int32_t* supp, const int32_t* cust, const int32_t* date, const int32_t* rev, uint64_t n,
                      const int32_t* ht_s, int32_t s_len, const int32_t* ht_c, int32_t c_len, const int32_t* ht_d,
                      int32_t d_len, int32_t d_keys_min, int32_t* res) {

@@ -98,6 +98,29 @@ void orc_probe_groupby(const int32_t* supp, const int32_t* part, const int32_t* 
                        const int32_t* ht_s, int32_t s_len, const int32_t* ht_p, int32_t p_len, const int32_t* ht_d,
                        int32_t d_len, int32_t d_keys_min, int32_t* res);
 
+/* Dimension predicates of the crystal-opt SSB builds (pred.cuh BlockPredEQ,
+ * GTE/AndLTE, OrEQ): rows whose filter value lies in [lo0, hi0] or
+ * [lo1, hi1] (filter NULL: every row); vals NULL builds a PHT_1. */
+void orc_pht_build_ranges(const int32_t* filter, int32_t lo0, int32_t hi0, int32_t lo1, int32_t hi1,
+                          const int32_t* keys, const int32_t* vals, uint64_t n, int32_t* ht, int32_t len,
+                          int32_t keys_min);
+
+/* The join + group-by loop every SSB join query of crystal-opt src/ssb
+ * (q21-q43.cu) and fastlanes src/ssb (fls_q21/q31/q41.cu) instantiates,
+ * over decoded columns: probes in order, group = (sum of PHT_2 payloads x
+ * multipliers - group_sub) % n_groups in wrapping 32-bit arithmetic, key words
+ * and a sum per record (sum_bits 64: int64 at words sum_slot..+1; 32: wrapping
+ * int32 at word sum_slot), measure agg or agg - agg_sub. */
+typedef struct orc_probe {
+	const int32_t* col;
+	const int32_t* ht;
+	int32_t        len, keys_min, kind; /* kind 1: PHT_1, 2: PHT_2 */
+} orc_probe;
+void orc_join_groupby(uint64_t n, const orc_probe* probes, uint32_t n_probes, const int32_t* agg,
+                      const int32_t* agg_sub, uint32_t n_keys, const int32_t* key_probe, const int32_t* key_mul,
+                      const int32_t* key_slot, int32_t group_sub, int32_t n_groups, uint32_t stride,
+                      uint32_t sum_slot, uint32_t sum_bits, int32_t* res);
+
 /* ---- learned selector MLP, double precision (the gradient checker) ------- */
 /* Parameter layout W1[64][16], b1[64], W2[64][64], b2[64], W3[5][64], b3[5];
  * ReLU hidden layers, mean softmax cross-entropy over the batch.  Writes the

@@ -40,6 +40,11 @@ def build(with_reference: bool = True) -> None:
     subprocess.run(["make", "-s", "-C", HERE, target], check=True)
 
 
+class OrcProbe(ctypes.Structure):
+    _fields_ = [("col", _i32p), ("ht", _i32p), ("len", ctypes.c_int32), ("keys_min", ctypes.c_int32),
+                ("kind", ctypes.c_int32)]
+
+
 class OrcVec(ctypes.Structure):
     _fields_ = [("scheme", ctypes.c_uint32), ("bw", ctypes.c_uint32), ("aux", ctypes.c_uint32),
                 ("n_words", ctypes.c_uint32), ("base", ctypes.c_int32)]
@@ -67,6 +72,11 @@ class Oracle:
                                       + [ctypes.c_int32, _i32p])
         L.orc_q41_groupby.argtypes = ([_i32p] * 6 + [ctypes.c_uint64] + [_i32p, ctypes.c_int32] * 4
                                       + [ctypes.c_int32, _i32p])
+        L.orc_pht_build_ranges.argtypes = ([_i32p] + [ctypes.c_int32] * 4 + [_i32p, _i32p, ctypes.c_uint64, _i32p]
+                                           + [ctypes.c_int32] * 2)
+        L.orc_join_groupby.argtypes = [ctypes.c_uint64, ctypes.POINTER(OrcProbe), ctypes.c_uint32, _i32p, _i32p,
+                                       ctypes.c_uint32, _i32p, _i32p, _i32p, ctypes.c_int32, ctypes.c_int32,
+                                       ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _i32p]
 
     # -- layout / packing -------------------------------------------------
     def tpos(self) -> np.ndarray:
@@ -213,6 +223,52 @@ class Oracle:
                                _p(ht_s, _i32p), ht_s.size, _p(ht_c, _i32p), ht_c.size // 2,
                                _p(ht_p, _i32p), ht_p.size, _p(ht_d, _i32p), ht_d.size // 2, d_keys_min,
                                _p(res, _i32p))
+        return res
+
+
+    @staticmethod
+    def filter_agg_ranges(cols, filters, agg_a: int, agg_b: int) -> int:
+        """crystal-opt src/ssb/q12.cu:68-100 (and q11, q13): rows with
+        lo <= cols[c] <= hi for every filter (c, lo, hi), exact int64 sum of
+        cols[agg_a] * cols[agg_b] (numpy integer arithmetic)."""
+        sel = np.ones(np.asarray(cols[0]).size, bool)
+        for c, lo, hi in filters:
+            x = np.asarray(cols[c]).astype(np.int64)
+            sel &= (x >= lo) & (x <= hi)
+        a = np.asarray(cols[agg_a])[sel].astype(np.int64)
+        b = np.asarray(cols[agg_b])[sel].astype(np.int64)
+        return int((a * b).sum())
+
+    def pht_build_ranges(self, filt, ranges, keys, vals, length, keys_min=0):
+        """Selective build of a PHT_1 (vals None) or PHT_2 over rows whose
+        filter value lies in one of one or two inclusive ranges."""
+        ht = np.zeros(length if vals is None else 2 * length, np.int32)
+        keys = np.ascontiguousarray(keys, np.int32)
+        v = None if vals is None else np.ascontiguousarray(vals, np.int32)
+        f = None if filt is None else np.ascontiguousarray(filt, np.int32)
+        (lo0, hi0), (lo1, hi1) = ranges[0], ranges[1] if len(ranges) == 2 else (1, 0)
+        self.L.orc_pht_build_ranges(None if f is None else _p(f, _i32p), lo0, hi0, lo1, hi1, _p(keys, _i32p),
+                                    None if v is None else _p(v, _i32p), keys.size, _p(ht, _i32p), length, keys_min)
+        return ht
+
+    def join_groupby(self, probes, agg, keys, group_sub, n_groups, res_stride, sum_slot, agg_sub=None,
+                     sum_bits=64):
+        """probes: [(fact column, table, table length, keys_min, kind)];
+        keys: [(probe, multiplier, record word or -1)].  Returns the records."""
+        cols = [np.ascontiguousarray(p[0], np.int32) for p in probes]
+        hts = [np.ascontiguousarray(p[1], np.int32) for p in probes]
+        arr = (OrcProbe * len(probes))()
+        for i, (p, c, h) in enumerate(zip(probes, cols, hts)):
+            arr[i] = OrcProbe(_p(c, _i32p), _p(h, _i32p), p[2], p[3], p[4])
+        agg = np.ascontiguousarray(agg, np.int32)
+        sub = None if agg_sub is None else np.ascontiguousarray(agg_sub, np.int32)
+        kp = np.array([k[0] for k in keys], np.int32)
+        km = np.array([k[1] for k in keys], np.int32)
+        ks = np.array([k[2] for k in keys], np.int32)
+        res = np.zeros(res_stride * n_groups, np.int32)
+        self.L.orc_join_groupby(agg.size, arr, len(probes), _p(agg, _i32p), None if sub is None else _p(sub, _i32p),
+                                len(keys), _p(kp, _i32p), _p(km, _i32p), _p(ks, _i32p), group_sub, n_groups,
+                                res_stride, sum_slot, sum_bits, _p(res, _i32p))
         return res
 
 
