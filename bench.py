@@ -38,7 +38,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["q11", "q21", "q31", "q41", "decode", "mixed"], default="q11")
+    ap.add_argument("--workload", choices=["q11", "q21", "q31", "q41", "ssb", "decode", "mixed"], default="q11")
     ap.add_argument("--rows", type=int, default=0, help="rows per GPU (0 = 2^27 for queries, 2^28 for decode)")
     ap.add_argument("--decode-bw", type=int, default=16, help="bit width of the FOR decode workload")
     ap.add_argument("--decode-scheme", choices=["for", "delta", "rle", "dict"], default="for",
@@ -265,6 +265,42 @@ def run_ours(a, dist: Dist):
                         "columns": "supp 17b, cust 18b, part 19b, date 12b, revenue 24b, supplycost 18b",
                         "filters": "supplier region 1/5, customer region 1/5, part manufacturer 2/5"}
         metric_key = a.workload
+    elif a.workload == "ssb":
+        # the thirteen SSB queries over one lineorder table (dimension tables
+        # and hash tables replicated per rank); results side by side in one
+        # int32 buffer, 8-byte aligned per query
+        t = datagen.ssb_tables(a.rows, seed=seed)
+        names = list(datagen.SSB_BITS)
+        hcols = [EncodedColumn.uniform(t[k], bw=datagen.SSB_BITS[k]) for k in names]
+        dcols = [c.to_device(dev) for c in hcols]
+        dmap = dict(zip(names, dcols))
+        suite, off = [], 0
+        for name in datagen.SSB_QUERIES:
+            dq = datagen.ssb_device_query(name, t, dmap, device=dev)
+            words = 2 if dq["kind"] == "filter" else dq["kw"]["res_stride"] * dq["kw"]["n_groups"]
+            suite.append((name, dq, off, words))
+            off += words + (words & 1)
+        del t
+        res = torch.zeros(off, dtype=torch.int32, device=dev)
+        suite_bytes = sum(sum(c.nbytes for c in dq["cols"]) for _, dq, _, _ in suite)
+
+        def run_query(dq, o, w):
+            if dq["kind"] == "filter":
+                ops.query_filter_agg(dq["cols"], dq["filters"], agg_a=3, agg_b=1, out=res[o:o + 2].view(torch.int64))
+            else:
+                ops.join_groupby(dq["cols"], dq["probes"], out=res[o:o + w], **dq["kw"])
+
+        def step():
+            for _, dq, o, w in suite:
+                run_query(dq, o, w)
+            return res
+        workload = {"workload": "SSB suite: Q1.1-Q4.3 (crystal-opt src/ssb q11..q43 shapes) over one lineorder "
+                                "table, 13 fused decode+query launches per step",
+                    "rows_per_gpu": a.rows, "rows_scanned_per_step": 13 * a.rows,
+                    "columns": ", ".join(f"{k[3:]} {b}b" for k, b in datagen.SSB_BITS.items()),
+                    "dimensions": "supplier 2^17, customer 2^18, part 2^19 keys, 2556 days; cities/nations/regions "
+                                  "and brands/categories/manufacturers in dbgen's hierarchy"}
+        metric_key = "ssb"
     else:
         from fastlanesgpu_b200 import LAYOUT_TRANSPOSED, SCHEME_DELTA, SCHEME_RLE
         if a.decode_scheme == "for":
@@ -304,10 +340,30 @@ def run_ours(a, dist: Dist):
         metric_key = f"decode_{a.decode_out}_{key}"
     comp_bytes = sum(c.nbytes for c in hcols)
     algo_bytes = comp_bytes + (out_bytes if a.workload == "decode" else 0)
+    if a.workload == "ssb":
+        algo_bytes = suite_bytes  # every query reads its own columns
 
     def collective():
         # the one exchange of the sharded query: combine the ranks' partial aggregates
         if not dist.pg:
+            return
+        if a.workload == "ssb":
+            for _, dq, o, w in suite:
+                if dq["kind"] == "filter":
+                    allreduce_sum(res[o:o + 2].view(torch.int64))
+                    continue
+                kw = dq["kw"]
+                rec = res[o:o + w].view(-1, kw["res_stride"])
+                sw = 1 if kw["sum_bits"] == 32 else 2
+                is_sum = torch.zeros(kw["res_stride"], dtype=torch.bool)
+                is_sum[kw["sum_slot"]:kw["sum_slot"] + sw] = True
+                keys = rec[:, ~is_sum].contiguous()
+                dist.pg.all_reduce(keys, op=dist.pg.ReduceOp.MAX)
+                rec[:, ~is_sum] = keys
+                sums = rec[:, is_sum].contiguous()
+                sums = sums.view(torch.int64) if sw == 2 else sums
+                allreduce_sum(sums)
+                rec[:, is_sum] = sums.view(torch.int32)
             return
         if a.workload in ("q21", "q31", "q41"):
             # reference layout per group: key words (equal on every rank that
@@ -377,8 +433,24 @@ def run_ours(a, dist: Dist):
     torch.cuda.synchronize()
     e2e_ms = dist.max(x0.elapsed_time(x1)) / n_e2e
     clk = clocks.stop()
+    per_query = None
+    if a.workload == "ssb":
+        # each query alone (outside the timed region), CUDA events, 20 runs
+        per_query = {}
+        for name, dq, o, w in suite:
+            q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            run_query(dq, o, w)
+            q0.record(stream)
+            for _ in range(20):
+                run_query(dq, o, w)
+            q1.record(stream)
+            torch.cuda.synchronize()
+            qb = sum(c.nbytes for c in dq["cols"])
+            qms = q0.elapsed_time(q1) / 20
+            per_query[name] = {"ms": round(qms, 4), "hbm_frac": round(qb / (qms / 1e3) / 1e9 / measured_peak_gbs()[0],
+                                                                       3)}
 
-    rows_total = a.rows * dist.world
+    rows_total = a.rows * dist.world * (13 if a.workload == "ssb" else 1)
     value = rows_total * a.steps / (ms / 1e3)
     ms_step = ms / a.steps
     peak, peak_src = measured_peak_gbs()
@@ -409,6 +481,10 @@ def run_ours(a, dist: Dist):
                               jit_launches=int(ops.jit_stats()["launches"])),
         "clocks": clk,
     }
+    if per_query is not None:
+        out["per_query"] = per_query
+        out["roofline"]["algorithmic_bytes_per_launch"] = algo_bytes
+        out["roofline"]["note"] = "a step is 13 query launches; bytes and time are the whole step's"
     return out, t if a.workload == "q11" else None, hcols
 
 
@@ -671,9 +747,10 @@ def run_reference(a, dist: Dist):
     from fastlanesgpu_b200 import datagen
     R = orc.Reference()
     threads = os.cpu_count() or 1
-    if a.workload == "mixed" or (a.workload == "decode" and a.decode_scheme != "for"):
+    if a.workload in ("mixed", "ssb") or (a.workload == "decode" and a.decode_scheme != "for"):
         return {"impl": "reference", "unavailable": "the reference has no CPU implementation of this workload "
-                "(learned selection, batching, or per-vector DELTA/RLE/DICT columns)"}
+                "(learned selection, batching, per-vector DELTA/RLE/DICT columns, or the SSB queries other "
+                "than its fls_q11/q21/q31/q41 loops)"}
     sample = min(a.rows, 1 << 24)
     if a.workload == "q11":
         t = datagen.lineorder_q11(sample, seed=1000)

@@ -103,3 +103,19 @@ def test_ssb_joins_full_size(both_paths, oracle, query):
         got = ops.join_groupby(dcols, probes, **kw).cpu().numpy()
         ops.check_device_error()
         assert np.array_equal(got, want), (query, jit)
+
+
+def test_ssb_suite_full_size(cuda, oracle):
+    """All thirteen SSB queries over one 2^27-row lineorder table against the
+    oracle (specialised kernels)."""
+    from test_gpu_ssb_suite import ssb_run, ssb_want
+    n = 1 << 27
+    t = datagen.ssb_tables(n, seed=2727)
+    dcols = {k: EncodedColumn.uniform(t[k], bw=b).to_device() for k, b in datagen.SSB_BITS.items()}
+    for name in datagen.SSB_QUERIES:
+        want, _ = ssb_want(oracle, name, t)
+        got, _ = ssb_run(name, t, dcols)
+        if isinstance(want, int):
+            assert got == want, name
+        else:
+            assert np.array_equal(got, want), name
