@@ -212,7 +212,7 @@ def run_ours(a, dist: Dist):
         ops.set_tuning(0, a.sparse_rows)
     ops.set_tuning(1, a.jit)
     ops.set_tuning(2, a.group_smem)
-    from fastlanesgpu_b200.shard import allreduce_sum, shard_seed
+    from fastlanesgpu_b200.shard import allreduce_sum, combine_group_records, shard_seed
     seed = shard_seed(1000, dist.rank)
     # ---------------------------------------------------------------- setup
     if a.workload == "q11":
@@ -351,33 +351,12 @@ def run_ours(a, dist: Dist):
             for _, dq, o, w in suite:
                 if dq["kind"] == "filter":
                     allreduce_sum(res[o:o + 2].view(torch.int64))
-                    continue
-                kw = dq["kw"]
-                rec = res[o:o + w].view(-1, kw["res_stride"])
-                sw = 1 if kw["sum_bits"] == 32 else 2
-                is_sum = torch.zeros(kw["res_stride"], dtype=torch.bool)
-                is_sum[kw["sum_slot"]:kw["sum_slot"] + sw] = True
-                keys = rec[:, ~is_sum].contiguous()
-                dist.pg.all_reduce(keys, op=dist.pg.ReduceOp.MAX)
-                rec[:, ~is_sum] = keys
-                sums = rec[:, is_sum].contiguous()
-                sums = sums.view(torch.int64) if sw == 2 else sums
-                allreduce_sum(sums)
-                rec[:, is_sum] = sums.view(torch.int32)
-            return
-        if a.workload in ("q21", "q31", "q41"):
-            # reference layout per group: key words (equal on every rank that
-            # saw the group, 0 elsewhere) + a uint64 sum
+                else:
+                    kw = dq["kw"]
+                    combine_group_records(res[o:o + w], kw["res_stride"], kw["sum_slot"], kw["sum_bits"])
+        elif a.workload in ("q21", "q31", "q41"):
             stride, sum_slot = (4, 2) if a.workload == "q21" else (jkw["res_stride"], jkw["sum_slot"])
-            r64 = res.view(torch.int64).view(-1, stride // 2)
-            sc = sum_slot // 2
-            keys = torch.cat([r64[:, :sc], r64[:, sc + 1:]], dim=1).contiguous()
-            sums = r64[:, sc].contiguous()
-            dist.pg.all_reduce(keys, op=dist.pg.ReduceOp.MAX)
-            allreduce_sum(sums)
-            r64[:, :sc].copy_(keys[:, :sc])
-            r64[:, sc + 1:].copy_(keys[:, sc:])
-            r64[:, sc].copy_(sums)
+            combine_group_records(res, stride, sum_slot)
         else:
             allreduce_sum(res)
 

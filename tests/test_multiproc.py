@@ -71,3 +71,71 @@ def test_gloo_two_ranks_allreduce_partials(oracle):
     want = oracle.filter_agg(t["date"], t["discount"], t["quantity"], t["price"], *f["date"], *f["discount"],
                              f["quantity"][1] + 1)
     assert got[0] == got[1] == want
+
+
+def _ssb_records(oracle, name, t, r0, r1):
+    """The oracle's records of SSB join query `name` over rows [r0, r1)."""
+    from fastlanesgpu_b200 import datagen
+    q = datagen.SSB_QUERIES[name]
+    keys = {"d": "d_datekey", "s": "s_suppkey", "c": "c_custkey", "p": "p_partkey"}
+    cols = [t[c][r0:r1] for c in q["cols"]]
+    probes = []
+    for col, dim, payload, filt, ranges in q["probes"]:
+        k = t[keys[dim]]
+        ht = oracle.pht_build_ranges(None if filt is None else t[filt], ranges or [(0, -1)], k,
+                                     None if payload is None else t[payload], k.size)
+        probes.append((cols[col], ht, k.size, 0, 1 if payload is None else 2))
+    return oracle.join_groupby(probes, cols[q["agg"]], q["keys"], q["sub"], q["groups"], q["stride"],
+                               q["sum_slot"], agg_sub=None if q["agg_sub"] is None else cols[q["agg_sub"]],
+                               sum_bits=q["sum_bits"])
+
+
+def _records_worker(rank, world, port, n, names, q):
+    import sys
+    import torch
+    import torch.distributed as dist
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, here)
+    sys.path.insert(0, os.path.join(here, "oracle"))
+    import datetime
+    import oracle as orc
+    from fastlanesgpu_b200 import datagen
+    from fastlanesgpu_b200.shard import combine_group_records, vector_range
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        t = datagen.ssb_tables(n, seed=9)
+        r0, r1 = vector_range(n, world, rank)
+        out = {}
+        for name in names:
+            spec = datagen.SSB_QUERIES[name]
+            res = torch.from_numpy(_ssb_records(orc.Oracle(), name, t, r0, r1))
+            combine_group_records(res, spec["stride"], spec["sum_slot"], spec["sum_bits"])
+            out[name] = res.numpy()
+        q.put((rank, out))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_two_ranks_combine_group_records(oracle):
+    """Row shards of SSB join queries with int64 sums (Q4.2: 6-word records)
+    and wrapping int32 sums (Q3.2, Q4.3) combine into the single-process
+    records."""
+    import multiprocessing as mp
+    from fastlanesgpu_b200 import datagen
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    n, names = 400_000, ["q32", "q42", "q43"]
+    port = _free_port()
+    ps = [ctx.Process(target=_records_worker, args=(r, 2, port, n, names, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    got = dict(q.get(timeout=300) for _ in range(2))
+    for p in ps:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    t = datagen.ssb_tables(n, seed=9)
+    for name in names:
+        want = _ssb_records(oracle, name, t, 0, n)
+        assert (want != 0).any()
+        assert np.array_equal(got[0][name], want) and np.array_equal(got[1][name], want), name
