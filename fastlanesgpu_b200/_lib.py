@@ -149,6 +149,10 @@ _SIGS = {
     "fls_encode_gpu_workspace_bytes": (ctypes.c_uint64, [ctypes.c_uint64]),
     "fls_encode_column_gpu": (ctypes.c_int, [_VP, ctypes.c_uint64, _VP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
                                              _VP, ctypes.c_uint64, _VP, _VP, _VP, ctypes.c_uint64, _VP]),
+    "fls_encode_learned_workspace_bytes": (ctypes.c_uint64, [ctypes.c_uint64]),
+    "fls_encode_learned_gpu": (ctypes.c_int, [_VP, ctypes.c_uint64, _VP, ctypes.c_float, ctypes.c_double,
+                                              ctypes.c_uint32, _VP, ctypes.c_uint64, _VP, _VP, _VP, _VP,
+                                              ctypes.c_uint64, _VP]),
     "fls_get_jit_stats": (ctypes.c_int, [ctypes.POINTER(JitStats)]),
     "fls_jit_last_log": (ctypes.c_char_p, []),
     "fls_jit_precompile": (ctypes.c_int, [ctypes.POINTER(FilterAggDesc)]),

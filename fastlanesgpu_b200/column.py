@@ -187,6 +187,34 @@ def encode_column_gpu(values, schemes=0, layout: int = LAYOUT_TRANSPOSED, round4
     return DeviceEncodedColumn(out, meta, n, layout, total, mx, mask)
 
 
+def encode_column_learned_gpu(values, params, threshold: float = 0.9, kappa: float = 0.0,
+                              layout: int = LAYOUT_TRANSPOSED, compact: bool = True):
+    """The learned encoder in one device call (fls_encode_learned_gpu): the MLP
+    with `params` (device float32, FLS_MLP_N_PARAMS) picks each vector's scheme,
+    the exhaustive choice replaces picks whose confidence is below
+    `threshold`, and the column is encoded on the GPU.  Returns
+    (DeviceEncodedColumn, per-vector schemes, number of fallback vectors)."""
+    import torch
+    n = int(values.numel())
+    nv = n_vectors(n)
+    dev = values.device
+    bound = int(lib().fls_encode_bound_words(n))
+    out = torch.empty(bound + 4, dtype=torch.int32, device=dev)
+    meta = torch.empty(nv * 4, dtype=torch.int32, device=dev)
+    info = torch.zeros(4, dtype=torch.int64, device=dev)
+    schemes = torch.empty(nv, dtype=torch.uint8, device=dev)
+    ws_bytes = int(lib().fls_encode_learned_workspace_bytes(n))
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    check(lib().fls_encode_learned_gpu(values.data_ptr(), n, params.data_ptr(), threshold, kappa, layout,
+                                       out.data_ptr(), bound + 4, meta.data_ptr(), info.data_ptr(), schemes.data_ptr(),
+                                       ws.data_ptr(), ws_bytes, torch.cuda.current_stream().cuda_stream),
+          "fls_encode_learned_gpu")
+    total, mx, mask, n_fb = (int(x) for x in info.cpu())
+    if compact:
+        out = out[:max(total, 4)].clone()
+    return DeviceEncodedColumn(out, meta, n, layout, total, mx, mask), schemes, n_fb
+
+
 def columns_array(cols) -> ctypes.Array:
     arr = (Column * len(cols))()
     for i, c in enumerate(cols):
@@ -194,6 +222,7 @@ def columns_array(cols) -> ctypes.Array:
     return arr
 
 
-__all__ = ["EncodedColumn", "DeviceColumn", "DeviceEncodedColumn", "encode_column_gpu", "META_DTYPE", "columns_array",
+__all__ = ["EncodedColumn", "DeviceColumn", "DeviceEncodedColumn", "encode_column_gpu", "encode_column_learned_gpu",
+           "META_DTYPE", "columns_array",
            "n_vectors", "_lib",
            "SCHEME_DELTA", "LAYOUT_TRANSPOSED"]

@@ -267,6 +267,87 @@ __global__ void __launch_bounds__(kEncWarps * 32) enc_plan_kernel(const __grid_c
 	}
 }
 
+// ------------------------------------------------ learned selection
+
+struct SelParams {
+	const int32_t*      values;
+	uint64_t            n, n_vec;
+	const uint8_t*      mlp_best; // the network's pick per vector
+	const float*        conf;     // and its probability
+	float               threshold;
+	uint32_t            pad_;
+	double              kappa;
+	uint8_t*            schemes;  // the chosen scheme per vector
+	unsigned long long* n_fallback;
+};
+
+// The exhaustive choice for vectors the network is unsure of (confidence
+// below threshold), else the network's pick.  The exact encoded sizes of
+// every scheme (payload + 16 B metadata) are the host exhaustive encoder's
+// (fls_host.cpp scheme_sizes), the choice the label rule of the learned
+// selector: argmin of size x (1 + kappa (decode cost - 1)) with the decode
+// costs FOR 1, DELTA 1.5, RLE 2, CONST 1, DICT 4.5, ties to the cheaper
+// decode (FOR, CONST, DELTA, RLE, DICT), in IEEE double with each product and
+// sum rounded separately (no fused multiply-add), as numpy computes it.
+__global__ void __launch_bounds__(kEncWarps * 32) enc_select_kernel(const __grid_constant__ SelParams S) {
+	extern __shared__ __align__(16) int32_t esmem[];
+	const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+	int32_t*       sv   = esmem + warp * kEncWarpWords;
+	int32_t *      a = sv + kValWords, *u = a + 1024;
+	EncParams      P {};
+	P.values = S.values;
+	P.n      = S.n;
+	for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * kEncWarps + warp; v < S.n_vec;
+	     v += static_cast<uint64_t>(gridDim.x) * kEncWarps) {
+		if (!(S.conf[v] < S.threshold)) {
+			if (lane == 0) { S.schemes[v] = S.mlp_best[v]; }
+			continue;
+		}
+		int32_t mn, mx;
+		stage_vector(P, v, sv, lane, mn, mx);
+		const uint32_t rbw = bits_of(static_cast<uint32_t>(mx) - static_cast<uint32_t>(mn));
+		uint32_t       mxd = 0;
+		{
+			const uint32_t c    = dev::chunk_of_lane(lane);
+			int32_t        prev = val_at(sv, 32u * c);
+			for (uint32_t t = 1; t < 32; ++t) {
+				const int32_t cur = val_at(sv, 32u * c + t);
+				mxd               = max(mxd, static_cast<uint32_t>(cur) - static_cast<uint32_t>(prev));
+				prev              = cur;
+			}
+		}
+		const uint32_t dbw    = bits_of(__reduce_max_sync(0xffffffffu, mxd));
+		const uint32_t n_runs = __reduce_add_sync(0xffffffffu, __popc(chunk_starts(sv, lane)));
+		const uint32_t n_dist = distinct_sorted(sv, a, u, lane);
+		if (lane == 0) {
+			uint32_t size[FLS_N_SCHEMES];
+			size[FLS_SCHEME_FOR]   = 16u + 4u * payload_words(FLS_SCHEME_FOR, rbw, 0u);
+			size[FLS_SCHEME_DELTA] = 16u + 4u * payload_words(FLS_SCHEME_DELTA, dbw, 0u);
+			size[FLS_SCHEME_RLE]   = 16u + 4u * payload_words(FLS_SCHEME_RLE, rbw, n_runs);
+			size[FLS_SCHEME_CONST] = mn == mx ? 16u : 0xffffffffu;
+			size[FLS_SCHEME_DICT]  = 16u + 4u * payload_words(FLS_SCHEME_DICT, rbw, n_dist);
+			const uint32_t order[FLS_N_SCHEMES] = {FLS_SCHEME_FOR, FLS_SCHEME_CONST, FLS_SCHEME_DELTA, FLS_SCHEME_RLE,
+			                                       FLS_SCHEME_DICT};
+			const double cost[FLS_N_SCHEMES] = {1.0, 1.5, 2.0, 1.0, 4.5}; // by scheme id
+			uint32_t     best = order[0];
+			double       best_score = 0.0;
+			for (uint32_t i = 0; i < FLS_N_SCHEMES; ++i) {
+				const uint32_t sc = order[i];
+				if (size[sc] == 0xffffffffu) { continue; }
+				const double f     = __dadd_rn(1.0, __dmul_rn(S.kappa, cost[sc] - 1.0));
+				const double score = __dmul_rn(static_cast<double>(size[sc]), f);
+				if (i == 0 || score < best_score) {
+					best       = sc;
+					best_score = score;
+				}
+			}
+			S.schemes[v] = static_cast<uint8_t>(best);
+			atomicAdd(S.n_fallback, 1ull);
+		}
+		__syncwarp();
+	}
+}
+
 // Exclusive scan of the payload words of one block of kScanBlock vectors
 // (blockDim = 256, 4 vectors per thread).  Returns the block total; with
 // `write` the offsets (plus `carry`) go into the metadata.
@@ -502,6 +583,78 @@ fls_status fls_encode_column_gpu(const int32_t* d_values, uint64_t n, const uint
 	enc_write_kernel<<<grid, kEncWarps * 32, smem, st>>>(P);
 	count_launch(5);
 	return cuda_check(cudaGetLastError(), "encode kernels launch");
+}
+
+uint64_t fls_encode_learned_workspace_bytes(uint64_t n) {
+	const uint64_t n_vec = (n + 1023u) / 1024u;
+	auto           a256  = [](uint64_t b) { return (b + 255u) & ~uint64_t {255u}; };
+	return a256(64u * n_vec) + a256(4u * n_vec) + 2u * a256(n_vec) + fls_encode_gpu_workspace_bytes(n);
+}
+
+fls_status fls_encode_learned_gpu(const int32_t* d_values, uint64_t n, const float* d_params, float threshold,
+                                  double kappa, uint32_t layout, uint32_t* d_out, uint64_t out_capacity_words,
+                                  fls_vec_meta* d_meta, uint64_t* d_info, uint8_t* d_schemes, void* d_workspace,
+                                  uint64_t workspace_bytes, fls_stream_t stream) {
+	if (!d_values || !d_params || !d_info || !d_workspace || n == 0) {
+		return set_error(FLS_ERR_INVALID_ARG, "fls_encode_learned_gpu: null pointer or n == 0");
+	}
+	if (!(kappa >= 0.0)) { return set_error(FLS_ERR_INVALID_ARG, "fls_encode_learned_gpu: kappa must be >= 0"); }
+	if (workspace_bytes < fls_encode_learned_workspace_bytes(n) || (reinterpret_cast<uintptr_t>(d_workspace) & 255u)) {
+		return set_error(FLS_ERR_CAPACITY,
+		                 "fls_encode_learned_gpu: workspace smaller than fls_encode_learned_workspace_bytes(n) "
+		                 "or not 256-byte aligned");
+	}
+	const uint64_t n_vec = (n + 1023u) / 1024u;
+	auto           a256  = [](uint64_t b) { return (b + 255u) & ~uint64_t {255u}; };
+	char*          w     = static_cast<char*>(d_workspace);
+	float*         stats = reinterpret_cast<float*>(w);
+	float*         conf  = reinterpret_cast<float*>(w + a256(64u * n_vec));
+	uint8_t*       best  = reinterpret_cast<uint8_t*>(w + a256(64u * n_vec) + a256(4u * n_vec));
+	uint8_t*       own   = best + a256(n_vec);
+	void*          enc   = own + a256(n_vec);
+	uint8_t*       pick  = d_schemes ? d_schemes : own;
+	cudaStream_t   st    = reinterpret_cast<cudaStream_t>(stream);
+	DeviceInfo     di;
+	fls_status     s = device_info(di);
+	if (s != FLS_OK) { return s; }
+	if ((s = fls_vector_stats_gpu(d_values, n, stats, stream)) != FLS_OK) { return s; }
+	if ((s = fls_mlp_infer(d_params, stats, n_vec, nullptr, best, conf, stream)) != FLS_OK) { return s; }
+	const size_t smem = 4u * kEncWarps * kEncWarpWords;
+	{
+		static std::mutex mu;
+		static uint64_t   configured = 0;
+		int               dev        = 0;
+		cudaGetDevice(&dev);
+		std::lock_guard<std::mutex> lk(mu);
+		if (dev >= 64 || !(configured & (1ull << dev))) {
+			if ((s = cuda_check(cudaFuncSetAttribute(enc_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			                                         static_cast<int>(smem)),
+			                    "cudaFuncSetAttribute")) != FLS_OK) {
+				return s;
+			}
+			if (dev < 64) { configured |= 1ull << dev; }
+		}
+	}
+	if ((s = cuda_check(cudaMemsetAsync(d_info + 3, 0, sizeof(uint64_t), st), "cudaMemsetAsync")) != FLS_OK) {
+		return s;
+	}
+	SelParams S {};
+	S.values     = d_values;
+	S.n          = n;
+	S.n_vec      = n_vec;
+	S.mlp_best   = best;
+	S.conf       = conf;
+	S.threshold  = threshold;
+	S.kappa      = kappa;
+	S.schemes    = pick;
+	S.n_fallback = reinterpret_cast<unsigned long long*>(d_info + 3);
+	const uint32_t grid = static_cast<uint32_t>(
+	    std::min<uint64_t>((n_vec + kEncWarps - 1) / kEncWarps, static_cast<uint64_t>(di.sms) * 8u));
+	enc_select_kernel<<<grid, kEncWarps * 32, smem, st>>>(S);
+	count_launch(1);
+	if ((s = cuda_check(cudaGetLastError(), "enc_select_kernel launch")) != FLS_OK) { return s; }
+	return fls_encode_column_gpu(d_values, n, pick, 0u, layout, 0, d_out, out_capacity_words, d_meta, d_info, enc,
+	                             fls_encode_gpu_workspace_bytes(n), stream);
 }
 
 } // extern "C"

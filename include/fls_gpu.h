@@ -371,6 +371,24 @@ fls_status fls_mlp_adam_step(float* d_params, const float* d_grads, float* d_m, 
 fls_status fls_mlp_infer(const float* d_params, const float* d_x, uint64_t n, float* d_probs, uint8_t* d_best,
                          float* d_conf, fls_stream_t stream);
 
+/* The learned encoder in one call, entirely on the device (no reference
+ * counterpart): the statistics of fls_vector_stats_gpu, the network's picks
+ * (fls_mlp_infer with d_params), and for each vector whose confidence is below
+ * `threshold` the exhaustive choice computed on the device -- the exact sizes
+ * of fls_encode_exhaustive under the selector's label rule, argmin of
+ * size x (1 + kappa (decode cost - 1)), costs FOR 1, DELTA 1.5, RLE 2,
+ * CONST 1, DICT 4.5, ties to the cheaper decode -- then the column encoded by
+ * fls_encode_column_gpu with those per-vector schemes (no FOR rounding).
+ * d_info (device uint64[4]): fls_encode_column_gpu's three values and the
+ * number of vectors that fell back to the exhaustive choice.  d_schemes
+ * (optional, device, one per vector) receives the choices.  d_workspace:
+ * fls_encode_learned_workspace_bytes(n) bytes, 256-byte aligned. */
+uint64_t   fls_encode_learned_workspace_bytes(uint64_t n);
+fls_status fls_encode_learned_gpu(const int32_t* d_values, uint64_t n, const float* d_params, float threshold,
+                                  double kappa, uint32_t layout, uint32_t* d_out, uint64_t out_capacity_words,
+                                  fls_vec_meta* d_meta, uint64_t* d_info, uint8_t* d_schemes, void* d_workspace,
+                                  uint64_t workspace_bytes, fls_stream_t stream);
+
 /* ------------------------------------- reference-shaped kernels (device) */
 
 /* fastlanes/src/ssb/fls_q11.cu:29-81 QueryKernel_v1, written against the

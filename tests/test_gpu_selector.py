@@ -79,3 +79,48 @@ def test_learned_encoding_is_lossless(trained):
     col = EncodedColumn.encode(vals, schemes)
     out = ops.unpack_global(col.to_device(), ORDER_ORIGINAL).cpu().numpy()
     assert np.array_equal(out, vals)
+
+
+@pytest.mark.parametrize("kappa", [0.0, 0.03])
+def test_device_exhaustive_choice_equals_host(cuda, kappa):
+    """fls_encode_learned_gpu with every vector below the confidence
+    threshold: the device's exhaustive choice equals the host exhaustive
+    encoder's sizes under the selector's label rule, on a ragged column of every
+    family (constant vectors included), and the column decodes losslessly."""
+    import torch
+    from fastlanesgpu_b200.column import encode_column_learned_gpu
+    from fastlanesgpu_b200.selector import decode_aware_labels
+    vals = training_corpus(3000, seed=31)[: 3000 * 1024 - 333]
+    sizes, _ = ops.encode_exhaustive(vals)
+    want = decode_aware_labels(sizes, kappa)
+    assert {0, 1, 2, 4} <= set(want.tolist())  # constant vectors tie FOR at 16 B and take FOR
+    params = LearnedSelector(seed=3).params
+    col, schemes, n_fb = encode_column_learned_gpu(torch.from_numpy(vals).cuda(), params, threshold=2.0, kappa=kappa)
+    ops.check_device_error()
+    assert n_fb == want.size
+    assert np.array_equal(schemes.cpu().numpy(), want)
+    out = ops.unpack_global(col, ORDER_ORIGINAL).cpu().numpy()[: vals.size]
+    assert np.array_equal(out, vals)
+
+
+def test_device_learned_encoder_equals_select_device(trained):
+    """The one-call device encoder gives the same schemes and the same encoded
+    column as the selector's device path (network picks, host exhaustive
+    fallback) followed by the GPU encoder; threshold 0 keeps every pick."""
+    import torch
+    from fastlanesgpu_b200.column import encode_column_gpu, encode_column_learned_gpu
+    sel, _ = trained
+    vals = training_corpus(1500, seed=77)[: 1500 * 1024 - 5]
+    dv = torch.from_numpy(vals).cuda()
+    want, info = sel.select_device(dv, vals, threshold=0.9, kappa=0.03)
+    col, schemes, n_fb = encode_column_learned_gpu(dv, sel.params, threshold=0.9, kappa=0.03)
+    ops.check_device_error()
+    assert n_fb == info["fallback_vectors"] > 0
+    assert torch.equal(schemes, want)
+    ref = encode_column_gpu(dv, want)
+    assert col.payload_words == ref.payload_words
+    assert torch.equal(col.data[: col.payload_words], ref.data[: ref.payload_words])
+    assert torch.equal(col.meta, ref.meta)
+    picks, _ = sel.predict(gpu_features(dv))
+    _, schemes0, n0 = encode_column_learned_gpu(dv, sel.params, threshold=0.0)
+    assert n0 == 0 and torch.equal(schemes0, picks)
