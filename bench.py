@@ -514,7 +514,7 @@ def run_mixed(a, dist: Dist):
 
     from fastlanesgpu_b200 import LAYOUT_TRANSPOSED, ORDER_ORIGINAL, EncodedColumn, datagen, ops
     from fastlanesgpu_b200.batch import Batch, graph_of
-    from fastlanesgpu_b200.column import encode_column_gpu
+    from fastlanesgpu_b200.column import encode_column_gpu, encode_column_learned_gpu
     from fastlanesgpu_b200.selector import LearnedSelector, corpus_device, decode_aware_labels, gpu_features
     dev = torch.device("cuda", dist.local)
     stream = torch.cuda.current_stream()
@@ -584,6 +584,25 @@ def run_mixed(a, dist: Dist):
               for i in range(len(cols))]
     torch.cuda.synchronize()
     ex_gpu_encode_s = time.perf_counter() - t0 + ln_upload_s
+    # the whole learned encoder as one device call per column
+    # (fls_encode_learned_gpu: statistics, MLP, exhaustive choice on the device
+    # for low-confidence vectors, encode), and the same call with every vector
+    # sent to the device's exhaustive choice
+    def one_call(threshold):
+        torch.cuda.synchronize()
+        t0_ = time.perf_counter()
+        out_ = [encode_column_learned_gpu(cat_dev[vstart[i] * 1024: vstart[i] * 1024 + lens[i]], sel.params,
+                                          threshold=threshold, kappa=a.decode_kappa, layout=LAYOUT_TRANSPOSED)
+                for i in range(len(cols))]
+        torch.cuda.synchronize()
+        return out_, time.perf_counter() - t0_
+    one_call(a.threshold)  # first use of the select kernel on this device
+    ln1, ln1_s = one_call(a.threshold)
+    exd, exd_s = one_call(2.0)
+    one_call_same = bool(torch.equal(torch.cat([sc for _, sc, _ in ln1]), schemes_dev))
+    size_ln1 = sum(c.nbytes for c, _, _ in ln1)
+    size_exd = sum(c.nbytes for c, _, _ in exd)
+    del ln1, exd
     size_ex = sum(c.nbytes for c in enc_ex)
     size_ex_gpu = sum(c.nbytes for c in ex_gpu)
     size_ln = sum(c.nbytes for c in dcols)
@@ -696,6 +715,10 @@ def run_mixed(a, dist: Dist):
                         "total_s": ln_upload_s + ln_select_s + ln_encode_s,
                         "parts_s": {k: v for k, v in info.items() if k.endswith("_s")}},
             "exhaustive_select_then_gpu_encode_s": ex_select_s + ex_gpu_encode_s,
+            "device_one_call": {"where": "fls_encode_learned_gpu per column, columns already on the GPU",
+                                "learned_s": ln1_s, "bytes_learned": size_ln1,
+                                "same_schemes_as_select_device": one_call_same,
+                                "exhaustive_on_device_s": exd_s, "bytes_exhaustive_on_device": size_exd},
             "encode_speedup": (ex_select_s + ex_encode_s) / (ln_upload_s + ln_select_s + ln_encode_s),
             "select_speedup": ex_select_s / (ln_upload_s + ln_select_s),
             "fallback_vectors": info["fallback_vectors"], "vectors": info["vectors"], "threshold": a.threshold,
