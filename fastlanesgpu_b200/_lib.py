@@ -149,6 +149,9 @@ _SIGS = {
     "fls_encode_gpu_workspace_bytes": (ctypes.c_uint64, [ctypes.c_uint64]),
     "fls_encode_column_gpu": (ctypes.c_int, [_VP, ctypes.c_uint64, _VP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
                                              _VP, ctypes.c_uint64, _VP, _VP, _VP, ctypes.c_uint64, _VP]),
+    "fls_column_container_bytes": (ctypes.c_uint64, [ctypes.POINTER(Column)]),
+    "fls_column_write_container": (ctypes.c_int, [ctypes.POINTER(Column), _VP, ctypes.c_uint64, _VP]),
+    "fls_column_open_container": (ctypes.c_int, [_VP, ctypes.c_uint64, ctypes.POINTER(Column)]),
     "fls_encode_learned_workspace_bytes": (ctypes.c_uint64, [ctypes.c_uint64]),
     "fls_encode_learned_gpu": (ctypes.c_int, [_VP, ctypes.c_uint64, _VP, ctypes.c_float, ctypes.c_double,
                                               ctypes.c_uint32, _VP, ctypes.c_uint64, _VP, _VP, _VP, _VP,

@@ -96,6 +96,45 @@ class EncodedColumn:
     def to_device(self, device=None) -> "DeviceColumn":
         return DeviceColumn(self, device)
 
+    # -- container (fls_column_write_container / fls_column_open_container) --
+    def to_bytes(self) -> bytes:
+        """The column as an encoded-column container (payload, metadata and a
+        checksummed footer)."""
+        words = np.ascontiguousarray(self.words, dtype=np.uint32)
+        meta = None if self.meta is None else np.ascontiguousarray(self.meta)
+        d = Column(data=words.ctypes.data, meta=0 if meta is None else meta.ctypes.data, n_values=self.n_values,
+                   n_words=int(words.size), layout=self.layout, scheme=self.scheme, bw=self.bw, base=self.base,
+                   max_vec_words=self.max_vec_words, scheme_mask=self.scheme_mask)
+        n = int(lib().fls_column_container_bytes(ctypes.byref(d)))
+        out = _aligned16(n)
+        check(lib().fls_column_write_container(ctypes.byref(d), out.ctypes.data, n, None), "fls_column_write_container")
+        return out.tobytes()
+
+    @classmethod
+    def from_bytes(cls, b) -> "EncodedColumn":
+        """A column from an encoded-column container; damaged or foreign bytes
+        raise FlsError (checked by the library before anything is read)."""
+        buf = _aligned16(len(b))
+        buf[:] = np.frombuffer(b, dtype=np.uint8)
+        d = Column()
+        check(lib().fls_column_open_container(buf.ctypes.data, buf.size, ctypes.byref(d)), "fls_column_open_container")
+        words = buf[: 4 * d.n_words].view(np.uint32).copy()
+        meta = None
+        if d.meta:
+            off = int(d.meta) - buf.ctypes.data
+            meta = buf[off: off + 16 * n_vectors(d.n_values)].view(META_DTYPE).copy()
+        return cls(words=words, meta=meta, n_values=int(d.n_values), layout=int(d.layout), scheme=int(d.scheme),
+                   bw=int(d.bw), base=int(d.base), max_vec_words=int(d.max_vec_words), scheme_mask=int(d.scheme_mask))
+
+    def save(self, path: str) -> None:
+        with open(path, "wb") as f:
+            f.write(self.to_bytes())
+
+    @classmethod
+    def load(cls, path: str) -> "EncodedColumn":
+        with open(path, "rb") as f:
+            return cls.from_bytes(f.read())
+
 
 class DeviceColumn:
     """An EncodedColumn resident in device memory, with its C descriptor."""
@@ -213,6 +252,13 @@ def encode_column_learned_gpu(values, params, threshold: float = 0.9, kappa: flo
     if compact:
         out = out[:max(total, 4)].clone()
     return DeviceEncodedColumn(out, meta, n, layout, total, mx, mask), schemes, n_fb
+
+
+def _aligned16(n: int) -> np.ndarray:
+    """A uint8 array of n bytes starting on a 16-byte boundary."""
+    raw = np.zeros(n + 16, dtype=np.uint8)
+    off = (-raw.ctypes.data) % 16
+    return raw[off: off + n]
 
 
 def columns_array(cols) -> ctypes.Array:

@@ -150,6 +150,21 @@ fls_status fls_encode_column_gpu(const int32_t* d_values, uint64_t n, const uint
                                  fls_vec_meta* d_meta, uint64_t* d_info, void* d_workspace, uint64_t workspace_bytes,
                                  fls_stream_t stream);
 
+/* Encoded-column container: the payload words and per-vector metadata of a
+ * column with HOST pointers (data, meta) in one byte string --
+ * [payload][zero pad to 16 B][metadata][80-byte footer: descriptor, CRC-32C
+ * of payload and metadata, version, magic "FLSCOLv1"] -- so encoded columns
+ * can be stored and read back without re-encoding.  The reference keeps raw
+ * int32 columns on disk (crystal_ssb_utils.h:108-127 storeColumn /
+ * loadColumn) and re-encodes them each run (compress_ssb.cu:357-454).
+ * fls_column_open_container checks the footer, both checksums and every
+ * vector's metadata against the payload (FLS_ERR_INVALID_ARG if damaged,
+ * FLS_ERR_UNSUPPORTED for another version) and fills `col` with pointers into
+ * `buf` (16-byte aligned); copy data and meta to the device to query it. */
+uint64_t   fls_column_container_bytes(const fls_column* col);
+fls_status fls_column_write_container(const fls_column* col, void* out, uint64_t out_bytes, uint64_t* written);
+fls_status fls_column_open_container(const void* buf, uint64_t bytes, fls_column* col);
+
 /* Exhaustive per-vector encoder (the selector's judge): exact encoded size in
  * bytes (payload + 16 B metadata) of every scheme for every vector
  * (sizes: n_vec*5, UINT32_MAX = not representable) and the argmin scheme, ties

@@ -77,3 +77,25 @@ def test_gpu_encoder_bad_scheme_is_flagged(cuda):
     host = EncodedColumn.encode(vals, 0, layout=LAYOUT_TRANSPOSED)
     got = dcol.to_host()
     assert np.array_equal(got.words[:host.payload_words], host.words[:host.payload_words])
+
+
+def test_container_columns_decode_on_gpu(cuda, tmp_path):
+    """Columns written to an encoded-column container and read back (host
+    encoder through a file; GPU encoder through bytes) decode to the original
+    values on the GPU."""
+    import torch
+    from fastlanesgpu_b200.column import encode_column_gpu
+    from fastlanesgpu_b200.selector import training_corpus
+    vals = training_corpus(300, seed=21)[: 300 * 1024 - 17]
+    _, best = ops.encode_exhaustive(vals)
+    col = EncodedColumn.encode(vals, best, layout=LAYOUT_TRANSPOSED)
+    p = tmp_path / "col.flsc"
+    col.save(str(p))
+    back = EncodedColumn.load(str(p))
+    out = ops.unpack_global(back.to_device(), ORDER_ORIGINAL).cpu().numpy()[: vals.size]
+    assert np.array_equal(out, vals)
+    g = encode_column_gpu(torch.from_numpy(vals).cuda(), torch.from_numpy(best).cuda()).to_host()
+    g2 = EncodedColumn.from_bytes(g.to_bytes())
+    want = int(vals.view(np.uint32).astype(np.uint64).sum())
+    assert int(ops.query_aggregate(g2.to_device()).cpu()[0]) & 0xFFFFFFFFFFFFFFFF == want
+    ops.check_device_error()
