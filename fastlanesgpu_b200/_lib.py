@@ -149,6 +149,16 @@ _SIGS = {
     "fls_encode_gpu_workspace_bytes": (ctypes.c_uint64, [ctypes.c_uint64]),
     "fls_encode_column_gpu": (ctypes.c_int, [_VP, ctypes.c_uint64, _VP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
                                              _VP, ctypes.c_uint64, _VP, _VP, _VP, ctypes.c_uint64, _VP]),
+    "fls_pack_u8": (ctypes.c_int, [_VP, _VP, ctypes.c_uint8]),
+    "fls_pack_u16": (ctypes.c_int, [_VP, _VP, ctypes.c_uint8]),
+    "fls_pack_u64": (ctypes.c_int, [_VP, _VP, ctypes.c_uint8]),
+    "fls_unpack_u8": (ctypes.c_int, [_VP, _VP, ctypes.c_uint8]),
+    "fls_unpack_u16": (ctypes.c_int, [_VP, _VP, ctypes.c_uint8]),
+    "fls_unpack_u64": (ctypes.c_int, [_VP, _VP, ctypes.c_uint8]),
+    "fls_pack_column": (ctypes.c_int, [_VP, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint8, ctypes.c_uint64, _VP]),
+    "fls_decode_u8": (ctypes.c_int, [_VP, ctypes.c_uint64, ctypes.c_uint8, ctypes.c_uint8, _VP, _VP, _VP]),
+    "fls_decode_u16": (ctypes.c_int, [_VP, ctypes.c_uint64, ctypes.c_uint8, ctypes.c_uint16, _VP, _VP, _VP]),
+    "fls_decode_u64": (ctypes.c_int, [_VP, ctypes.c_uint64, ctypes.c_uint8, ctypes.c_uint64, _VP, _VP, _VP]),
     "fls_column_container_bytes": (ctypes.c_uint64, [ctypes.POINTER(Column)]),
     "fls_column_write_container": (ctypes.c_int, [ctypes.POINTER(Column), _VP, ctypes.c_uint64, _VP]),
     "fls_column_open_container": (ctypes.c_int, [_VP, ctypes.c_uint64, ctypes.POINTER(Column)]),

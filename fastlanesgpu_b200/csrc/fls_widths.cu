@@ -1,0 +1,191 @@
+// fls_widths.cu -- GPU decode of FastLanes columns of 8-, 16- and 64-bit
+// lanes (FOR with one base and bit width per column), to HBM and/or fused
+// with a sum.  The reference decodes only 32-bit lanes on the GPU
+// (fls_gen/unpack/unpack.cuh); its host packer covers all four widths
+// (fastlanes/src/pack.cpp:29521, 29552, 29607, 29710), whose layout this
+// reads: 1024/T lanes, row r of lane i is value (1024/T)*r + i, word k of
+// lane i at (1024/T)*k + i, 128-byte rows, 128*bw bytes per vector.
+//
+// 8/16-bit lanes: one warp per vector; thread t reads the 32-bit word t of
+// each 128-byte row, which holds 32/T consecutive lanes, and extracts row r
+// of all of them at once (SIMD within a register: every lane of a word has
+// the same bit offset r*bw, so one shift and a per-lane mask serve all; the
+// base is added lane-wise without carries between lanes).  64-bit lanes: a
+// half-warp per vector, one lane per thread.  Both read and write 128-byte
+// rows per instruction.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "fls_pipeline.cuh"
+
+namespace fls {
+namespace {
+
+template <int B>
+struct Narrow {
+	static constexpr uint32_t kRep  = B == 8 ? 0x01010101u : 0x00010001u; // one per lane of a word
+	static constexpr uint32_t kLow  = (1u << B) - 1u;
+	static constexpr uint32_t kHigh = (1u << (B - 1)) * kRep; // lane top bits
+};
+
+// Lane-wise sum of the 32/B lanes of x.
+template <int B>
+__device__ __forceinline__ uint32_t lane_sum(uint32_t x) {
+	if constexpr (B == 8) {
+		const uint32_t t = (x & 0x00ff00ffu) + ((x >> 8) & 0x00ff00ffu);
+		return (t & 0xffffu) + (t >> 16);
+	} else {
+		return (x & 0xffffu) + (x >> 16);
+	}
+}
+
+template <int B>
+__global__ void __launch_bounds__(256) decode_narrow_kernel(const uint32_t* __restrict in, uint64_t n, uint64_t n_vec,
+                                                            uint32_t bw, uint32_t base_rep, uint32_t* __restrict out,
+                                                            unsigned long long* sum) {
+	using N                = Narrow<B>;
+	constexpr uint32_t L   = 32u / B;    // lanes per thread word
+	constexpr uint32_t S   = 1024u / B;  // lanes per vector
+	const uint32_t     t   = threadIdx.x & 31u;
+	const uint64_t     w0  = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t     nw  = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+	const uint32_t     vm  = (bw >= static_cast<uint32_t>(B) ? N::kLow : (1u << bw) - 1u) * N::kRep;
+	unsigned long long acc = 0;
+	for (uint64_t v = w0; v < n_vec; v += nw) {
+		const uint32_t* src  = in + v * 32u * bw;
+		uint32_t*       dst  = out ? out + v * 32u * B : nullptr;
+		const uint64_t  rem  = n - v * 1024u; // values of this vector inside the column
+		uint32_t        part = 0;
+#pragma unroll
+		for (uint32_t r = 0; r < static_cast<uint32_t>(B); ++r) {
+			const uint32_t o = r * bw, k = o / B, s = o % B;
+			uint32_t       x = 0;
+			if (bw) {
+				x = (__ldg(src + 32u * k + t) >> s) & ((N::kLow >> s) * N::kRep);
+				if (s + bw > static_cast<uint32_t>(B)) {
+					x |= (__ldg(src + 32u * (k + 1u) + t) << (B - s)) & (((N::kLow << (B - s)) & N::kLow) * N::kRep);
+				}
+				x &= vm;
+			}
+			const uint32_t y = ((x & ~N::kHigh) + (base_rep & ~N::kHigh)) ^ ((x ^ base_rep) & N::kHigh);
+			if (dst) { __stcs(dst + 32u * r + t, y); }
+			if (sum) {
+				uint32_t keep = y;
+				if (rem < 1024u) { // the column's last, partial vector
+					keep = 0;
+#pragma unroll
+					for (uint32_t j = 0; j < L; ++j) {
+						if (S * r + L * t + j < rem) { keep |= y & (N::kLow << (B * j)); }
+					}
+				}
+				part += lane_sum<B>(keep);
+			}
+		}
+		acc += part;
+	}
+	if (sum) {
+#pragma unroll
+		for (int off = 16; off > 0; off >>= 1) { acc += __shfl_xor_sync(0xffffffffu, acc, off); }
+		if (t == 0 && acc) { atomicAdd(sum, acc); }
+	}
+}
+
+__global__ void __launch_bounds__(256) decode_u64_kernel(const uint64_t* __restrict in, uint64_t n, uint64_t n_vec,
+                                                         uint32_t bw, uint64_t base, uint64_t* __restrict out,
+                                                         unsigned long long* sum) {
+	const uint32_t     i   = threadIdx.x & 15u; // lane of the vector
+	const uint64_t     h0  = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 4;
+	const uint64_t     nh  = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 4;
+	const uint64_t     m   = bw >= 64 ? ~0ull : (1ull << bw) - 1ull;
+	unsigned long long acc = 0;
+	// every half-warp runs the same number of iterations, so full-warp
+	// shuffles at the end see every lane
+	const uint64_t iters = (n_vec + nh - 1) / nh;
+	for (uint64_t it = 0; it < iters; ++it) {
+		const uint64_t v = h0 + it * nh;
+		if (v >= n_vec) { continue; }
+		const uint64_t* src = in + v * 16u * bw;
+		const uint64_t  rem = n - v * 1024u;
+#pragma unroll 8
+		for (uint32_t r = 0; r < 64; ++r) {
+			const uint32_t o = r * bw, k = o >> 6, s = o & 63u;
+			uint64_t       x = 0;
+			if (bw) {
+				x = __ldg(reinterpret_cast<const unsigned long long*>(src) + 16u * k + i) >> s;
+				if (s + bw > 64u) { x |= __ldg(reinterpret_cast<const unsigned long long*>(src) + 16u * (k + 1u) + i) << (64u - s); }
+				x &= m;
+			}
+			const uint64_t y = x + base;
+			if (out) { __stcs(reinterpret_cast<unsigned long long*>(out) + v * 1024u + 16u * r + i, y); }
+			if (sum && 16u * r + i < rem) { acc += y; }
+		}
+	}
+	if (sum) {
+#pragma unroll
+		for (int off = 16; off > 0; off >>= 1) { acc += __shfl_xor_sync(0xffffffffu, acc, off); }
+		if ((threadIdx.x & 31u) == 0 && acc) { atomicAdd(sum, acc); }
+	}
+}
+
+fls_status launch_decode(uint32_t bits, const void* d_in, uint64_t n, uint8_t bw, uint64_t base, void* d_out,
+                         uint64_t* d_sum, fls_stream_t stream, const char* who) {
+	if (!d_in || n == 0 || (!d_out && !d_sum)) {
+		return set_error(FLS_ERR_INVALID_ARG, std::string(who) + ": null pointer, n == 0 or no output");
+	}
+	if (bw > bits) { return set_error(FLS_ERR_BAD_BW, std::string(who) + ": bit width larger than the values"); }
+	if ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) & 15u) {
+		return set_error(FLS_ERR_ALIGNMENT, std::string(who) + ": buffers must be 16-byte aligned");
+	}
+	DeviceInfo di;
+	fls_status s = device_info(di);
+	if (s != FLS_OK) { return s; }
+	cudaStream_t   st    = reinterpret_cast<cudaStream_t>(stream);
+	const uint64_t n_vec = (n + 1023u) / 1024u;
+	if (d_sum && (s = cuda_check(cudaMemsetAsync(d_sum, 0, sizeof(uint64_t), st), "cudaMemsetAsync")) != FLS_OK) {
+		return s;
+	}
+	auto* sum = reinterpret_cast<unsigned long long*>(d_sum);
+	if (bits == 64) {
+		const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>((n_vec + 15u) / 16u, static_cast<uint64_t>(di.sms) * 16u));
+		decode_u64_kernel<<<grid, 256, 0, st>>>(static_cast<const uint64_t*>(d_in), n, n_vec, bw, base,
+		                                         static_cast<uint64_t*>(d_out), sum);
+	} else {
+		const uint32_t rep  = bits == 8 ? static_cast<uint32_t>(base & 0xffu) * 0x01010101u
+		                                : static_cast<uint32_t>(base & 0xffffu) * 0x00010001u;
+		const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>((n_vec + 7u) / 8u, static_cast<uint64_t>(di.sms) * 16u));
+		if (bits == 8) {
+			decode_narrow_kernel<8><<<grid, 256, 0, st>>>(static_cast<const uint32_t*>(d_in), n, n_vec, bw, rep,
+			                                              static_cast<uint32_t*>(d_out), sum);
+		} else {
+			decode_narrow_kernel<16><<<grid, 256, 0, st>>>(static_cast<const uint32_t*>(d_in), n, n_vec, bw, rep,
+			                                               static_cast<uint32_t*>(d_out), sum);
+		}
+	}
+	count_launch();
+	return cuda_check(cudaGetLastError(), "decode kernel launch");
+}
+
+} // namespace
+} // namespace fls
+
+using namespace fls;
+
+extern "C" {
+
+fls_status fls_decode_u8(const uint8_t* d_in, uint64_t n, uint8_t bw, uint8_t base, uint8_t* d_out, uint64_t* d_sum,
+                         fls_stream_t stream) {
+	return launch_decode(8, d_in, n, bw, base, d_out, d_sum, stream, "fls_decode_u8");
+}
+
+fls_status fls_decode_u16(const uint16_t* d_in, uint64_t n, uint8_t bw, uint16_t base, uint16_t* d_out,
+                          uint64_t* d_sum, fls_stream_t stream) {
+	return launch_decode(16, d_in, n, bw, base, d_out, d_sum, stream, "fls_decode_u16");
+}
+
+fls_status fls_decode_u64(const uint64_t* d_in, uint64_t n, uint8_t bw, uint64_t base, uint64_t* d_out,
+                          uint64_t* d_sum, fls_stream_t stream) {
+	return launch_decode(64, d_in, n, bw, base, d_out, d_sum, stream, "fls_decode_u64");
+}
+
+} // extern "C"

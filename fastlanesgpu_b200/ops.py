@@ -362,3 +362,59 @@ def get_tuning(param: int) -> int:
 
 def kernel_launch_count() -> int:
     return int(lib().fls_kernel_launch_count())
+
+
+# ------------------------------------------------- 8/16/64-bit lane widths
+
+_WIDTH_DTYPES = {8: np.uint8, 16: np.uint16, 32: np.uint32, 64: np.uint64}
+
+
+def pack_vector(values: np.ndarray, bw: int) -> np.ndarray:
+    """FastLanes packing of one vector of 1024 uint8/uint16/uint64 values
+    (fls_pack_u8/u16/u64): (1024/T)*bw words of the values' type."""
+    v = np.ascontiguousarray(values)
+    bits = v.dtype.itemsize * 8
+    assert v.size == 1024 and bits in (8, 16, 64)
+    out = np.zeros(1024 // bits * bw + 1, dtype=v.dtype)
+    check(getattr(lib(), f"fls_pack_u{bits}")(v.ctypes.data, out.ctypes.data, bw), f"fls_pack_u{bits}")
+    return out[: 1024 // bits * bw]
+
+
+def unpack_vector(packed: np.ndarray, bw: int) -> np.ndarray:
+    p = np.ascontiguousarray(packed)
+    bits = p.dtype.itemsize * 8
+    src = np.concatenate([p, np.zeros(1, p.dtype)])
+    out = np.zeros(1024, dtype=p.dtype)
+    check(getattr(lib(), f"fls_unpack_u{bits}")(src.ctypes.data, out.ctypes.data, bw), f"fls_unpack_u{bits}")
+    return out
+
+
+def pack_column_width(values: np.ndarray, bw: int, base: int = 0) -> np.ndarray:
+    """A column of uint8/uint16/uint32/uint64 values minus `base`, packed
+    vector after vector (fls_pack_column); returns the packed words."""
+    v = np.ascontiguousarray(values)
+    bits = v.dtype.itemsize * 8
+    n_vec = (v.size + 1023) // 1024
+    out = np.zeros(n_vec * 1024 // bits * bw + 16 // v.dtype.itemsize, dtype=v.dtype)
+    check(lib().fls_pack_column(v.ctypes.data, v.size, bits, bw, base & ((1 << bits) - 1), out.ctypes.data),
+          "fls_pack_column")
+    return out
+
+
+def decode_width(packed, n: int, bits: int, bw: int, base: int = 0, out=None, want_sum: bool = True):
+    """GPU decode of a packed 8/16/64-bit column (fls_decode_u8/u16/u64):
+    packed is a 16-byte aligned device tensor of the packed bytes.  Returns
+    (decoded values tensor of the width's torch dtype or None, uint64 sum as
+    a Python int or None)."""
+    import torch
+    n_vec = (n + 1023) // 1024
+    tdt = {8: torch.uint8, 16: torch.int16, 64: torch.int64}[bits]
+    if out is None:
+        out = torch.empty(n_vec * 1024, dtype=tdt, device=packed.device)
+    s = torch.zeros(1, dtype=torch.int64, device=packed.device) if want_sum else None
+    check(getattr(lib(), f"fls_decode_u{bits}")(packed.data_ptr(), n, bw, base & ((1 << bits) - 1),
+                                               None if out is False else out.data_ptr(),
+                                               None if s is None else s.data_ptr(), _stream()),
+          f"fls_decode_u{bits}")
+    total = None if s is None else int(s.cpu()[0]) & 0xFFFFFFFFFFFFFFFF
+    return (None if out is False else out), total

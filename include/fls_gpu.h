@@ -150,6 +150,35 @@ fls_status fls_encode_column_gpu(const int32_t* d_values, uint64_t n, const uint
                                  fls_vec_meta* d_meta, uint64_t* d_info, void* d_workspace, uint64_t workspace_bytes,
                                  fls_stream_t stream);
 
+/* FastLanes packing of the other lane widths: 1024 values of T bits in
+ * 1024/T lanes, row r of lane i = value (1024/T)*r + i, masked to bw bits,
+ * LSB-first, word k of lane i at out[(1024/T)*k + i]; every width has
+ * 128-byte rows (128*bw bytes per vector).  fastlanes/src/pack.cpp:29521 (u8),
+ * 29552 (u16), 29710 (u64); the inverses are those declared in
+ * fls_gen/unpack/unpack.hpp:7-10 (the reference has no host body for them). */
+fls_status fls_pack_u8(const uint8_t* in, uint8_t* out, uint8_t bw);
+fls_status fls_pack_u16(const uint16_t* in, uint16_t* out, uint8_t bw);
+fls_status fls_pack_u64(const uint64_t* in, uint64_t* out, uint8_t bw);
+fls_status fls_unpack_u8(const uint8_t* in, uint8_t* out, uint8_t bw);
+fls_status fls_unpack_u16(const uint16_t* in, uint16_t* out, uint8_t bw);
+fls_status fls_unpack_u64(const uint64_t* in, uint64_t* out, uint8_t bw);
+/* A column of n values of value_bits (8, 16, 32, 64) bits, minus `base`
+ * (modulo 2^value_bits), packed vector after vector at bw bits (the last vector
+ * padded with the last value): ceil(n/1024) * 128*bw bytes.  FLS_ERR_BAD_BW if
+ * a value does not fit.  Host memory. */
+fls_status fls_pack_column(const void* in, uint64_t n, uint32_t value_bits, uint8_t bw, uint64_t base, void* out);
+/* GPU decode of such a column (d_in, 16-byte aligned): d_out (optional,
+ * ceil(n/1024)*1024 values of the column's width) receives every vector with
+ * the base added modulo 2^T, *d_sum (optional, device) the uint64 sum of the n
+ * values (modulo 2^64).  The reference decodes 32-bit lanes only on the GPU
+ * (fls_gen/unpack/unpack.cuh); 32-bit columns use fls_decode_u32. */
+fls_status fls_decode_u8(const uint8_t* d_in, uint64_t n, uint8_t bw, uint8_t base, uint8_t* d_out, uint64_t* d_sum,
+                         fls_stream_t stream);
+fls_status fls_decode_u16(const uint16_t* d_in, uint64_t n, uint8_t bw, uint16_t base, uint16_t* d_out,
+                          uint64_t* d_sum, fls_stream_t stream);
+fls_status fls_decode_u64(const uint64_t* d_in, uint64_t n, uint8_t bw, uint64_t base, uint64_t* d_out,
+                          uint64_t* d_sum, fls_stream_t stream);
+
 /* Encoded-column container: the payload words and per-vector metadata of a
  * column with HOST pointers (data, meta) in one byte string --
  * [payload][zero pad to 16 B][metadata][80-byte footer: descriptor, CRC-32C

@@ -691,3 +691,48 @@ uint64_t orc_splitmix64(uint64_t* state) {
 	z          = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
 	return z ^ (z >> 31);
 }
+
+/* FastLanes packing of the other lane widths (pack.cpp:5-1742 8-bit,
+ * the 16-bit block after it, 7280-29520 64-bit; dispatch at 29521, 29552,
+ * 29710): a vector of 1024 T-bit values has S = 1024/T lanes; lane i packs
+ * rows r = 0..T-1 (value S*r + i), masked to bw bits, LSB-first into T-bit
+ * words, word k of lane i at out[S*k + i]. */
+#define ORC_PACK_WIDTH(T, B)                                                                                          \
+	void orc_pack_##B(const T* in, T* out, unsigned bw) {                                                         \
+		const unsigned S = 1024u / (B);                                                                       \
+		const T        m = bw >= (B) ? (T)~(T)0 : (T)((((T)1) << bw) - 1u);                                  \
+		for (unsigned i = 0; i < S; ++i) {                                                                    \
+			unsigned k = 0, fill = 0;                                                                     \
+			T        acc = 0;                                                                             \
+			if (bw == 0) { continue; }                                                                    \
+			for (unsigned r = 0; r < (B); ++r) {                                                          \
+				const T v = (T)(in[S * r + i] & m);                                                   \
+				acc |= (T)(v << fill);                                                                \
+				if (fill + bw >= (B)) {                                                               \
+					out[S * k++ + i] = acc;                                                        \
+					acc  = fill + bw > (B) ? (T)(v >> ((B) - fill)) : (T)0;                        \
+					fill = fill + bw - (B);                                                        \
+				} else {                                                                              \
+					fill += bw;                                                                    \
+				}                                                                                     \
+			}                                                                                             \
+		}                                                                                                     \
+	}                                                                                                             \
+	void orc_unpack_##B(const T* in, T* out, unsigned bw) {                                                       \
+		const unsigned S = 1024u / (B);                                                                       \
+		const T        m = bw >= (B) ? (T)~(T)0 : (T)((((T)1) << bw) - 1u);                                  \
+		for (unsigned i = 0; i < S; ++i) {                                                                    \
+			for (unsigned r = 0; r < (B); ++r) {                                                          \
+				const unsigned bit = r * bw, k = bit / (B), s = bit % (B);                            \
+				T              v   = 0;                                                               \
+				if (bw) {                                                                             \
+					v = (T)(in[S * k + i] >> s);                                                   \
+					if (s + bw > (B)) { v |= (T)(in[S * (k + 1) + i] << ((B) - s)); }              \
+				}                                                                                     \
+				out[S * r + i] = (T)(v & m);                                                          \
+			}                                                                                             \
+		}                                                                                                     \
+	}
+ORC_PACK_WIDTH(uint8_t, 8)
+ORC_PACK_WIDTH(uint16_t, 16)
+ORC_PACK_WIDTH(uint64_t, 64)

@@ -98,6 +98,15 @@ void orc_probe_groupby(const int32_t* supp, const int32_t* part, const int32_t* 
                        const int32_t* ht_s, int32_t s_len, const int32_t* ht_p, int32_t p_len, const int32_t* ht_d,
                        int32_t d_len, int32_t d_keys_min, int32_t* res);
 
+/* FastLanes bit-packing of 8-, 16- and 64-bit lanes (pack.cpp:29521,
+ * 29552, 29710) and its inverse: 1024 values, 1024/T lanes, bw <= T. */
+void orc_pack_8(const uint8_t* in, uint8_t* out, unsigned bw);
+void orc_unpack_8(const uint8_t* in, uint8_t* out, unsigned bw);
+void orc_pack_16(const uint16_t* in, uint16_t* out, unsigned bw);
+void orc_unpack_16(const uint16_t* in, uint16_t* out, unsigned bw);
+void orc_pack_64(const uint64_t* in, uint64_t* out, unsigned bw);
+void orc_unpack_64(const uint64_t* in, uint64_t* out, unsigned bw);
+
 /* Dimension predicates of the crystal-opt SSB builds (pred.cuh BlockPredEQ,
  * GTE/AndLTE, OrEQ): rows whose filter value lies in [lo0, hi0] or
  * [lo1, hi1] (filter NULL: every row); vals NULL builds a PHT_1. */
