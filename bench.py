@@ -41,6 +41,8 @@ def parse_args():
     ap.add_argument("--workload", choices=["q11", "q21", "q31", "q41", "ssb", "decode", "mixed"], default="q11")
     ap.add_argument("--rows", type=int, default=0, help="rows per GPU (0 = 2^27 for queries, 2^28 for decode)")
     ap.add_argument("--decode-bw", type=int, default=16, help="bit width of the FOR decode workload")
+    ap.add_argument("--decode-width", type=int, choices=[8, 16, 32, 64], default=32,
+                    help="decode workload, FOR: value width of the FastLanes lanes (8/16/64: fls_decode_u8/u16/u64)")
     ap.add_argument("--decode-scheme", choices=["for", "delta", "rle", "dict"], default="for",
                     help="decode input: uniform FOR bit-packing, delta over sorted keys (geometric gaps p=0.3), "
                          "RLE (geometric runs of mean 16, values in [0,2^16)), dictionary (Zipf 1.1 over 2^20)")
@@ -303,7 +305,9 @@ def run_ours(a, dist: Dist):
         metric_key = "ssb"
     else:
         from fastlanesgpu_b200 import LAYOUT_TRANSPOSED, SCHEME_DELTA, SCHEME_RLE
-        if a.decode_scheme == "for":
+        if a.decode_scheme == "for" and a.decode_width != 32:
+            vals, hcols = None, []  # built below
+        elif a.decode_scheme == "for":
             vals = datagen.uniform_bits(a.rows, a.decode_bw, seed=seed)
             hcols = [EncodedColumn.uniform(vals, bw=a.decode_bw)]
             what, key = f"bit-pack + FOR, bw {a.decode_bw} (uniform column)", f"for_bw{a.decode_bw}"
@@ -322,7 +326,42 @@ def run_ours(a, dist: Dist):
             what, key = "dictionary, Zipf 1.1 over [0,2^20)", "dict"
         del vals
         dcols = [c.to_device(dev) for c in hcols]
-        if a.decode_out == "sum":
+        if a.decode_scheme == "for" and a.decode_width != 32:
+            # the same decode over lanes of another width: values uniform in
+            # [0, 2^bw), bw capped at the width
+            bits, bw_w = a.decode_width, min(a.decode_bw, a.decode_width)
+            dt = {8: np.uint8, 16: np.uint16, 64: np.uint64}[bits]
+            raw = np.random.default_rng(seed).integers(0, 2**64 - 1, a.rows, dtype=np.uint64, endpoint=True)
+            if bw_w < 64:
+                raw &= np.uint64((1 << bw_w) - 1)
+            packed = ops.pack_column_width(raw.astype(dt), bw_w, 0)
+            del raw
+            n_vec_w = (a.rows + 1023) // 1024
+
+            class _Packed:  # host column for the end-to-end copies
+                words, meta, nbytes = packed.view(np.uint32), None, n_vec_w * 128 * bw_w
+
+            class _DevPacked:
+                data = torch.from_numpy(packed.view(np.int32)).to(dev)
+                n_vec = n_vec_w
+            hcols, dcols = [_Packed], [_DevPacked]
+            tdt = {8: torch.uint8, 16: torch.int16, 64: torch.int64}[bits]
+            if a.decode_out == "sum":
+                res = torch.zeros(1, dtype=torch.int64, device=dev)
+
+                def step():
+                    ops.decode_width_into(_DevPacked.data, a.rows, bits, bw_w, 0, None, res)
+                    return res
+            else:
+                res = torch.empty(n_vec_w * 1024, dtype=tdt, device=dev)
+
+                def step():
+                    ops.decode_width_into(_DevPacked.data, a.rows, bits, bw_w, 0, res, None)
+                    return res
+            out_bytes = (bits // 8) * n_vec_w * 1024 if a.decode_out == "hbm" else 0
+            what = f"bit-pack {bits}-bit lanes, bw {bw_w} (uniform column, fls_decode_u{bits})"
+            key = f"u{bits}_bw{bw_w}"
+        elif a.decode_out == "sum":
             res = torch.zeros(1, dtype=torch.int64, device=dev)
 
             def step():
@@ -334,7 +373,8 @@ def run_ours(a, dist: Dist):
             def step():
                 ops.unpack_global(dcols[0], out=res)
                 return res
-        out_bytes = 4 * dcols[0].n_vec * 1024 if a.decode_out == "hbm" else 0
+        if not (a.decode_scheme == "for" and a.decode_width != 32):
+            out_bytes = 4 * dcols[0].n_vec * 1024 if a.decode_out == "hbm" else 0
         workload = {"workload": f"decode {'to HBM' if a.decode_out == 'hbm' else 'fused with uint64 sum'}: {what}",
                     "rows_per_gpu": a.rows}
         metric_key = f"decode_{a.decode_out}_{key}"
@@ -749,10 +789,11 @@ def run_reference(a, dist: Dist):
     from fastlanesgpu_b200 import datagen
     R = orc.Reference()
     threads = os.cpu_count() or 1
-    if a.workload in ("mixed", "ssb") or (a.workload == "decode" and a.decode_scheme != "for"):
+    if a.workload in ("mixed", "ssb") or (a.workload == "decode" and (a.decode_scheme != "for" or
+                                                                        a.decode_width != 32)):
         return {"impl": "reference", "unavailable": "the reference has no CPU implementation of this workload "
-                "(learned selection, batching, per-vector DELTA/RLE/DICT columns, or the SSB queries other "
-                "than its fls_q11/q21/q31/q41 loops)"}
+                "(learned selection, batching, per-vector DELTA/RLE/DICT columns, 8/16/64-bit lanes (it only "
+                "packs them), or the SSB queries other than its fls_q11/q21/q31/q41 loops)"}
     sample = min(a.rows, 1 << 24)
     if a.workload == "q11":
         t = datagen.lineorder_q11(sample, seed=1000)

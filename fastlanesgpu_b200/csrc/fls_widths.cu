@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "fls_pipeline.cuh"
 
@@ -40,57 +41,84 @@ __device__ __forceinline__ uint32_t lane_sum(uint32_t x) {
 	}
 }
 
-template <int B>
+// One vector of 8/16-bit lanes: row r of the 32/B lanes of thread word t.
+// OUT / SUM: write the values / add them to part; TAIL: the column's last,
+// partial vector (rem values).  Branch-free per row, so the loads of all rows
+// can issue before the first is used.
+template <int B, bool OUT, bool SUM, bool TAIL>
+__device__ __forceinline__ void narrow_vector(const uint32_t* __restrict src, uint32_t* __restrict dst, uint32_t bw,
+                                              uint32_t vm, uint32_t base_rep, uint32_t t, uint64_t rem,
+                                              uint32_t& part) {
+	using N              = Narrow<B>;
+	constexpr uint32_t L = 32u / B;   // lanes per thread word
+	constexpr uint32_t S = 1024u / B; // lanes per vector
+	const uint32_t     last = bw ? bw - 1u : 0u;
+#pragma unroll
+	for (uint32_t r = 0; r < static_cast<uint32_t>(B); ++r) {
+		// the second word row is read unconditionally, clamped inside the vector
+		const uint32_t o = r * bw, k = o / B, s = o % B;
+		const uint32_t lo_word = __ldg(src + 32u * k + t);
+		const uint32_t hi_word = __ldg(src + 32u * min(k + 1u, last) + t);
+		const uint32_t hi      = (hi_word << (B - s)) & (((N::kLow << (B - s)) & N::kLow) * N::kRep);
+		const uint32_t x       = (((lo_word >> s) & ((N::kLow >> s) * N::kRep)) |
+		                    (s + bw > static_cast<uint32_t>(B) ? hi : 0u)) & vm;
+		const uint32_t y = ((x & ~N::kHigh) + (base_rep & ~N::kHigh)) ^ ((x ^ base_rep) & N::kHigh);
+		if constexpr (OUT) { __stcs(dst + 32u * r + t, y); }
+		if constexpr (SUM) {
+			uint32_t keep = y;
+			if constexpr (TAIL) {
+				keep = 0;
+#pragma unroll
+				for (uint32_t j = 0; j < L; ++j) {
+					keep |= (S * r + L * t + j < rem) ? (y & (N::kLow << (B * j))) : 0u;
+				}
+			}
+			part += lane_sum<B>(keep);
+		}
+	}
+}
+
+// 8/16-bit lanes: one warp per vector (a 0-bit column reads no payload).
+template <int B, bool OUT, bool SUM>
 __global__ void __launch_bounds__(256) decode_narrow_kernel(const uint32_t* __restrict in, uint64_t n, uint64_t n_vec,
                                                             uint32_t bw, uint32_t base_rep, uint32_t* __restrict out,
                                                             unsigned long long* sum) {
 	using N                = Narrow<B>;
-	constexpr uint32_t L   = 32u / B;    // lanes per thread word
-	constexpr uint32_t S   = 1024u / B;  // lanes per vector
 	const uint32_t     t   = threadIdx.x & 31u;
-	const uint64_t     w0  = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t     wg  = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
 	const uint64_t     nw  = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
 	const uint32_t     vm  = (bw >= static_cast<uint32_t>(B) ? N::kLow : (1u << bw) - 1u) * N::kRep;
 	unsigned long long acc = 0;
-	for (uint64_t v = w0; v < n_vec; v += nw) {
+	for (uint64_t v = wg; v < n_vec; v += nw) {
 		const uint32_t* src  = in + v * 32u * bw;
-		uint32_t*       dst  = out ? out + v * 32u * B : nullptr;
-		const uint64_t  rem  = n - v * 1024u; // values of this vector inside the column
+		uint32_t*       dst  = OUT ? out + v * 32u * B : nullptr;
+		const uint64_t  rem  = n - v * 1024u;
 		uint32_t        part = 0;
-#pragma unroll
-		for (uint32_t r = 0; r < static_cast<uint32_t>(B); ++r) {
-			const uint32_t o = r * bw, k = o / B, s = o % B;
-			uint32_t       x = 0;
-			if (bw) {
-				x = (__ldg(src + 32u * k + t) >> s) & ((N::kLow >> s) * N::kRep);
-				if (s + bw > static_cast<uint32_t>(B)) {
-					x |= (__ldg(src + 32u * (k + 1u) + t) << (B - s)) & (((N::kLow << (B - s)) & N::kLow) * N::kRep);
-				}
-				x &= vm;
+		if (bw == 0) {
+			// every value is the base
+			for (uint32_t r = 0; r < static_cast<uint32_t>(B); ++r) {
+				if constexpr (OUT) { __stcs(dst + 32u * r + t, base_rep); }
 			}
-			const uint32_t y = ((x & ~N::kHigh) + (base_rep & ~N::kHigh)) ^ ((x ^ base_rep) & N::kHigh);
-			if (dst) { __stcs(dst + 32u * r + t, y); }
-			if (sum) {
-				uint32_t keep = y;
-				if (rem < 1024u) { // the column's last, partial vector
-					keep = 0;
-#pragma unroll
-					for (uint32_t j = 0; j < L; ++j) {
-						if (S * r + L * t + j < rem) { keep |= y & (N::kLow << (B * j)); }
-					}
-				}
-				part += lane_sum<B>(keep);
+			if constexpr (SUM) {
+				const uint64_t cnt = rem < 1024u ? rem : 1024u;
+				if (t == 0) { acc += cnt * (base_rep & N::kLow); }
 			}
+		} else if (rem >= 1024u) {
+			narrow_vector<B, OUT, SUM, false>(src, dst, bw, vm, base_rep, t, rem, part);
+		} else {
+			narrow_vector<B, OUT, SUM, true>(src, dst, bw, vm, base_rep, t, rem, part);
 		}
 		acc += part;
 	}
-	if (sum) {
+	if constexpr (SUM) {
 #pragma unroll
 		for (int off = 16; off > 0; off >>= 1) { acc += __shfl_xor_sync(0xffffffffu, acc, off); }
 		if (t == 0 && acc) { atomicAdd(sum, acc); }
 	}
 }
 
+// 64-bit lanes: a half-warp per vector, one lane per thread.
+template <bool OUT, bool SUM>
 __global__ void __launch_bounds__(256) decode_u64_kernel(const uint64_t* __restrict in, uint64_t n, uint64_t n_vec,
                                                          uint32_t bw, uint64_t base, uint64_t* __restrict out,
                                                          unsigned long long* sum) {
@@ -98,6 +126,7 @@ __global__ void __launch_bounds__(256) decode_u64_kernel(const uint64_t* __restr
 	const uint64_t     h0  = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 4;
 	const uint64_t     nh  = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 4;
 	const uint64_t     m   = bw >= 64 ? ~0ull : (1ull << bw) - 1ull;
+	const uint32_t     last = bw ? bw - 1u : 0u;
 	unsigned long long acc = 0;
 	// every half-warp runs the same number of iterations, so full-warp
 	// shuffles at the end see every lane
@@ -105,26 +134,44 @@ __global__ void __launch_bounds__(256) decode_u64_kernel(const uint64_t* __restr
 	for (uint64_t it = 0; it < iters; ++it) {
 		const uint64_t v = h0 + it * nh;
 		if (v >= n_vec) { continue; }
-		const uint64_t* src = in + v * 16u * bw;
-		const uint64_t  rem = n - v * 1024u;
-#pragma unroll 8
-		for (uint32_t r = 0; r < 64; ++r) {
-			const uint32_t o = r * bw, k = o >> 6, s = o & 63u;
-			uint64_t       x = 0;
-			if (bw) {
-				x = __ldg(reinterpret_cast<const unsigned long long*>(src) + 16u * k + i) >> s;
-				if (s + bw > 64u) { x |= __ldg(reinterpret_cast<const unsigned long long*>(src) + 16u * (k + 1u) + i) << (64u - s); }
-				x &= m;
+		const auto*    src = reinterpret_cast<const unsigned long long*>(in + v * 16u * bw);
+		const uint64_t rem = n - v * 1024u;
+		if (bw == 0) { // every value is the base; no payload to read
+			for (uint32_t r = 0; r < 64; ++r) {
+				if constexpr (OUT) { __stcs(reinterpret_cast<unsigned long long*>(out) + v * 1024u + 16u * r + i, base); }
+				if constexpr (SUM) { acc += 16u * r + i < rem ? base : 0ull; }
 			}
-			const uint64_t y = x + base;
-			if (out) { __stcs(reinterpret_cast<unsigned long long*>(out) + v * 1024u + 16u * r + i, y); }
-			if (sum && 16u * r + i < rem) { acc += y; }
+			continue;
+		}
+#pragma unroll 16
+		for (uint32_t r = 0; r < 64; ++r) {
+			// both word rows read unconditionally (the second clamped inside the
+			// vector) and combined by selection: no branch between the rows
+			const uint32_t o = r * bw, k = o >> 6, s = o & 63u;
+			const uint64_t lo_word = __ldg(src + 16u * k + i);
+			const uint64_t hi_word = __ldg(src + 16u * min(k + 1u, last) + i);
+			const uint64_t hi      = (hi_word << 1) << (63u - s); // hi_word << (64 - s), defined for s = 0
+			const uint64_t x       = ((lo_word >> s) | (s + bw > 64u ? hi : 0ull)) & m;
+			const uint64_t y       = x + base;
+			if constexpr (OUT) { __stcs(reinterpret_cast<unsigned long long*>(out) + v * 1024u + 16u * r + i, y); }
+			if constexpr (SUM) { acc += 16u * r + i < rem ? y : 0ull; }
 		}
 	}
-	if (sum) {
+	if constexpr (SUM) {
 #pragma unroll
 		for (int off = 16; off > 0; off >>= 1) { acc += __shfl_xor_sync(0xffffffffu, acc, off); }
 		if ((threadIdx.x & 31u) == 0 && acc) { atomicAdd(sum, acc); }
+	}
+}
+
+template <class K>
+void launch_mode(bool out, bool sum, K&& k) {
+	if (out && sum) {
+		k(std::integral_constant<int, 3> {});
+	} else if (out) {
+		k(std::integral_constant<int, 1> {});
+	} else {
+		k(std::integral_constant<int, 2> {});
 	}
 }
 
@@ -148,19 +195,25 @@ fls_status launch_decode(uint32_t bits, const void* d_in, uint64_t n, uint8_t bw
 	auto* sum = reinterpret_cast<unsigned long long*>(d_sum);
 	if (bits == 64) {
 		const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>((n_vec + 15u) / 16u, static_cast<uint64_t>(di.sms) * 16u));
-		decode_u64_kernel<<<grid, 256, 0, st>>>(static_cast<const uint64_t*>(d_in), n, n_vec, bw, base,
-		                                         static_cast<uint64_t*>(d_out), sum);
+		launch_mode(d_out != nullptr, d_sum != nullptr, [&](auto mode) {
+			constexpr int M = decltype(mode)::value;
+			decode_u64_kernel<(M & 1) != 0, (M & 2) != 0><<<grid, 256, 0, st>>>(
+			    static_cast<const uint64_t*>(d_in), n, n_vec, bw, base, static_cast<uint64_t*>(d_out), sum);
+		});
 	} else {
 		const uint32_t rep  = bits == 8 ? static_cast<uint32_t>(base & 0xffu) * 0x01010101u
 		                                : static_cast<uint32_t>(base & 0xffffu) * 0x00010001u;
 		const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>((n_vec + 7u) / 8u, static_cast<uint64_t>(di.sms) * 16u));
-		if (bits == 8) {
-			decode_narrow_kernel<8><<<grid, 256, 0, st>>>(static_cast<const uint32_t*>(d_in), n, n_vec, bw, rep,
-			                                              static_cast<uint32_t*>(d_out), sum);
-		} else {
-			decode_narrow_kernel<16><<<grid, 256, 0, st>>>(static_cast<const uint32_t*>(d_in), n, n_vec, bw, rep,
-			                                               static_cast<uint32_t*>(d_out), sum);
-		}
+		launch_mode(d_out != nullptr, d_sum != nullptr, [&](auto mode) {
+			constexpr int M = decltype(mode)::value;
+			if (bits == 8) {
+				decode_narrow_kernel<8, (M & 1) != 0, (M & 2) != 0><<<grid, 256, 0, st>>>(
+				    static_cast<const uint32_t*>(d_in), n, n_vec, bw, rep, static_cast<uint32_t*>(d_out), sum);
+			} else {
+				decode_narrow_kernel<16, (M & 1) != 0, (M & 2) != 0><<<grid, 256, 0, st>>>(
+				    static_cast<const uint32_t*>(d_in), n, n_vec, bw, rep, static_cast<uint32_t*>(d_out), sum);
+			}
+		});
 	}
 	count_launch();
 	return cuda_check(cudaGetLastError(), "decode kernel launch");

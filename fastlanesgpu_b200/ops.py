@@ -401,6 +401,15 @@ def pack_column_width(values: np.ndarray, bw: int, base: int = 0) -> np.ndarray:
     return out
 
 
+def decode_width_into(packed, n: int, bits: int, bw: int, base: int, out=None, sum_out=None) -> None:
+    """Stream-ordered form of decode_width: writes into `out` (device tensor of
+    the width's values, or None) and `sum_out` (device int64[1], or None)."""
+    check(getattr(lib(), f"fls_decode_u{bits}")(packed.data_ptr(), n, bw, base & ((1 << bits) - 1),
+                                               None if out is None else out.data_ptr(),
+                                               None if sum_out is None else sum_out.data_ptr(), _stream()),
+          f"fls_decode_u{bits}")
+
+
 def decode_width(packed, n: int, bits: int, bw: int, base: int = 0, out=None, want_sum: bool = True):
     """GPU decode of a packed 8/16/64-bit column (fls_decode_u8/u16/u64):
     packed is a 16-byte aligned device tensor of the packed bytes.  Returns
