@@ -63,8 +63,13 @@ struct DecodeSumOp {
 		dev::decode_vals(sv.s, sv.vi, ws.dict(), lane, vals);
 		const uint32_t     m = valid_rows(cfg, v, lane);
 		unsigned long long p[4] = {0, 0, 0, 0};
+		if (m == 0xffffffffu) { // every vector but the column's last
 #pragma unroll
-		for (uint32_t r = 0; r < 32; ++r) { p[r & 3] += ((m >> r) & 1u) ? vals[r] : 0u; }
+			for (uint32_t r = 0; r < 32; ++r) { p[r & 3] += vals[r]; }
+		} else {
+#pragma unroll
+			for (uint32_t r = 0; r < 32; ++r) { p[r & 3] += ((m >> r) & 1u) ? vals[r] : 0u; }
+		}
 		S.acc += (p[0] + p[1]) + (p[2] + p[3]);
 	}
 	__device__ void finish(State& S, uint32_t lane, const StageCfg&) const {
