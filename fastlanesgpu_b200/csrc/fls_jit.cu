@@ -174,11 +174,15 @@ Entry& compiled_entry(const std::string& key) {
 // Stage plan of a specialised kernel: tiles of k vectors, S stages per warp,
 // as many warps (up to the launch configuration's) as shared memory holds
 // next to cta_words of CTA-wide tables.
+// join: the probe + group-by kernels, which take up to jit_max_warps() warps;
+// the filter and decode kernels keep the launch configuration's (16 by
+// default: measured faster for them).
 fls_status plan_fixed(const DeviceInfo& di, const fls_column* sc, uint32_t n, uint32_t cta_words,
-                      fixed::StageParams& S, uint32_t& grid, size_t& smem) {
+                      fixed::StageParams& S, uint32_t& grid, size_t& smem, bool join = false) {
 	fls_status st       = FLS_OK;
 	uint32_t   W0 = 0, S0 = 0, ctas = 0, tile_bytes = 0;
 	fls_get_launch_config(&W0, &S0, &ctas, &tile_bytes);
+	if (join) { W0 = jit_max_warps(); }
 	std::memset(&S, 0, sizeof(S));
 	uint32_t sum_vec = 0;
 	for (uint32_t c = 0; c < n; ++c) {
@@ -502,7 +506,7 @@ bool jit_compile(const fls_join_groupby_desc* d, const JitProbeShape& sh) {
 	fixed::StageParams S;
 	uint32_t           grid;
 	size_t             smem;
-	if (plan_fixed(di, sc, sh.n_staged, sh.cta_words, S, grid, smem) != FLS_OK) { return false; }
+	if (plan_fixed(di, sc, sh.n_staged, sh.cta_words, S, grid, smem, true) != FLS_OK) { return false; }
 	std::lock_guard<std::mutex> lk(g_mu);
 	return compiled_entry(make_key('P', S.warps, sh.key)).state > 0;
 }
@@ -529,7 +533,7 @@ fls_status jit_probe_groupby(const fls_join_groupby_desc* d, int32_t* d_res, int
 	DeviceInfo         di;
 	fls_status         s = device_info(di);
 	if (s != FLS_OK) { return s; }
-	if ((s = plan_fixed(di, sc, sh.n_staged, sh.cta_words, P.S, grid, smem)) != FLS_OK) { return s; }
+	if ((s = plan_fixed(di, sc, sh.n_staged, sh.cta_words, P.S, grid, smem, true)) != FLS_OK) { return s; }
 	P.S.err = device_error_word();
 	for (uint32_t i = 0; i < sh.n_staged; ++i) { P.base[i] = static_cast<uint32_t>(sc[i].base); }
 	for (uint32_t q = 0; q < d->n_probes; ++q) {

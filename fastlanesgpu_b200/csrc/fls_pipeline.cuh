@@ -32,7 +32,12 @@ using dev::VecInfo;
 
 constexpr uint32_t kMaxCols    = FLS_MAX_QUERY_COLS;
 constexpr uint32_t kMaxTile    = 32;       // vectors per tile (one lane per vector at issue)
-constexpr uint32_t kMaxWarps   = 16;       // warps per CTA
+constexpr uint32_t kMaxWarps   = 16;       // warps per CTA (general kernels)
+// Warps per CTA of the specialised join kernels unless the caller set a
+// launch configuration: their launch bounds follow the shape, and joins whose
+// tables leave room for more than 16 warps run faster with them (the filter
+// and decode kernels measured faster at 16).
+constexpr uint32_t kJitDefaultWarps = 20;
 constexpr uint32_t kWaitPolls  = 1u << 17; // bounded mbarrier waits (x <= 20 us each)
 constexpr uint32_t kDictWords  = 1024;     // per-warp dictionary scratch
 constexpr uint32_t kTBufWords  = 33 * 32;  // per-warp transpose buffer
@@ -293,6 +298,7 @@ void       count_launch(uint64_t n = 1);
 int        tuning_sparse_rows();
 int        tuning_jit();
 int        tuning_group_smem();
+uint32_t   jit_max_warps(); // most warps per CTA of the specialised join kernels
 
 // Validates one column descriptor and converts it for a kernel.
 fls_status make_devcol(const fls_column& c, DevCol& d);

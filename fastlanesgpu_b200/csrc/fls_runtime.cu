@@ -24,6 +24,7 @@ struct LaunchCfg {
 };
 std::mutex g_cfg_mu;
 LaunchCfg  g_cfg;
+bool       g_warps_set = false; // warps chosen by the caller (fls_set_launch_config)
 
 LaunchCfg launch_cfg() {
 	std::lock_guard<std::mutex> lk(g_cfg_mu);
@@ -38,6 +39,11 @@ std::vector<uint32_t*>  g_err_addr;
 } // namespace
 
 void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+uint32_t jit_max_warps() {
+	std::lock_guard<std::mutex> lk(g_cfg_mu);
+	return g_warps_set ? g_cfg.warps : kJitDefaultWarps;
+}
 
 namespace {
 constexpr int    kDefaultSparseRows = 4;
@@ -258,6 +264,7 @@ fls_status fls_set_launch_config(uint32_t warps_per_cta, uint32_t stages, uint32
 	const LaunchCfg d;
 	std::lock_guard<std::mutex> lk(g_cfg_mu);
 	g_cfg.warps       = warps_per_cta ? warps_per_cta : d.warps;
+	g_warps_set       = warps_per_cta != 0;
 	g_cfg.stages      = stages ? stages : d.stages;
 	g_cfg.ctas_per_sm = ctas_per_sm ? ctas_per_sm : d.ctas_per_sm;
 	g_cfg.tile_bytes  = tile_bytes ? tile_bytes : d.tile_bytes;

@@ -460,7 +460,9 @@ fls_status fls_crystal_q21_probe(const int32_t* suppkey, uint32_t supp_bw, const
 /* Launch shape of the staged decode/query kernels: warps per CTA (<= 16),
  * pipeline stages per warp, CTAs per SM and the target bytes of one staged
  * tile of consecutive vectors (0 = library default for each).  Used by the
- * autotuner; applies to subsequent calls from all threads. */
+ * autotuner; applies to subsequent calls from all threads.  Until warps are
+ * set here, the specialised join + group-by kernels (FLS_TUNE_JIT) use up to
+ * 20 warps per CTA where shared memory allows, every other kernel 16. */
 fls_status fls_set_launch_config(uint32_t warps_per_cta, uint32_t stages, uint32_t ctas_per_sm, uint32_t tile_bytes);
 fls_status fls_get_launch_config(uint32_t* warps_per_cta, uint32_t* stages, uint32_t* ctas_per_sm,
                                  uint32_t* tile_bytes);
