@@ -78,9 +78,17 @@ __device__ __forceinline__ void narrow_vector(const uint32_t* __restrict src, ui
 	}
 }
 
+// Resident 256-thread blocks per SM asked of the compiler (it trades
+// registers for warps), measured per form on B200 at 2^28 values: decode to
+// HBM 4, 8-bit sums and 64-bit lanes 3, 16-bit sums 2.
+template <int B, bool OUT, bool SUM>
+constexpr int narrow_min_blocks() {
+	return OUT && !SUM ? 4 : (B == 16 && !OUT ? 2 : 3);
+}
+
 // 8/16-bit lanes: one warp per vector (a 0-bit column reads no payload).
 template <int B, bool OUT, bool SUM>
-__global__ void __launch_bounds__(256) decode_narrow_kernel(const uint32_t* __restrict in, uint64_t n, uint64_t n_vec,
+__global__ void __launch_bounds__(256, narrow_min_blocks<B, OUT, SUM>()) decode_narrow_kernel(const uint32_t* __restrict in, uint64_t n, uint64_t n_vec,
                                                             uint32_t bw, uint32_t base_rep, uint32_t* __restrict out,
                                                             unsigned long long* sum) {
 	using N                = Narrow<B>;
@@ -119,7 +127,7 @@ __global__ void __launch_bounds__(256) decode_narrow_kernel(const uint32_t* __re
 
 // 64-bit lanes: a half-warp per vector, one lane per thread.
 template <bool OUT, bool SUM>
-__global__ void __launch_bounds__(256) decode_u64_kernel(const uint64_t* __restrict in, uint64_t n, uint64_t n_vec,
+__global__ void __launch_bounds__(256, 3) decode_u64_kernel(const uint64_t* __restrict in, uint64_t n, uint64_t n_vec,
                                                          uint32_t bw, uint64_t base, uint64_t* __restrict out,
                                                          unsigned long long* sum) {
 	const uint32_t     i   = threadIdx.x & 15u; // lane of the vector
