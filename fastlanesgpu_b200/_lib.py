@@ -149,6 +149,7 @@ _SIGS = {
     "fls_encode_gpu_workspace_bytes": (ctypes.c_uint64, [ctypes.c_uint64]),
     "fls_encode_column_gpu": (ctypes.c_int, [_VP, ctypes.c_uint64, _VP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
                                              _VP, ctypes.c_uint64, _VP, _VP, _VP, ctypes.c_uint64, _VP]),
+    "fls_selftest_bounded_wait": (ctypes.c_int, [ctypes.c_uint32, _VP]),
     "fls_pack_u8": (ctypes.c_int, [_VP, _VP, ctypes.c_uint8]),
     "fls_pack_u16": (ctypes.c_int, [_VP, _VP, ctypes.c_uint8]),
     "fls_pack_u64": (ctypes.c_int, [_VP, _VP, ctypes.c_uint8]),

@@ -229,6 +229,25 @@ fls_status plan_stages(const fls_column* cols, uint32_t n_cols, uint32_t extra_w
 	return FLS_OK;
 }
 
+namespace {
+// Self-test of the bounded waits every pipeline uses: one warp waits on an
+// mbarrier that nothing arrives on, with the pipelines' own bounded wait, so
+// it gives up after `polls` tries, raises the timeout bit and returns; the
+// host then reads FLS_ERR_TIMEOUT from fls_check_device_error and the context
+// stays usable.  No fault, trap or unbounded wait is involved.
+__global__ void wait_selftest_kernel(uint32_t polls, uint32_t* err) {
+	__shared__ uint64_t bar;
+	if (threadIdx.x == 0) {
+		dev::mbar_init(&bar, 1);
+		dev::fence_mbar_init();
+	}
+	__syncwarp();
+	const bool done = dev::mbar_wait_bounded(&bar, 0, polls);
+	if (!done && threadIdx.x == 0) { atomicOr(err, kErrTimeout); }
+}
+
+} // namespace
+
 } // namespace fls
 
 using namespace fls;
@@ -254,6 +273,16 @@ fls_status fls_check_device_error(fls_stream_t stream) {
 		return set_error(FLS_ERR_TIMEOUT, msg);
 	}
 	return set_error(FLS_ERR_DEVICE, msg);
+}
+
+fls_status fls_selftest_bounded_wait(uint32_t polls, fls_stream_t stream) {
+	if (polls == 0 || polls > 1024) { return set_error(FLS_ERR_INVALID_ARG, "fls_selftest_bounded_wait: polls in 1..1024"); }
+	DeviceInfo di;
+	fls_status s = device_info(di);
+	if (s != FLS_OK) { return s; }
+	wait_selftest_kernel<<<1, 32, 0, reinterpret_cast<cudaStream_t>(stream)>>>(polls, device_error_word());
+	count_launch();
+	return cuda_check(cudaGetLastError(), "wait_selftest_kernel launch");
 }
 
 fls_status fls_set_launch_config(uint32_t warps_per_cta, uint32_t stages, uint32_t ctas_per_sm, uint32_t tile_bytes) {

@@ -427,3 +427,10 @@ def decode_width(packed, n: int, bits: int, bw: int, base: int = 0, out=None, wa
           f"fls_decode_u{bits}")
     total = None if s is None else int(s.cpu()[0]) & 0xFFFFFFFFFFFFFFFF
     return (None if out is False else out), total
+
+
+def selftest_bounded_wait(polls: int = 64) -> None:
+    """Runs the pipelines' bounded device wait on a barrier nothing arrives
+    on (fls_selftest_bounded_wait); the next check_device_error raises
+    FLS_ERR_TIMEOUT."""
+    check(lib().fls_selftest_bounded_wait(polls, _stream()), "fls_selftest_bounded_wait")

@@ -99,6 +99,13 @@ const char* fls_last_error(void);
  * Returns FLS_OK, FLS_ERR_DEVICE or FLS_ERR_TIMEOUT. */
 fls_status fls_check_device_error(fls_stream_t stream);
 
+/* Self-test of failure detection (no reference counterpart): one warp runs
+ * the bounded mbarrier wait of the staged pipelines on a barrier that nothing
+ * arrives on, gives up after `polls` (1..1024, about 20 us each at most) tries
+ * and raises the timeout bit, so the next fls_check_device_error returns
+ * FLS_ERR_TIMEOUT; the context stays usable.  Nothing faults or hangs. */
+fls_status fls_selftest_bounded_wait(uint32_t polls, fls_stream_t stream);
+
 /* ------------------------------------------------- host encoders (CPU) */
 
 /* fastlanes/src/pack.cpp:29607 generated::pack::fallback::scalar::pack(u32):
