@@ -139,3 +139,53 @@ def test_gloo_two_ranks_combine_group_records(oracle):
         want = _ssb_records(oracle, name, t, 0, n)
         assert (want != 0).any()
         assert np.array_equal(got[0][name], want) and np.array_equal(got[1][name], want), name
+
+
+def _leaving_worker(rank, world, port, q):
+    import datetime
+    import sys
+    import time
+    import torch
+    import torch.distributed as dist
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, here)
+    from fastlanesgpu_b200.shard import allreduce_sum
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    x = torch.ones(1, dtype=torch.int64)
+    allreduce_sum(x)  # one good step on both ranks
+    if rank == 1:
+        q.put((rank, "left", int(x.item())))
+        q.close()
+        q.join_thread()  # the message is out before the process ends
+        os._exit(0)  # leaves between steps, without its next collective
+    t0 = time.time()
+    try:
+        allreduce_sum(x)
+        q.put((rank, "no error", time.time() - t0))
+    except Exception as e:  # the peer is gone: the collective ends with an error
+        q.put((rank, type(e).__name__, time.time() - t0))
+    q.close()
+    q.join_thread()
+    os._exit(0)
+
+
+def test_gloo_rank_that_leaves_ends_the_next_collective_with_an_error():
+    """Failure detection on the host: after one good step, rank 1 exits
+    between steps; rank 0's next all-reduce raises within the process group's
+    short timeout instead of waiting for good."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_leaving_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    got = {}
+    for _ in range(2):
+        r, what, val = q.get(timeout=120)
+        got[r] = (what, val)
+    for p in ps:
+        p.join(timeout=60)
+    assert got[1] == ("left", 2)
+    assert got[0][0] != "no error" and got[0][1] < 60, got
