@@ -55,6 +55,8 @@ def parse_args():
     ap.add_argument("--sparse-rows", type=int, default=0, help="FLS_TUNE_SPARSE_ROWS (0 = default)")
     ap.add_argument("--jit", type=int, choices=[0, 1], default=1,
                     help="FLS_TUNE_JIT: 1 = kernel specialised to the query's shape, 0 = general kernel")
+    ap.add_argument("--late-measure", type=int, choices=[0, 1], default=None,
+                    help="FLS_TUNE_LATE_MEASURE: 1 = join measures read from global memory for selected rows only")
     ap.add_argument("--group-smem", type=int, choices=[0, 1], default=1,
                     help="FLS_TUNE_GROUP_SMEM: 1 = per-CTA group sums in shared memory, 0 = a global atomic per row")
     ap.add_argument("--mixed-columns", type=int, default=64, help="mixed workload: number of columns")
@@ -214,6 +216,8 @@ def run_ours(a, dist: Dist):
         ops.set_tuning(0, a.sparse_rows)
     ops.set_tuning(1, a.jit)
     ops.set_tuning(2, a.group_smem)
+    if a.late_measure is not None:
+        ops.set_tuning(3, a.late_measure)
     from fastlanesgpu_b200.shard import allreduce_sum, combine_group_records, shard_seed
     seed = shard_seed(1000, dist.rank)
     # ---------------------------------------------------------------- setup
@@ -497,6 +501,7 @@ def run_ours(a, dist: Dist):
         "gpu_launches": int(launches),
         "launch_config": dict(zip(["warps", "stages", "ctas_per_sm", "tile_bytes"], ops.get_launch_config()),
                               sparse_rows=ops.get_tuning(0), jit=ops.get_tuning(1), group_smem=ops.get_tuning(2),
+                              late_measure=ops.get_tuning(3),
                               jit_launches=int(ops.jit_stats()["launches"])),
         "clocks": clk,
     }

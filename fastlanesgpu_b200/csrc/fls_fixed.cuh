@@ -68,6 +68,7 @@ struct ProbeParams {
 	uint32_t       sum32;            // 1: wrapping int32 sum in one record word, 0: int64 in two
 	const uint32_t* bits;            // presence bitmaps at the tables' shared-memory offsets
 	int32_t*       res;
+	const uint32_t* gcol[2];         // columns kNS, kNS + 1 (not staged): packed words in global memory
 };
 
 struct DecodeParams {
@@ -83,13 +84,14 @@ struct DecodeParams {
 // sizes mean equal offsets.
 static_assert(sizeof(StageParams) == 128 && alignof(StageParams) == 8, "StageParams layout");
 static_assert(sizeof(FilterParams) == 240, "FilterParams layout");
-static_assert(sizeof(ProbeParams) == 312, "ProbeParams layout");
+static_assert(sizeof(ProbeParams) == 328, "ProbeParams layout");
 static_assert(sizeof(DecodeParams) == 152, "DecodeParams layout");
 
 // Bit widths of the staged columns and where they sit in a stage.
 template <int LAYOUT, int... BWS>
 struct Shape {
 	static constexpr int NC      = sizeof...(BWS);
+	static constexpr int kNS     = NC; // columns staged in shared memory (the first kNS)
 	static constexpr int kLayout = LAYOUT;
 	__host__ __device__ static constexpr int bw(int c) {
 		int i = 0, r = 0;
@@ -131,13 +133,14 @@ struct FilterQuery : Shape<LAYOUT, BWS...> {
 // in shared memory (a group claims its slot, or else adds to its record
 // directly) and adds the slots' non-zero sums to the records once, at its end.
 template <int LAYOUT, int NP, int AGG, int SUB, int NK, int K0, int K1, int K2, int KINDS, int SMEM, int PBIT,
-          int DIRECT, int GSM, int... BWS>
+          int DIRECT, int GSM, int NS, int... BWS>
 struct ProbeQuery : Shape<LAYOUT, BWS...> {
 	static constexpr int kNP  = NP;
 	static constexpr int kAgg = AGG;
 	static constexpr int kSub = SUB;
 	static constexpr int kNK  = NK;
 	static constexpr bool kGroupSmem = GSM != 0;
+	static constexpr int  kNS        = NS; // staged columns; the measure columns past them stay in global memory
 	__host__ __device__ static constexpr int key_probe(int k) { return k == 0 ? K0 : k == 1 ? K1 : K2; }
 	__host__ __device__ static constexpr bool pht2(int q) { return (KINDS >> q) & 1; }
 	__host__ __device__ static constexpr bool in_smem(int q) { return (SMEM >> q) & 1; }
@@ -146,6 +149,8 @@ struct ProbeQuery : Shape<LAYOUT, BWS...> {
 	__host__ __device__ static constexpr bool dense_ok(int q) { return !pht2(q) || in_smem(q) || pbit(q); }
 	__host__ __device__ static constexpr bool direct(int q) { return (DIRECT >> q) & 1; }
 	static_assert(NP >= 1 && NP <= FLS_MAX_PROBES, "1..4 probes");
+	static_assert(NS >= NP && NS <= static_cast<int>(sizeof...(BWS)) && static_cast<int>(sizeof...(BWS)) - NS <= 2,
+	              "probe columns staged; at most two columns in global memory");
 };
 
 // MODE 0: decode fused with a uint64 sum; MODE 1: decode to HBM in stored
@@ -288,6 +293,28 @@ __device__ __forceinline__ bool row_pass(const FilterParams& P, const Vec<Q>& V,
 template <class Q, int C>
 __device__ __forceinline__ int32_t row_value(const uint32_t* base, const Vec<Q>& V, uint32_t lane, uint32_t r) {
 	return static_cast<int32_t>(row_field<Q::bw(C)>(V.template col<C>(), lane, r) + base[C]);
+}
+
+// Field of row r of `lane` in vector v of a column left in global memory
+// (uniform FOR: vector v at word 32*BW*v, word k of the lane at 32k + lane);
+// the second word is read only when the field straddles, so every read stays
+// inside the vector.
+template <int BW>
+__device__ __forceinline__ uint32_t global_field(const uint32_t* __restrict__ col, uint64_t v, uint32_t lane,
+                                                 uint32_t r) {
+	if constexpr (BW == 0) {
+		return 0u;
+	} else {
+		const uint32_t* p   = col + v * (32u * BW);
+		const uint32_t  bit = r * BW, k = bit >> 5, s = bit & 31u;
+		const uint32_t  lo  = __ldg(p + 32u * k + lane);
+		if constexpr (BW == 32) {
+			return lo;
+		} else {
+			const uint32_t hi = s + BW > 32u ? __ldg(p + 32u * (k + 1u) + lane) : 0u;
+			return __funnelshift_r(lo, hi, s) & ((1u << BW) - 1u);
+		}
+	}
 }
 
 // Filters F0.. and the aggregate, one selected row at a time (warp-uniform
@@ -575,9 +602,21 @@ __device__ __forceinline__ void emit(const ProbeParams& P, uint32_t* tables,
 	if (!cached) { add_record_sum(P, rec, static_cast<unsigned long long>(static_cast<long long>(measure))); }
 }
 
+// Value of measure column C for a selected row: from the stage, or (column
+// past the staged ones) from global memory.
+template <class Q, int C>
+__device__ __forceinline__ uint32_t measure_value(const ProbeParams& P, const Vec<Q>& V, uint64_t v, uint32_t lane,
+                                                  uint32_t r) {
+	if constexpr (C < Q::kNS) {
+		return static_cast<uint32_t>(row_value<Q, C>(P.base, V, lane, r));
+	} else {
+		return global_field<Q::bw(C)>(P.gcol[C - Q::kNS], v, lane, r) + P.base[C];
+	}
+}
+
 template <class Q>
-__device__ __forceinline__ void row_phase(const ProbeParams& P, uint32_t* tables, const Vec<Q>& V, uint32_t lane,
-                                          uint32_t mask, int f0) {
+__device__ __forceinline__ void row_phase(const ProbeParams& P, uint32_t* tables, const Vec<Q>& V, uint64_t v,
+                                          uint32_t lane, uint32_t mask, int f0) {
 	const int n_it = max_rows(mask);
 	for (int it0 = 0; it0 < n_it; it0 += kRowBatch) {
 		const int rem = n_it - it0; // warp-uniform
@@ -593,12 +632,31 @@ __device__ __forceinline__ void row_phase(const ProbeParams& P, uint32_t* tables
 			for (int k = 0; k < FLS_MAX_GROUP_KEYS; ++k) { kv[k][j] = 0; }
 		}
 		probe_rows<Q, 0>(P, tables, V, lane, rows, pass, kv, rem, f0);
+		if constexpr (Q::kAgg >= Q::kNS || Q::kSub >= Q::kNS) {
+			// measures in global memory: the batch's reads first, all in flight
+			uint32_t m[kRowBatch];
 #pragma unroll
-		for (int j = 0; j < kRowBatch; ++j) {
-			if (j < rem && pass[j]) {
-				uint32_t m = static_cast<uint32_t>(row_value<Q, Q::kAgg>(P.base, V, lane, rows[j]));
-				if constexpr (Q::kSub >= 0) { m -= static_cast<uint32_t>(row_value<Q, Q::kSub>(P.base, V, lane, rows[j])); }
-				emit<Q>(P, tables, kv, j, static_cast<int32_t>(m));
+			for (int j = 0; j < kRowBatch; ++j) {
+				m[j] = 0u;
+				if (j < rem && pass[j]) {
+					m[j] = measure_value<Q, Q::kAgg>(P, V, v, lane, rows[j]);
+					if constexpr (Q::kSub >= 0) { m[j] -= measure_value<Q, Q::kSub>(P, V, v, lane, rows[j]); }
+				}
+			}
+#pragma unroll
+			for (int j = 0; j < kRowBatch; ++j) {
+				if (j < rem && pass[j]) { emit<Q>(P, tables, kv, j, static_cast<int32_t>(m[j])); }
+			}
+		} else {
+#pragma unroll
+			for (int j = 0; j < kRowBatch; ++j) {
+				if (j < rem && pass[j]) {
+					uint32_t m = static_cast<uint32_t>(row_value<Q, Q::kAgg>(P.base, V, lane, rows[j]));
+					if constexpr (Q::kSub >= 0) {
+						m -= static_cast<uint32_t>(row_value<Q, Q::kSub>(P.base, V, lane, rows[j]));
+					}
+					emit<Q>(P, tables, kv, j, static_cast<int32_t>(m));
+				}
 			}
 		}
 	}
@@ -700,7 +758,7 @@ struct ProbeBody {
 		int      f0   = Q::kNP;
 		dense_probes<Q, 0>(P, tables, V, lane, mask, f0);
 		if (!__any_sync(0xffffffffu, mask)) { return; }
-		row_phase<Q>(P, tables, V, lane, mask, f0);
+		row_phase<Q>(P, tables, V, v, lane, mask, f0);
 	}
 
 	// GSM: once every warp of the CTA is done, the CTA adds each claimed
@@ -775,7 +833,7 @@ struct DecodeBody {
 // Words per vector and stage offset (in vectors' words) of column `lane`.
 template <class Q, int C>
 __device__ __forceinline__ void lane_column(uint32_t lane, uint32_t& vw, uint32_t& pre) {
-	if constexpr (C < Q::NC) {
+	if constexpr (C < Q::kNS) {
 		constexpr uint32_t w = Q::vec_words(C), p = Q::prefix(C);
 		if (lane == C) {
 			vw  = w;
@@ -791,7 +849,7 @@ __device__ __forceinline__ void issue(const StageParams& S, uint32_t* stage, uin
                                       uint64_t pol) {
 	const uint64_t v0 = t * S.tile;
 	const uint64_t kk = S.n_vec - v0 < S.tile ? S.n_vec - v0 : S.tile;
-	if (lane < static_cast<uint32_t>(Q::NC)) {
+	if (lane < static_cast<uint32_t>(Q::kNS)) {
 		uint32_t vw = 0, pre = 0;
 		lane_column<Q, 0>(lane, vw, pre);
 		const uint32_t bytes = static_cast<uint32_t>(kk) * vw * 4u;

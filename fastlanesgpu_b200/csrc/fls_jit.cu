@@ -439,9 +439,15 @@ bool jit_probe_shape(const fls_join_groupby_desc* d, JitProbeShape& sh) {
 		sh.staged[sh.n_staged] = static_cast<uint32_t>(c);
 		return static_cast<int>(sh.n_staged++);
 	};
-	sh.agg = slot_of(static_cast<int32_t>(d->agg_col));
-	sh.sub = slot_of(d->agg_sub_col);
-	for (uint32_t i = 0; i < sh.n_staged; ++i) {
+	// The measure columns: staged like the probe columns, or (late measures)
+	// left in global memory, past the staged ones, and read for the selected
+	// rows only.  A measure that is also a probe column is staged anyway.
+	const uint32_t n_probe_cols = sh.n_staged;
+	sh.agg                      = slot_of(static_cast<int32_t>(d->agg_col));
+	sh.sub                      = slot_of(d->agg_sub_col);
+	sh.n_global                 = tuning_late_measure() ? sh.n_staged - n_probe_cols : 0u;
+	sh.n_staged -= sh.n_global;
+	for (uint32_t i = 0; i < sh.n_staged + sh.n_global; ++i) {
 		if (!uniform_for(d->cols[sh.staged[i]], d->cols[sh.staged[0]].layout)) { return false; }
 	}
 	// Tables go to shared memory in probe order while they fit the budget:
@@ -487,14 +493,14 @@ bool jit_probe_shape(const fls_join_groupby_desc* d, JitProbeShape& sh) {
 	sh.gsum_off = sh.cta_words;
 	if (sh.gsm) { sh.cta_words += 3u * sh.gslots + (4u - (3u * sh.gslots) % 4u) % 4u; }
 	fls_column sc[FLS_MAX_QUERY_COLS];
-	for (uint32_t i = 0; i < sh.n_staged; ++i) { sc[i] = d->cols[sh.staged[i]]; }
+	for (uint32_t i = 0; i < sh.n_staged + sh.n_global; ++i) { sc[i] = d->cols[sh.staged[i]]; }
 	int kp[FLS_MAX_GROUP_KEYS] = {-1, -1, -1};
 	for (uint32_t k = 0; k < d->n_keys; ++k) { kp[k] = d->key_probe[k]; }
 	char head[160];
-	std::snprintf(head, sizeof(head), "%u, %u, %d, %d, %u, %d, %d, %d, %u, %u, %u, %u, %d",
+	std::snprintf(head, sizeof(head), "%u, %u, %d, %d, %u, %d, %d, %d, %u, %u, %u, %u, %d, %u",
 	              static_cast<unsigned>(sc[0].layout), d->n_probes, sh.agg, sh.sub, d->n_keys, kp[0], kp[1], kp[2], kinds,
-	              in_smem, pbit, direct, sh.gsm ? 1 : 0);
-	sh.key = key_args(sc, sh.n_staged, head);
+	              in_smem, pbit, direct, sh.gsm ? 1 : 0, sh.n_staged);
+	sh.key = key_args(sc, sh.n_staged + sh.n_global, head);
 	return true;
 }
 
@@ -535,7 +541,10 @@ fls_status jit_probe_groupby(const fls_join_groupby_desc* d, int32_t* d_res, int
 	if (s != FLS_OK) { return s; }
 	if ((s = plan_fixed(di, sc, sh.n_staged, sh.cta_words, P.S, grid, smem, true)) != FLS_OK) { return s; }
 	P.S.err = device_error_word();
-	for (uint32_t i = 0; i < sh.n_staged; ++i) { P.base[i] = static_cast<uint32_t>(sc[i].base); }
+	for (uint32_t i = 0; i < sh.n_staged + sh.n_global; ++i) {
+		P.base[i] = static_cast<uint32_t>(d->cols[sh.staged[i]].base);
+	}
+	for (uint32_t g = 0; g < sh.n_global; ++g) { P.gcol[g] = d->cols[sh.staged[sh.n_staged + g]].data; }
 	for (uint32_t q = 0; q < d->n_probes; ++q) {
 		P.ht[q]       = d->probes[q].ht;
 		P.len[q]      = d->probes[q].ht_len;

@@ -298,6 +298,7 @@ void       count_launch(uint64_t n = 1);
 int        tuning_sparse_rows();
 int        tuning_jit();
 int        tuning_group_smem();
+int        tuning_late_measure();
 uint32_t   jit_max_warps(); // most warps per CTA of the specialised join kernels
 
 // Validates one column descriptor and converts it for a kernel.
@@ -339,6 +340,7 @@ struct JitProbeShape {
 	uint32_t    cta_words = 0;
 	uint32_t    tables_words = 0;  // words of the tables (the presence bitmaps' buffer)
 	uint32_t    bitmaps      = 0;  // probes whose presence bitmap is staged
+	uint32_t    n_global     = 0;     // measure columns left in global memory (after the staged ones)
 	bool        gsm          = false; // group sums in shared memory
 	uint32_t    gslots       = 0;     // their slots (a power of two)
 	uint32_t    gsum_off     = 0;     // their offset (words) in the CTA scratch

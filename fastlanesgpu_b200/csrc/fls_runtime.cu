@@ -50,11 +50,13 @@ constexpr int    kDefaultSparseRows = 4;
 std::atomic<int> g_sparse_rows {kDefaultSparseRows};
 std::atomic<int> g_jit {1};
 std::atomic<int> g_group_smem {1};
+std::atomic<int> g_late_measure {0};
 } // namespace
 
 int tuning_sparse_rows() { return g_sparse_rows.load(std::memory_order_relaxed); }
 int tuning_jit() { return g_jit.load(std::memory_order_relaxed); }
 int tuning_group_smem() { return g_group_smem.load(std::memory_order_relaxed); }
+int tuning_late_measure() { return g_late_measure.load(std::memory_order_relaxed); }
 
 fls_status cuda_check(cudaError_t e, const char* what) {
 	if (e == cudaSuccess) { return FLS_OK; }
@@ -326,6 +328,10 @@ fls_status fls_set_tuning(uint32_t param, int64_t value) {
 		if (value < 0 || value > 1) { return set_error(FLS_ERR_INVALID_ARG, "group smem must be 0 or 1"); }
 		g_group_smem.store(static_cast<int>(value));
 		return FLS_OK;
+	case FLS_TUNE_LATE_MEASURE:
+		if (value < 0 || value > 1) { return set_error(FLS_ERR_INVALID_ARG, "late measure must be 0 or 1"); }
+		g_late_measure.store(static_cast<int>(value));
+		return FLS_OK;
 	default: return set_error(FLS_ERR_INVALID_ARG, "unknown tuning parameter");
 	}
 }
@@ -336,6 +342,7 @@ fls_status fls_get_tuning(uint32_t param, int64_t* value) {
 	case FLS_TUNE_SPARSE_ROWS: *value = tuning_sparse_rows(); return FLS_OK;
 	case FLS_TUNE_JIT: *value = tuning_jit(); return FLS_OK;
 	case FLS_TUNE_GROUP_SMEM: *value = tuning_group_smem(); return FLS_OK;
+	case FLS_TUNE_LATE_MEASURE: *value = tuning_late_measure(); return FLS_OK;
 	default: return set_error(FLS_ERR_INVALID_ARG, "unknown tuning parameter");
 	}
 }

@@ -496,7 +496,12 @@ typedef enum fls_tune_param {
 	 * slots to the group records once per CTA, instead of one global int64
 	 * atomic per selected row (few live groups make those atomics contend).
 	 * 0: one global atomic per row.  Results are identical either way. */
-	FLS_TUNE_GROUP_SMEM = 2
+	FLS_TUNE_GROUP_SMEM = 2,
+	/* 1: the specialised join + group-by kernels leave the measure columns
+	 * (aggregated and subtracted) in global memory and read their fields for
+	 * the selected rows only, instead of staging them whole with the probe
+	 * columns.  0 (default): staged.  Results are identical either way. */
+	FLS_TUNE_LATE_MEASURE = 3
 } fls_tune_param;
 fls_status fls_set_tuning(uint32_t param, int64_t value);
 fls_status fls_get_tuning(uint32_t param, int64_t* value);

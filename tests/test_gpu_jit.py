@@ -254,8 +254,16 @@ def _numpy_probe(keys, measure, probes_np, agg_vals, ka, kb, mul, sub, ng):
     return res32
 
 
+@pytest.fixture(params=[0, 1], ids=["staged", "late"])
+def late_measure(request):
+    from fastlanesgpu_b200._lib import TUNE_LATE_MEASURE
+    ops.set_tuning(TUNE_LATE_MEASURE, request.param)
+    yield request.param
+    ops.set_tuning(TUNE_LATE_MEASURE, 0)
+
+
 @pytest.mark.parametrize("seed", range(12))
-def test_jit_probe_random_shapes(jit_on, seed):
+def test_jit_probe_random_shapes(jit_on, late_measure, seed):
     import torch
     g = np.random.default_rng(500 + seed)
     n = int(g.choice([17, 1024, 3000, 50 * 1024 + 9, 200 * 1024]))

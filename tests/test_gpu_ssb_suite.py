@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from fastlanesgpu_b200 import EncodedColumn, datagen, ops
-from fastlanesgpu_b200._lib import TUNE_JIT
+from fastlanesgpu_b200._lib import TUNE_JIT, TUNE_LATE_MEASURE
 
 pytestmark = pytest.mark.gpu
 
@@ -60,8 +60,9 @@ def test_ssb_query_against_oracle(ssb_data, oracle, name):
     t, dcols = ssb_data
     want, tables = ssb_want(oracle, name, t)
     try:
-        for jit in (1, 0):
+        for jit, late in ((1, 0), (1, 1), (0, 0)):
             ops.set_tuning(TUNE_JIT, jit)
+            ops.set_tuning(TUNE_LATE_MEASURE, late)
             before = ops.jit_stats()["launches"]
             got, dq = ssb_run(name, t, dcols)
             assert ops.jit_stats()["launches"] - before == jit, (name, jit)
@@ -73,4 +74,5 @@ def test_ssb_query_against_oracle(ssb_data, oracle, name):
                 assert (want != 0).any() and np.array_equal(got, want), (name, jit)
     finally:
         ops.set_tuning(TUNE_JIT, 1)
+        ops.set_tuning(TUNE_LATE_MEASURE, 0)
     assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
