@@ -1,10 +1,14 @@
-"""Autotuner of the staged kernels' launch shape.
+"""Autotuner of the staged kernels' launch shape and of the join kernels'
+variants.
 
 Sweeps warps per CTA, pipeline stages, tile bytes (vectors per staged tile)
-and the dense/row-at-a-time threshold for a workload, times each candidate
-with CUDA events after warm-up, keeps the fastest and caches it in a JSON file
-keyed by the workload's signature (default ~/.cache/fastlanesgpu_b200/
-autotune.json, or $FLS_AUTOTUNE_CACHE)."""
+and the dense/row-at-a-time threshold for a workload (DEFAULT_SPACE), or the
+join kernels' choices that depend on the query's selectivity -- measure
+columns staged or read late, group sums per CTA or per row (JOIN_SPACE) --,
+times each candidate with CUDA events after warm-up, keeps the fastest and
+caches it in a JSON file keyed by the workload's signature (default
+~/.cache/fastlanesgpu_b200/autotune.json, or $FLS_AUTOTUNE_CACHE).  Results
+never depend on the choice."""
 from __future__ import annotations
 
 import itertools
@@ -19,6 +23,15 @@ DEFAULT_SPACE = {
     "tile_bytes": [2048, 6144, 16384],
     "sparse_rows": [2, 4, 8],
 }
+
+# The join + group-by kernels' variants whose best choice depends on how many
+# rows pass the probes, which the library cannot see before a query runs.
+JOIN_SPACE = {
+    "late_measure": [0, 1],
+    "group_smem": [1, 0],
+}
+
+_TUNING = {"sparse_rows": 0, "group_smem": 2, "late_measure": 3}
 
 
 def cache_path() -> str:
@@ -35,8 +48,13 @@ def _load(path):
 
 
 def apply(cfg: dict) -> None:
-    ops.set_launch_config(cfg["warps"], cfg["stages"], 0, cfg["tile_bytes"])
-    ops.set_tuning(0, cfg["sparse_rows"])
+    """Applies the settings `cfg` names (launch shape and tuning parameters);
+    the others keep their current values."""
+    if any(k in cfg for k in ("warps", "stages", "tile_bytes")):
+        ops.set_launch_config(cfg.get("warps", 0), cfg.get("stages", 0), 0, cfg.get("tile_bytes", 0))
+    for k, param in _TUNING.items():
+        if k in cfg:
+            ops.set_tuning(param, cfg[k])
 
 
 def time_ms(fn, warmup: int = 3, iters: int = 10) -> float:
@@ -82,5 +100,8 @@ def tune(signature: str, fn, space: dict | None = None, iters: int = 10, use_cac
 
 
 def reset() -> None:
+    """Library defaults for everything the tuner sets."""
     ops.set_launch_config(0, 0, 0, 0)
     ops.set_tuning(0, 0)
+    ops.set_tuning(2, 1)
+    ops.set_tuning(3, 0)

@@ -101,3 +101,27 @@ def test_autotuner_picks_and_caches(cuda, tmp_path):
         assert again["config"] == best["config"]
     finally:
         autotune.reset()
+
+
+def test_autotuner_join_space(cuda, oracle, tmp_path):
+    """JOIN_SPACE picks the join kernel's variants for one query (late
+    measures, group sums per CTA) by timing them; every candidate gives the
+    oracle's records, and the choice is applied and cached."""
+    from fastlanesgpu_b200 import autotune, datagen
+    from test_gpu_ssb_suite import ssb_want
+    t = datagen.ssb_tables(1 << 20, seed=5)
+    dcols = {k: EncodedColumn.uniform(t[k], bw=b).to_device() for k, b in datagen.SSB_BITS.items()}
+    dq = datagen.ssb_device_query("q43", t, dcols)
+    want, _ = ssb_want(oracle, "q43", t)
+    got = []
+    run = lambda: got.append(ops.join_groupby(dq["cols"], dq["probes"], **dq["kw"]))  # noqa: E731
+    path = str(tmp_path / "tune.json")
+    try:
+        best = autotune.tune("q43-test", run, space=autotune.JOIN_SPACE, iters=2, path=path)
+        assert len(best["candidates"]) == 4 and set(best["config"]) == {"late_measure", "group_smem"}
+        assert ops.get_tuning(3) == best["config"]["late_measure"]
+        assert all(np.array_equal(g.cpu().numpy(), want) for g in got)
+        again = autotune.tune("q43-test", run, space=autotune.JOIN_SPACE, iters=2, path=path)
+        assert again["config"] == best["config"]
+    finally:
+        autotune.reset()
