@@ -59,6 +59,8 @@ def parse_args():
                     help="FLS_TUNE_LATE_MEASURE: 1 = join measures read from global memory for selected rows only")
     ap.add_argument("--tune-joins", type=int, choices=[0, 1], default=1,
                     help="ssb workload: choose each join's variants with the autotuner (JOIN_SPACE) before timing")
+    ap.add_argument("--table-kb", type=int, default=0,
+                    help="FLS_TUNE_TABLE_KB: shared-memory budget of the join kernels' hash tables (0 = default 72)")
     ap.add_argument("--group-smem", type=int, choices=[0, 1], default=1,
                     help="FLS_TUNE_GROUP_SMEM: 1 = per-CTA group sums in shared memory, 0 = a global atomic per row")
     ap.add_argument("--mixed-columns", type=int, default=64, help="mixed workload: number of columns")
@@ -220,6 +222,7 @@ def run_ours(a, dist: Dist):
     ops.set_tuning(2, a.group_smem)
     if a.late_measure is not None:
         ops.set_tuning(3, a.late_measure)
+    ops.set_tuning(4, a.table_kb)
     from fastlanesgpu_b200.shard import allreduce_sum, combine_group_records, shard_seed
     seed = shard_seed(1000, dist.rank)
     # ---------------------------------------------------------------- setup
@@ -303,7 +306,8 @@ def run_ours(a, dist: Dist):
         from fastlanesgpu_b200 import autotune
         if a.tune_joins:
             # the library's autotuner picks each join's variants (late or
-            # staged measures, group sums per CTA or per row) by timing them,
+            # staged measures, group sums per CTA or per row, shared-memory
+            # budget of the hash tables) by timing them,
             # before the timed region; the step applies each query's choice
             for name, dq, o, w in suite:
                 if dq["kind"] == "join":
@@ -519,7 +523,7 @@ def run_ours(a, dist: Dist):
         "gpu_launches": int(launches),
         "launch_config": dict(zip(["warps", "stages", "ctas_per_sm", "tile_bytes"], ops.get_launch_config()),
                               sparse_rows=ops.get_tuning(0), jit=ops.get_tuning(1), group_smem=ops.get_tuning(2),
-                              late_measure=ops.get_tuning(3),
+                              late_measure=ops.get_tuning(3), table_kb=ops.get_tuning(4),
                               jit_launches=int(ops.jit_stats()["launches"])),
         "clocks": clk,
     }

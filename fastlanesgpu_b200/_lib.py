@@ -22,7 +22,7 @@ SCHEME_NAMES = ["FOR", "DELTA", "RLE", "CONST", "DICT"]
 LAYOUT_NORMAL, LAYOUT_TRANSPOSED = 0, 1
 ORDER_STORED, ORDER_ORIGINAL = 0, 1
 MAX_QUERY_COLS, MAX_FILTERS, MAX_PROBES = 8, 4, 4
-TUNE_SPARSE_ROWS, TUNE_JIT, TUNE_GROUP_SMEM, TUNE_LATE_MEASURE = 0, 1, 2, 3
+TUNE_SPARSE_ROWS, TUNE_JIT, TUNE_GROUP_SMEM, TUNE_LATE_MEASURE, TUNE_TABLE_KB = 0, 1, 2, 3, 4
 MLP_IN, MLP_HIDDEN, MLP_OUT = 16, 64, 5
 MLP_N_PARAMS = 64 * 16 + 64 + 64 * 64 + 64 + 5 * 64 + 5
 

@@ -4,7 +4,8 @@ variants.
 Sweeps warps per CTA, pipeline stages, tile bytes (vectors per staged tile)
 and the dense/row-at-a-time threshold for a workload (DEFAULT_SPACE), or the
 join kernels' choices that depend on the query's selectivity -- measure
-columns staged or read late, group sums per CTA or per row (JOIN_SPACE) --,
+columns staged or read late, group sums per CTA or per row, how much shared
+memory the hash tables take from the staged vectors (JOIN_SPACE) --,
 times each candidate with CUDA events after warm-up, keeps the fastest and
 caches it in a JSON file keyed by the workload's signature (default
 ~/.cache/fastlanesgpu_b200/autotune.json, or $FLS_AUTOTUNE_CACHE).  Results
@@ -29,9 +30,10 @@ DEFAULT_SPACE = {
 JOIN_SPACE = {
     "late_measure": [0, 1],
     "group_smem": [1, 0],
+    "table_kb": [72, 144],
 }
 
-_TUNING = {"sparse_rows": 0, "group_smem": 2, "late_measure": 3}
+_TUNING = {"sparse_rows": 0, "group_smem": 2, "late_measure": 3, "table_kb": 4}
 
 
 def cache_path() -> str:
@@ -105,3 +107,4 @@ def reset() -> None:
     ops.set_tuning(0, 0)
     ops.set_tuning(2, 1)
     ops.set_tuning(3, 0)
+    ops.set_tuning(4, 0)

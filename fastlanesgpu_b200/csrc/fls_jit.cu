@@ -456,8 +456,9 @@ bool jit_probe_shape(const fls_join_groupby_desc* d, JitProbeShape& sh) {
 	// direct when base + [0, 2^bw) - keys_min lies in [0, len).
 	uint32_t kinds = 0, in_smem = 0, pbit = 0, direct = 0;
 	sh.cta_words   = 0;
-	auto place     = [&](uint64_t words, uint32_t q) {
-        if (sh.cta_words + words > kJitTableWords) { return false; }
+	const uint32_t budget = tuning_table_words();
+	auto           place  = [&](uint64_t words, uint32_t q) {
+        if (sh.cta_words + words > budget) { return false; }
         sh.smem_off[q] = sh.cta_words;
         sh.cta_words += static_cast<uint32_t>((words + 3u) & ~3ull);
         return true;

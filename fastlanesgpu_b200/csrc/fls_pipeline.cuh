@@ -299,6 +299,7 @@ int        tuning_sparse_rows();
 int        tuning_jit();
 int        tuning_group_smem();
 int        tuning_late_measure();
+uint32_t   tuning_table_words(); // table budget in 4-byte words
 uint32_t   jit_max_warps(); // most warps per CTA of the specialised join kernels
 
 // Validates one column descriptor and converts it for a kernel.
@@ -329,7 +330,9 @@ fls_status jit_filter_agg(const fls_column* cols, const fls_filter* filters, uin
 
 // Probe + group-by shapes: staged columns (probe keys in probe order, then the
 // measure column if no probe reads it), which tables live in shared memory.
-constexpr uint32_t kJitTableWords = 72u * 1024u / 4u; // shared-memory budget for hash tables
+constexpr uint32_t kJitTableKB    = 72u;  // default shared-memory budget for hash tables
+constexpr uint32_t kJitMaxTableKB = 144u; // largest budget: 144 KB of tables + 24 KB of group slots
+                                          // leave room for one warp of the widest staged row
 constexpr uint32_t kJitGroupSlots = 2048u;            // most group-sum slots per CTA in shared memory
 struct JitProbeShape {
 	uint32_t    staged[FLS_MAX_QUERY_COLS];

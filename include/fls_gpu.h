@@ -501,7 +501,15 @@ typedef enum fls_tune_param {
 	 * (aggregated and subtracted) in global memory and read their fields for
 	 * the selected rows only, instead of staging them whole with the probe
 	 * columns.  0 (default): staged.  Results are identical either way. */
-	FLS_TUNE_LATE_MEASURE = 3
+	FLS_TUNE_LATE_MEASURE = 3,
+	/* Shared-memory budget, in KB, of the specialised join kernels' hash
+	 * tables (PHT_1 as bitmaps, PHT_2 verbatim or as presence bitmaps, placed
+	 * in probe order while they fit; the others are probed in global memory).
+	 * A larger budget keeps more tables on chip and leaves less room for the
+	 * staged vectors, so fewer warps per CTA.  Default 72; 0 restores it; at
+	 * most 144.  fls_join_workspace_bytes depends on it.  Results are
+	 * identical either way. */
+	FLS_TUNE_TABLE_KB = 4
 } fls_tune_param;
 fls_status fls_set_tuning(uint32_t param, int64_t value);
 fls_status fls_get_tuning(uint32_t param, int64_t* value);

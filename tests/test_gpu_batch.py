@@ -105,7 +105,7 @@ def test_autotuner_picks_and_caches(cuda, tmp_path):
 
 def test_autotuner_join_space(cuda, oracle, tmp_path):
     """JOIN_SPACE picks the join kernel's variants for one query (late
-    measures, group sums per CTA) by timing them; every candidate gives the
+    measures, group sums per CTA, table budget) by timing them; every candidate gives the
     oracle's records, and the choice is applied and cached."""
     from fastlanesgpu_b200 import autotune, datagen
     from test_gpu_ssb_suite import ssb_want
@@ -118,8 +118,9 @@ def test_autotuner_join_space(cuda, oracle, tmp_path):
     path = str(tmp_path / "tune.json")
     try:
         best = autotune.tune("q43-test", run, space=autotune.JOIN_SPACE, iters=2, path=path)
-        assert len(best["candidates"]) == 4 and set(best["config"]) == {"late_measure", "group_smem"}
+        assert len(best["candidates"]) == 8 and set(best["config"]) == {"late_measure", "group_smem", "table_kb"}
         assert ops.get_tuning(3) == best["config"]["late_measure"]
+        assert ops.get_tuning(4) == best["config"]["table_kb"]
         assert all(np.array_equal(g.cpu().numpy(), want) for g in got)
         again = autotune.tune("q43-test", run, space=autotune.JOIN_SPACE, iters=2, path=path)
         assert again["config"] == best["config"]

@@ -2,12 +2,13 @@
 seeded SSB-shaped schema, through the library's two query operators: the
 hash tables built on the device with the queries' dimension predicates equal
 the oracle's builds, and every result equals the oracle's loop, with the
-specialised and the general kernels."""
+specialised and the general kernels, with measures staged or read late and
+with the default and the largest shared-memory budget for the tables."""
 import numpy as np
 import pytest
 
 from fastlanesgpu_b200 import EncodedColumn, datagen, ops
-from fastlanesgpu_b200._lib import TUNE_JIT, TUNE_LATE_MEASURE
+from fastlanesgpu_b200._lib import TUNE_JIT, TUNE_LATE_MEASURE, TUNE_TABLE_KB
 
 pytestmark = pytest.mark.gpu
 
@@ -60,9 +61,10 @@ def test_ssb_query_against_oracle(ssb_data, oracle, name):
     t, dcols = ssb_data
     want, tables = ssb_want(oracle, name, t)
     try:
-        for jit, late in ((1, 0), (1, 1), (0, 0)):
+        for jit, late, table_kb in ((1, 0, 0), (1, 1, 0), (1, 0, 144), (1, 1, 144), (0, 0, 0)):
             ops.set_tuning(TUNE_JIT, jit)
             ops.set_tuning(TUNE_LATE_MEASURE, late)
+            ops.set_tuning(TUNE_TABLE_KB, table_kb)
             before = ops.jit_stats()["launches"]
             got, dq = ssb_run(name, t, dcols)
             assert ops.jit_stats()["launches"] - before == jit, (name, jit)
@@ -75,4 +77,5 @@ def test_ssb_query_against_oracle(ssb_data, oracle, name):
     finally:
         ops.set_tuning(TUNE_JIT, 1)
         ops.set_tuning(TUNE_LATE_MEASURE, 0)
+        ops.set_tuning(TUNE_TABLE_KB, 0)
     assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()

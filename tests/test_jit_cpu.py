@@ -131,3 +131,33 @@ def test_join_workspace_bytes():
         assert ops.join_workspace_bytes(cols, probes, **kw) == 0
     finally:
         ops.set_tuning(TUNE_JIT, 1)
+
+
+def test_table_budget_tuning():
+    """FLS_TUNE_TABLE_KB bounds the shared memory of the join kernels' tables
+    (default 72 KB, at most 144, 0 restores the default).  Q2.1 over the SSB
+    schema (supplier PHT_1 of 2^17 slots, part PHT_2 of 2^19, date PHT_2 of
+    2556): at 72 KB the supplier bitmap (4096 words) and the date table
+    verbatim (5112) sit on chip and the part table stays in global memory; at
+    144 KB the part presence bitmap (16384) sits between them, the workspace
+    covers all three, and the kernel for that placement compiles."""
+    from fastlanesgpu_b200._lib import TUNE_TABLE_KB
+    assert ops.get_tuning(TUNE_TABLE_KB) == 72
+    for bad in (-1, 145):
+        with pytest.raises(FlsError):
+            ops.set_tuning(TUNE_TABLE_KB, bad)
+    bits = datagen.SSB_BITS
+    cols = [_col(bits[k]) for k in ("lo_suppkey", "lo_partkey", "lo_orderdate", "lo_revenue")]
+    probes = [(0, 0x200000, 1 << 17, 0, 1), (1, 0x400000, 1 << 19, 0, 2), (2, 0x800000, datagen.N_DAYS, 0, 2)]
+    kw = dict(agg_col=3, keys=[(1, 7, 1), (2, 1, 0)], group_sub=1992, n_groups=7000, res_stride=4, sum_slot=2)
+    try:
+        assert ops.join_workspace_bytes(cols, probes, **kw) == 4 * (4096 + 5112)
+        ops.set_tuning(TUNE_TABLE_KB, 144)
+        assert ops.get_tuning(TUNE_TABLE_KB) == 144
+        assert ops.join_workspace_bytes(cols, probes, **kw) == 4 * (4096 + 16384 + 5112)
+        ops.jit_precompile_join(cols, probes, **kw)
+        assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
+        ops.set_tuning(TUNE_TABLE_KB, 0)
+        assert ops.get_tuning(TUNE_TABLE_KB) == 72
+    finally:
+        ops.set_tuning(TUNE_TABLE_KB, 0)
