@@ -128,7 +128,8 @@ struct FilterQuery : Shape<LAYOUT, BWS...> {
 // for shared memory has its presence bitmap there (a slot hits when its 64-bit
 // entry is not zero), its payloads stay in global memory; DIRECT bit q: the
 // host proved every key of probe q's column lands in [keys_min, keys_min +
-// len) (from the column's base and bit width), so its slot is key - keys_min.
+// len) (from the column's base and bit width), so its slot is key - keys_min;
+// DIRECT bit 8 + q: also base == keys_min, so the slot is the packed field.
 // GSM: each CTA sums its groups in a direct-mapped cache of group-sum slots
 // in shared memory (a group claims its slot, or else adds to its record
 // directly) and adds the slots' non-zero sums to the records once, at its end.
@@ -148,6 +149,9 @@ struct ProbeQuery : Shape<LAYOUT, BWS...> {
 	// Probes whose hit test reads shared memory only (or a PHT_1 array).
 	__host__ __device__ static constexpr bool dense_ok(int q) { return !pht2(q) || in_smem(q) || pbit(q); }
 	__host__ __device__ static constexpr bool direct(int q) { return (DIRECT >> q) & 1; }
+	__host__ __device__ static constexpr bool field_slot(int q) { return direct(q) && ((DIRECT >> (8 + q)) & 1); }
+	// Probes whose hit test is one bit of a shared-memory bitmap.
+	__host__ __device__ static constexpr bool smem_bits(int q) { return (in_smem(q) && !pht2(q)) || pbit(q); }
 	static_assert(NP >= 1 && NP <= FLS_MAX_PROBES, "1..4 probes");
 	static_assert(NS >= NP && NS <= static_cast<int>(sizeof...(BWS)) && static_cast<int>(sizeof...(BWS)) - NS <= 2,
 	              "probe columns staged; at most two columns in global memory");
@@ -479,12 +483,22 @@ __device__ __forceinline__ void dense_probes(const ProbeParams& P, const uint32_
 		const uint32_t kb  = P.base[q] - static_cast<uint32_t>(P.kmin[q]);
 		const int32_t  len = P.len[q];
 		uint32_t       hit[4] = {0, 0, 0, 0};
-		dev::unpack_rows<Q::bw(q)>(V.template col<q>(), lane, [&](int r, uint32_t x) {
-			uint32_t   h;
-			const bool ok = hash_slot<Q::direct(q)>(x + kb, len, h, P.S.err);
-			const bool b  = ok & table_hit<Q, q>(P, tables, h);
-			hit[r & 3] |= (b ? 1u : 0u) << r;
-		});
+		if constexpr (Q::direct(q) && Q::smem_bits(q)) {
+			// slot h's bit: word h / 32, shifted right by h mod 32 (the funnel
+			// shift takes the amount mod 32), moved to bit r
+			const uint32_t* bm = tables + P.smem_off[q];
+			dev::unpack_rows<Q::bw(q)>(V.template col<q>(), lane, [&](int r, uint32_t x) {
+				const uint32_t h = Q::field_slot(q) ? x : x + kb;
+				hit[r & 3] |= (__funnelshift_r(bm[h >> 5], 0u, h) << r) & (1u << r);
+			});
+		} else {
+			dev::unpack_rows<Q::bw(q)>(V.template col<q>(), lane, [&](int r, uint32_t x) {
+				uint32_t   h;
+				const bool ok = hash_slot<Q::direct(q)>(x + kb, len, h, P.S.err);
+				const bool b  = ok & table_hit<Q, q>(P, tables, h);
+				hit[r & 3] |= (b ? 1u : 0u) << r;
+			});
+		}
 		mask &= (hit[0] | hit[1]) | (hit[2] | hit[3]);
 		dense_probes<Q, q + 1>(P, tables, V, lane, mask, f0);
 	} else {

@@ -468,7 +468,7 @@ bool jit_probe_shape(const fls_join_groupby_desc* d, JitProbeShape& sh) {
 		const fls_column& kc = d->cols[p.col];
 		const int64_t     lo = static_cast<int64_t>(kc.base) - p.keys_min;
 		const int64_t     hi = lo + (kc.bw >= 32 ? (int64_t {1} << 32) : (int64_t {1} << kc.bw)) - 1;
-		if (kc.bw < 32 && lo >= 0 && hi < p.ht_len) { direct |= 1u << q; }
+		if (kc.bw < 32 && lo >= 0 && hi < p.ht_len) { direct |= (lo == 0 ? 0x101u : 1u) << q; }
 		const uint64_t bits_words = (static_cast<uint64_t>(p.ht_len) + 31u) / 32u;
 		sh.smem_off[q]            = 0;
 		if (p.kind == 1) {

@@ -357,6 +357,59 @@ def test_jit_probe_out_of_range_keys_flagged(jit_on):
     torch.cuda.synchronize()
 
 
+@pytest.mark.parametrize("late", [0, 1])
+def test_jit_row_phase_flags_only_rows_that_reach_the_probe(jit_on, late):
+    """In the row phase a key with a negative remainder at a later probe sets
+    the error word only when its row passed the probes before it, as in the
+    reference's probe chain (a rejected row reads no further table).  Probe 0, a PHT_2 of 2^14 slots kept in
+    global memory by a 1 KB table budget, rejects every third slot; probe 1's
+    keys (keys_min 100) are 50 on exactly the rows probe 0 rejects: no flag and
+    the restated records.  The same key on one row that probe 0 accepts: the
+    flag is set, and that row is dropped."""
+    import torch
+    from fastlanesgpu_b200 import FlsError
+    from fastlanesgpu_b200._lib import TUNE_LATE_MEASURE, TUNE_TABLE_KB
+    g = np.random.default_rng(4242)
+    n, l0, l1, ng = 8 * 1024 + 5, 1 << 14, 1000, 36
+    slots0 = np.arange(l0)
+    ht0 = np.zeros(2 * l0, np.int32)
+    present0 = slots0 % 3 != 0
+    ht0[0::2][present0] = 1 + slots0[present0]
+    ht0[1::2][present0] = slots0[present0] % 5
+    slots1 = np.arange(l1)
+    ht1 = np.zeros(2 * l1, np.int32)
+    present1 = g.random(l1) < 0.6
+    ht1[0::2][present1] = 1 + slots1[present1]
+    ht1[1::2][present1] = slots1[present1] % 7
+    k0 = g.integers(0, l0, n).astype(np.int32)
+    hit0 = present0[k0]
+    k1 = np.where(hit0, g.integers(100, 1100, n), 50).astype(np.int32)
+    measure = g.integers(-2**20, 2**20, n).astype(np.int32)
+    probes_np = [(0, ht0, l0, 0, 2), (1, ht1, l1, 100, 2)]
+    probes = [(q, torch.from_numpy(ht).cuda(), ln, kmin, kind) for q, ht, ln, kmin, kind in probes_np]
+    m_col = EncodedColumn.uniform(measure, bw=21, base=-2**20).to_device()
+    try:
+        ops.set_tuning(TUNE_TABLE_KB, 1)
+        ops.set_tuning(TUNE_LATE_MEASURE, late)
+        cols = [EncodedColumn.uniform(k0, bw=14).to_device(), EncodedColumn.uniform(k1, bw=11).to_device(), m_col]
+        want = _numpy_probe([k0, k1], measure, probes_np, None, 0, 1, 7, 0, ng)
+        got, used = _probe_run(cols, probes, 2, 0, 1, 7, 0, ng, jit=True)
+        assert used == 1 and np.array_equal(got, want)
+        k1b = k1.copy()
+        k1b[int(np.nonzero(hit0)[0][17])] = 50
+        cols[1] = EncodedColumn.uniform(k1b, bw=11).to_device()
+        want_b = _numpy_probe([k0, k1b], measure, probes_np, None, 0, 1, 7, 0, ng)
+        assert not np.array_equal(want_b, want)
+        got_b = ops.probe_groupby(cols, probes, 2, 0, 1, 7, 0, ng).cpu().numpy()
+        with pytest.raises(FlsError):
+            ops.check_device_error()
+        assert np.array_equal(got_b, want_b)
+    finally:
+        ops.set_tuning(TUNE_TABLE_KB, 0)
+        ops.set_tuning(TUNE_LATE_MEASURE, 0)
+    assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
+
+
 # ------------------------------------------------------------------ decode
 
 @pytest.mark.parametrize("bw", [0, 1, 3, 8, 13, 16, 24, 27, 28, 31, 32])
