@@ -57,11 +57,13 @@ def parse_args():
                     help="FLS_TUNE_JIT: 1 = kernel specialised to the query's shape, 0 = general kernel")
     ap.add_argument("--late-measure", type=int, choices=[0, 1], default=None,
                     help="FLS_TUNE_LATE_MEASURE: 1 = join measures read from global memory for selected rows only")
-    ap.add_argument("--tune-joins", type=int, choices=[0, 1], default=1,
-                    help="ssb workload: choose each join's variants with the autotuner (JOIN_SPACE) before timing")
+    ap.add_argument("--tune-joins", type=int, choices=[0, 1], default=None,
+                    help="join workloads (q21, q31, q41, each join of ssb): choose the join variants with the "
+                         "autotuner (JOIN_SPACE) before timing; default 1 unless --late-measure, --table-kb or "
+                         "--group-smem is given (ssb: always 1 by default)")
     ap.add_argument("--table-kb", type=int, default=0,
                     help="FLS_TUNE_TABLE_KB: shared-memory budget of the join kernels' hash tables (0 = default 72)")
-    ap.add_argument("--group-smem", type=int, choices=[0, 1], default=1,
+    ap.add_argument("--group-smem", type=int, choices=[0, 1], default=None,
                     help="FLS_TUNE_GROUP_SMEM: 1 = per-CTA group sums in shared memory, 0 = a global atomic per row")
     ap.add_argument("--mixed-columns", type=int, default=64, help="mixed workload: number of columns")
     ap.add_argument("--mixed-max-log", type=int, default=26, help="mixed workload: longest column is 2^this rows")
@@ -219,10 +221,13 @@ def run_ours(a, dist: Dist):
     if a.sparse_rows:
         ops.set_tuning(0, a.sparse_rows)
     ops.set_tuning(1, a.jit)
-    ops.set_tuning(2, a.group_smem)
+    if a.group_smem is not None:
+        ops.set_tuning(2, a.group_smem)
     if a.late_measure is not None:
         ops.set_tuning(3, a.late_measure)
     ops.set_tuning(4, a.table_kb)
+    explicit_variants = a.late_measure is not None or a.table_kb != 0 or a.group_smem is not None
+    tune_joins = a.tune_joins if a.tune_joins is not None else int(a.workload == "ssb" or not explicit_variants)
     from fastlanesgpu_b200.shard import allreduce_sum, combine_group_records, shard_seed
     seed = shard_seed(1000, dist.rank)
     # ---------------------------------------------------------------- setup
@@ -304,7 +309,7 @@ def run_ours(a, dist: Dist):
                 ops.join_groupby(dq["cols"], dq["probes"], out=res[o:o + w], **dq["kw"])
 
         from fastlanesgpu_b200 import autotune
-        if a.tune_joins:
+        if tune_joins:
             # the library's autotuner picks each join's variants (late or
             # staged measures, group sums per CTA or per row, shared-memory
             # budget of the hash tables) by timing them,
@@ -312,7 +317,8 @@ def run_ours(a, dist: Dist):
             for name, dq, o, w in suite:
                 if dq["kind"] == "join":
                     best = autotune.tune(f"ssb-{name}", lambda: run_query(dq, o, w), space=autotune.JOIN_SPACE,
-                                         iters=5, use_cache=False)
+                                         iters=10, use_cache=False, prefer=autotune.JOIN_DEFAULT, margin=0.02,
+                                         retime=3)
                     dq["tuned"] = best["config"]
             autotune.reset()
 
@@ -404,6 +410,14 @@ def run_ours(a, dist: Dist):
         workload = {"workload": f"decode {'to HBM' if a.decode_out == 'hbm' else 'fused with uint64 sum'}: {what}",
                     "rows_per_gpu": a.rows}
         metric_key = f"decode_{a.decode_out}_{key}"
+    if a.workload in ("q21", "q31", "q41") and tune_joins:
+        # the library's autotuner picks the join variants (late or staged
+        # measures, group sums per CTA or per row, shared-memory budget of
+        # the hash tables) by timing them, before the timed region
+        from fastlanesgpu_b200 import autotune
+        best = autotune.tune(f"{a.workload}-{a.rows}", step, space=autotune.JOIN_SPACE, iters=20, use_cache=False,
+                             prefer=autotune.JOIN_DEFAULT, margin=0.02, retime=3)
+        workload["join_variants"] = best["config"]
     comp_bytes = sum(c.nbytes for c in hcols)
     algo_bytes = comp_bytes + (out_bytes if a.workload == "decode" else 0)
     if a.workload == "ssb":

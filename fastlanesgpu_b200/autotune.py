@@ -74,9 +74,13 @@ def time_ms(fn, warmup: int = 3, iters: int = 10) -> float:
 
 
 def tune(signature: str, fn, space: dict | None = None, iters: int = 10, use_cache: bool = True,
-         path: str | None = None) -> dict:
+         path: str | None = None, prefer: dict | None = None, margin: float = 0.0, retime: int = 0) -> dict:
     """Best launch configuration for `fn` (a callable enqueueing the workload);
-    applies it and returns {config, ms, candidates}."""
+    applies it and returns {config, ms, candidates}.  retime > 0: the
+    `retime` fastest candidates (and `prefer`) are timed again, interleaved,
+    and ranked by the sum of both timings.  prefer: a configuration (usually
+    the library default) kept unless another is faster by more than
+    `margin` (a fraction), so timing noise does not move a workload off it."""
     path = path or cache_path()
     cache = _load(path) if use_cache else {}
     if use_cache and signature in cache:
@@ -88,9 +92,25 @@ def tune(signature: str, fn, space: dict | None = None, iters: int = 10, use_cac
     for combo in itertools.product(*[space[k] for k in keys]):
         cfg = dict(zip(keys, combo))
         apply(cfg)
-        results.append((time_ms(fn, iters=iters), cfg))
+        results.append([time_ms(fn, iters=iters), cfg])
     results.sort(key=lambda x: x[0])
-    best = {"config": results[0][1], "ms": results[0][0],
+    if retime > 0:
+        again = results[:retime] + [r for r in results[retime:] if prefer is not None and r[1] == prefer]
+        for r in again:
+            apply(r[1])
+            r[0] += time_ms(fn, iters=iters)
+        for r in results:
+            if r not in again:
+                r[0] *= 2.0
+        results.sort(key=lambda x: x[0])
+        for r in results:
+            r[0] /= 2.0
+    chosen = results[0]
+    if prefer is not None:
+        pref = next((r for r in results if r[1] == prefer), None)
+        if pref is not None and chosen[0] > pref[0] * (1.0 - margin):
+            chosen = pref
+    best = {"config": chosen[1], "ms": chosen[0],
             "candidates": [{"ms": m, **c} for m, c in results]}
     apply(best["config"])
     if use_cache:
@@ -99,6 +119,10 @@ def tune(signature: str, fn, space: dict | None = None, iters: int = 10, use_cac
         with open(path, "w") as f:
             json.dump(cache, f, indent=1)
     return best
+
+
+# The library's defaults for the JOIN_SPACE variants.
+JOIN_DEFAULT = {"late_measure": 0, "group_smem": 1, "table_kb": 72}
 
 
 def reset() -> None:

@@ -124,5 +124,12 @@ def test_autotuner_join_space(cuda, oracle, tmp_path):
         assert all(np.array_equal(g.cpu().numpy(), want) for g in got)
         again = autotune.tune("q43-test", run, space=autotune.JOIN_SPACE, iters=2, path=path)
         assert again["config"] == best["config"]
+        # re-timing the leaders and a preferred configuration no other beats
+        # by 100 %: the preferred one is kept and applied
+        kept = autotune.tune("q43-keep", run, space=autotune.JOIN_SPACE, iters=2, use_cache=False,
+                             prefer=autotune.JOIN_DEFAULT, margin=1.0, retime=2)
+        assert kept["config"] == autotune.JOIN_DEFAULT and len(kept["candidates"]) == 8
+        assert ops.get_tuning(3) == 0 and ops.get_tuning(2) == 1 and ops.get_tuning(4) == 72
+        assert all(np.array_equal(g.cpu().numpy(), want) for g in got)
     finally:
         autotune.reset()
