@@ -4,7 +4,7 @@ A 16-64-64-5 FP32 MLP, trained on the GPU by the library's own kernels
 (fls_mlp_gradients / fls_mlp_adam_step), reads 16 per-vector statistics
 (fls_vector_stats_gpu) and picks one of the five schemes for each 1024-value
 vector.  The exhaustive encoder (fls_encode_exhaustive: exact size of every
-scheme) produces the training labels, judges the selector's regret and is the
+scheme) produces the training labels, measures the selector's regret and is the
 fallback for vectors whose top softmax probability is below a threshold.  The
 encoder recomputes bit widths exactly for whatever scheme is picked, so the
 encoded data is lossless regardless of the pick.

@@ -201,7 +201,7 @@ uint64_t   fls_column_container_bytes(const fls_column* col);
 fls_status fls_column_write_container(const fls_column* col, void* out, uint64_t out_bytes, uint64_t* written);
 fls_status fls_column_open_container(const void* buf, uint64_t bytes, fls_column* col);
 
-/* Exhaustive per-vector encoder (the selector's judge): exact encoded size in
+/* Exhaustive per-vector encoder (the selector's labels and regret): exact encoded size in
  * bytes (payload + 16 B metadata) of every scheme for every vector
  * (sizes: n_vec*5, UINT32_MAX = not representable) and the argmin scheme, ties
  * broken by the measured decode-cost order CONST < FOR < DELTA < RLE < DICT. */
