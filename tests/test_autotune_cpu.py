@@ -61,3 +61,23 @@ def test_prefer_retimed_with_leaders(fake):
     assert fake["calls"].count((1, 0)) == 2 and fake["calls"].count((0, 0)) == 2
     # (0, 0): 0.8 + 0.8; prefer: 1.2 + 0.7 = 1.9 / 2 = 0.95; 0.8 > 0.95 * 0.8, so prefer is kept
     assert best["config"] == prefer
+
+
+def test_reset_restores_every_default():
+    """reset() puts back the library defaults of everything apply() can set:
+    launch shape, sparse-row threshold, group sums per CTA, late measures,
+    table budget (host-side settings, no GPU needed)."""
+    from fastlanesgpu_b200 import ops
+    before = (ops.get_launch_config(), [ops.get_tuning(p) for p in (0, 2, 3, 4)])
+    try:
+        autotune.apply({"warps": 8, "stages": 3, "tile_bytes": 2048, "sparse_rows": 12, "group_smem": 0,
+                        "late_measure": 1, "table_kb": 144})
+        assert ops.get_launch_config()[0] == 8 and ops.get_launch_config()[1] == 3
+        assert [ops.get_tuning(p) for p in (0, 2, 3, 4)] == [12, 0, 1, 144]
+        autotune.apply({"table_kb": 100})  # a partial configuration leaves the rest
+        assert [ops.get_tuning(p) for p in (0, 2, 3, 4)] == [12, 0, 1, 100]
+        autotune.reset()
+        assert [ops.get_tuning(p) for p in (0, 2, 3, 4)] == [4, 1, 0, 72]
+        assert (ops.get_launch_config(), [ops.get_tuning(p) for p in (0, 2, 3, 4)]) == before
+    finally:
+        autotune.reset()
