@@ -9,14 +9,16 @@
 // arrays); it has no encoded-data format, so this layout is this library's:
 //
 //   [payload: n_words x u32][zero pad to 16 B][meta: n_vec x fls_vec_meta]
-//   [footer: 80 B]
+//   [footer: 96 B]
 //
 // all little-endian.  The footer comes last (a reader finds it from the end),
 // holds the column descriptor, the metadata offset, CRC-32C checksums of the
-// payload and metadata bytes, a version and the magic "FLSCOLv1".  Opening a
-// container checks every field and every vector's metadata against the
-// payload before handing out a descriptor, so a damaged or hostile file is
-// refused on the host instead of reaching a kernel.
+// payload and metadata bytes and of the footer itself, a version and the
+// magic "FLSCOLv1".  Opening a container checks the three checksums, every
+// field and every vector's metadata against the payload before handing out a
+// descriptor, so a damaged or hostile file is refused on the host instead of
+// reaching a kernel (a damaged descriptor -- a FOR base, the layout, the row
+// count -- would otherwise decode to other values without any fault).
 #include <cstring>
 #include <mutex>
 
@@ -26,8 +28,8 @@ namespace fls {
 namespace {
 
 constexpr char     kMagic[8]    = {'F', 'L', 'S', 'C', 'O', 'L', 'v', '1'};
-constexpr uint32_t kVersion     = 1;
-constexpr uint64_t kFooterBytes = 80;
+constexpr uint32_t kVersion     = 2; // 1 had no footer checksum
+constexpr uint64_t kFooterBytes = 96;
 
 struct Footer {
 	uint64_t n_values;
@@ -39,6 +41,8 @@ struct Footer {
 	uint32_t max_vec_words, scheme_mask;
 	uint32_t has_meta;
 	uint32_t crc_words, crc_meta;
+	uint32_t crc_footer; // CRC-32C of the footer with this field zero
+	uint32_t reserved[3];
 	uint32_t version;
 	char     magic[8];
 };
@@ -140,6 +144,7 @@ fls_status fls_column_write_container(const fls_column* col, void* out, uint64_t
 	}
 	f.version = kVersion;
 	std::memcpy(f.magic, kMagic, sizeof(kMagic));
+	f.crc_footer = crc32c(&f, kFooterBytes);
 	std::memcpy(o + need - kFooterBytes, &f, kFooterBytes);
 	if (written) { *written = need; }
 	return FLS_OK;
@@ -160,9 +165,16 @@ fls_status fls_column_open_container(const void* buf, uint64_t bytes, fls_column
 	if (f.version != kVersion) {
 		return set_error(FLS_ERR_UNSUPPORTED, "container: version " + std::to_string(f.version) + " not supported");
 	}
+	{
+		Footer z          = f;
+		z.crc_footer      = 0;
+		if (crc32c(&z, kFooterBytes) != f.crc_footer) {
+			return set_error(FLS_ERR_INVALID_ARG, "container: footer checksum mismatch");
+		}
+	}
 	const uint64_t body = bytes - kFooterBytes;
 	if (f.n_values == 0 || f.n_vec != n_vectors(f.n_values) || f.n_words > body / 4u || f.layout > FLS_LAYOUT_TRANSPOSED ||
-	    f.has_meta > 1u) {
+	    f.has_meta > 1u || f.reserved[0] || f.reserved[1] || f.reserved[2]) {
 		return set_error(FLS_ERR_INVALID_ARG, "container: inconsistent column description");
 	}
 	const uint64_t pay_b = 4u * f.n_words;

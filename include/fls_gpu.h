@@ -188,12 +188,12 @@ fls_status fls_decode_u64(const uint64_t* d_in, uint64_t n, uint8_t bw, uint64_t
 
 /* Encoded-column container: the payload words and per-vector metadata of a
  * column with HOST pointers (data, meta) in one byte string --
- * [payload][zero pad to 16 B][metadata][80-byte footer: descriptor, CRC-32C
- * of payload and metadata, version, magic "FLSCOLv1"] -- so encoded columns
+ * [payload][zero pad to 16 B][metadata][96-byte footer: descriptor, CRC-32C
+ * of payload, metadata and footer, version 2, magic "FLSCOLv1"] -- so encoded columns
  * can be stored and read back without re-encoding.  The reference keeps raw
  * int32 columns on disk (crystal_ssb_utils.h:108-127 storeColumn /
  * loadColumn) and re-encodes them each run (compress_ssb.cu:357-454).
- * fls_column_open_container checks the footer, both checksums and every
+ * fls_column_open_container checks the footer, the three checksums and every
  * vector's metadata against the payload (FLS_ERR_INVALID_ARG if damaged,
  * FLS_ERR_UNSUPPORTED for another version) and fills `col` with pointers into
  * `buf` (16-byte aligned); copy data and meta to the device to query it. */

@@ -2,7 +2,7 @@
 fls_column_open_container) on the host: round trips of uniform and
 per-vector columns of every scheme, and refusal of damaged, truncated,
 foreign or inconsistent bytes -- including metadata that points outside the
-payload under valid checksums."""
+payload under valid checksums, and every single-bit change of the footer."""
 import struct
 
 import numpy as np
@@ -12,7 +12,8 @@ from fastlanesgpu_b200 import EncodedColumn, FlsError, datagen
 from fastlanesgpu_b200._lib import (LAYOUT_NORMAL, LAYOUT_TRANSPOSED, SCHEME_CONST, SCHEME_DELTA, SCHEME_DICT,
                                     SCHEME_FOR, SCHEME_RLE)
 
-FOOTER = 80
+FOOTER = 96
+CRC_FOOTER = 68  # footer offset of the footer's own checksum
 
 
 def _crc32c(data: bytes) -> int:
@@ -26,6 +27,14 @@ def _crc32c(data: bytes) -> int:
     for byte in data:
         c = table[(c ^ byte) & 0xFF] ^ (c >> 8)
     return c ^ 0xFFFFFFFF
+
+
+def _reseal(d: bytearray):
+    """Recomputes the footer checksum after a deliberate change of a footer
+    field, so the open reaches the checks behind it."""
+    foot = len(d) - FOOTER
+    struct.pack_into("<I", d, foot + CRC_FOOTER, 0)
+    struct.pack_into("<I", d, foot + CRC_FOOTER, _crc32c(bytes(d[foot:])))
 
 
 def _same(a: EncodedColumn, b: EncodedColumn):
@@ -88,7 +97,7 @@ def test_damaged_bytes_are_refused():
     d[-8:] = b"NOTACOL!"
     _refused(d, 1, "magic")
     d = bytearray(b)
-    d[-12:-8] = struct.pack("<I", 2)          # version field of the footer
+    d[-12:-8] = struct.pack("<I", 1)          # version field of the footer (1: no footer checksum)
     _refused(d, 7, "version")
 
 
@@ -110,6 +119,7 @@ def test_metadata_outside_payload_is_refused_despite_checksums():
         else:
             struct.pack_into("<H", d, rec + 14, value)
         struct.pack_into("<I", d, foot + 64, _crc32c(bytes(d[meta_off: meta_off + 16 * n_vec])))
+        _reseal(d)
         _refused(d, 1, "vector")
 
 
@@ -119,10 +129,52 @@ def test_inconsistent_description_is_refused():
     foot = len(b) - FOOTER
     d = bytearray(b)
     struct.pack_into("<I", d, foot + 40, 30)           # bit width larger than the payload holds
+    _reseal(d)
     _refused(d, 1, "uniform")
     d = bytearray(b)
     struct.pack_into("<Q", d, foot + 0, 10 ** 7)       # rows the payload does not hold
+    _reseal(d)
     _refused(d, 1)
     d = bytearray(b)
     struct.pack_into("<I", d, foot + 32, 5)            # layout
+    _reseal(d)
     _refused(d, 1)
+    d = bytearray(b)
+    struct.pack_into("<I", d, foot + 72, 1)            # reserved word
+    _reseal(d)
+    _refused(d, 1, "inconsistent")
+
+
+@pytest.mark.parametrize("uniform", [True, False])
+def test_every_footer_bit_flip_is_refused(uniform):
+    """A damaged descriptor would decode to other values without any fault
+    (a FOR base, the layout, the row count), so the footer carries its own
+    checksum: each of its 768 single-bit changes is refused."""
+    col = EncodedColumn.uniform(datagen.uniform_bits(3000, 9, seed=3), bw=9) if uniform else _per_vector()
+    b = col.to_bytes()
+    foot = len(b) - FOOTER
+    for bit in range(8 * FOOTER):
+        d = bytearray(b)
+        d[foot + bit // 8] ^= 1 << (bit % 8)
+        with pytest.raises(FlsError):
+            EncodedColumn.from_bytes(bytes(d))
+    d = bytearray(b)
+    struct.pack_into("<i", d, foot + 44, col.base + 1)  # the FOR base alone
+    _refused(d, 1, "footer checksum")
+
+
+def test_random_bit_flips_are_refused_or_harmless():
+    """Seeded single-bit changes anywhere in a per-vector container: refused,
+    or (in the zero padding between payload and metadata, which nothing
+    reads) the same column."""
+    col = _per_vector()
+    b = col.to_bytes()
+    g = np.random.default_rng(11)
+    for pos in g.integers(0, len(b), 400):
+        d = bytearray(b)
+        d[int(pos)] ^= 1 << int(g.integers(0, 8))
+        try:
+            got = EncodedColumn.from_bytes(bytes(d))
+        except FlsError:
+            continue
+        _same(col, got)
