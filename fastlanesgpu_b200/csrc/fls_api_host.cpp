@@ -29,6 +29,13 @@ fls_status set_error(fls_status st, const std::string& msg) {
 }
 void clear_error() { t_last_error.clear(); }
 
+fls_status check_n_values(uint64_t n, const char* who) {
+	if (n == 0 || n > FLS_MAX_VALUES) {
+		return set_error(FLS_ERR_INVALID_ARG, std::string(who) + ": the value count must be in 1..FLS_MAX_VALUES (2^40)");
+	}
+	return FLS_OK;
+}
+
 } // namespace fls
 
 using namespace fls;

@@ -524,6 +524,7 @@ fls_status fls_encode_column_gpu(const int32_t* d_values, uint64_t n, const uint
 	if (!d_values || !d_out || !d_meta || !d_info || !d_workspace || n == 0) {
 		return set_error(FLS_ERR_INVALID_ARG, "fls_encode_column_gpu: null pointer or n == 0");
 	}
+	if (fls_status s = check_n_values(n, "fls_encode_column_gpu"); s != FLS_OK) { return s; }
 	if (!d_schemes && scheme >= FLS_N_SCHEMES) { return set_error(FLS_ERR_INVALID_ARG, "fls_encode_column_gpu: bad scheme"); }
 	if (layout > FLS_LAYOUT_TRANSPOSED) { return set_error(FLS_ERR_INVALID_ARG, "fls_encode_column_gpu: bad layout"); }
 	if ((reinterpret_cast<uintptr_t>(d_out) | reinterpret_cast<uintptr_t>(d_meta)) & 15u) {
@@ -598,6 +599,7 @@ fls_status fls_encode_learned_gpu(const int32_t* d_values, uint64_t n, const flo
 	if (!d_values || !d_params || !d_info || !d_workspace || n == 0) {
 		return set_error(FLS_ERR_INVALID_ARG, "fls_encode_learned_gpu: null pointer or n == 0");
 	}
+	if (fls_status s = check_n_values(n, "fls_encode_learned_gpu"); s != FLS_OK) { return s; }
 	if (!(kappa >= 0.0)) { return set_error(FLS_ERR_INVALID_ARG, "fls_encode_learned_gpu: kappa must be >= 0"); }
 	if (workspace_bytes < fls_encode_learned_workspace_bytes(n) || (reinterpret_cast<uintptr_t>(d_workspace) & 255u)) {
 		return set_error(FLS_ERR_CAPACITY,

@@ -99,6 +99,34 @@ fls_status check_vectors(const fls_vec_meta* meta, uint64_t n_vec, uint64_t n_wo
 	return FLS_OK;
 }
 
+// The column description a container may hold, checked by the writer before
+// any byte is written and by the reader before a descriptor is handed out, so
+// a column that one refuses the other refuses too.  Sizes are compared by
+// division: n_values is capped at FLS_MAX_VALUES, and no product of a count
+// and a vector size is formed that could wrap.
+fls_status check_description(uint64_t n_values, uint64_t n_words, uint32_t layout, uint32_t scheme, uint32_t bw,
+                             const fls_vec_meta* meta, uint32_t max_vec_words, uint32_t scheme_mask) {
+	if (n_values == 0 || n_values > FLS_MAX_VALUES || layout > FLS_LAYOUT_TRANSPOSED) {
+		return set_error(FLS_ERR_INVALID_ARG, "container: inconsistent column description (row count or layout)");
+	}
+	const uint64_t n_vec = n_vectors(n_values);
+	if (meta) {
+		if (max_vec_words > kMaxVecWords) {
+			return set_error(FLS_ERR_INVALID_ARG, "container: largest vector payload out of range");
+		}
+		return check_vectors(meta, n_vec, n_words, max_vec_words, scheme_mask);
+	}
+	if ((scheme != FLS_SCHEME_FOR && scheme != FLS_SCHEME_DELTA) || bw > 32 ||
+	    (scheme == FLS_SCHEME_DELTA && layout != FLS_LAYOUT_TRANSPOSED)) {
+		return set_error(FLS_ERR_INVALID_ARG, "container: bad uniform column (scheme, bit width or layout)");
+	}
+	const uint64_t per = scheme == FLS_SCHEME_FOR ? 32u * bw : 32u + 32u * bw;
+	if (per != 0 && n_vec > n_words / per) {
+		return set_error(FLS_ERR_INVALID_ARG, "container: uniform column larger than its payload");
+	}
+	return FLS_OK;
+}
+
 } // namespace
 } // namespace fls
 
@@ -110,16 +138,17 @@ uint64_t fls_column_container_bytes(const fls_column* col) { return col ? contai
 
 fls_status fls_column_write_container(const fls_column* col, void* out, uint64_t out_bytes, uint64_t* written) {
 	if (!col || !out || !col->data) { return set_error(FLS_ERR_INVALID_ARG, "fls_column_write_container: null pointer"); }
-	if (col->n_values == 0) { return set_error(FLS_ERR_INVALID_ARG, "fls_column_write_container: empty column"); }
+	if (col->n_values == 0 || col->n_values > FLS_MAX_VALUES || col->n_words > (UINT64_MAX >> 4)) {
+		return set_error(FLS_ERR_INVALID_ARG, "fls_column_write_container: empty column or more than FLS_MAX_VALUES rows");
+	}
 	const uint64_t need = container_bytes(*col);
 	if (out_bytes < need) {
 		return set_error(FLS_ERR_CAPACITY, "fls_column_write_container: output smaller than fls_column_container_bytes");
 	}
+	fls_status s = check_description(col->n_values, col->n_words, col->layout, col->scheme, col->bw, col->meta,
+	                                 col->max_vec_words, col->scheme_mask);
+	if (s != FLS_OK) { return s; }
 	const uint64_t n_vec = n_vectors(col->n_values);
-	if (col->meta) {
-		fls_status s = check_vectors(col->meta, n_vec, col->n_words, col->max_vec_words, col->scheme_mask);
-		if (s != FLS_OK) { return s; }
-	}
 	uint8_t*       o     = static_cast<uint8_t*>(out);
 	const uint64_t pay_b = 4u * col->n_words;
 	std::memcpy(o, col->data, pay_b);
@@ -173,8 +202,8 @@ fls_status fls_column_open_container(const void* buf, uint64_t bytes, fls_column
 		}
 	}
 	const uint64_t body = bytes - kFooterBytes;
-	if (f.n_values == 0 || f.n_vec != n_vectors(f.n_values) || f.n_words > body / 4u || f.layout > FLS_LAYOUT_TRANSPOSED ||
-	    f.has_meta > 1u || f.reserved[0] || f.reserved[1] || f.reserved[2]) {
+	if (f.n_values == 0 || f.n_values > FLS_MAX_VALUES || f.n_vec != n_vectors(f.n_values) || f.n_words > body / 4u ||
+	    f.layout > FLS_LAYOUT_TRANSPOSED || f.has_meta > 1u || f.reserved[0] || f.reserved[1] || f.reserved[2]) {
 		return set_error(FLS_ERR_INVALID_ARG, "container: inconsistent column description");
 	}
 	const uint64_t pay_b = 4u * f.n_words;
@@ -188,18 +217,12 @@ fls_status fls_column_open_container(const void* buf, uint64_t bytes, fls_column
 	}
 	if (crc32c(b, pay_b) != f.crc_words) { return set_error(FLS_ERR_INVALID_ARG, "container: payload checksum mismatch"); }
 	const fls_vec_meta* meta = f.has_meta ? reinterpret_cast<const fls_vec_meta*>(b + f.meta_offset) : nullptr;
-	if (meta) {
-		if (crc32c(meta, 16u * f.n_vec) != f.crc_meta) {
-			return set_error(FLS_ERR_INVALID_ARG, "container: metadata checksum mismatch");
-		}
-		fls_status s = check_vectors(meta, f.n_vec, f.n_words, f.max_vec_words, f.scheme_mask);
-		if (s != FLS_OK) { return s; }
-	} else {
-		const uint64_t per = f.scheme == FLS_SCHEME_FOR ? 32u * f.bw : 32u + 32u * f.bw;
-		if ((f.scheme != FLS_SCHEME_FOR && f.scheme != FLS_SCHEME_DELTA) || f.bw > 32 || per * f.n_vec > f.n_words) {
-			return set_error(FLS_ERR_INVALID_ARG, "container: bad uniform column (scheme, bit width or size)");
-		}
+	if (meta && crc32c(meta, 16u * f.n_vec) != f.crc_meta) {
+		return set_error(FLS_ERR_INVALID_ARG, "container: metadata checksum mismatch");
 	}
+	fls_status s = check_description(f.n_values, f.n_words, f.layout, f.scheme, f.bw, meta, f.max_vec_words,
+	                                 f.scheme_mask);
+	if (s != FLS_OK) { return s; }
 	fls_column c {};
 	c.data          = reinterpret_cast<const uint32_t*>(b);
 	c.meta          = meta;

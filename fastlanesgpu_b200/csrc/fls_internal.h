@@ -28,6 +28,9 @@ void     scheme_sizes(const int32_t* v, uint32_t* size5);
 uint8_t  best_scheme(const uint32_t* size5);
 void     vector_stats(const int32_t* v, float* f16);
 
+// FLS_ERR_INVALID_ARG unless 0 < n <= FLS_MAX_VALUES (`who` names the caller).
+fls_status check_n_values(uint64_t n, const char* who);
+
 // Largest payload of one vector in words (DICT with 1024 distinct 32-bit values).
 constexpr uint32_t kMaxVecWords = 32u * 10u + 1024u;
 

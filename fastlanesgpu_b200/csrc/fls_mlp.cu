@@ -384,6 +384,7 @@ extern "C" {
 
 fls_status fls_vector_stats_gpu(const int32_t* d_values, uint64_t n, float* d_stats, fls_stream_t stream) {
 	if (!d_values || !d_stats || n == 0) { return set_error(FLS_ERR_INVALID_ARG, "fls_vector_stats_gpu: bad arguments"); }
+	if (fls_status s = check_n_values(n, "fls_vector_stats_gpu"); s != FLS_OK) { return s; }
 	DeviceInfo di;
 	fls_status s = device_info(di);
 	if (s != FLS_OK) { return s; }

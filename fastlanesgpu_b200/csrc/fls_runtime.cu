@@ -112,7 +112,7 @@ fls_status make_devcol(const fls_column& c, DevCol& d) {
 		return set_error(FLS_ERR_ALIGNMENT, "column metadata must be 16-byte aligned");
 	}
 	if (c.layout > FLS_LAYOUT_TRANSPOSED) { return set_error(FLS_ERR_INVALID_ARG, "bad column layout"); }
-	if (c.n_values == 0) { return set_error(FLS_ERR_INVALID_ARG, "column has no values"); }
+	if (fls_status s = check_n_values(c.n_values, "column"); s != FLS_OK) { return s; }
 	d.data    = c.data;
 	d.meta    = c.meta;
 	d.n_words = c.n_words;
@@ -132,7 +132,7 @@ fls_status make_devcol(const fls_column& c, DevCol& d) {
 		d.slot_words         = dev::payload_words(c.scheme, c.bw, 0);
 		d.vec_words          = d.slot_words;
 		const uint64_t n_vec = (c.n_values + 1023u) / 1024u;
-		if (static_cast<uint64_t>(d.slot_words) * n_vec > c.n_words) {
+		if (d.slot_words != 0 && n_vec > c.n_words / d.slot_words) {
 			return set_error(FLS_ERR_CAPACITY, "column data smaller than n_values at this bit width");
 		}
 	} else {

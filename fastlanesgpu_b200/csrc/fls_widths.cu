@@ -189,6 +189,7 @@ fls_status launch_decode(uint32_t bits, const void* d_in, uint64_t n, uint8_t bw
 		return set_error(FLS_ERR_INVALID_ARG, std::string(who) + ": null pointer, n == 0 or no output");
 	}
 	if (bw > bits) { return set_error(FLS_ERR_BAD_BW, std::string(who) + ": bit width larger than the values"); }
+	if (fls_status s = check_n_values(n, who); s != FLS_OK) { return s; }
 	if ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) & 15u) {
 		return set_error(FLS_ERR_ALIGNMENT, std::string(who) + ": buffers must be 16-byte aligned");
 	}

@@ -75,6 +75,11 @@ typedef struct fls_vec_meta {
 	uint16_t aux;    /* RLE: number of runs; DICT: dictionary size        */
 } fls_vec_meta;
 
+/* Largest column the library accepts: 2^40 values (2^30 vectors).  Larger
+ * counts are refused with FLS_ERR_INVALID_ARG before any size arithmetic, so
+ * that vector counts and payload sizes derived from n_values cannot wrap. */
+#define FLS_MAX_VALUES (1ull << 40)
+
 /* An encoded column resident in device memory.  With meta == NULL the column
  * is "uniform" like the reference's (one scheme/bw/base for all vectors,
  * vector v at word 32*bw*v for FOR, (32+32*bw)*v for DELTA). */
@@ -407,6 +412,9 @@ fls_status fls_mlp_gradients(const float* d_params, const float* d_x, const uint
  *   - batch > FLS_MLP_STATIC_MAX_BATCH returns FLS_ERR_CAPACITY (nothing runs).
  *   - The first call on a device looks up the array's device address (with
  *     that device current); make that first call before any stream capture.
+ *     The address is kept for the life of the process: resetting the device
+ *     (cudaDeviceReset, or a reset of its primary context) after that first
+ *     call is not supported, since the array may then live elsewhere.
  *   - It calls no cudaMalloc / cudaFree.  All calls share the one array: each
  *     call writes every scratch element it later reads, so nothing carries
  *     over between calls, but calls that overlap on the GPU (other streams,

@@ -145,6 +145,40 @@ def test_inconsistent_description_is_refused():
     _refused(d, 1, "inconsistent")
 
 
+def test_row_count_that_would_wrap_is_refused():
+    """A resealed footer whose row count makes (vector count x words per
+    vector) wrap modulo 2^64 -- a uniform 32-bit DELTA column of about 1.8e19
+    rows -- is refused (the library caps columns at FLS_MAX_VALUES = 2^40
+    rows and compares sizes by division), as is a row count at the cap that
+    the payload does not hold."""
+    col = EncodedColumn.uniform(datagen.sorted_geometric(4096, seed=1), SCHEME_DELTA, layout=LAYOUT_TRANSPOSED)
+    assert col.bw <= 32
+    b = bytearray(col.to_bytes())
+    foot = len(b) - FOOTER
+    struct.pack_into("<I", b, foot + 40, 32)              # bit width 32: 1056 words per vector
+    n_vec = (1 << 64) // 1056 + 1                          # n_vec * 1056 wraps to a few words
+    assert (n_vec * 1056) % (1 << 64) < 4096 and n_vec * 1024 < (1 << 64)
+    for n_values, vec in ((n_vec * 1024, n_vec), (1 << 40, 1 << 30), ((1 << 40) + 1, (1 << 30) + 1)):
+        d = bytearray(b)
+        struct.pack_into("<Q", d, foot + 0, n_values)
+        struct.pack_into("<Q", d, foot + 16, vec)
+        _reseal(d)
+        _refused(d, 1)
+
+
+def test_writer_refuses_what_the_reader_refuses():
+    """The writer checks the same column description as the reader before
+    writing any byte: a uniform DELTA column in the normal layout, a bit
+    width above 32 and a payload too small for the rows are refused at write
+    time."""
+    for field, value in (("layout", LAYOUT_NORMAL), ("bw", 33), ("n_values", 10 ** 6)):
+        col = EncodedColumn.uniform(datagen.sorted_geometric(4096, seed=1), SCHEME_DELTA, layout=LAYOUT_TRANSPOSED)
+        setattr(col, field, value)
+        with pytest.raises(FlsError) as e:
+            col.to_bytes()
+        assert e.value.status == 1 and "container" in str(e.value)
+
+
 @pytest.mark.parametrize("uniform", [True, False])
 def test_every_footer_bit_flip_is_refused(uniform):
     """A damaged descriptor would decode to other values without any fault
