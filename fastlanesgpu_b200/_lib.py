@@ -100,6 +100,7 @@ _VP = ctypes.c_void_p
 _SIGS = {
     "fls_last_error": (ctypes.c_char_p, []),
     "fls_check_device_error": (ctypes.c_int, [_VP]),
+    "fls_bind_error_word": (ctypes.c_int, [_VP, _VP]),
     "fls_pack_u32": (ctypes.c_int, [_VP, _VP, ctypes.c_uint8]),
     "fls_transpose_i_u32": (ctypes.c_int, [_VP, _VP]),
     "fls_untranspose_u32": (ctypes.c_int, [_VP, _VP]),

@@ -289,7 +289,7 @@ fls_status batch_launch(const fls_batch* b, const DevCol* cols, const fls_batch_
 	P.n_slots    = n_slots;
 	P.has_dict   = b->has_dict;
 	P.warps      = warps;
-	P.err        = device_error_word();
+	P.err        = device_error_word(st);
 	const uint64_t want = (b->items.size() + warps - 1) / warps;
 	const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>(want, static_cast<uint64_t>(di.sms) * ctas));
 	batch_kernel<<<grid, 32u * warps, 4ull * L.total * warps, st>>>(P);

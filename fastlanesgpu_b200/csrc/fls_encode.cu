@@ -554,7 +554,7 @@ fls_status fls_encode_column_gpu(const int32_t* d_values, uint64_t n, const uint
 	P.words   = static_cast<uint32_t*>(d_workspace);
 	P.bsum    = reinterpret_cast<uint64_t*>(static_cast<char*>(d_workspace) + ((4u * n_vec + 255u) & ~uint64_t {255u}));
 	P.info    = d_info;
-	P.err     = device_error_word();
+	P.err     = device_error_word(st);
 	const size_t smem = 4u * kEncWarps * kEncWarpWords;
 	{
 		static std::mutex mu;

@@ -370,7 +370,7 @@ fls_status jit_filter_agg(const fls_column* cols, const fls_filter* filters, uin
 	fls_status          s = device_info(di);
 	if (s != FLS_OK) { return s; }
 	if ((s = plan_fixed(di, sc, sh.n_staged, 0u, P.S, grid, smem)) != FLS_OK) { return s; }
-	P.S.err = device_error_word();
+	P.S.err = device_error_word(stream);
 	for (uint32_t i = 0; i < sh.n_staged; ++i) { P.base[i] = static_cast<uint32_t>(sc[i].base); }
 	for (uint32_t f = 0; f < n_filters; ++f) {
 		P.lo[f]    = static_cast<uint32_t>(filters[f].lo);
@@ -541,7 +541,7 @@ fls_status jit_probe_groupby(const fls_join_groupby_desc* d, int32_t* d_res, int
 	fls_status         s = device_info(di);
 	if (s != FLS_OK) { return s; }
 	if ((s = plan_fixed(di, sc, sh.n_staged, sh.cta_words, P.S, grid, smem, true)) != FLS_OK) { return s; }
-	P.S.err = device_error_word();
+	P.S.err = device_error_word(stream);
 	for (uint32_t i = 0; i < sh.n_staged + sh.n_global; ++i) {
 		P.base[i] = static_cast<uint32_t>(d->cols[sh.staged[i]].base);
 	}
@@ -601,7 +601,7 @@ fls_status jit_decode(const fls_column* col, int mode, uint32_t* d_out, uint64_t
 	fls_status          s = device_info(di);
 	if (s != FLS_OK) { return s; }
 	if ((s = plan_fixed(di, col, 1, 0u, P.S, grid, smem)) != FLS_OK) { return s; }
-	P.S.err = device_error_word();
+	P.S.err = device_error_word(stream);
 	P.base  = static_cast<uint32_t>(col->base);
 	P.sum   = reinterpret_cast<unsigned long long*>(d_sum);
 	P.out   = d_out;

@@ -293,7 +293,10 @@ struct DeviceInfo {
 
 fls_status device_info(DeviceInfo& di);
 fls_status cuda_check(cudaError_t e, const char* what);
-uint32_t*  device_error_word(); // device address of this device's error word
+// Device address of the error word that kernels launched on `stream` record
+// errors in: the word bound to the stream (fls_bind_error_word), else the
+// device's default word.
+uint32_t*  device_error_word(cudaStream_t stream);
 void       count_launch(uint64_t n = 1);
 int        tuning_sparse_rows();
 int        tuning_jit();
@@ -390,7 +393,9 @@ fls_status launch_staged(const StageCfg& cfg, const Op& op, uint32_t grid, uint3
 		}
 	}
 	if (grid == 0) { return FLS_OK; }
-	kern<<<grid, threads, smem, stream>>>(cfg, op);
+	StageCfg c = cfg;
+	c.err      = device_error_word(stream);
+	kern<<<grid, threads, smem, stream>>>(c, op);
 	count_launch();
 	return cuda_check(cudaGetLastError(), "staged kernel launch");
 }

@@ -789,7 +789,7 @@ fls_status fls_pht_build_ranges(const int32_t* d_filter, int32_t lo0, int32_t hi
 	const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>(want, static_cast<uint64_t>(di.sms) * 8u));
 	pht_build_kernel<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(d_filter, lo0, hi0, lo1, hi1, d_keys,
 	                                                                           d_vals, n, d_ht, ht_len, keys_min,
-	                                                                           device_error_word());
+	                                                                           device_error_word(reinterpret_cast<cudaStream_t>(stream)));
 	count_launch();
 	return cuda_check(cudaGetLastError(), "pht_build_kernel launch");
 }

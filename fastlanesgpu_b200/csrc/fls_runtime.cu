@@ -12,9 +12,11 @@
 
 namespace fls {
 
-// One error word per device (a module-scope variable exists once per device
-// context); kernels receive its address as a parameter.
-__device__ uint32_t g_err_word = 0;
+// The default error word of each device (a module-scope variable exists once
+// per device context), for streams without a word of their own: [0] holds the
+// bits kernels OR in, [1] receives the bits fls_check_device_error takes out of
+// [0] with one atomic exchange.  Kernels receive the address as a parameter.
+__device__ uint32_t g_err_word[2] = {0u, 0u};
 
 namespace {
 std::atomic<uint64_t> g_launches {0};
@@ -36,6 +38,22 @@ uint32_t round4(uint32_t w) { return (w + 3u) & ~3u; }
 std::mutex              g_dev_mu;
 std::vector<DeviceInfo> g_dev_cache;
 std::vector<uint32_t*>  g_err_addr;
+
+// Error words bound to streams by fls_bind_error_word: (device, stream) ->
+// caller-owned pair of device words.  A short list: callers bind one word per
+// stream they use.
+struct ErrBinding {
+	int          dev;
+	cudaStream_t stream;
+	uint32_t*    words;
+};
+constexpr size_t        kMaxBindings = 4096;
+std::mutex              g_bind_mu;
+std::vector<ErrBinding> g_bind;
+
+// Moves the error bits of words[0] into words[1] with one atomic exchange, in
+// stream order, so no bit raised after the read is lost.
+__global__ void err_take_kernel(uint32_t* words) { words[1] = atomicExch(&words[0], 0u); }
 } // namespace
 
 void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
@@ -95,9 +113,15 @@ fls_status device_info(DeviceInfo& di) {
 	return FLS_OK;
 }
 
-uint32_t* device_error_word() {
+uint32_t* device_error_word(cudaStream_t stream) {
 	int dev = 0;
 	cudaGetDevice(&dev);
+	{
+		std::lock_guard<std::mutex> lk(g_bind_mu);
+		for (const ErrBinding& b : g_bind) {
+			if (b.dev == dev && b.stream == stream) { return b.words; }
+		}
+	}
 	std::lock_guard<std::mutex> lk(g_dev_mu);
 	return dev < static_cast<int>(g_err_addr.size()) ? g_err_addr[dev] : nullptr;
 }
@@ -182,7 +206,7 @@ fls_status plan_stages(const fls_column* cols, uint32_t n_cols, uint32_t extra_w
 	cfg.all_uniform = uniform ? 1u : 0u;
 	cfg.has_dict = dict ? 1u : 0u;
 	cfg.n_vec    = (cfg.n_values + 1023u) / 1024u;
-	cfg.err      = device_error_word();
+	cfg.err      = device_error_word(nullptr); // launch_staged sets the launching stream's word
 	LaunchCfg lc = launch_cfg();
 	uint32_t  W = lc.warps, S = lc.stages;
 	// Tile: enough consecutive vectors for ~tile_bytes per stage, but keep at
@@ -258,15 +282,52 @@ using namespace fls;
 
 extern "C" {
 
-fls_status fls_check_device_error(fls_stream_t stream) {
-	fls_status s = cuda_check(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)), "cudaStreamSynchronize");
+fls_status fls_bind_error_word(fls_stream_t stream, uint32_t* d_words) {
+	if (reinterpret_cast<uintptr_t>(d_words) & 7u) {
+		return set_error(FLS_ERR_ALIGNMENT, "fls_bind_error_word: the word pair must be 8-byte aligned");
+	}
+	DeviceInfo di;
+	fls_status s = device_info(di);
 	if (s != FLS_OK) { return s; }
-	uint32_t word = 0, zero = 0;
-	if ((s = cuda_check(cudaMemcpyFromSymbol(&word, g_err_word, sizeof(word)), "read error word")) != FLS_OK) {
+	int dev = 0;
+	cudaGetDevice(&dev);
+	const cudaStream_t          st = reinterpret_cast<cudaStream_t>(stream);
+	std::lock_guard<std::mutex> lk(g_bind_mu);
+	for (size_t i = 0; i < g_bind.size(); ++i) {
+		if (g_bind[i].dev == dev && g_bind[i].stream == st) {
+			if (d_words) {
+				g_bind[i].words = d_words;
+			} else {
+				g_bind.erase(g_bind.begin() + static_cast<std::ptrdiff_t>(i));
+			}
+			return FLS_OK;
+		}
+	}
+	if (!d_words) { return FLS_OK; }
+	if (g_bind.size() >= kMaxBindings) {
+		return set_error(FLS_ERR_CAPACITY, "fls_bind_error_word: too many bound streams (unbind with NULL)");
+	}
+	g_bind.push_back(ErrBinding {dev, st, d_words});
+	return FLS_OK;
+}
+
+fls_status fls_check_device_error(fls_stream_t stream) {
+	DeviceInfo di;
+	fls_status s = device_info(di);
+	if (s != FLS_OK) { return s; }
+	cudaStream_t st    = reinterpret_cast<cudaStream_t>(stream);
+	uint32_t*    words = device_error_word(st);
+	if (!words) { return set_error(FLS_ERR_CUDA, "no error word for this device"); }
+	err_take_kernel<<<1, 1, 0, st>>>(words);
+	count_launch();
+	if ((s = cuda_check(cudaGetLastError(), "err_take_kernel launch")) != FLS_OK) { return s; }
+	uint32_t word = 0;
+	if ((s = cuda_check(cudaMemcpyAsync(&word, words + 1, sizeof(word), cudaMemcpyDeviceToHost, st),
+	                    "read error word")) != FLS_OK) {
 		return s;
 	}
+	if ((s = cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize")) != FLS_OK) { return s; }
 	if (word == 0) { return FLS_OK; }
-	cudaMemcpyToSymbol(g_err_word, &zero, sizeof(zero));
 	std::string msg = "device error:";
 	if (word & kErrBadMeta) { msg += " bad-vector-metadata"; }
 	if (word & kErrBounds) { msg += " vector-out-of-bounds"; }
@@ -284,7 +345,8 @@ fls_status fls_selftest_bounded_wait(uint32_t polls, fls_stream_t stream) {
 	DeviceInfo di;
 	fls_status s = device_info(di);
 	if (s != FLS_OK) { return s; }
-	wait_selftest_kernel<<<1, 32, 0, reinterpret_cast<cudaStream_t>(stream)>>>(polls, device_error_word());
+	wait_selftest_kernel<<<1, 32, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+	    polls, device_error_word(reinterpret_cast<cudaStream_t>(stream)));
 	count_launch();
 	return cuda_check(cudaGetLastError(), "wait_selftest_kernel launch");
 }

@@ -334,9 +334,20 @@ def crystal_q21_probe(cols, n_rows: int, ht_s, ht_p, ht_d, d_keys_min: int = 0, 
     return out
 
 
-def check_device_error() -> None:
-    """Synchronise the current stream and raise if a kernel flagged bad input."""
-    check(lib().fls_check_device_error(_stream()), "device")
+def check_device_error(stream=None) -> None:
+    """Take the error bits of `stream` (default: the current stream) and raise
+    if a kernel launched on it flagged bad input or a timeout."""
+    st = _stream() if stream is None else stream.cuda_stream
+    check(lib().fls_check_device_error(st), "device")
+
+
+def bind_error_word(words, stream=None) -> None:
+    """Give `stream` (default: the current stream) its own error word: `words`
+    is a zeroed device tensor of two int32 (None removes the binding)."""
+    st = _stream() if stream is None else stream.cuda_stream
+    if words is not None:
+        assert words.is_cuda and words.numel() * words.element_size() >= 8
+    check(lib().fls_bind_error_word(st, None if words is None else words.data_ptr()), "fls_bind_error_word")
 
 
 def set_launch_config(warps: int = 0, stages: int = 0, ctas_per_sm: int = 0, tile_bytes: int = 0) -> None:

@@ -100,9 +100,24 @@ typedef struct fls_column {
 
 /* Human-readable text of the last error raised on this host thread. */
 const char* fls_last_error(void);
-/* Synchronise `stream`, then read and clear the device error word.
- * Returns FLS_OK, FLS_ERR_DEVICE or FLS_ERR_TIMEOUT. */
+/* Reads and clears the error word of `stream`: one atomic exchange on the
+ * device, in stream order, takes the bits (a bit raised after it stays for the
+ * next check), then the stream is synchronised.  Returns FLS_OK,
+ * FLS_ERR_DEVICE or FLS_ERR_TIMEOUT.  The reference reports device-side
+ * problems by exit() or trap (fastlanes/src/include/gpu_utils.h:41-58,
+ * fls_gen/unpack/hardcoded_16.cuh:755). */
 fls_status fls_check_device_error(fls_stream_t stream);
+/* Gives `stream` an error word of its own (no reference counterpart): d_words
+ * is a caller-owned pair of device uint32 words, zeroed by the caller and
+ * 8-byte aligned.  Kernels this library launches on `stream` (on the current
+ * device) record errors in d_words[0], and fls_check_device_error(stream)
+ * reports exactly those; d_words[1] receives the bits each check takes out.
+ * Streams without a word share the device's default word, so a check on one
+ * of them may report another unbound stream's error.  Binding again replaces
+ * the word; d_words == NULL removes the binding.  The binding is looked up
+ * when a call enqueues its kernels: keep the words alive while work that was
+ * enqueued with them may run. */
+fls_status fls_bind_error_word(fls_stream_t stream, uint32_t* d_words);
 
 /* Self-test of failure detection (no reference counterpart): one warp runs
  * the bounded mbarrier wait of the staged pipelines on a barrier that nothing
