@@ -49,6 +49,10 @@ def parse_args():
     ap.add_argument("--decode-out", choices=["sum", "hbm"], default="sum",
                     help="decode fused with a uint64 sum, or decode to HBM")
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--secondary", choices=["all", "none"], default="all",
+                    help="with the default workload on 1 GPU: also measure the other configurations (Q2.1, Q3.1 and "
+                         "Q4.1 joins, the FOR decode sweep over bit widths 1..32 and DELTA/RLE/DICT decode at 2^28 "
+                         "values, learned vs exhaustive encoding and the batch) and add them to the line")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch", default="", help="warps,stages,ctas_per_sm,tile_bytes (0 = default)")
@@ -252,6 +256,7 @@ def run_ours(a, dist: Dist):
         ht_p = ops.build_pht(dt["p_partkey"], dt["p_partkey"].numel(), vals=dt["p_brand1"], filt=dt["p_category"],
                              filter_eq=1)
         ht_d = ops.build_pht(dt["d_datekey"], datagen.N_DAYS, vals=dt["d_year"])
+        tabs = {"ht_s": ht_s, "ht_p": ht_p, "ht_d": ht_d}
         probes = [(0, ht_s, ht_s.numel(), 0, 1), (1, ht_p, ht_p.numel() // 2, 0, 2),
                   (2, ht_d, ht_d.numel() // 2, 0, 2)]
         res = torch.zeros(4 * datagen.N_GROUPS, dtype=torch.int32, device=dev)
@@ -265,6 +270,7 @@ def run_ours(a, dist: Dist):
         metric_key = "q21"
     elif a.workload in ("q31", "q41"):
         t, tables, hcols, dcols, probes, jkw = datagen.ssb_join(a.workload, a.rows, seed, device=dev)
+        tabs = tables
         res = torch.zeros(jkw["res_stride"] * jkw["n_groups"], dtype=torch.int32, device=dev)
 
         def step():
@@ -552,36 +558,106 @@ def run_ours(a, dist: Dist):
         out["per_query"] = per_query
         out["roofline"]["algorithmic_bytes_per_launch"] = algo_bytes
         out["roofline"]["note"] = "a step is 13 query launches; bytes and time are the whole step's"
-    return out, t if a.workload == "q11" else None, hcols
+    ctx = {"workload": a.workload, "hcols": hcols, "res": res,
+           "tabs": {k: v.cpu().numpy() for k, v in tabs.items()} if a.workload in ("q21", "q31", "q41") else None}
+    return out, ctx
 
 
-def cpu_baseline_q11(a, hcols, budget_s: float):
-    """The reference's CPU implementation (its own unpack compiled from its
-    sources + the fls_q11.cu scalar loop), all host threads, on a bounded
-    prefix sample of the same table."""
+M64 = (1 << 64) - 1
+
+REF_HOW = {
+    "q11": "the reference's unpack (unpack_fused.cuh, host-compiled from its sources) + the fls_q11.cu loop",
+    "q21": "the reference's unpack (host-compiled from its sources) + the fls_q21.cu probe_v1 loop",
+    "q31": "the reference's unpack (host-compiled from its sources) + the fls_q31.cu probe_v1 loop",
+    "q41": "the reference's unpack (host-compiled from its sources) + the fls_q41.cu probe_v1 loop",
+    "decode": "the reference's unpack (unpack.cuh, host-compiled from its sources) + uint64 sum",
+}
+
+
+def cpu_info() -> dict:
+    """The host CPU: model name (/proc/cpuinfo) and the cores this process may use."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except Exception:
+        usable = os.cpu_count() or 1
+    return {"model": model, "logical_cpus": os.cpu_count(), "usable_cpus": usable}
+
+
+def _time_cpu(fn, args, budget_s: float, min_reps: int = 3, max_reps: int = 100000):
+    """fn(*args) once untimed, then at least min_reps timed runs and more
+    until budget_s is spent: (median seconds, runs, last result)."""
+    res = fn(*args)
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while len(times) < min_reps or (time.perf_counter() < t_end and len(times) < max_reps):
+        t0 = time.perf_counter()
+        res = fn(*args)
+        times.append(time.perf_counter() - t0)
+    return statistics.median(times), len(times), res
+
+
+def reference_call(R, workload: str, words, bws, n_rows: int, tabs, threads: int, decode_bw: int = 0):
+    """(function, arguments) of the reference's CPU implementation of a
+    workload over packed words (uniform FOR columns in the reference's
+    format) and, for the joins, the perfect hash tables."""
+    from fastlanesgpu_b200 import datagen
+    if workload == "q11":
+        f = datagen.Q11_FILTER
+        return R.q11_sum, (words, bws, n_rows, *f["date"], *f["discount"], f["quantity"][1] + 1, threads)
+    if workload == "q21":
+        return R.q21_groupby, (words, bws, n_rows, tabs["ht_s"], tabs["ht_p"], tabs["ht_d"], 0, threads)
+    if workload == "q31":
+        return R.q31_groupby, (words, bws, n_rows, tabs["ht_s"], tabs["ht_c"], tabs["ht_d"], 0, threads)
+    if workload == "q41":
+        return R.q41_groupby, (words, bws, n_rows, tabs["ht_s"], tabs["ht_c"], tabs["ht_p"], tabs["ht_d"], 0,
+                               threads)
+    return R.decode_sum, (words[0], decode_bw, (n_rows + 1023) // 1024, threads)
+
+
+def _same_result(workload: str, ref, res) -> bool:
+    """The reference's result equals the GPU's (device tensor `res`)."""
+    import numpy as np
+    if workload in ("q21", "q31", "q41"):
+        return bool(np.array_equal(np.asarray(ref), res.cpu().numpy()))
+    got = int(res.cpu()[0])
+    return (got & M64) == (int(ref) & M64)
+
+
+def cpu_baseline(a, ctx, budget_s: float) -> dict:
+    """The reference's CPU implementation of the benched workload (its own
+    unpack compiled from its sources + its scalar query loop), timed on the
+    host cores over the WHOLE benched table with all usable threads, and on a
+    prefix with one thread; its result on the whole table is compared with
+    the GPU's result (the bench line fails on a mismatch)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
     import oracle as orc
-    from fastlanesgpu_b200 import datagen
     R = orc.Reference()
-    threads = os.cpu_count() or 1
-    sample = min(a.rows, 1 << 24)
-    n_vec = (sample + 1023) // 1024
-    words = [np.ascontiguousarray(c.words[:n_vec * 32 * c.bw + 4]) for c in hcols]
-    bws = [c.bw for c in hcols]
-    f = datagen.Q11_FILTER
-    args = (words, bws, sample, *f["date"], *f["discount"], f["quantity"][1] + 1, threads)
-    R.q11_sum(*args)  # warm-up
-    times = []
-    t_end = time.perf_counter() + budget_s
-    while time.perf_counter() < t_end or len(times) < 3:
-        t0 = time.perf_counter()
-        R.q11_sum(*args)
-        times.append(time.perf_counter() - t0)
-    med = statistics.median(times)
-    return {"value": sample / med, "unit": "rows/s", "cores": threads, "kind": "reference",
-            "sample": f"first {sample} rows of the table, {len(times)} repetitions, median; reference unpack "
-                      f"(unpack_fused.cuh host-compiled) + fls_q11.cu loop, OpenMP {threads} threads"}
+    info = cpu_info()
+    threads = info["usable_cpus"]
+    w = ctx["workload"]
+    words = [np.ascontiguousarray(c.words).view(np.uint32) for c in ctx["hcols"]]
+    bws = [c.bw for c in ctx["hcols"]]
+    fn, args = reference_call(R, w, words, bws, a.rows, ctx["tabs"], threads, a.decode_bw)
+    med, reps, ref = _time_cpu(fn, args, budget_s)
+    n1 = min(a.rows, 1 << 22)
+    fn1, args1 = reference_call(R, w, words, bws, n1, ctx["tabs"], 1, a.decode_bw)
+    med1, reps1, _ = _time_cpu(fn1, args1, budget_s / 4, min_reps=1)
+    return {"value": a.rows / med, "unit": "rows/s", "cores": threads, "kind": "reference", "cpu": info,
+            "sample": f"the whole benched table ({a.rows} rows), {reps} runs after one untimed, median; "
+                      f"{REF_HOW[w]}, OpenMP {threads} threads",
+            "single_thread": {"value": n1 / med1, "unit": "rows/s", "cores": 1,
+                              "sample": f"first {n1} rows of the table, {reps1} runs, median, 1 thread"},
+            "result_equal": _same_result(w, ref, ctx["res"])}
 
 
 def _pad_vectors(v):
@@ -828,88 +904,268 @@ def run_mixed(a, dist: Dist):
 
 
 def run_reference(a, dist: Dist):
-    """--impl reference: the reference's own CPU implementation of the path (its
-    unpack compiled from its sources, the fls_q11.cu / fls_q21.cu scalar loops),
-    all host threads, on a bounded sample of the same workload."""
+    """--impl reference: the reference's own CPU implementation of the path
+    (its unpack compiled from its sources, its fls_q11.cu / fls_q21.cu /
+    fls_q31.cu / fls_q41.cu scalar loops) on the host cores, with every usable
+    thread, over the same workload at full size: --warmup untimed and --steps
+    timed passes over the whole table (the timed passes stop early only if
+    they would exceed about two minutes; `steps` then says how many ran)."""
     import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
     from fastlanesgpu_b200 import datagen
+    from fastlanesgpu_b200.shard import shard_seed
     R = orc.Reference()
-    threads = os.cpu_count() or 1
+    info = cpu_info()
+    threads = info["usable_cpus"]
     if a.workload in ("mixed", "ssb") or (a.workload == "decode" and (a.decode_scheme != "for" or
                                                                         a.decode_width != 32)):
         return {"impl": "reference", "unavailable": "the reference has no CPU implementation of this workload "
                 "(learned selection, batching, per-vector DELTA/RLE/DICT columns, 8/16/64-bit lanes (it only "
                 "packs them), or the SSB queries other than its fls_q11/q21/q31/q41 loops)"}
-    sample = min(a.rows, 1 << 24)
+    n = a.rows
+    seed = shard_seed(1000, 0)  # the table the GPU arm benches on rank 0
+    tabs, bws, decode_bw = None, None, a.decode_bw
     if a.workload == "q11":
-        t = datagen.lineorder_q11(sample, seed=1000)
-        names = ["date", "discount", "quantity", "price"]
-        words = [R.pack_column(t[k], datagen.Q11_BITS[k], threads) for k in names]
-        bws = [datagen.Q11_BITS[k] for k in names]
-        f = datagen.Q11_FILTER
-        args = (words, bws, sample, *f["date"], *f["discount"], f["quantity"][1] + 1, threads)
-        fn, what = R.q11_sum, "fused decode + filter-aggregate (Q1.1 shape)"
-        how = "the reference's unpack (host-compiled from its sources) + fls_q11.cu loop"
-    elif a.workload in ("q31", "q41"):
+        t = datagen.lineorder_q11(n, seed=seed)
+        names, bits = ["date", "discount", "quantity", "price"], datagen.Q11_BITS
+        what = "fused decode + filter-aggregate (Q1.1 shape)"
+    elif a.workload in ("q21", "q31", "q41"):
         O = orc.Oracle()
-        if a.workload == "q31":
-            t = datagen.q31_tables(sample, seed=1000)
-            hs = O.pht2_build(t["s_region"], 1, t["s_suppkey"], t["s_nation"], t["s_suppkey"].size)
-            hc = O.pht2_build(t["c_region"], 1, t["c_custkey"], t["c_nation"], t["c_custkey"].size)
-            hd = O.pht2_build(t["d_in_range"], 1, t["d_datekey"], t["d_year"], datagen.N_DAYS)
+        if a.workload == "q21":
+            t = datagen.q21_tables(n, seed=seed)
+            tabs = {"ht_s": O.pht1_build(t["s_region"], 1, t["s_suppkey"], t["s_suppkey"].size),
+                    "ht_p": O.pht2_build(t["p_category"], 1, t["p_partkey"], t["p_brand1"], t["p_partkey"].size),
+                    "ht_d": O.pht2_build(None, 0, t["d_datekey"], t["d_year"], datagen.N_DAYS)}
+            names, bits = ["lo_suppkey", "lo_partkey", "lo_orderdate", "lo_revenue"], datagen.Q21_BITS
+            what = "fused decode + 3-way perfect-hash probe + 7000-group int64 group-by (Q2.1 shape)"
+        elif a.workload == "q31":
+            t = datagen.q31_tables(n, seed=seed)
+            tabs = {"ht_s": O.pht2_build(t["s_region"], 1, t["s_suppkey"], t["s_nation"], t["s_suppkey"].size),
+                    "ht_c": O.pht2_build(t["c_region"], 1, t["c_custkey"], t["c_nation"], t["c_custkey"].size),
+                    "ht_d": O.pht2_build(t["d_in_range"], 1, t["d_datekey"], t["d_year"], datagen.N_DAYS)}
             names, bits = ["lo_suppkey", "lo_custkey", "lo_orderdate", "lo_revenue"], datagen.Q31_BITS
-            tabs, fn, shape = (hs, hc, hd), R.q31_groupby, "Q3.1"
+            what = "fused decode + perfect-hash probes + int64 group-by (Q3.1 shape)"
         else:
-            t = datagen.q41_tables(sample, seed=1000)
-            hs = O.pht1_build(t["s_region"], 1, t["s_suppkey"], t["s_suppkey"].size)
-            hc = O.pht2_build(t["c_region"], 1, t["c_custkey"], t["c_nation"], t["c_custkey"].size)
-            hp = O.pht1_build(t["p_mfgr_low"], 1, t["p_partkey"], t["p_partkey"].size)
-            hd = O.pht2_build(None, 0, t["d_datekey"], t["d_year"], datagen.N_DAYS)
+            t = datagen.q41_tables(n, seed=seed)
+            tabs = {"ht_s": O.pht1_build(t["s_region"], 1, t["s_suppkey"], t["s_suppkey"].size),
+                    "ht_c": O.pht2_build(t["c_region"], 1, t["c_custkey"], t["c_nation"], t["c_custkey"].size),
+                    "ht_p": O.pht1_build(t["p_mfgr_low"], 1, t["p_partkey"], t["p_partkey"].size),
+                    "ht_d": O.pht2_build(None, 0, t["d_datekey"], t["d_year"], datagen.N_DAYS)}
             names = ["lo_suppkey", "lo_custkey", "lo_partkey", "lo_orderdate", "lo_revenue", "lo_supplycost"]
-            bits, tabs, fn, shape = datagen.Q41_BITS, (hs, hc, hp, hd), R.q41_groupby, "Q4.1"
-        words = [R.pack_column(t[k], bits[k], threads) for k in names]
-        args = (words, [bits[k] for k in names], sample, *tabs, 0, threads)
-        what = f"fused decode + perfect-hash probes + int64 group-by ({shape} shape)"
-        how = f"the reference's unpack (host-compiled from its sources) + fls_{a.workload}.cu probe_v1 loop"
-    elif a.workload == "q21":
-        t = datagen.q21_tables(sample, seed=1000)
-        O = orc.Oracle()
-        ht_s = O.pht1_build(t["s_region"], 1, t["s_suppkey"], t["s_suppkey"].size)
-        ht_p = O.pht2_build(t["p_category"], 1, t["p_partkey"], t["p_brand1"], t["p_partkey"].size)
-        ht_d = O.pht2_build(None, 0, t["d_datekey"], t["d_year"], datagen.N_DAYS)
-        names = ["lo_suppkey", "lo_partkey", "lo_orderdate", "lo_revenue"]
-        words = [R.pack_column(t[k], datagen.Q21_BITS[k], threads) for k in names]
-        bws = [datagen.Q21_BITS[k] for k in names]
-        args = (words, bws, sample, ht_s, ht_p, ht_d, 0, threads)
-        fn, what = R.q21_groupby, "fused decode + 3-way perfect-hash probe + 7000-group int64 group-by (Q2.1 shape)"
-        how = "the reference's unpack (host-compiled from its sources) + fls_q21.cu probe_v1 loop"
+            bits = datagen.Q41_BITS
+            what = "fused decode + perfect-hash probes + int64 group-by (Q4.1 shape)"
     else:
-        vals = datagen.uniform_bits(sample, a.decode_bw, seed=1000)
-        packed = R.pack_column(vals, a.decode_bw, threads)
-        args = (packed, a.decode_bw, sample // 1024, threads)
-        fn, what = R.decode_sum, f"decode fused with uint64 sum: bit-pack + FOR, bw {a.decode_bw}"
-        how = "the reference's unpack (host-compiled from its sources) + uint64 sum"
-    for _ in range(max(1, min(a.warmup, 3))):
+        t = {"v": datagen.uniform_bits(n, a.decode_bw, seed=seed)}
+        names, bits = ["v"], {"v": a.decode_bw}
+        what = f"decode fused with uint64 sum: bit-pack + FOR, bw {a.decode_bw}"
+    # the reference's own packer (pack.cpp) encodes the columns
+    words = [R.pack_column(t[k], bits[k], threads) for k in names]
+    bws = [bits[k] for k in names]
+    del t
+    fn, args = reference_call(R, a.workload, words, bws, n, tabs, threads, decode_bw)
+    for _ in range(a.warmup):
         fn(*args)
-    steps = max(1, min(a.steps, 10))
     times = []
-    for _ in range(steps):
+    budget = 120.0
+    for i in range(a.steps):
         t0 = time.perf_counter()
         fn(*args)
         times.append(time.perf_counter() - t0)
-    value = sample * len(times) / sum(times)
+        if sum(times) / (i + 1) * a.steps > budget and sum(times) > budget:
+            break
+    ms = 1e3 * sum(times) / len(times)
+    value = n / (ms / 1e3)
+    n1 = min(n, 1 << 22)
+    fn1, args1 = reference_call(R, a.workload, words, bws, n1, tabs, 1, decode_bw)
+    med1, reps1, _ = _time_cpu(fn1, args1, 3.0, min_reps=1)
     return {
         "impl": "reference", "metric": "fused decode+query rows/s", "value": value, "unit": "rows/s",
-        "n_gpus": a.gpus, "steps": steps, "warmup": max(1, min(a.warmup, 3)),
-        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int32->int64", "data": "synthetic (seeded)",
-        "config": {"workload": what, "rows_per_gpu": a.rows, "sample_rows_per_step": sample},
-        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "reference",
-                         "sample": f"{sample} rows per step of the same table shape; {how}, OpenMP {threads} threads"},
+        "n_gpus": a.gpus, "steps": len(times), "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32->int64", "data": "synthetic (seeded)",
+        "config": {"workload": what, "rows_per_gpu": n, "rows_per_step": n},
+        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "reference", "cpu": info,
+                         "sample": f"the whole table ({n} rows) per step, {len(times)} timed steps after "
+                                   f"{a.warmup} untimed, mean; {REF_HOW[a.workload]}, OpenMP {threads} threads",
+                         "single_thread": {"value": n1 / med1, "unit": "rows/s", "cores": 1,
+                                           "sample": f"first {n1} rows, {reps1} runs, median, 1 thread"}},
         "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+
+
+def _time_gpu(fn, steps: int, warmup: int = 3) -> float:
+    """Milliseconds per call of fn: CUDA events on the current stream around
+    `steps` calls, after `warmup` untimed ones (inputs larger than L2)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def secondary_joins(a, dist, steps: int) -> dict:
+    """Q2.1, Q3.1 and Q4.1 (2^27 rows each) through the same path as the
+    headline, each checked against the reference's CPU implementation on the
+    whole table, with the median SM clock of its timed region."""
+    import argparse as _ap
+
+    import torch
+    out = {}
+    for w in ("q21", "q31", "q41"):
+        b = _ap.Namespace(**vars(a))
+        b.workload, b.steps, b.e2e_steps, b.rows = w, steps, 3, a.rows
+        line, ctx = run_ours(b, dist)
+        cb = cpu_baseline(b, ctx, 2.0)
+        clk = line["clocks"]
+        ms = line["ms_per_step"]
+        ent = {"workload": line["config"]["workload"], "rows": b.rows, "steps": steps, "ms_per_step": ms,
+               "rows_per_s": line["value"],
+               "roofline": {k: line["roofline"][k] for k in ("achieved", "frac", "algorithmic_bytes_per_launch",
+                                                             "traffic")},
+               "clocks": clk, "join_variants": line["config"].get("join_variants"),
+               "e2e_rows_per_s": line["e2e"]["value"],
+               "cpu_baseline": {k: cb[k] for k in ("value", "cores", "single_thread")},
+               "result_equal": cb["result_equal"]}
+        if clk.get("sm_mhz") and clk.get("sm_max_mhz"):
+            ent["ms_x_sm_mhz"] = ms * clk["sm_mhz"]
+            ent["ms_at_max_sm_clock"] = ms * clk["sm_mhz"] / clk["sm_max_mhz"]
+        out[w] = ent
+        del ctx, line
+        torch.cuda.empty_cache()
+    return out
+
+
+def decode_sweep(a, dist, steps: int) -> dict:
+    """Uniform FOR bit-packed columns of 2^28 values at every bit width 1..32,
+    decoded to HBM and fused with a uint64 sum.  Values uniform in [0, 2^bw)
+    pack to uniformly random words (every bit of a packed vector belongs to
+    exactly one value), so the packed words are drawn directly on the device.
+    Checks per width: the fused sum equals the sum of the decoded array and the
+    reference's own unpack + sum over the whole column on the host (which is
+    also timed, all threads), and three vectors decode element-wise as the
+    reference's unpack decodes them."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as orc
+    import torch
+
+    from fastlanesgpu_b200 import ops
+    from fastlanesgpu_b200.column import DeviceUniformColumn
+    R = orc.Reference()
+    threads = cpu_info()["usable_cpus"]
+    dev = torch.device("cuda", dist.local)
+    n = 1 << 28
+    n_vec = n // 1024
+    peak = measured_peak_gbs()[0]
+    g = torch.Generator(device=dev)
+    g.manual_seed(2800)
+    dec = torch.empty(n, dtype=torch.int32, device=dev)
+    s = torch.zeros(1, dtype=torch.int64, device=dev)
+    clocks = ClockSampler(dist.local)
+    clocks.start()
+    w0 = time.time()
+    per_bw, ok = {}, True
+    for bw in range(1, 33):
+        words = torch.randint(0, 256, (4 * n_vec * 32 * bw,), dtype=torch.uint8, device=dev,
+                              generator=g).view(torch.int32)
+        col = DeviceUniformColumn(words, n, bw)
+        ms_sum = _time_gpu(lambda: ops.query_aggregate(col, out=s), steps, max(3, a.warmup))
+        ms_hbm = _time_gpu(lambda: ops.unpack_global(col, out=dec), steps, max(3, a.warmup))
+        got_sum = int(s.cpu()[0]) & M64
+        dec_sum = int((dec.to(torch.int64) & 0xFFFFFFFF).sum()) & M64
+        host = words.cpu().numpy().view(np.uint32)
+        t0 = time.perf_counter()
+        ref_sum = R.decode_sum(host, bw, n_vec, threads) & M64
+        ref_s = time.perf_counter() - t0
+        vec_ok = all(np.array_equal(dec[v * 1024:(v + 1) * 1024].cpu().numpy().view(np.uint32),
+                                    R.unpack(host[v * 32 * bw:(v + 1) * 32 * bw], bw).view(np.uint32))
+                     for v in (0, n_vec // 2, n_vec - 1))
+        equal = got_sum == dec_sum == ref_sum and vec_ok
+        ok = ok and equal
+        b_in = n_vec * 128 * bw
+        per_bw[bw] = {"sum_ms": ms_sum, "sum_frac": b_in / (ms_sum / 1e3) / 1e9 / peak,
+                      "sum_values_per_s": n / (ms_sum / 1e3),
+                      "hbm_ms": ms_hbm, "hbm_frac": (b_in + 4 * n) / (ms_hbm / 1e3) / 1e9 / peak,
+                      "cpu_reference_values_per_s": n / ref_s, "result_equal": equal}
+        del words, col, host
+    clocks.mark(w0, time.time())
+    clk = clocks.stop()
+    del dec
+    torch.cuda.empty_cache()
+    return {"workload": "decode of a uniform FOR bit-packed column of 2^28 values at bit widths 1..32, to HBM "
+                        "(algorithmic bytes 128*bw per vector + 4 B per value written) and fused with a uint64 sum "
+                        "(128*bw per vector)", "steps": steps, "peak_gbs": peak, "clocks": clk,
+            "cpu_reference": f"{REF_HOW['decode']}, OpenMP {threads} threads, one pass over the whole column",
+            "all_equal": ok, "per_bw": per_bw}
+
+
+def decode_schemes(a, dist, steps: int) -> dict:
+    """DELTA (sorted keys, geometric gaps p=0.3), RLE (geometric runs of mean
+    16, values in [0, 2^16)) and DICT (Zipf 1.1 over [0, 2^20)) columns of 2^28
+    values, generated and encoded on the GPU (per-vector metadata), decoded to
+    HBM (stored order) and fused with a uint64 sum; checked by decoding in
+    original order against the input values and by the input's sum."""
+    import torch
+
+    from fastlanesgpu_b200 import LAYOUT_TRANSPOSED, ORDER_ORIGINAL, SCHEME_DELTA, SCHEME_DICT, SCHEME_RLE, datagen, ops
+    from fastlanesgpu_b200.column import encode_column_gpu
+    dev = torch.device("cuda", dist.local)
+    n = 1 << 28
+    peak = measured_peak_gbs()[0]
+    out = {}
+    for name, scheme, gen in (
+            ("delta", SCHEME_DELTA, lambda: datagen.sorted_geometric_device(n, 0.3, seed=2801, device=dev)),
+            ("rle", SCHEME_RLE, lambda: datagen.geometric_runs_device(n, 16.0, 16, seed=2802, device=dev)),
+            ("dict", SCHEME_DICT, lambda: datagen.zipf_device(n, s=1.1, domain=1 << 20, seed=2803, device=dev))):
+        vals = gen()
+        col = encode_column_gpu(vals, scheme, layout=LAYOUT_TRANSPOSED)
+        dec = torch.empty(col.n_vec * 1024, dtype=torch.int32, device=dev)
+        s = torch.zeros(1, dtype=torch.int64, device=dev)
+        ms_sum = _time_gpu(lambda: ops.query_aggregate(col, out=s), steps, max(3, a.warmup))
+        ms_hbm = _time_gpu(lambda: ops.unpack_global(col, out=dec), steps, max(3, a.warmup))
+        want = int((vals.to(torch.int64) & 0xFFFFFFFF).sum()) & M64
+        equal = (int(s.cpu()[0]) & M64) == want
+        ops.unpack_global(col, order=ORDER_ORIGINAL, out=dec)
+        equal = equal and bool(torch.equal(dec[:n], vals))
+        ops.check_device_error()
+        b = col.nbytes
+        out[name] = {"encoded_bytes": b, "bits_per_value": 8 * b / n, "sum_ms": ms_sum,
+                     "sum_frac": b / (ms_sum / 1e3) / 1e9 / peak, "sum_values_per_s": n / (ms_sum / 1e3),
+                     "hbm_ms": ms_hbm, "hbm_frac": (b + 4 * n) / (ms_hbm / 1e3) / 1e9 / peak,
+                     "result_equal": equal}
+        del vals, col, dec
+        torch.cuda.empty_cache()
+    return out
+
+
+def mixed_summary(a, dist) -> dict:
+    """The learned-encoding + batched workload (64 mixed columns, MLP trained on
+    the GPU, 256 batched filter-aggregate queries), condensed."""
+    import argparse as _ap
+    b = _ap.Namespace(**vars(a))
+    b.steps = max(20, min(a.steps, 200))
+    m = run_mixed(b, dist)
+    le, bt = m["learned_encoding"], m["batched"]
+    dc = le["device_one_call"]
+    return {"workload": m["config"]["workload"], "rows_scanned_per_step": m["config"]["rows_scanned_per_step"],
+            "batch_rows_per_s": m["value"], "batch_roofline_frac": m["roofline"]["frac"],
+            "bytes_exhaustive": le["bytes_exhaustive"], "bytes_learned": le["bytes_learned"], "regret": le["regret"],
+            "host_exhaustive_s": le["exhaustive"]["total_s"], "host_exhaustive_where": le["exhaustive"]["where"],
+            "learned_gpu_pipeline_s": le["learned"]["total_s"],
+            "learned_vs_host_exhaustive": le["encode_speedup"],
+            "device_learned_s": dc["learned_s"], "device_exhaustive_s": dc["exhaustive_on_device_s"],
+            "learned_vs_device_exhaustive": dc["exhaustive_on_device_s"] / dc["learned_s"],
+            "bytes_device_learned": dc["bytes_learned"], "bytes_device_exhaustive": dc["bytes_exhaustive_on_device"],
+            "fallback_vectors": le["fallback_vectors"], "vectors": le["vectors"], "lossless": le["lossless"],
+            "batch_ms": bt["ms_batch_graph"], "per_query_launches_ms": bt["ms_per_query_launches"],
+            "batch_speedup": bt["speedup"], "results_equal": bt["results_equal"], "clocks": m["clocks"]}
 
 
 def main():
@@ -920,19 +1176,40 @@ def main():
             print(json.dumps(run_reference(a, dist)), flush=True)
         return
     dist.init()
+    failed = False
     try:
         if a.workload == "mixed":
             if dist.world > 1:
                 raise SystemExit("--workload mixed runs on one GPU")
             print(json.dumps(run_mixed(a, dist)), flush=True)
             return
-        out, _, hcols = run_ours(a, dist)
+        out, ctx = run_ours(a, dist)
+        checkable = a.workload in ("q11", "q21", "q31", "q41") or (
+            a.workload == "decode" and a.decode_scheme == "for" and a.decode_width == 32 and a.decode_out == "sum")
+        if dist.rank == 0 and dist.world == 1 and checkable and not a.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(a, ctx, a.cpu_seconds)
+            out["result_check"] = {"against": "the reference's CPU implementation on the whole benched table "
+                                              "(cpu_baseline leg)", "equal": out["cpu_baseline"]["result_equal"]}
+            failed = not out["result_check"]["equal"]
+        del ctx
+        if dist.world == 1 and a.workload == "q11" and a.secondary == "all" and not failed:
+            sec = {"note": "other configurations, each timed with CUDA events after warm-up; inputs larger than L2"}
+            sec_steps = max(a.steps, 200)
+            sec.update(secondary_joins(a, dist, max(a.steps, 1000)))
+            sec["decode_for_2p28"] = decode_sweep(a, dist, sec_steps)
+            sec["decode_schemes_2p28"] = decode_schemes(a, dist, sec_steps)
+            sec["mixed"] = mixed_summary(a, dist)
+            out["secondary"] = sec
+            failed = not (all(sec[w]["result_equal"] for w in ("q21", "q31", "q41")) and
+                          sec["decode_for_2p28"]["all_equal"] and
+                          all(v["result_equal"] for v in sec["decode_schemes_2p28"].values()) and
+                          sec["mixed"]["results_equal"] and sec["mixed"]["lossless"])
         if dist.rank == 0:
-            if dist.world == 1 and a.workload == "q11" and not a.no_cpu_baseline:
-                out["cpu_baseline"] = cpu_baseline_q11(a, hcols, a.cpu_seconds)
             print(json.dumps(out), flush=True)
     finally:
         dist.close()
+    if failed:
+        raise SystemExit("bench: a result differs from the reference's (see result_check / secondary)")
 
 
 if __name__ == "__main__":

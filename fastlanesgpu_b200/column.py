@@ -163,6 +163,37 @@ class DeviceColumn:
         return self.host.nbytes
 
 
+class DeviceUniformColumn:
+    """A uniform column (one scheme, bit width and FOR base, the reference's
+    column format) whose packed words are already in device memory (int32
+    tensor, 16-byte aligned): vector v at word 32*bw*v (FOR) or (32+32*bw)*v
+    (DELTA, transposed).  Same interface as DeviceColumn."""
+
+    def __init__(self, data, n_values: int, bw: int, base: int = 0, scheme: int = SCHEME_FOR,
+                 layout: int = LAYOUT_NORMAL):
+        self.host = None
+        self.data, self.meta = data, None
+        self._n_values, self.bw = n_values, bw
+        per = 32 * bw if scheme == SCHEME_FOR else 32 + 32 * bw
+        self.payload_words = n_vectors(n_values) * per
+        if int(data.numel()) < self.payload_words:
+            raise ValueError("device words smaller than the column")
+        self.desc = Column(data=data.data_ptr(), meta=0, n_values=n_values, n_words=int(data.numel()), layout=layout,
+                           scheme=scheme, bw=bw, base=base, max_vec_words=0, scheme_mask=1 << scheme)
+
+    @property
+    def n_values(self) -> int:
+        return self._n_values
+
+    @property
+    def n_vec(self) -> int:
+        return n_vectors(self._n_values)
+
+    @property
+    def nbytes(self) -> int:
+        return self.payload_words * 4
+
+
 class DeviceEncodedColumn:
     """A per-vector encoded column produced on the GPU (fls_encode_column_gpu):
     the device words and metadata with their C descriptor; same interface as
@@ -268,7 +299,7 @@ def columns_array(cols) -> ctypes.Array:
     return arr
 
 
-__all__ = ["EncodedColumn", "DeviceColumn", "DeviceEncodedColumn", "encode_column_gpu", "encode_column_learned_gpu",
+__all__ = ["EncodedColumn", "DeviceColumn", "DeviceUniformColumn", "DeviceEncodedColumn", "encode_column_gpu", "encode_column_learned_gpu",
            "META_DTYPE", "columns_array",
            "n_vectors", "_lib",
            "SCHEME_DELTA", "LAYOUT_TRANSPOSED"]

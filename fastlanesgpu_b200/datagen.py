@@ -220,6 +220,33 @@ def mixed_columns(n_cols: int = 64, lo_log: int = 16, hi_log: int = 26, seed: in
     return cols
 
 
+def sorted_geometric_device(n: int, p: float = 0.3, seed: int = 3, device="cuda"):
+    """Sorted keys with geometric(p) gaps (>= 1), drawn with torch on `device`
+    (int32 tensor; the distribution of sorted_geometric)."""
+    import torch
+    dev = torch.device(device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    u = torch.rand(n, generator=g, device=dev, dtype=torch.float64)
+    gaps = torch.floor(torch.log1p(-u) / torch.log1p(torch.tensor(-p, dtype=torch.float64, device=dev))) + 1
+    return torch.cumsum(gaps.to(torch.int64), 0).to(torch.int32)
+
+
+def geometric_runs_device(n: int, mean_run: float = 16.0, value_bits: int = 16, seed: int = 4, device="cuda"):
+    """Runs of geometric length (mean `mean_run`: a run starts at each row with
+    probability 1/mean_run) of uniform values in [0, 2^value_bits), drawn with
+    torch on `device` (int32 tensor; the distribution of geometric_runs)."""
+    import torch
+    dev = torch.device(device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    starts = torch.rand(n, generator=g, device=dev) < 1.0 / mean_run
+    starts[0] = True
+    run = torch.cumsum(starts.to(torch.int64), 0) - 1
+    vals = torch.randint(0, 1 << value_bits, (int(run[-1]) + 1,), generator=g, device=dev, dtype=torch.int64)
+    return vals[run].to(torch.int32)
+
+
 def ssb_join(query: str, n: int, seed: int, device="cuda"):
     """Device columns, hash tables and the join + group-by arguments of the
     Q3.1 / Q4.1 shapes (fls_q31.cu / fls_q41.cu): (tables, hash tables, host
