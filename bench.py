@@ -38,7 +38,11 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["q11", "q21", "q31", "q41", "ssb", "decode", "mixed"], default="q11")
+    ap.add_argument("--workload", choices=["q11", "q21", "q31", "q41", "ssb", "ssb-real", "decode", "mixed"],
+                    default="q11")
+    ap.add_argument("--ssb-dir", default="",
+                    help="ssb-real: directory of the Star Schema Benchmark columns loaded from dbgen's tables "
+                         "(<column>.i32; default $FLS_SSB_DIR/sf10 or <tmp>/fls_ssb/sf10)")
     ap.add_argument("--rows", type=int, default=0, help="rows per GPU (0 = 2^27 for queries, 2^28 for decode)")
     ap.add_argument("--decode-bw", type=int, default=16, help="bit width of the FOR decode workload")
     ap.add_argument("--decode-width", type=int, choices=[8, 16, 32, 64], default=32,
@@ -231,7 +235,8 @@ def run_ours(a, dist: Dist):
         ops.set_tuning(3, a.late_measure)
     ops.set_tuning(4, a.table_kb)
     explicit_variants = a.late_measure is not None or a.table_kb != 0 or a.group_smem is not None
-    tune_joins = a.tune_joins if a.tune_joins is not None else int(a.workload == "ssb" or not explicit_variants)
+    tune_joins = a.tune_joins if a.tune_joins is not None else int(a.workload in ("ssb", "ssb-real") or
+                                                                    not explicit_variants)
     from fastlanesgpu_b200.shard import allreduce_sum, combine_group_records, shard_seed
     seed = shard_seed(1000, dist.rank)
     # ---------------------------------------------------------------- setup
@@ -287,18 +292,28 @@ def run_ours(a, dist: Dist):
                         "columns": "supp 17b, cust 18b, part 19b, date 12b, revenue 24b, supplycost 18b",
                         "filters": "supplier region 1/5, customer region 1/5, part manufacturer 2/5"}
         metric_key = a.workload
-    elif a.workload == "ssb":
+    elif a.workload in ("ssb", "ssb-real"):
         # the thirteen SSB queries over one lineorder table (dimension tables
         # and hash tables replicated per rank); results side by side in one
         # int32 buffer, 8-byte aligned per query
-        t = datagen.ssb_tables(a.rows, seed=seed)
-        names = list(datagen.SSB_BITS)
-        hcols = [EncodedColumn.uniform(t[k], bw=datagen.SSB_BITS[k]) for k in names]
+        if a.workload == "ssb":
+            t = datagen.ssb_tables(a.rows, seed=seed)
+            names = list(datagen.SSB_BITS)
+            hcols = [EncodedColumn.uniform(t[k], bw=datagen.SSB_BITS[k]) for k in names]
+            make_query = datagen.ssb_device_query
+        else:
+            # dbgen's tables in the reference loader's encoding, every rank the same
+            t = datagen.ssb_dbgen_load(a.ssb_dir or datagen.ssb_dbgen_default_dir(10))
+            a.rows = int(t["lo_orderdate"].size)
+            enc = datagen.ssb_dbgen_columns(t)
+            names = list(enc)
+            hcols = [enc[k] for k in names]
+            make_query = datagen.ssb_dbgen_query
         dcols = [c.to_device(dev) for c in hcols]
         dmap = dict(zip(names, dcols))
         suite, off = [], 0
         for name in datagen.SSB_QUERIES:
-            dq = datagen.ssb_device_query(name, t, dmap, device=dev)
+            dq = make_query(name, t, dmap, device=dev)
             words = 2 if dq["kind"] == "filter" else dq["kw"]["res_stride"] * dq["kw"]["n_groups"]
             suite.append((name, dq, off, words))
             off += words + (words & 1)
@@ -332,15 +347,20 @@ def run_ours(a, dist: Dist):
             for _, dq, o, w in suite:
                 run_query(dq, o, w)
             return res
-        workload = {"workload": "SSB suite: Q1.1-Q4.3 (crystal-opt src/ssb q11..q43 shapes) over one lineorder "
-                                "table, 13 fused decode+query launches per step",
+        what = ("SSB suite: Q1.1-Q4.3 (crystal-opt src/ssb q11..q43 shapes) over one lineorder table, 13 fused "
+                "decode+query launches per step")
+        if a.workload == "ssb-real":
+            what += (f"; the Star Schema Benchmark's own data (dbgen, {a.rows} lineorder rows, the reference loader's "
+                     "encoding), FastLanes FOR columns at the smallest bit widths")
+        workload = {"workload": what,
                     "rows_per_gpu": a.rows, "rows_scanned_per_step": 13 * a.rows,
-                    "columns": ", ".join(f"{k[3:]} {b}b" for k, b in datagen.SSB_BITS.items()),
-                    "dimensions": "supplier 2^17, customer 2^18, part 2^19 keys, 2556 days; cities/nations/regions "
-                                  "and brands/categories/manufacturers in dbgen's hierarchy",
+                    "columns": ", ".join(f"{k[3:]} {c.bw}b" for k, c in zip(names, hcols)),
+                    "dimensions": ("supplier 2^17, customer 2^18, part 2^19 keys, 2556 days; cities/nations/regions "
+                                   "and brands/categories/manufacturers in dbgen's hierarchy") if a.workload == "ssb"
+                    else ", ".join(f"{k} {t[k].size}" for k in ("s_suppkey", "c_custkey", "p_partkey", "d_datekey")),
                     "join_variants": {name: dq.get("tuned", "defaults") for name, dq, _, _ in suite
                                       if dq["kind"] == "join"}}
-        metric_key = "ssb"
+        metric_key = a.workload
     else:
         from fastlanesgpu_b200 import LAYOUT_TRANSPOSED, SCHEME_DELTA, SCHEME_RLE
         if a.decode_scheme == "for" and a.decode_width != 32:
@@ -426,14 +446,14 @@ def run_ours(a, dist: Dist):
         workload["join_variants"] = best["config"]
     comp_bytes = sum(c.nbytes for c in hcols)
     algo_bytes = comp_bytes + (out_bytes if a.workload == "decode" else 0)
-    if a.workload == "ssb":
+    if a.workload in ("ssb", "ssb-real"):
         algo_bytes = suite_bytes  # every query reads its own columns
 
     def collective():
         # the one exchange of the sharded query: combine the ranks' partial aggregates
         if not dist.pg:
             return
-        if a.workload == "ssb":
+        if a.workload in ("ssb", "ssb-real"):
             for _, dq, o, w in suite:
                 if dq["kind"] == "filter":
                     allreduce_sum(res[o:o + 2].view(torch.int64))
@@ -501,7 +521,7 @@ def run_ours(a, dist: Dist):
     e2e_ms = dist.max(x0.elapsed_time(x1)) / n_e2e
     clk = clocks.stop()
     per_query = None
-    if a.workload == "ssb":
+    if a.workload in ("ssb", "ssb-real"):
         # each query alone (outside the timed region), CUDA events, 20 runs
         per_query = {}
         for name, dq, o, w in suite:
@@ -517,13 +537,14 @@ def run_ours(a, dist: Dist):
             per_query[name] = {"ms": round(qms, 4), "hbm_frac": round(qb / (qms / 1e3) / 1e9 / measured_peak_gbs()[0],
                                                                        3)}
 
+    answers = ssb_real_answers(a.rows, suite, res) if a.workload == "ssb-real" else None
     if a.workload == "decode" and a.decode_out == "hbm":
         exchange = "no exchange (each rank keeps its decoded shard)"
-    elif a.workload in ("q21", "q31", "q41", "ssb"):
+    elif a.workload in ("q21", "q31", "q41", "ssb", "ssb-real"):
         exchange = "group records combined per step (all-reduce MAX of the key words, SUM of the group sums)"
     else:
         exchange = "one int64 all-reduce per step"
-    rows_total = a.rows * dist.world * (13 if a.workload == "ssb" else 1)
+    rows_total = a.rows * dist.world * (13 if a.workload in ("ssb", "ssb-real") else 1)
     value = rows_total * a.steps / (ms / 1e3)
     ms_step = ms / a.steps
     peak, peak_src = measured_peak_gbs()
@@ -554,6 +575,8 @@ def run_ours(a, dist: Dist):
                               jit_launches=int(ops.jit_stats()["launches"])),
         "clocks": clk,
     }
+    if answers is not None:
+        out["reference_answers"] = answers
     if per_query is not None:
         out["per_query"] = per_query
         out["roofline"]["algorithmic_bytes_per_launch"] = algo_bytes
@@ -564,6 +587,35 @@ def run_ours(a, dist: Dist):
 
 
 M64 = (1 << 64) - 1
+
+
+def ssb_real_answers(rows: int, suite, res) -> dict:
+    """The SSB results on dbgen's data against the answers the reference holds
+    (fastlanes/src/include/ssb_utils.h:178-183 and data/result_of_queries,
+    committed as tests/golden/ssb_answers.json): Q1.1 at scale factors 0.1, 1
+    and 10, Q1.2 and Q1.3 at 1, every group of Q2.1, Q3.1 and Q4.1 at 10."""
+    import numpy as np
+    with open(os.path.join(ROOT, "tests", "golden", "ssb_answers.json")) as f:
+        ans = json.load(f)
+    sf = {600597: "0.1", 6001171: "1", 59986214: "10"}.get(rows)
+    got = {name: (dq, o, w) for name, dq, o, w in suite}
+    checked, equal = [], True
+    for name, by_sf in ans["scalar"].items():
+        if sf in by_sf:
+            dq, o, w = got[name]
+            v = int(res[o:o + 2].view(__import__("torch").int64).cpu()[0])
+            checked.append(name)
+            equal = equal and v == by_sf[sf]
+    if sf == "10":
+        for name, key_words in (("q21", 2), ("q31", 3), ("q41", 2)):
+            dq, o, w = got[name]
+            kw = dq["kw"]
+            rec = res[o:o + w].cpu().numpy().reshape(-1, kw["res_stride"])
+            sums = rec[:, kw["sum_slot"]:kw["sum_slot"] + 2].copy().view(np.int64)[:, 0]
+            rows_ = sorted([int(x) for x in r[:key_words]] + [int(s_)] for r, s_ in zip(rec, sums) if s_ != 0)
+            checked.append(name)
+            equal = equal and rows_ == sorted(ans["groups_sf10"][name])
+    return {"scale_factor": sf, "checked": checked, "equal": bool(equal and checked)}
 
 REF_HOW = {
     "q11": "the reference's unpack (unpack_fused.cuh, host-compiled from its sources) + the fls_q11.cu loop",
@@ -918,7 +970,7 @@ def run_reference(a, dist: Dist):
     R = orc.Reference()
     info = cpu_info()
     threads = info["usable_cpus"]
-    if a.workload in ("mixed", "ssb") or (a.workload == "decode" and (a.decode_scheme != "for" or
+    if a.workload in ("mixed", "ssb", "ssb-real") or (a.workload == "decode" and (a.decode_scheme != "for" or
                                                                         a.decode_width != 32)):
         return {"impl": "reference", "unavailable": "the reference has no CPU implementation of this workload "
                 "(learned selection, batching, per-vector DELTA/RLE/DICT columns, 8/16/64-bit lanes (it only "
@@ -1178,9 +1230,9 @@ def main():
     dist.init()
     failed = False
     try:
+        if a.workload in ("mixed", "ssb-real") and dist.world > 1:
+            raise SystemExit(f"--workload {a.workload} runs on one GPU")
         if a.workload == "mixed":
-            if dist.world > 1:
-                raise SystemExit("--workload mixed runs on one GPU")
             print(json.dumps(run_mixed(a, dist)), flush=True)
             return
         out, ctx = run_ours(a, dist)
@@ -1191,6 +1243,8 @@ def main():
             out["result_check"] = {"against": "the reference's CPU implementation on the whole benched table "
                                               "(cpu_baseline leg)", "equal": out["cpu_baseline"]["result_equal"]}
             failed = not out["result_check"]["equal"]
+        if "reference_answers" in out:
+            failed = failed or not out["reference_answers"]["equal"]
         del ctx
         if dist.world == 1 and a.workload == "q11" and a.secondary == "all" and not failed:
             sec = {"note": "other configurations, each timed with CUDA events after warm-up; inputs larger than L2"}

@@ -1,8 +1,11 @@
 """Seeded synthetic inputs with the shapes, sizes and value distributions of the
-workloads the reference measures (its SSB data is not available; these stand
-in for it).  All generators use numpy's PCG64 with an explicit seed.
+workloads the reference measures, and the Star Schema Benchmark queries on
+them and on SSB's own data (dbgen's tables, loaded in the reference loader's
+integer encoding).  All generators use numpy's PCG64 with an explicit seed.
 """
 from __future__ import annotations
+
+import os
 
 import numpy as np
 
@@ -442,3 +445,86 @@ def ssb_device_query(name: str, t: dict, dcols: dict, device="cuda"):
     kw = dict(agg_col=q["agg"], keys=q["keys"], group_sub=q["sub"], n_groups=q["groups"], res_stride=q["stride"],
               sum_slot=q["sum_slot"], sum_bits=q["sum_bits"], agg_sub_col=-1 if q["agg_sub"] is None else q["agg_sub"])
     return dict(kind="join", cols=cols, tables=tables, probes=probes, kw=kw)
+
+
+# ------------------------------------------------ SSB on dbgen's tables
+# The same thirteen queries on the tables of SSB's own generator (dbgen), in
+# the reference loader's integer encoding: dates are yyyymmdd day keys, the
+# dimension keys run from 1 to the table's row count, and the hash tables are
+# those of crystal-opt src/ssb and fastlanes/src/ssb: a supplier, customer or
+# part table has one slot per dimension row, slot = key % rows
+# (HASH(key, len, 0), crystal-opt/join.cuh:26), and the date table has
+# 19981230 - 19920101 + 1 slots from key 19920101 (fls_q21.cu:290,309).
+
+SSB_DATE_MIN = 19920101
+SSB_DATE_SLOTS = 19981230 - 19920101 + 1
+
+# Q1.x date predicates on yyyymmdd keys (crystal-opt src/ssb/q11.cu: year
+# 1993; q12.cu: January 1994; q13.cu: week 6 of 1994 = 4-10 February).
+SSB_DBGEN_DATE_FILTER = {"q11": (19930101, 19931231), "q12": (19940101, 19940131), "q13": (19940204, 19940210)}
+
+
+def ssb_dbgen_dims(t: dict) -> dict:
+    """(key column, hash table slots, keys_min) of each dimension."""
+    return {"d": ("d_datekey", SSB_DATE_SLOTS, SSB_DATE_MIN), "s": ("s_suppkey", int(t["s_suppkey"].size), 0),
+            "c": ("c_custkey", int(t["c_custkey"].size), 0), "p": ("p_partkey", int(t["p_partkey"].size), 0)}
+
+
+def ssb_dbgen_columns(t: dict, names=None) -> dict:
+    """Fact columns encoded as the reference encodes them: uniform FOR with the
+    column minimum as base (fls_q21.cu:373-375 subtracts lo_orderdate's) and
+    the smallest bit width that holds max - min."""
+    from .column import EncodedColumn
+    out = {}
+    for k in names or SSB_BITS:
+        v = t[k]
+        out[k] = EncodedColumn.uniform(v, base=int(v.min()))
+    return out
+
+
+def ssb_dbgen_query(name: str, t: dict, dcols: dict, device="cuda"):
+    """ssb_device_query for dbgen's tables (see ssb_dbgen_dims and
+    SSB_DBGEN_DATE_FILTER): the same predicates, group formulas and record
+    layouts."""
+    import torch
+
+    from . import ops
+    q = SSB_QUERIES[name]
+    cols = [dcols[c] for c in q["cols"]]
+    if q["kind"] == "filter":
+        lo, hi = SSB_DBGEN_DATE_FILTER[name]
+        filters = [(0, lo, hi)] + list(q["filters"][1:])
+        return dict(kind="filter", cols=cols, filters=filters, agg_a=3, agg_b=1)
+    dims = ssb_dbgen_dims(t)
+    tables, probes = [], []
+    for col, dim, payload, filt, ranges in q["probes"]:
+        key_col, length, kmin = dims[dim]
+        to = lambda k: torch.from_numpy(t[k]).to(device)  # noqa: E731
+        ht = ops.build_pht(to(key_col), length, vals=None if payload is None else to(payload),
+                           filt=None if filt is None else to(filt), ranges=ranges, keys_min=kmin)
+        tables.append(ht)
+        probes.append((col, ht, length, kmin, 1 if payload is None else 2))
+    kw = dict(agg_col=q["agg"], keys=q["keys"], group_sub=q["sub"], n_groups=q["groups"], res_stride=q["stride"],
+              sum_slot=q["sum_slot"], sum_bits=q["sum_bits"], agg_sub_col=-1 if q["agg_sub"] is None else q["agg_sub"])
+    return dict(kind="join", cols=cols, tables=tables, probes=probes, kw=kw)
+
+
+SSB_DBGEN_COLUMNS = ["lo_custkey", "lo_partkey", "lo_suppkey", "lo_orderdate", "lo_quantity", "lo_extendedprice",
+                     "lo_discount", "lo_revenue", "lo_supplycost", "s_suppkey", "s_city", "s_nation", "s_region",
+                     "c_custkey", "c_city", "c_nation", "c_region", "p_partkey", "p_mfgr", "p_category", "p_brand1",
+                     "d_datekey", "d_year", "d_yearmonthnum", "d_weeknuminyear"]
+
+
+def ssb_dbgen_default_dir(sf: float) -> str:
+    import tempfile
+    base = os.environ.get("FLS_SSB_DIR") or os.path.join(tempfile.gettempdir(), "fls_ssb")
+    return os.path.join(base, f"sf{sf:g}")
+
+
+def ssb_dbgen_load(path: str) -> dict:
+    """SSB columns loaded from dbgen's tables: <path>/<column>.i32, raw int32
+    in the reference loader's encoding (written by the loader next to the
+    oracle, oracle/ssb_load.c)."""
+    if not os.path.exists(os.path.join(path, "complete")):
+        raise FileNotFoundError(f"no loaded SSB tables in {path} (generate them with python oracle/ssb_data.py)")
+    return {k: np.fromfile(os.path.join(path, k + ".i32"), dtype=np.int32) for k in SSB_DBGEN_COLUMNS}
