@@ -1,0 +1,39 @@
+"""The drop-in device API without a GPU: the reference's own kernel files --
+its SSB query kernels (fastlanes/src/ssb) and its decode microbenchmarks
+(fastlanes/src/bitpack_*.cu, delta_*.cu) -- compile for sm_100a, unchanged,
+against include/fls_crystal.cuh through the headers under include/compat
+(first on the include path, ahead of the reference's own include directory).
+Runs where the reference sources and nvcc are present; the kernels
+themselves run in tests/test_gpu_dropin_reference.py."""
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_SRC = "/root/reference/fastlanes/src"
+FILES = ["ssb/fls_q11.cu", "ssb/fls_q21.cu", "ssb/fls_q31.cu", "ssb/fls_q41.cu", "ssb/compress_ssb.cu",
+         "ssb/compress_ssb_sorted.cu", "ssb/fls_q11_bitpacked_opt_v3.cu", "ssb/fls_q11_bitpacked_opt_v4.cu",
+         "ssb/fls_q21_bitpacked_opt_v4.cu", "ssb/fls_q31_bitpacked_opt_v5.cu", "ssb/fls_q41_bitpacked_opt_v3.cu",
+         "ssb/fls_q41_bitpacked_opt_v4.cu", "bitpack_shared_memory.cu", "bitpack_register.cu",
+         "delta_shared_memory.cu", "delta_global_memory.cu"]
+
+
+def _compile(f, out_dir):
+    cmd = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++20", "-O1", "-w", "-include", "algorithm",
+           '-DCMAKE_SOURCE_DIR=std::string("/")', "-I", os.path.join(ROOT, "include", "compat"),
+           "-I", os.path.join(ROOT, "oracle", "ref", "dropin_stub"), "-I", os.path.join(REF_SRC, "include"),
+           "-I", REF_SRC, "-c", "-o", os.path.join(out_dir, f.replace("/", "_") + ".o"), os.path.join(REF_SRC, f)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    return f, r.returncode, (r.stdout + r.stderr)[-1500:]
+
+
+def test_reference_kernel_files_compile_against_dropin_headers(tmp_path):
+    if not os.path.isdir(REF_SRC) or shutil.which("nvcc") is None:
+        pytest.skip("needs the reference sources and nvcc")
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        results = list(ex.map(lambda f: _compile(f, str(tmp_path)), FILES))
+    failed = [(f, log) for f, rc, log in results if rc != 0]
+    assert not failed, failed
