@@ -1161,9 +1161,11 @@ def decode_sweep(a, dist, steps: int) -> dict:
 def decode_schemes(a, dist, steps: int) -> dict:
     """DELTA (sorted keys, geometric gaps p=0.3), RLE (geometric runs of mean
     16, values in [0, 2^16)) and DICT (Zipf 1.1 over [0, 2^20)) columns of 2^28
-    values, generated and encoded on the GPU (per-vector metadata), decoded to
-    HBM (stored order) and fused with a uint64 sum; checked by decoding in
-    original order against the input values and by the input's sum."""
+    values, generated and encoded on the GPU (per-vector metadata), and the
+    same runs in the reference's tile-based RLE format (RFOR, host-encoded),
+    decoded to HBM (stored order) and fused with a uint64 sum; checked by
+    decoding in original order against the input values and by the input's
+    sum."""
     import torch
 
     from fastlanesgpu_b200 import LAYOUT_TRANSPOSED, ORDER_ORIGINAL, SCHEME_DELTA, SCHEME_DICT, SCHEME_RLE, datagen, ops
@@ -1172,19 +1174,31 @@ def decode_schemes(a, dist, steps: int) -> dict:
     n = 1 << 28
     peak = measured_peak_gbs()[0]
     out = {}
+    from fastlanesgpu_b200.column import RforColumn
     for name, scheme, gen in (
             ("delta", SCHEME_DELTA, lambda: datagen.sorted_geometric_device(n, 0.3, seed=2801, device=dev)),
             ("rle", SCHEME_RLE, lambda: datagen.geometric_runs_device(n, 16.0, 16, seed=2802, device=dev)),
-            ("dict", SCHEME_DICT, lambda: datagen.zipf_device(n, s=1.1, domain=1 << 20, seed=2803, device=dev))):
+            ("dict", SCHEME_DICT, lambda: datagen.zipf_device(n, s=1.1, domain=1 << 20, seed=2803, device=dev)),
+            ("rfor", None, lambda: datagen.geometric_runs_device(n, 16.0, 16, seed=2804, device=dev))):
         vals = gen()
-        col = encode_column_gpu(vals, scheme, layout=LAYOUT_TRANSPOSED)
-        dec = torch.empty(col.n_vec * 1024, dtype=torch.int32, device=dev)
         s = torch.zeros(1, dtype=torch.int64, device=dev)
-        ms_sum = _time_gpu(lambda: ops.query_aggregate(col, out=s), steps, max(3, a.warmup))
-        ms_hbm = _time_gpu(lambda: ops.unpack_global(col, out=dec), steps, max(3, a.warmup))
+        if scheme is None:
+            # the reference's tile-based RLE (tile_based/src/rlebinpack.cpp), encoded on the host
+            col = RforColumn.encode(vals.cpu().numpy()).to_device(dev)
+            dec = torch.empty(n, dtype=torch.int32, device=dev)
+            sum_fn, hbm_fn = (lambda: ops.rfor_decode_sum(col, out=s)), (lambda: ops.rfor_decode(col, out=dec))
+        else:
+            col = encode_column_gpu(vals, scheme, layout=LAYOUT_TRANSPOSED)
+            dec = torch.empty(col.n_vec * 1024, dtype=torch.int32, device=dev)
+            sum_fn, hbm_fn = (lambda: ops.query_aggregate(col, out=s)), (lambda: ops.unpack_global(col, out=dec))
+        ms_sum = _time_gpu(sum_fn, steps, max(3, a.warmup))
+        ms_hbm = _time_gpu(hbm_fn, steps, max(3, a.warmup))
         want = int((vals.to(torch.int64) & 0xFFFFFFFF).sum()) & M64
         equal = (int(s.cpu()[0]) & M64) == want
-        ops.unpack_global(col, order=ORDER_ORIGINAL, out=dec)
+        if scheme is None:
+            ops.rfor_decode(col, out=dec)
+        else:
+            ops.unpack_global(col, order=ORDER_ORIGINAL, out=dec)
         equal = equal and bool(torch.equal(dec[:n], vals))
         ops.check_device_error()
         b = col.nbytes

@@ -20,6 +20,7 @@ STATUS_NAMES = {0: "FLS_OK", 1: "FLS_ERR_INVALID_ARG", 2: "FLS_ERR_BAD_BW", 3: "
 SCHEME_FOR, SCHEME_DELTA, SCHEME_RLE, SCHEME_CONST, SCHEME_DICT = 0, 1, 2, 3, 4
 SCHEME_NAMES = ["FOR", "DELTA", "RLE", "CONST", "DICT"]
 LAYOUT_NORMAL, LAYOUT_TRANSPOSED = 0, 1
+RFOR_TILE = 512  # values per tile of the RFOR format (FLS_RFOR_TILE)
 ORDER_STORED, ORDER_ORIGINAL = 0, 1
 MAX_QUERY_COLS, MAX_FILTERS, MAX_PROBES = 8, 4, 4
 TUNE_SPARSE_ROWS, TUNE_JIT, TUNE_GROUP_SMEM, TUNE_LATE_MEASURE, TUNE_TABLE_KB = 0, 1, 2, 3, 4
@@ -85,6 +86,12 @@ class JoinGroupbyDesc(ctypes.Structure):
                 ("key_slot", ctypes.c_int32 * MAX_GROUP_KEYS), ("group_sub", ctypes.c_int32),
                 ("n_groups", ctypes.c_int32), ("res_stride", ctypes.c_uint32), ("sum_slot", ctypes.c_uint32),
                 ("sum_bits", ctypes.c_uint32)]
+
+
+class RforColumnDesc(ctypes.Structure):
+    _fields_ = [("values", ctypes.c_void_p), ("run_lengths", ctypes.c_void_p), ("val_offsets", ctypes.c_void_p),
+                ("rl_offsets", ctypes.c_void_p), ("n_values", ctypes.c_uint64), ("n_val_words", ctypes.c_uint64),
+                ("n_rl_words", ctypes.c_uint64)]
 
 
 class JitStats(ctypes.Structure):
@@ -176,6 +183,10 @@ _SIGS = {
     "fls_query_join_groupby": (ctypes.c_int, [ctypes.POINTER(JoinGroupbyDesc), _VP, _VP]),
     "fls_query_join_groupby_ws": (ctypes.c_int, [ctypes.POINTER(JoinGroupbyDesc), _VP, _VP, ctypes.c_uint64, _VP]),
     "fls_join_workspace_bytes": (ctypes.c_uint64, [ctypes.POINTER(JoinGroupbyDesc)]),
+    "fls_rfor_bound_words": (ctypes.c_uint64, [ctypes.c_uint64]),
+    "fls_rfor_encode": (ctypes.c_int, [_VP, ctypes.c_uint64, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "fls_rfor_decode_u32": (ctypes.c_int, [ctypes.POINTER(RforColumnDesc), _VP, _VP]),
+    "fls_rfor_decode_sum_u32": (ctypes.c_int, [ctypes.POINTER(RforColumnDesc), _VP, _VP]),
 }
 
 _LIB = None

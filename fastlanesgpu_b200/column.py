@@ -285,6 +285,68 @@ def encode_column_learned_gpu(values, params, threshold: float = 0.9, kappa: flo
     return DeviceEncodedColumn(out, meta, n, layout, total, mx, mask), schemes, n_fb
 
 
+@dataclass
+class RforColumn:
+    """A column in the reference's tile-based run-length format (RFOR,
+    tile_based/src/rlebinpack.cpp): per 512-value tile the runs' values and
+    lengths, each FOR bit-packed in its own stream, with per-tile word
+    offsets into both streams."""
+    values: np.ndarray       # uint32 value stream
+    run_lengths: np.ndarray  # uint32 run-length stream
+    val_offsets: np.ndarray  # uint32, tiles + 1
+    rl_offsets: np.ndarray   # uint32, tiles + 1
+    n_values: int
+
+    @property
+    def n_tiles(self) -> int:
+        return (self.n_values + _lib.RFOR_TILE - 1) // _lib.RFOR_TILE
+
+    @property
+    def nbytes(self) -> int:
+        """Encoded bytes a decode reads: both streams and both offset arrays."""
+        return 4 * (self.values.size + self.run_lengths.size + self.val_offsets.size + self.rl_offsets.size)
+
+    @classmethod
+    def encode(cls, values: np.ndarray) -> "RforColumn":
+        v = np.ascontiguousarray(values).view(np.uint32)
+        n = int(v.size)
+        bound = int(lib().fls_rfor_bound_words(n))
+        tiles = (n + _lib.RFOR_TILE - 1) // _lib.RFOR_TILE
+        vs, rs = np.zeros(bound, np.uint32), np.zeros(bound, np.uint32)
+        vo, ro = np.zeros(tiles + 1, np.uint32), np.zeros(tiles + 1, np.uint32)
+        nv, nr = ctypes.c_uint64(), ctypes.c_uint64()
+        check(lib().fls_rfor_encode(_ptr(v), n, _ptr(vs), _ptr(rs), _ptr(vo), _ptr(ro), ctypes.addressof(nv),
+                                    ctypes.addressof(nr)), "fls_rfor_encode")
+        return cls(vs[:nv.value].copy(), rs[:nr.value].copy(), vo, ro, n)
+
+    def to_device(self, device=None) -> "DeviceRforColumn":
+        return DeviceRforColumn(self, device)
+
+
+class DeviceRforColumn:
+    """An RforColumn in device memory, with its C descriptor."""
+
+    def __init__(self, col: RforColumn, device=None):
+        import torch
+        dev = torch.device("cuda") if device is None else torch.device(device)
+        self.host = col
+        t = lambda a: torch.from_numpy(a.view(np.int32)).to(dev)  # noqa: E731
+        self.values, self.run_lengths = t(col.values), t(col.run_lengths)
+        self.val_offsets, self.rl_offsets = t(col.val_offsets), t(col.rl_offsets)
+        self.desc = _lib.RforColumnDesc(values=self.values.data_ptr(), run_lengths=self.run_lengths.data_ptr(),
+                                        val_offsets=self.val_offsets.data_ptr(), rl_offsets=self.rl_offsets.data_ptr(),
+                                        n_values=col.n_values, n_val_words=int(col.values.size),
+                                        n_rl_words=int(col.run_lengths.size))
+
+    @property
+    def n_values(self) -> int:
+        return self.host.n_values
+
+    @property
+    def nbytes(self) -> int:
+        return self.host.nbytes
+
+
 def _aligned16(n: int) -> np.ndarray:
     """A uint8 array of n bytes starting on a 16-byte boundary."""
     raw = np.zeros(n + 16, dtype=np.uint8)
@@ -299,7 +361,8 @@ def columns_array(cols) -> ctypes.Array:
     return arr
 
 
-__all__ = ["EncodedColumn", "DeviceColumn", "DeviceUniformColumn", "DeviceEncodedColumn", "encode_column_gpu", "encode_column_learned_gpu",
+__all__ = ["EncodedColumn", "DeviceColumn", "DeviceUniformColumn", "DeviceEncodedColumn", "RforColumn",
+           "DeviceRforColumn", "encode_column_gpu", "encode_column_learned_gpu",
            "META_DTYPE", "columns_array",
            "n_vectors", "_lib",
            "SCHEME_DELTA", "LAYOUT_TRANSPOSED"]

@@ -78,6 +78,185 @@ struct DecodeSumOp {
 	}
 };
 
+// ------------------------------------------------------------------------
+// Decode fused with a sum for columns whose vectors all share one scheme
+// (DELTA, RLE or DICT; scheme_mask has one bit), as the encoder produces for
+// sorted keys, runs and dictionaries.  The scheme is a template parameter, so
+// the per-vector scheme switch and the value array of the general operator
+// disappear: each decoded value goes straight into the lane's sum.  The bit
+// width stays a warp-uniform switch per vector (vectors of one column differ
+// in width).  Values whose 32-row lane sum cannot exceed 32 bits (every value
+// below 2^27, known from the vector's base and width) are summed in 32 bits.
+//
+// The reference times delta decode + sum as delta_shared_memory.cu:24-61
+// (unpack to shared memory, d_rsum_32, BlockLoad, BlockSum per 1024 values).
+
+template <int BW>
+__device__ __forceinline__ unsigned long long delta_lane_sum(const uint32_t* __restrict__ s, uint32_t lane,
+                                                             uint32_t rows) {
+	dev::LaneWords<BW> lw;
+	dev::load_words<BW>(s + 32, lane, lw);
+	uint32_t           x   = s[lane];
+	unsigned long long acc = 0;
+	if (rows == 0xffffffffu) {
+#pragma unroll
+		for (int st = 0; st < 32; ++st) {
+			x += dev::extract<BW>(lw, static_cast<int>(dev::rsum_row(st)));
+			acc += x;
+		}
+	} else {
+#pragma unroll
+		for (int st = 0; st < 32; ++st) {
+			const int r = static_cast<int>(dev::rsum_row(st));
+			x += dev::extract<BW>(lw, r);
+			acc += ((rows >> r) & 1u) ? x : 0u;
+		}
+	}
+	return acc;
+}
+
+// True when every value of the vector (base + a bw-bit field) is below 2^27.
+__device__ __forceinline__ bool small_values(const VecInfo& m) {
+	const uint64_t top = static_cast<uint64_t>(static_cast<uint32_t>(m.base)) +
+	                     (m.bw >= 32 ? 0xffffffffull : ((1ull << m.bw) - 1ull));
+	return top < (1ull << 27);
+}
+
+template <bool Small>
+__device__ __forceinline__ unsigned long long rle_lane_sum(const uint32_t* __restrict__ s,
+                                                           const uint32_t* __restrict__ dict, uint32_t lane,
+                                                           uint32_t rows) {
+	uint32_t           idx  = reinterpret_cast<const uint16_t*>(s)[lane];
+	const uint32_t     bits = s[16 + lane];
+	uint32_t           s32  = 0;
+	unsigned long long s64  = 0;
+#pragma unroll
+	for (int st = 0; st < 32; ++st) {
+		const int r = static_cast<int>(dev::rsum_row(st));
+		idx += (bits >> r) & 1u;
+		const uint32_t v = ((rows >> r) & 1u) ? dict[idx & 1023u] : 0u;
+		if constexpr (Small) {
+			s32 += v;
+		} else {
+			s64 += v;
+		}
+	}
+	return Small ? static_cast<unsigned long long>(s32) : s64;
+}
+
+template <int CBW, bool Small>
+__device__ __forceinline__ unsigned long long dict_lane_sum(const uint32_t* __restrict__ s,
+                                                            const uint32_t* __restrict__ dict, uint32_t lane,
+                                                            uint32_t rows) {
+	dev::LaneWords<CBW> lw;
+	dev::load_words<CBW>(s, lane, lw);
+	uint32_t           s32 = 0;
+	unsigned long long s64 = 0;
+#pragma unroll
+	for (int r = 0; r < 32; ++r) {
+		const uint32_t v = ((rows >> r) & 1u) ? dict[dev::extract<CBW>(lw, r) & 1023u] : 0u;
+		if constexpr (Small) {
+			s32 += v;
+		} else {
+			s64 += v;
+		}
+	}
+	return Small ? static_cast<unsigned long long>(s32) : s64;
+}
+
+// Sequentially FOR-packed dictionary of n entries at bit width BW into dst
+// (base added), lanes striding over the entries.
+template <int BW>
+__device__ __forceinline__ void unpack_dict_bw(const uint32_t* __restrict__ src, uint32_t n, int32_t base,
+                                               uint32_t* __restrict__ dst, uint32_t lane) {
+	const uint32_t b = static_cast<uint32_t>(base);
+	for (uint32_t k = lane; k < n; k += 32) {
+		uint32_t v = 0;
+		if constexpr (BW == 32) {
+			v = src[k];
+		} else if constexpr (BW > 0) {
+			const uint32_t bit = k * BW, w = bit >> 5, sh = bit & 31u;
+			const uint32_t hi  = (sh + BW > 32u) ? src[w + 1] : 0u; // never past the dictionary
+			v                  = __funnelshift_r(src[w], hi, sh) & ((1u << BW) - 1u);
+		}
+		dst[k] = v + b;
+	}
+	__syncwarp();
+}
+
+__device__ __forceinline__ void unpack_dict_any(const uint32_t* __restrict__ src, uint32_t n, uint32_t bw,
+                                                int32_t base, uint32_t* __restrict__ dst, uint32_t lane) {
+	switch (bw) {
+#define FLS_DICT_UNPACK(B)                                                                                             \
+	case B: unpack_dict_bw<B>(src, n, base, dst, lane); break;
+		FLS_BW_CASES_0_32(FLS_DICT_UNPACK)
+#undef FLS_DICT_UNPACK
+	default: break;
+	}
+}
+
+template <uint32_t SCHEME>
+struct SchemeSumOp {
+	using State = AccState;
+	unsigned long long* sum;
+	__device__ void cta_setup(State&, uint32_t*, const StageCfg&) const {}
+	__device__ void process(State& S, uint64_t v, const WarpStage& ws, uint32_t st, uint32_t i, uint32_t lane,
+	                        const StageCfg& cfg) const {
+		const StagedVec sv = staged(ws, st, i, 0);
+		if (sv.bad()) { return; }
+		const uint32_t rows = valid_rows(cfg, v, lane);
+		if (sv.vi.scheme != SCHEME) { // the host saw one scheme; any other vector is flagged, not read
+			if (lane == 0) { raise_err(cfg.err, kErrBadMeta); }
+			return;
+		}
+		if constexpr (SCHEME == FLS_SCHEME_DELTA) {
+			switch (sv.vi.bw) {
+#define FLS_DELTA_SUM(B)                                                                                               \
+	case B: S.acc += delta_lane_sum<B>(sv.s, lane, rows); break;
+				FLS_BW_CASES_0_32(FLS_DELTA_SUM)
+#undef FLS_DELTA_SUM
+			default: break;
+			}
+		} else if constexpr (SCHEME == FLS_SCHEME_RLE) {
+			uint32_t* dict = ws.dict();
+			unpack_dict_any(sv.s + 48, sv.vi.aux, sv.vi.bw, sv.vi.base, dict, lane);
+			S.acc += small_values(sv.vi) ? rle_lane_sum<true>(sv.s, dict, lane, rows)
+			                             : rle_lane_sum<false>(sv.s, dict, lane, rows);
+			__syncwarp();
+		} else {
+			uint32_t*      dict = ws.dict();
+			const uint32_t cbw  = dev::bits_of(sv.vi.aux - 1u);
+			unpack_dict_any(sv.s + 32u * cbw, sv.vi.aux, sv.vi.bw, sv.vi.base, dict, lane);
+			const bool small = small_values(sv.vi);
+			switch (cbw) {
+#define FLS_DICT_SUM(B)                                                                                                \
+	case B:                                                                                                            \
+		S.acc += small ? dict_lane_sum<B, true>(sv.s, dict, lane, rows) : dict_lane_sum<B, false>(sv.s, dict, lane, rows); \
+		break;
+				FLS_BW_CASES_0_10(FLS_DICT_SUM)
+#undef FLS_DICT_SUM
+			default: break;
+			}
+			__syncwarp();
+		}
+	}
+	__device__ void finish(State& S, uint32_t lane, const StageCfg&) const {
+		const unsigned long long s = warp_sum_u64(S.acc);
+		if (lane == 0 && s) { atomicAdd(sum, s); }
+	}
+};
+
+// The single scheme of a per-vector column that has a specialised sum, or
+// FLS_N_SCHEMES.
+uint32_t single_scheme(const fls_column& c) {
+	if (!c.meta) { return FLS_N_SCHEMES; }
+	const uint32_t m = c.scheme_mask;
+	if (m == (1u << FLS_SCHEME_DELTA)) { return FLS_SCHEME_DELTA; }
+	if (m == (1u << FLS_SCHEME_RLE)) { return FLS_SCHEME_RLE; }
+	if (m == (1u << FLS_SCHEME_DICT)) { return FLS_SCHEME_DICT; }
+	return FLS_N_SCHEMES;
+}
+
 } // namespace
 } // namespace fls
 
@@ -119,6 +298,15 @@ fls_status fls_decode_sum_u32(const fls_column* col, uint64_t* d_sum, fls_stream
 		bool used = false;
 		s         = jit_decode(col, 0, nullptr, d_sum, st, used);
 		if (s != FLS_OK || used) { return s; }
+	}
+	if (tuning_jit()) {
+		auto* sum = reinterpret_cast<unsigned long long*>(d_sum);
+		switch (single_scheme(*col)) {
+		case FLS_SCHEME_DELTA: return launch_staged(cfg, SchemeSumOp<FLS_SCHEME_DELTA> {sum}, grid, threads, smem, st);
+		case FLS_SCHEME_RLE: return launch_staged(cfg, SchemeSumOp<FLS_SCHEME_RLE> {sum}, grid, threads, smem, st);
+		case FLS_SCHEME_DICT: return launch_staged(cfg, SchemeSumOp<FLS_SCHEME_DICT> {sum}, grid, threads, smem, st);
+		default: break;
+		}
 	}
 	DecodeSumOp op {};
 	op.sum = reinterpret_cast<unsigned long long*>(d_sum);

@@ -118,6 +118,24 @@ def query_aggregate(col: DeviceColumn, out=None):
     return out
 
 
+def rfor_decode(col, out=None):
+    """Decode an RFOR column (DeviceRforColumn) to n_values int32 values (device)."""
+    import torch
+    if out is None:
+        out = torch.empty(col.n_values, dtype=torch.int32, device=col.values.device)
+    check(lib().fls_rfor_decode_u32(ctypes.byref(col.desc), out.data_ptr(), _stream()), "fls_rfor_decode_u32")
+    return out
+
+
+def rfor_decode_sum(col, out=None):
+    """RFOR decode fused with a uint64 sum of all values (device int64[1])."""
+    import torch
+    if out is None:
+        out = torch.empty(1, dtype=torch.int64, device=col.values.device)
+    check(lib().fls_rfor_decode_sum_u32(ctypes.byref(col.desc), out.data_ptr(), _stream()), "fls_rfor_decode_sum_u32")
+    return out
+
+
 def query_filter_agg(cols, filters, agg_a: int = -1, agg_b: int = -1, out=None):
     """Filters [(col, lo, hi)] (inclusive int32 ranges) ANDed; returns the int64
     sum of cols[agg_a] (* cols[agg_b]) over the selected rows, or the count."""

@@ -221,6 +221,42 @@ uint64_t   fls_column_container_bytes(const fls_column* col);
 fls_status fls_column_write_container(const fls_column* col, void* out, uint64_t out_bytes, uint64_t* written);
 fls_status fls_column_open_container(const void* buf, uint64_t bytes, fls_column* col);
 
+/* ------------------------------------------------------------ RFOR
+ * The reference's tile-based run-length format ("RFOR", tile_based/src/
+ * rlebinpack.cpp:9-146, decoded by LoadRBinPack in tile_based/src/include/
+ * rlebinpack_kernel.cuh:20-145): values in tiles of 512; per tile the runs'
+ * values and lengths, each FOR-packed in its own stream.  Both streams start
+ * with a 4-word header {512, 4, rows encoded, first value}; tile t's block in
+ * a stream starts at word offsets[t]: {minimum, bit width in each of the 4
+ * bytes, run count, then the count fields (x - minimum) packed LSB first, field
+ * i at bit i*bw, max(1, ceil(count*bw/32)) words}.  offsets has one entry per
+ * tile plus the end.  The rows are padded to whole tiles with the last value
+ * (as the reference pads, rlebinpack.cpp:219).  The reference's encoder
+ * packs 32-bit fields with a shift by 32 (undefined in C++); this encoder
+ * packs them as the format defines.
+ *
+ * fls_rfor_bound_words: words one stream may take for n rows.
+ * fls_rfor_encode (host): into caller buffers of that bound (values, run
+ * lengths) and of (n+511)/512 + 1 words (each offsets array).
+ * fls_rfor_decode_u32 / fls_rfor_decode_sum_u32 (device): one warp per tile;
+ * a tile whose block is inconsistent (counts, widths, offsets, run lengths
+ * not summing to the tile) is skipped and flagged (fls_check_device_error). */
+typedef struct fls_rfor_column {
+	const uint32_t* values;      /* device: value stream        */
+	const uint32_t* run_lengths; /* device: run-length stream   */
+	const uint32_t* val_offsets; /* device: tiles + 1 words     */
+	const uint32_t* rl_offsets;  /* device: tiles + 1 words     */
+	uint64_t        n_values;    /* rows (the last tile may be partial) */
+	uint64_t        n_val_words; /* size of the value stream (bounds checks) */
+	uint64_t        n_rl_words;  /* size of the run-length stream */
+} fls_rfor_column;
+#define FLS_RFOR_TILE 512
+uint64_t   fls_rfor_bound_words(uint64_t n);
+fls_status fls_rfor_encode(const uint32_t* values, uint64_t n, uint32_t* val_stream, uint32_t* rl_stream,
+                           uint32_t* val_offsets, uint32_t* rl_offsets, uint64_t* n_val_words, uint64_t* n_rl_words);
+fls_status fls_rfor_decode_u32(const fls_rfor_column* col, uint32_t* d_out, fls_stream_t stream);
+fls_status fls_rfor_decode_sum_u32(const fls_rfor_column* col, uint64_t* d_sum, fls_stream_t stream);
+
 /* Exhaustive per-vector encoder (the selector's labels and regret): exact encoded size in
  * bytes (payload + 16 B metadata) of every scheme for every vector
  * (sizes: n_vec*5, UINT32_MAX = not representable) and the argmin scheme, ties

@@ -685,6 +685,105 @@ void orc_vector_stats(const int32_t* v, float* f) {
 	f[15] = 1.0f;
 }
 
+/* ---- tile-based RLE (RFOR): tile_based/src/rlebinpack.cpp:9-146 ------- */
+
+uint64_t orc_rfor_bound(uint64_t n) { return 4u + ((n + 511u) / 512u) * (3u + 512u); }
+
+/* Appends one block (min, widths, count, packed fields) at stream[*o]. */
+static void rfor_block(uint32_t* stream, uint64_t* o, const uint32_t* x, uint32_t count) {
+	uint32_t mn = x[0];
+	for (uint32_t k = 1; k < count; ++k) { mn = x[k] < mn ? x[k] : mn; }
+	uint32_t bw = 0;
+	for (uint32_t k = 0; k < count; ++k) {
+		const unsigned b = orc_bit_width(x[k] - mn);
+		bw               = b > bw ? b : bw;
+	}
+	stream[(*o)++] = mn;
+	stream[(*o)++] = bw + (bw << 8) + (bw << 16) + (bw << 24);
+	stream[(*o)++] = count;
+	/* field after field, LSB first, carrying into the next word */
+	uint64_t w = *o, shift = 0;
+	stream[w]  = 0;
+	for (uint32_t k = 0; k < count; ++k) {
+		const uint32_t v = x[k] - mn;
+		if (bw == 0) { continue; }
+		if (shift == 32) {
+			stream[++w] = 0;
+			shift       = 0;
+		}
+		stream[w] |= v << shift;
+		if (shift + bw > 32) {
+			stream[++w] = v >> (32 - shift);
+			shift       = shift + bw - 32;
+		} else {
+			shift += bw;
+		}
+	}
+	*o = w + 1;
+}
+
+void orc_rfor_encode(const uint32_t* in, uint64_t n, uint32_t* val, uint32_t* rl, uint32_t* val_off, uint32_t* rl_off,
+                     uint64_t* n_val, uint64_t* n_rl) {
+	uint64_t vo = 4, ro = 4;
+	val[0] = rl[0] = 512;
+	val[1] = rl[1] = 4;
+	val[2] = rl[2] = (uint32_t)n;
+	val[3] = rl[3] = in[0];
+	uint32_t v[512], l[512];
+	for (uint64_t t = 0; t < n / 512; ++t) {
+		const uint32_t* x = in + 512 * t;
+		uint32_t        count = 0, run = 1;
+		for (uint32_t i = 1; i < 512; ++i) {
+			if (x[i] != x[i - 1]) {
+				v[count]   = x[i - 1];
+				l[count++] = run;
+				run        = 1;
+			} else {
+				++run;
+			}
+		}
+		v[count]   = x[511];
+		l[count++] = run;
+		val_off[t] = (uint32_t)vo;
+		rl_off[t]  = (uint32_t)ro;
+		rfor_block(val, &vo, v, count);
+		rfor_block(rl, &ro, l, count);
+	}
+	val_off[n / 512] = (uint32_t)vo;
+	rl_off[n / 512]  = (uint32_t)ro;
+	*n_val           = vo;
+	*n_rl            = ro;
+}
+
+static uint32_t rfor_field(const uint32_t* p, uint32_t k, uint32_t bw) {
+	if (bw == 0) { return 0; }
+	const uint64_t bit = (uint64_t)k * bw;
+	uint64_t       two = p[bit >> 5];
+	if ((bit & 31) + bw > 32) { two |= (uint64_t)p[(bit >> 5) + 1] << 32; }
+	return (uint32_t)((two >> (bit & 31)) & ((1ull << bw) - 1ull));
+}
+
+int orc_rfor_decode(const uint32_t* val, const uint32_t* rl, const uint32_t* val_off, const uint32_t* rl_off,
+                    uint64_t n, uint32_t* out) {
+	for (uint64_t t = 0; t * 512 < n; ++t) {
+		const uint32_t* vb = val + val_off[t];
+		const uint32_t* rb = rl + rl_off[t];
+		const uint32_t  count = vb[2], vbw = vb[1] & 255, rbw = rb[1] & 255;
+		if (count == 0 || count > 512 || rb[2] != count || vbw > 32 || rbw > 32) { return -1; }
+		uint32_t p = 0;
+		for (uint32_t k = 0; k < count; ++k) {
+			const uint32_t x   = vb[0] + rfor_field(vb + 3, k, vbw);
+			const uint32_t len = rb[0] + rfor_field(rb + 3, k, rbw);
+			for (uint32_t i = 0; i < len; ++i, ++p) {
+				if (p >= 512) { return -1; }
+				if (t * 512 + p < n) { out[t * 512 + p] = x; }
+			}
+		}
+		if (p != 512) { return -1; }
+	}
+	return 0;
+}
+
 uint64_t orc_splitmix64(uint64_t* state) {
 	uint64_t z = (*state += 0x9e3779b97f4a7c15ull);
 	z          = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;

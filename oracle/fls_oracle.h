@@ -139,6 +139,25 @@ double orc_mlp_loss_grad(const float* params, const float* x, const uint8_t* y, 
 /* 16 selector statistics of one vector (the same definitions as the library). */
 void orc_vector_stats(const int32_t* v, float* f16);
 
+/* ---- tile-based RLE (RFOR) ------------------------------------------------
+ * tile_based/src/rlebinpack.cpp:9-146 (encoder; n a multiple of 512, the
+ * caller pads with the last value as rlebinpack.cpp:217-219 does): both
+ * streams start {512, 4, n, in[0]}; per tile the runs (value, length) with
+ * min, bit width of (x - min) (ceil(log2(x+1)), :75-83), a block {min,
+ * bw * 0x01010101, count, fields packed LSB first} whose packed part takes
+ * max(1, ceil(count*bw/32)) words (:101-128); offsets[t] = block start,
+ * offsets[tiles] = end (:141-142).  Streams must hold orc_rfor_bound(n) words;
+ * returns the words written to each through n_val / n_rl.  Widths of 32 are
+ * packed as the format defines (the reference shifts by 32 there).
+ * orc_rfor_decode: the decoder's semantics (rlebinpack_kernel.cuh:20-145):
+ * position p of a tile holds the value of the run whose cumulative length
+ * first exceeds p.  Returns -1 on an inconsistent block. */
+uint64_t orc_rfor_bound(uint64_t n);
+void orc_rfor_encode(const uint32_t* in, uint64_t n, uint32_t* val, uint32_t* rl, uint32_t* val_off, uint32_t* rl_off,
+                     uint64_t* n_val, uint64_t* n_rl);
+int orc_rfor_decode(const uint32_t* val, const uint32_t* rl, const uint32_t* val_off, const uint32_t* rl_off,
+                    uint64_t n, uint32_t* out);
+
 /* ---- synthetic inputs (SplitMix64; shared with the Python tests) --------- */
 uint64_t orc_splitmix64(uint64_t* state);
 

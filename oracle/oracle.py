@@ -60,6 +60,10 @@ class Oracle:
         L.orc_bit_width.restype = ctypes.c_uint
         L.orc_vector_rle.restype = ctypes.c_int
         L.orc_encode_vec.restype = ctypes.c_int
+        L.orc_rfor_bound.restype = ctypes.c_uint64
+        L.orc_rfor_bound.argtypes = [ctypes.c_uint64]
+        L.orc_rfor_encode.argtypes = [_u32p, ctypes.c_uint64] + [_u32p] * 4 + [ctypes.c_void_p] * 2
+        L.orc_rfor_decode.argtypes = [_u32p] * 4 + [ctypes.c_uint64, _u32p]
         L.orc_filter_agg.restype = ctypes.c_int64
         L.orc_filter_agg.argtypes = [_i32p, _i32p, _i32p, _i32p, ctypes.c_uint64] + [ctypes.c_int32] * 5
         L.orc_pht1_build.argtypes = [_i32p, ctypes.c_int32, _i32p, ctypes.c_uint64, _i32p, ctypes.c_int32,
@@ -132,6 +136,27 @@ class Oracle:
         d4 = np.zeros(4, np.uint16)
         n = self.L.orc_vector_rle(_p(vec, _i32p), _p(idx, _u8p), _p(dic, _i32p), _p(d4, _u16p))
         return n, idx, dic[:n].copy(), d4
+
+    # -- tile-based RLE (RFOR) --------------------------------------------
+    def rfor_encode(self, values):
+        """tile_based/src/rlebinpack.cpp:9-146 on values padded to whole tiles
+        with the last value: (value stream, run-length stream, val_offsets,
+        rl_offsets)."""
+        v = np.ascontiguousarray(values).view(np.uint32)
+        n = (v.size + 511) // 512 * 512
+        x = np.concatenate([v, np.full(n - v.size, v[-1], np.uint32)])
+        bound = int(self.L.orc_rfor_bound(n))
+        val, rl = np.zeros(bound, np.uint32), np.zeros(bound, np.uint32)
+        vo, ro = np.zeros(n // 512 + 1, np.uint32), np.zeros(n // 512 + 1, np.uint32)
+        nv, nr = ctypes.c_uint64(), ctypes.c_uint64()
+        self.L.orc_rfor_encode(_p(x, _u32p), n, _p(val, _u32p), _p(rl, _u32p), _p(vo, _u32p), _p(ro, _u32p),
+                               ctypes.byref(nv), ctypes.byref(nr))
+        return val[:nv.value].copy(), rl[:nr.value].copy(), vo, ro
+
+    def rfor_decode(self, val, rl, vo, ro, n):
+        out = np.zeros(n, np.uint32)
+        rc = self.L.orc_rfor_decode(_p(val, _u32p), _p(rl, _u32p), _p(vo, _u32p), _p(ro, _u32p), n, _p(out, _u32p))
+        return None if rc != 0 else out
 
     # -- encoded vectors ---------------------------------------------------
     def encode_vec(self, vec, scheme: int, transposed: bool = True, round4: bool = False):
@@ -365,6 +390,20 @@ class Reference:
         d4 = np.zeros(4, np.uint16)
         n = self.L.ref_vector_rle(_p(vec, _i32p), _p(idx, _u8p), _p(dic, _i32p), _p(d4, _u16p))
         return n, idx, dic[:n].copy(), d4
+
+    def rfor_encode(self, values):
+        """The reference's rleBinPack (tile_based/src/rlebinpack.cpp) on values
+        padded to whole tiles with the last value, as its main pads them."""
+        v = np.ascontiguousarray(values).view(np.uint32)
+        n = (v.size + 511) // 512 * 512
+        x = np.concatenate([v, np.full(n - v.size, v[-1], np.uint32)])
+        bound = 4 + (n // 512) * 515
+        val, rl = np.zeros(bound, np.uint32), np.zeros(bound, np.uint32)
+        vo, ro = np.zeros(n // 512 + 1, np.uint32), np.zeros(n // 512 + 1, np.uint32)
+        sz = np.zeros(2, np.uint32)
+        self.L.ref_rfor_encode(_p(x, _u32p), n, _p(val, _u32p), _p(rl, _u32p), _p(vo, _u32p), _p(ro, _u32p),
+                               _p(sz, _u32p))
+        return val[:sz[0]].copy(), rl[:sz[1]].copy(), vo, ro
 
     def q11_sum(self, cols, bws, n_rows, date_lo, date_hi, disc_lo, disc_hi, qty_lt, threads):
         args = []

@@ -36,6 +36,13 @@ int ref_unpack_h16(const uint32_t* in, uint16_t* out, unsigned bw);
  * discarded).  Returns the total number of dictionary entries. */
 int ref_vector_rle(const int32_t* vec, uint8_t* idx, int32_t* dict, uint16_t* dict4);
 
+/* tile_based/src/rlebinpack.cpp:9-146 rleBinPack (RFOR): n a multiple of 512;
+ * value / run_length zero-initialised by the caller (the encoder adds into
+ * them), of at least 4 + (n/512)*515 words; offsets of n/512 + 1 words.
+ * sizes2 receives the words written to each stream. */
+void ref_rfor_encode(const uint32_t* in, uint32_t n, uint32_t* value, uint32_t* run_length, uint32_t* val_offsets,
+                     uint32_t* rl_offsets, uint32_t* sizes2);
+
 /* generated/cuda/normal_t32_uf1/cuda_normal_t32_1024_uf1_unpack_helper.hpp:
  * the reference's golden arrays rand_arr_{bw}_b{bw}_w32_arr[1024], bw 0..32 */
 const uint32_t* ref_helper_arr(unsigned bw);

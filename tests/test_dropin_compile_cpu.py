@@ -37,3 +37,25 @@ def test_reference_kernel_files_compile_against_dropin_headers(tmp_path):
         results = list(ex.map(lambda f: _compile(f, str(tmp_path)), FILES))
     failed = [(f, log) for f, rc, log in results if rc != 0]
     assert not failed, failed
+
+
+def test_dropin_libraries_load_with_their_launchers():
+    """The libraries built from the reference's kernel files (oracle/_ref,
+    make -C oracle dropin) resolve every symbol at load time and export the
+    launchers the GPU tests call."""
+    import ctypes
+    want = {"q21": ["dropin_q21_build", "dropin_q21_probe", "dropin_q21_widths", "dropin_q21_take_error"],
+            "q31": ["dropin_q31_build", "dropin_q31_probe", "dropin_q31_widths", "dropin_q31_take_error"],
+            "q41": ["dropin_q41_build", "dropin_q41_probe", "dropin_q41_widths", "dropin_q41_take_error"],
+            "delta": ["dropin_delta_sum", "dropin_delta_take_error"]}
+    found = 0
+    for name, syms in want.items():
+        path = os.path.join(ROOT, "oracle", "_ref", f"libdropin_{name}.so")
+        if not os.path.exists(path):
+            continue
+        L = ctypes.CDLL(path)
+        for s in syms:
+            assert hasattr(L, s), (name, s)
+        found += 1
+    if found == 0:
+        pytest.skip("drop-in libraries not built (make -C oracle dropin needs the reference sources)")
