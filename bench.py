@@ -317,6 +317,9 @@ def run_ours(a, dist: Dist):
             words = 2 if dq["kind"] == "filter" else dq["kw"]["res_stride"] * dq["kw"]["n_groups"]
             suite.append((name, dq, off, words))
             off += words + (words & 1)
+        dims = ("supplier 2^17, customer 2^18, part 2^19 keys, 2556 days; cities/nations/regions and "
+                "brands/categories/manufacturers in dbgen's hierarchy") if a.workload == "ssb" else \
+            ", ".join(f"{k} {t[k].size}" for k in ("s_suppkey", "c_custkey", "p_partkey", "d_datekey"))
         del t
         res = torch.zeros(off, dtype=torch.int32, device=dev)
         suite_bytes = sum(sum(c.nbytes for c in dq["cols"]) for _, dq, _, _ in suite)
@@ -355,9 +358,7 @@ def run_ours(a, dist: Dist):
         workload = {"workload": what,
                     "rows_per_gpu": a.rows, "rows_scanned_per_step": 13 * a.rows,
                     "columns": ", ".join(f"{k[3:]} {c.bw}b" for k, c in zip(names, hcols)),
-                    "dimensions": ("supplier 2^17, customer 2^18, part 2^19 keys, 2556 days; cities/nations/regions "
-                                   "and brands/categories/manufacturers in dbgen's hierarchy") if a.workload == "ssb"
-                    else ", ".join(f"{k} {t[k].size}" for k in ("s_suppkey", "c_custkey", "p_partkey", "d_datekey")),
+                    "dimensions": dims,
                     "join_variants": {name: dq.get("tuned", "defaults") for name, dq, _, _ in suite
                                       if dq["kind"] == "join"}}
         metric_key = a.workload
