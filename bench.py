@@ -47,9 +47,10 @@ def parse_args():
     ap.add_argument("--decode-bw", type=int, default=16, help="bit width of the FOR decode workload")
     ap.add_argument("--decode-width", type=int, choices=[8, 16, 32, 64], default=32,
                     help="decode workload, FOR: value width of the FastLanes lanes (8/16/64: fls_decode_u8/u16/u64)")
-    ap.add_argument("--decode-scheme", choices=["for", "delta", "rle", "dict"], default="for",
+    ap.add_argument("--decode-scheme", choices=["for", "delta", "rle", "dict", "rfor"], default="for",
                     help="decode input: uniform FOR bit-packing, delta over sorted keys (geometric gaps p=0.3), "
-                         "RLE (geometric runs of mean 16, values in [0,2^16)), dictionary (Zipf 1.1 over 2^20)")
+                         "RLE (geometric runs of mean 16, values in [0,2^16)), dictionary (Zipf 1.1 over 2^20), "
+                         "the reference's tile-based RLE format (rfor; the same runs)")
     ap.add_argument("--decode-out", choices=["sum", "hbm"], default="sum",
                     help="decode fused with a uint64 sum, or decode to HBM")
     ap.add_argument("--e2e-steps", type=int, default=10)
@@ -374,6 +375,11 @@ def run_ours(a, dist: Dist):
             vals = datagen.sorted_geometric(a.rows, p=0.3, seed=seed)
             hcols = [EncodedColumn.encode(vals, SCHEME_DELTA, layout=LAYOUT_TRANSPOSED)]
             what, key = "delta over sorted keys with geometric gaps (p=0.3), per-vector bw", "delta"
+        elif a.decode_scheme == "rfor":
+            from fastlanesgpu_b200.column import RforColumn
+            vals = datagen.geometric_runs(a.rows, mean_run=16.0, value_bits=16, seed=seed)
+            hcols = [RforColumn.encode(vals)]
+            what, key = "tile-based RLE (RFOR), geometric runs (mean 16) of values in [0,2^16)", "rfor"
         elif a.decode_scheme == "rle":
             vals = datagen.geometric_runs(a.rows, mean_run=16.0, value_bits=16, seed=seed)
             hcols = [EncodedColumn.encode(vals, SCHEME_RLE, layout=LAYOUT_TRANSPOSED)]
@@ -420,6 +426,20 @@ def run_ours(a, dist: Dist):
             out_bytes = (bits // 8) * n_vec_w * 1024 if a.decode_out == "hbm" else 0
             what = f"bit-pack {bits}-bit lanes, bw {bw_w} (uniform column, fls_decode_u{bits})"
             key = f"u{bits}_bw{bw_w}"
+        elif a.decode_scheme == "rfor":
+            if a.decode_out == "sum":
+                res = torch.zeros(1, dtype=torch.int64, device=dev)
+
+                def step():
+                    ops.rfor_decode_sum(dcols[0], out=res)
+                    return res
+            else:
+                res = torch.empty(a.rows, dtype=torch.int32, device=dev)
+
+                def step():
+                    ops.rfor_decode(dcols[0], out=res)
+                    return res
+            out_bytes = 4 * a.rows if a.decode_out == "hbm" else 0
         elif a.decode_out == "sum":
             res = torch.zeros(1, dtype=torch.int64, device=dev)
 
@@ -432,7 +452,7 @@ def run_ours(a, dist: Dist):
             def step():
                 ops.unpack_global(dcols[0], out=res)
                 return res
-        if not (a.decode_scheme == "for" and a.decode_width != 32):
+        if not (a.decode_scheme == "for" and a.decode_width != 32) and a.decode_scheme != "rfor":
             out_bytes = 4 * dcols[0].n_vec * 1024 if a.decode_out == "hbm" else 0
         workload = {"workload": f"decode {'to HBM' if a.decode_out == 'hbm' else 'fused with uint64 sum'}: {what}",
                     "rows_per_gpu": a.rows}
@@ -499,10 +519,16 @@ def run_ours(a, dist: Dist):
     # every encoded buffer of every column: packed words and, for per-vector
     # columns, the vector metadata
     copies = []
-    for c, dc in zip(hcols, dcols):
-        copies.append((dc.data, torch.from_numpy(c.words.view("int32")).pin_memory()))
-        if c.meta is not None:
-            copies.append((dc.meta, torch.from_numpy(c.meta.view(np.uint8)).pin_memory()))
+    if a.workload == "decode" and a.decode_scheme == "rfor":
+        hc, dc = hcols[0], dcols[0]
+        for dst, src in ((dc.values, hc.values), (dc.run_lengths, hc.run_lengths), (dc.val_offsets, hc.val_offsets),
+                         (dc.rl_offsets, hc.rl_offsets)):
+            copies.append((dst, torch.from_numpy(src.view("int32")).pin_memory()))
+    else:
+        for c, dc in zip(hcols, dcols):
+            copies.append((dc.data, torch.from_numpy(c.words.view("int32")).pin_memory()))
+            if c.meta is not None:
+                copies.append((dc.meta, torch.from_numpy(c.meta.view(np.uint8)).pin_memory()))
     h2d = sum(hp.numel() * hp.element_size() for _, hp in copies)
     d2h = res.numel() * res.element_size()
     host_res = torch.empty_like(res, device="cpu").pin_memory()
@@ -806,13 +832,17 @@ def run_mixed(a, dist: Dist):
     # for low-confidence vectors, encode), and the same call with every vector
     # sent to the device's exhaustive choice
     def one_call(threshold):
+        # every column's call enqueued back to back; the encoders' info words
+        # are read once all have run (no host round trip per column)
         torch.cuda.synchronize()
         t0_ = time.perf_counter()
-        out_ = [encode_column_learned_gpu(cat_dev[vstart[i] * 1024: vstart[i] * 1024 + lens[i]], sel.params,
-                                          threshold=threshold, kappa=a.decode_kappa, layout=LAYOUT_TRANSPOSED)
+        pend = [encode_column_learned_gpu(cat_dev[vstart[i] * 1024: vstart[i] * 1024 + lens[i]], sel.params,
+                                          threshold=threshold, kappa=a.decode_kappa, layout=LAYOUT_TRANSPOSED,
+                                          compact=False, defer=True)
                 for i in range(len(cols))]
         torch.cuda.synchronize()
-        return out_, time.perf_counter() - t0_
+        dt = time.perf_counter() - t0_
+        return [p.finish() for p in pend], dt
     one_call(a.threshold)  # first use of the select kernel on this device
     ln1, ln1_s = one_call(a.threshold)
     exd, exd_s = one_call(2.0)

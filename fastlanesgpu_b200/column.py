@@ -257,13 +257,30 @@ def encode_column_gpu(values, schemes=0, layout: int = LAYOUT_TRANSPOSED, round4
     return DeviceEncodedColumn(out, meta, n, layout, total, mx, mask)
 
 
+class PendingEncode:
+    """A GPU encode enqueued without reading its results back: finish() reads
+    the encoder's info words (one device-to-host copy) and returns what
+    encode_column_learned_gpu returns.  Deferring the read lets many columns
+    be encoded back to back with no host round trip in between."""
+
+    def __init__(self, out, meta, info, schemes, n, layout, compact):
+        self.out, self.meta, self.info, self.schemes = out, meta, info, schemes
+        self.n, self.layout, self.compact = n, layout, compact
+
+    def finish(self):
+        total, mx, mask, n_fb = (int(x) for x in self.info.cpu())
+        out = self.out[:max(total, 4)].clone() if self.compact else self.out
+        return DeviceEncodedColumn(out, self.meta, self.n, self.layout, total, mx, mask), self.schemes, n_fb
+
+
 def encode_column_learned_gpu(values, params, threshold: float = 0.9, kappa: float = 0.0,
-                              layout: int = LAYOUT_TRANSPOSED, compact: bool = True):
+                              layout: int = LAYOUT_TRANSPOSED, compact: bool = True, defer: bool = False):
     """The learned encoder in one device call (fls_encode_learned_gpu): the MLP
     with `params` (device float32, FLS_MLP_N_PARAMS) picks each vector's scheme,
     the exhaustive choice replaces picks whose confidence is below
     `threshold`, and the column is encoded on the GPU.  Returns
-    (DeviceEncodedColumn, per-vector schemes, number of fallback vectors)."""
+    (DeviceEncodedColumn, per-vector schemes, number of fallback vectors), or
+    with defer=True a PendingEncode whose finish() returns them."""
     import torch
     n = int(values.numel())
     nv = n_vectors(n)
@@ -279,10 +296,8 @@ def encode_column_learned_gpu(values, params, threshold: float = 0.9, kappa: flo
                                        out.data_ptr(), bound + 4, meta.data_ptr(), info.data_ptr(), schemes.data_ptr(),
                                        ws.data_ptr(), ws_bytes, torch.cuda.current_stream().cuda_stream),
           "fls_encode_learned_gpu")
-    total, mx, mask, n_fb = (int(x) for x in info.cpu())
-    if compact:
-        out = out[:max(total, 4)].clone()
-    return DeviceEncodedColumn(out, meta, n, layout, total, mx, mask), schemes, n_fb
+    pending = PendingEncode(out, meta, info, schemes, n, layout, compact)
+    return pending if defer else pending.finish()
 
 
 @dataclass

@@ -98,6 +98,23 @@ __device__ __forceinline__ unsigned long long delta_lane_sum(const uint32_t* __r
 	dev::load_words<BW>(s + 32, lane, lw);
 	uint32_t           x   = s[lane];
 	unsigned long long acc = 0;
+	if constexpr (BW <= 22) {
+		if (rows == 0xffffffffu) {
+			// Value s is base + p_s with p_s the running sum of the deltas.
+			// For BW <= 22, p_31 < 2^27 and the sum of the 32 p_s < 2^32, so
+			// the p_s sum in 32 bits and the base is added once -- exact
+			// unless base + p_31 wraps (then the full path below runs).
+			uint32_t p = 0, ps = 0;
+#pragma unroll
+			for (int st = 0; st < 32; ++st) {
+				p += dev::extract<BW>(lw, static_cast<int>(dev::rsum_row(st)));
+				ps += p;
+			}
+			if (static_cast<uint64_t>(x) + p < (1ull << 32)) {
+				return 32ull * x + ps;
+			}
+		}
+	}
 	if (rows == 0xffffffffu) {
 #pragma unroll
 		for (int st = 0; st < 32; ++st) {

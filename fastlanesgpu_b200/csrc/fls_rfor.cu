@@ -49,21 +49,52 @@ __device__ __forceinline__ uint32_t field(const uint32_t* __restrict__ p, uint32
 	return __funnelshift_r(lo, hi, sh) & m;
 }
 
+// The run index and value of position 32 j + lane for the 16 rows of a tile,
+// handed to f(p, v); pre = run starts before mask word `lane`, minus one.
+template <bool FULL, class F>
+__device__ __forceinline__ void expand_rows(const uint32_t* bits, const uint32_t* vals, uint32_t pre, uint32_t lane,
+                                            uint32_t live, F&& f) {
+	const uint32_t upto = 0xffffffffu >> (31u - lane);
+#pragma unroll
+	for (uint32_t j = 0; j < kTile / 32; ++j) {
+		const uint32_t w   = bits[j];
+		const uint32_t idx = __shfl_sync(0xffffffffu, pre, j) + __popc(w & upto);
+		const uint32_t p   = 32u * j + lane;
+		if (FULL || p < live) { f(p, vals[idx]); }
+	}
+}
+
 template <bool SUM>
-__global__ void __launch_bounds__(kRforWarps * 32) rfor_kernel(const __grid_constant__ RforParams P) {
+__global__ void __launch_bounds__(kRforWarps * 32, 5) rfor_kernel(const __grid_constant__ RforParams P) {
 	__shared__ uint32_t s_vals[kRforWarps][kTile];
+	__shared__ uint16_t s_lens[kRforWarps][kTile];
 	__shared__ uint32_t s_bits[kRforWarps][kTile / 32];
 	const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
 	uint32_t*      vals = s_vals[warp];
+	uint16_t*      lens = s_lens[warp];
 	uint32_t*      bits = s_bits[warp];
 	unsigned long long acc = 0;
-	for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * kRforWarps + warp; t < P.n_tiles;
-	     t += static_cast<uint64_t>(gridDim.x) * kRforWarps) {
+	const uint64_t stride = static_cast<uint64_t>(gridDim.x) * kRforWarps;
+	uint64_t       t      = static_cast<uint64_t>(blockIdx.x) * kRforWarps + warp;
+	// block extents of the next tile, loaded one tile ahead
+	uint32_t nvo = 0, nve = 0, nro = 0, nre = 0;
+	if (t < P.n_tiles) {
+		nvo = __ldg(P.val_off + t);
+		nve = __ldg(P.val_off + t + 1);
+		nro = __ldg(P.rl_off + t);
+		nre = __ldg(P.rl_off + t + 1);
+	}
+	for (; t < P.n_tiles; t += stride) {
 		// the tile's blocks: {minimum, bit width per byte, count, fields}
-		const uint64_t vo = __ldg(P.val_off + t), ve = __ldg(P.val_off + t + 1);
-		const uint64_t ro = __ldg(P.rl_off + t), re = __ldg(P.rl_off + t + 1);
-		bool           ok = vo + 3u <= ve && ve <= P.n_val_words && ro + 3u <= re && re <= P.n_rl_words;
-		uint32_t       vmin = 0, vbw = 0, cnt = 0, rmin = 0, rbw = 0;
+		const uint64_t vo = nvo, ve = nve, ro = nro, re = nre; // 32-bit word offsets
+		if (t + stride < P.n_tiles) {
+			nvo = __ldg(P.val_off + t + stride);
+			nve = __ldg(P.val_off + t + stride + 1);
+			nro = __ldg(P.rl_off + t + stride);
+			nre = __ldg(P.rl_off + t + stride + 1);
+		}
+		bool     ok = vo + 3u <= ve && ve <= P.n_val_words && ro + 3u <= re && re <= P.n_rl_words;
+		uint32_t vmin = 0, vbw = 0, cnt = 0, rmin = 0, rbw = 0;
 		if (ok) {
 			vmin = __ldg(P.vals + vo);
 			vbw  = __ldg(P.vals + vo + 1) & 0xffu;
@@ -79,11 +110,17 @@ __global__ void __launch_bounds__(kRforWarps * 32) rfor_kernel(const __grid_cons
 		}
 		const uint32_t* vf = P.vals + vo + 3u;
 		const uint32_t* rf = P.rls + ro + 3u;
-		// 1. run lengths of this lane's chunk of runs, and where the chunk starts
+		// 1. this lane's chunk of runs: values and lengths to shared memory,
+		//    and where the chunk starts
 		const uint32_t chunk = (cnt + 31u) >> 5;
 		const uint32_t k0 = min(cnt, lane * chunk), k1 = min(cnt, k0 + chunk);
 		uint32_t       len = 0;
-		for (uint32_t k = k0; k < k1; ++k) { len += rmin + field(rf, k, rbw); }
+		for (uint32_t k = k0; k < k1; ++k) {
+			const uint32_t l = rmin + field(rf, k, rbw);
+			vals[k] = vmin + field(vf, k, vbw);
+			lens[k] = static_cast<uint16_t>(min(l, kTile)); // a longer run fails the cover check below
+			len += l;
+		}
 		uint32_t incl = len;
 #pragma unroll
 		for (int o = 1; o < 32; o <<= 1) {
@@ -94,39 +131,40 @@ __global__ void __launch_bounds__(kRforWarps * 32) rfor_kernel(const __grid_cons
 			if (lane == 0) { raise_err(P.err, kErrBadMeta); }
 			continue;
 		}
-		// 2. values to shared memory, run starts into the mask
+		// 2. run starts into the mask (each lane reads back its own lengths)
 		if (lane < kTile / 32) { bits[lane] = 0u; }
 		__syncwarp();
 		uint32_t pos = incl - len;
 		for (uint32_t k = k0; k < k1; ++k) {
-			vals[k] = vmin + field(vf, k, vbw);
 			if (pos < kTile) { atomicOr(&bits[pos >> 5], 1u << (pos & 31u)); } // runs of length 0 end at the tile's end
-			pos += rmin + field(rf, k, rbw);
+			pos += lens[k];
 		}
 		__syncwarp();
-		// 3. run index of position 32 j + lane, prefix counts of the mask words
-		uint32_t c = lane < kTile / 32 ? __popc(bits[lane]) : 0u;
+		// 3. run index of position 32 j + lane from prefix counts of the mask words
+		const uint32_t own = lane < kTile / 32 ? __popc(bits[lane]) : 0u;
+		uint32_t       c   = own;
 #pragma unroll
 		for (int o = 1; o < 16; o <<= 1) {
 			const uint32_t x = __shfl_up_sync(0xffffffffu, c, o);
 			if (lane >= static_cast<uint32_t>(o)) { c += x; }
 		}
-		const uint32_t pre  = c - (lane < kTile / 32 ? __popc(bits[lane]) : 0u); // starts before word lane
+		const uint32_t pre  = c - own - 1u; // starts before word lane, minus one
 		const uint64_t row0 = t * kTile;
 		const uint32_t live = static_cast<uint32_t>(min(static_cast<uint64_t>(kTile), P.n_values - row0));
-		const uint32_t upto = 0xffffffffu >> (31u - lane);
-#pragma unroll
-		for (uint32_t j = 0; j < kTile / 32; ++j) {
-			const uint32_t w   = bits[j];
-			const uint32_t idx = __shfl_sync(0xffffffffu, pre, j) + __popc(w & upto) - 1u;
-			const uint32_t v   = vals[idx];
-			const uint32_t p   = 32u * j + lane;
-			if (p < live) {
-				if constexpr (SUM) {
-					acc += v;
-				} else {
-					__stcs(P.out + row0 + p, v);
-				}
+		if constexpr (SUM) {
+			auto add = [&](uint32_t, uint32_t v) { acc += v; };
+			if (live == kTile) {
+				expand_rows<true>(bits, vals, pre, lane, live, add);
+			} else {
+				expand_rows<false>(bits, vals, pre, lane, live, add);
+			}
+		} else {
+			uint32_t* out = P.out + row0;
+			auto      put = [&](uint32_t p, uint32_t v) { __stcs(out + p, v); };
+			if (live == kTile) {
+				expand_rows<true>(bits, vals, pre, lane, live, put);
+			} else {
+				expand_rows<false>(bits, vals, pre, lane, live, put);
 			}
 		}
 		__syncwarp();

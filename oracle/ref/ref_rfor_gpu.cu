@@ -28,14 +28,24 @@ __global__ void ref_rfor_tiles(int* col, uint* val_block_start, uint* val_data, 
 }
 } // namespace
 
-// Decodes every tile of the streams into out (n values); device pointers.
-extern "C" int ref_rfor_decode_gpu(const uint32_t* val, const uint32_t* val_offsets, const uint32_t* rl,
-                                   const uint32_t* rl_offsets, uint32_t n, int32_t* out) {
+// Launches the decode of every tile of the streams into out (n values) on the
+// legacy default stream, without waiting; device pointers.  Returns the
+// launch status.
+extern "C" int ref_rfor_decode_gpu_launch(const uint32_t* val, const uint32_t* val_offsets, const uint32_t* rl,
+                                          const uint32_t* rl_offsets, uint32_t n, int32_t* out) {
 	const unsigned tiles = (n + kTile - 1) / kTile;
 	// 8 KB of shared memory: the 4 KB the benchmark gives, plus room for CUB's
 	// scan and exchange storage, which LoadRBinPack places in its second half.
 	ref_rfor_tiles<<<tiles, kThreads, 8192>>>(out, const_cast<uint*>(val_offsets), const_cast<uint*>(val),
 	                                          const_cast<uint*>(rl_offsets), const_cast<uint*>(rl),
 	                                          static_cast<int>(n));
-	return static_cast<int>(cudaDeviceSynchronize());
+	return static_cast<int>(cudaGetLastError());
+}
+
+// Decodes every tile of the streams into out (n values) and waits; device
+// pointers.
+extern "C" int ref_rfor_decode_gpu(const uint32_t* val, const uint32_t* val_offsets, const uint32_t* rl,
+                                   const uint32_t* rl_offsets, uint32_t n, int32_t* out) {
+	const int s = ref_rfor_decode_gpu_launch(val, val_offsets, rl, rl_offsets, n, out);
+	return s != 0 ? s : static_cast<int>(cudaDeviceSynchronize());
 }

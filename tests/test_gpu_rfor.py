@@ -86,3 +86,42 @@ def test_reference_gpu_decoder_reads_the_same_streams(cuda, name):
                                  ctypes.c_uint32(vals.size), p(out)) == 0
     assert np.array_equal(out.cpu().numpy(), vals), name
     assert np.array_equal(ops.rfor_decode(d).cpu().numpy(), vals)
+
+
+def test_decode_time_against_reference_gpu_decoder(cuda):
+    """Both decoders on 2^26 values of geometric runs (mean 16) of values in
+    [0, 2^16): each result equals the input, and the CUDA-event time of each
+    (20 launches after 5, on the default stream) is printed."""
+    import ctypes
+
+    import torch
+    L = _ref_gpu()
+    n = 1 << 26
+    vals = datagen.geometric_runs(n, mean_run=16.0, value_bits=16, seed=2804)
+    d = RforColumn.encode(vals).to_device()
+    out = torch.empty(n, dtype=torch.int32, device=cuda)
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+
+    def ref():
+        assert L.ref_rfor_decode_gpu_launch(p(d.values), p(d.val_offsets), p(d.run_lengths), p(d.rl_offsets),
+                                            ctypes.c_uint32(n), p(out)) == 0
+
+    def ours():
+        ops.rfor_decode(d, out=out)
+    ms = {}
+    for name, f in (("reference LoadRBinPack", ref), ("fls_rfor_decode_u32", ours)):
+        out.fill_(-1)
+        for _ in range(5):
+            f()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(20):
+            f()
+        e1.record()
+        torch.cuda.synchronize()
+        ms[name] = e0.elapsed_time(e1) / 20
+        ops.check_device_error()
+        assert torch.equal(out.cpu(), torch.from_numpy(vals)), name
+    print("\nRFOR decode of 2^26 values to HBM, ms per launch:",
+          ", ".join(f"{k} {v:.4f}" for k, v in ms.items()))
