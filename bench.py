@@ -72,6 +72,8 @@ def parse_args():
                          "--group-smem is given (ssb: always 1 by default)")
     ap.add_argument("--table-kb", type=int, default=0,
                     help="FLS_TUNE_TABLE_KB: shared-memory budget of the join kernels' hash tables (0 = default 72)")
+    ap.add_argument("--half-vectors", type=int, choices=[0, 1], default=None,
+                    help="FLS_TUNE_HALF_VECTORS: join kernels stage half vectors (1) or whole ones (0)")
     ap.add_argument("--group-smem", type=int, choices=[0, 1], default=None,
                     help="FLS_TUNE_GROUP_SMEM: 1 = per-CTA group sums in shared memory, 0 = a global atomic per row")
     ap.add_argument("--mixed-columns", type=int, default=64, help="mixed workload: number of columns")
@@ -235,7 +237,10 @@ def run_ours(a, dist: Dist):
     if a.late_measure is not None:
         ops.set_tuning(3, a.late_measure)
     ops.set_tuning(4, a.table_kb)
-    explicit_variants = a.late_measure is not None or a.table_kb != 0 or a.group_smem is not None
+    if a.half_vectors is not None:
+        ops.set_tuning(5, a.half_vectors)
+    explicit_variants = (a.late_measure is not None or a.table_kb != 0 or a.group_smem is not None or
+                         a.half_vectors is not None)
     tune_joins = a.tune_joins if a.tune_joins is not None else int(a.workload in ("ssb", "ssb-real") or
                                                                     not explicit_variants)
     from fastlanesgpu_b200.shard import allreduce_sum, combine_group_records, shard_seed
@@ -599,6 +604,7 @@ def run_ours(a, dist: Dist):
         "launch_config": dict(zip(["warps", "stages", "ctas_per_sm", "tile_bytes"], ops.get_launch_config()),
                               sparse_rows=ops.get_tuning(0), jit=ops.get_tuning(1), group_smem=ops.get_tuning(2),
                               late_measure=ops.get_tuning(3), table_kb=ops.get_tuning(4),
+                              half_vectors=ops.get_tuning(5),
                               jit_launches=int(ops.jit_stats()["launches"])),
         "clocks": clk,
     }

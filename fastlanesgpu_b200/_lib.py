@@ -23,7 +23,7 @@ LAYOUT_NORMAL, LAYOUT_TRANSPOSED = 0, 1
 RFOR_TILE = 512  # values per tile of the RFOR format (FLS_RFOR_TILE)
 ORDER_STORED, ORDER_ORIGINAL = 0, 1
 MAX_QUERY_COLS, MAX_FILTERS, MAX_PROBES = 8, 4, 4
-TUNE_SPARSE_ROWS, TUNE_JIT, TUNE_GROUP_SMEM, TUNE_LATE_MEASURE, TUNE_TABLE_KB = 0, 1, 2, 3, 4
+TUNE_SPARSE_ROWS, TUNE_JIT, TUNE_GROUP_SMEM, TUNE_LATE_MEASURE, TUNE_TABLE_KB, TUNE_HALF_VECTORS = 0, 1, 2, 3, 4, 5
 MLP_IN, MLP_HIDDEN, MLP_OUT = 16, 64, 5
 MLP_N_PARAMS = 64 * 16 + 64 + 64 * 64 + 64 + 5 * 64 + 5
 

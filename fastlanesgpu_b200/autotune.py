@@ -33,7 +33,7 @@ JOIN_SPACE = {
     "table_kb": [72, 144],
 }
 
-_TUNING = {"sparse_rows": 0, "group_smem": 2, "late_measure": 3, "table_kb": 4}
+_TUNING = {"sparse_rows": 0, "group_smem": 2, "late_measure": 3, "table_kb": 4, "half_vectors": 5}
 
 
 def cache_path() -> str:

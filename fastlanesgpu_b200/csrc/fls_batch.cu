@@ -176,29 +176,47 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) batch_kernel(const __grid_c
 				// the aggregated column decoded row by row into the sums).
 				uint32_t x[32];
 				dev::decode_vals(sf, vf, base + L.dict, lane, x);
-				uint32_t m[kGroupQueries];
-#pragma unroll
-				for (uint32_t j = 0; j < kGroupQueries; ++j) {
-					uint32_t mj = 0;
-#pragma unroll
-					for (int r = 0; r < 32; ++r) { mj |= (x[r] - lo[j] <= range[j] ? 1u : 0u) << r; }
-					m[j] = live[j] ? (mj & valid) : 0u;
-					cnt[j] += static_cast<unsigned>(__popc(m[j]));
-				}
 				long long p[kGroupQueries] = {0, 0, 0, 0};
-				if (same) {
+				if (same && valid == 0xffffffffu) {
+					// A whole vector whose sums are over the filtered values: each
+					// query adds the rows in its range straight from the registers.
 #pragma unroll
-					for (int r = 0; r < 32; ++r) {
-						const long long a = static_cast<int32_t>(x[r]);
+					for (uint32_t j = 0; j < kGroupQueries; ++j) {
+						if (!live[j]) { continue; } // warp-uniform: one group per work item
+						uint32_t c = 0;
 #pragma unroll
-						for (uint32_t j = 0; j < kGroupQueries; ++j) { p[j] += ((m[j] >> r) & 1u) ? a : 0ll; }
+						for (int r = 0; r < 32; ++r) {
+							if (x[r] - lo[j] <= range[j]) {
+								p[j] += static_cast<int32_t>(x[r]);
+								++c;
+							}
+						}
+						cnt[j] += c;
 					}
 				} else {
-					dev::decode_each<true>(sa, va, base + L.dict, lane, [&](int r, uint32_t y) {
-						const long long a = static_cast<int32_t>(y);
+					uint32_t m[kGroupQueries];
 #pragma unroll
-						for (uint32_t j = 0; j < kGroupQueries; ++j) { p[j] += ((m[j] >> r) & 1u) ? a : 0ll; }
-					});
+					for (uint32_t j = 0; j < kGroupQueries; ++j) {
+						uint32_t mj = 0;
+#pragma unroll
+						for (int r = 0; r < 32; ++r) { mj |= (x[r] - lo[j] <= range[j] ? 1u : 0u) << r; }
+						m[j] = live[j] ? (mj & valid) : 0u;
+						cnt[j] += static_cast<unsigned>(__popc(m[j]));
+					}
+					if (same) {
+#pragma unroll
+						for (int r = 0; r < 32; ++r) {
+							const long long a = static_cast<int32_t>(x[r]);
+#pragma unroll
+							for (uint32_t j = 0; j < kGroupQueries; ++j) { p[j] += ((m[j] >> r) & 1u) ? a : 0ll; }
+						}
+					} else {
+						dev::decode_each<true>(sa, va, base + L.dict, lane, [&](int r, uint32_t y) {
+							const long long a = static_cast<int32_t>(y);
+#pragma unroll
+							for (uint32_t j = 0; j < kGroupQueries; ++j) { p[j] += ((m[j] >> r) & 1u) ? a : 0ll; }
+						});
+					}
 				}
 #pragma unroll
 				for (uint32_t j = 0; j < kGroupQueries; ++j) { sum[j] += p[j]; }
@@ -288,10 +306,17 @@ fls_status batch_launch(const fls_batch* b, const DevCol* cols, const fls_batch_
 	P.slot_words = b->slot_words;
 	P.n_slots    = n_slots;
 	P.has_dict   = b->has_dict;
+	// Every SM gets warps: fewer work items than SMs x warps take fewer warps
+	// per CTA, not fewer CTAs (the items are pulled from one counter).
+	const uint64_t n_items = b->items.size();
+	uint64_t       grid64  = std::min<uint64_t>((n_items + warps - 1) / warps, static_cast<uint64_t>(di.sms) * ctas);
+	if (grid64 < static_cast<uint64_t>(di.sms)) {
+		grid64 = std::min<uint64_t>(n_items, static_cast<uint64_t>(di.sms));
+		warps  = static_cast<uint32_t>((n_items + grid64 - 1) / grid64);
+	}
+	const uint32_t grid = static_cast<uint32_t>(grid64);
 	P.warps      = warps;
 	P.err        = device_error_word(st);
-	const uint64_t want = (b->items.size() + warps - 1) / warps;
-	const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>(want, static_cast<uint64_t>(di.sms) * ctas));
 	batch_kernel<<<grid, 32u * warps, 4ull * L.total * warps, st>>>(P);
 	count_launch();
 	return cuda_check(cudaGetLastError(), "batch_kernel launch");

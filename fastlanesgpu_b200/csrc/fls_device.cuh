@@ -159,6 +159,21 @@ __device__ __forceinline__ void unpack_rows(const uint32_t* __restrict__ s, uint
 	for (int r = 0; r < 32; ++r) { f(r, extract<BW>(lw, r)); }
 }
 
+// Rows 16 H .. 16 H + 15 of a lane stream: f(r, packed value).  `s` is the
+// stream's base as unpack_rows takes it; only the word rows that hold these
+// rows are read (rows 0..15 end in word row ceil(BW/2) - 1, rows 16..31 start
+// in word row floor(BW/2)), so for H = 1 `s` may point below the staged half.
+template <int BW, int H, class F>
+__device__ __forceinline__ void unpack_half_rows(const uint32_t* __restrict__ s, uint32_t lane, F&& f) {
+	static_assert(H == 0 || H == 1, "half 0 or 1");
+	constexpr int k0 = H ? BW / 2 : 0, k1 = H ? BW : (BW + 1) / 2;
+	LaneWords<BW> lw;
+#pragma unroll
+	for (int k = k0; k < k1; ++k) { lw.w[k] = s[32 * k + lane]; }
+#pragma unroll
+	for (int r = 16 * H; r < 16 * H + 16; ++r) { f(r, extract<BW>(lw, r)); }
+}
+
 // DELTA: 32 lane bases then packed deltas; running sum in rsum order.
 template <int BW, class F>
 __device__ __forceinline__ void rsum_rows(const uint32_t* __restrict__ s, uint32_t lane, F&& f) {

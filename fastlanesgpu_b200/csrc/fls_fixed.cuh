@@ -104,6 +104,17 @@ struct Shape {
 		for (int i = 0; i < c; ++i) { s += 32 * bw(i); }
 		return s;
 	}
+	// Half-vector tiles: a tile holds rows 0..15 or rows 16..31 of every lane,
+	// ceil(bw/2) word rows of each column (half 1 starts at word row
+	// floor(bw/2)).
+	static constexpr bool kHalf = false;
+	__host__ __device__ static constexpr int half_words(int c) { return 32 * ((bw(c) + 1) / 2); }
+	__host__ __device__ static constexpr int half_skip(int c) { return 32 * (bw(c) / 2); }
+	__host__ __device__ static constexpr int half_prefix(int c) {
+		int s = 0;
+		for (int i = 0; i < c; ++i) { s += half_words(i); }
+		return s;
+	}
 	static_assert(NC >= 1 && NC <= FLS_MAX_QUERY_COLS, "1..8 staged columns");
 };
 
@@ -133,9 +144,13 @@ struct FilterQuery : Shape<LAYOUT, BWS...> {
 // GSM: each CTA sums its groups in a direct-mapped cache of group-sum slots
 // in shared memory (a group claims its slot, or else adds to its record
 // directly) and adds the slots' non-zero sums to the records once, at its end.
+// HALF: tiles are half vectors (rows 0..15 or 16..31 of every lane), so a
+// stage takes half the shared memory and twice the warps fit beside the
+// tables.
 template <int LAYOUT, int NP, int AGG, int SUB, int NK, int K0, int K1, int K2, int KINDS, int SMEM, int PBIT,
-          int DIRECT, int GSM, int NS, int... BWS>
+          int DIRECT, int GSM, int HALF, int NS, int... BWS>
 struct ProbeQuery : Shape<LAYOUT, BWS...> {
+	static constexpr bool kHalf = HALF != 0;
 	static constexpr int kNP  = NP;
 	static constexpr int kAgg = AGG;
 	static constexpr int kSub = SUB;
@@ -185,17 +200,39 @@ __device__ __forceinline__ uint32_t row_field(const uint32_t* __restrict__ s, ui
 
 __device__ __forceinline__ int max_rows(uint32_t mask) { return __reduce_max_sync(0xffffffffu, __popc(mask)); }
 
-// Where the columns of tile vector i sit in the stage.
+// Where the columns of tile vector i sit in the stage.  Half-vector tiles
+// (h = the half): the base of column C's lane streams such that word row k
+// is at 32 k + lane, for the word rows the half holds (for h = 1 this lies
+// below the staged words, which start at word row floor(bw/2)).
 template <class Q>
 struct Vec {
 	const uint32_t* stage;
-	uint32_t        k, i;
+	uint32_t        k, i, h;
 	template <int C>
 	__device__ __forceinline__ const uint32_t* col() const {
-		constexpr uint32_t pre = Q::prefix(C), vw = Q::vec_words(C);
-		return stage + k * pre + i * vw;
+		if constexpr (Q::kHalf) {
+			return stage + Q::half_prefix(C) - (h ? Q::half_skip(C) : 0);
+		} else {
+			constexpr uint32_t pre = Q::prefix(C), vw = Q::vec_words(C);
+			return stage + k * pre + i * vw;
+		}
 	}
 };
+
+// f(r, packed field of column C) for the rows of this lane the tile holds:
+// all 32, or the 16 of a half-vector tile.
+template <class Q, int C, class F>
+__device__ __forceinline__ void unpack_tile_rows(const Vec<Q>& V, uint32_t lane, F&& f) {
+	if constexpr (Q::kHalf) {
+		if (V.h) {
+			dev::unpack_half_rows<Q::bw(C), 1>(V.template col<C>(), lane, f);
+		} else {
+			dev::unpack_half_rows<Q::bw(C), 0>(V.template col<C>(), lane, f);
+		}
+	} else {
+		dev::unpack_rows<Q::bw(C)>(V.template col<C>(), lane, f);
+	}
+}
 
 __device__ __forceinline__ uint32_t valid_rows(const StageParams& S, int layout, uint64_t v, uint32_t lane) {
 	const uint64_t start = v * 1024u;
@@ -487,12 +524,12 @@ __device__ __forceinline__ void dense_probes(const ProbeParams& P, const uint32_
 			// slot h's bit: word h / 32, shifted right by h mod 32 (the funnel
 			// shift takes the amount mod 32), moved to bit r
 			const uint32_t* bm = tables + P.smem_off[q];
-			dev::unpack_rows<Q::bw(q)>(V.template col<q>(), lane, [&](int r, uint32_t x) {
+			unpack_tile_rows<Q, q>(V, lane, [&](int r, uint32_t x) {
 				const uint32_t h = Q::field_slot(q) ? x : x + kb;
 				hit[r & 3] |= (__funnelshift_r(bm[h >> 5], 0u, h) << r) & (1u << r);
 			});
 		} else {
-			dev::unpack_rows<Q::bw(q)>(V.template col<q>(), lane, [&](int r, uint32_t x) {
+			unpack_tile_rows<Q, q>(V, lane, [&](int r, uint32_t x) {
 				uint32_t   h;
 				const bool ok = hash_slot<Q::direct(q)>(x + kb, len, h, P.S.err);
 				const bool b  = ok & table_hit<Q, q>(P, tables, h);
@@ -632,6 +669,8 @@ template <class Q>
 __device__ __forceinline__ void row_phase(const ProbeParams& P, uint32_t* tables, const Vec<Q>& V, uint64_t v,
                                           uint32_t lane, uint32_t mask, int f0) {
 	const int n_it = max_rows(mask);
+	// A slot without a row reads the tile's first row (its fields are staged).
+	const uint32_t idle = Q::kHalf ? 16u * V.h : 0u;
 	for (int it0 = 0; it0 < n_it; it0 += kRowBatch) {
 		const int rem = n_it - it0; // warp-uniform
 		uint32_t  rows[kRowBatch];
@@ -640,7 +679,7 @@ __device__ __forceinline__ void row_phase(const ProbeParams& P, uint32_t* tables
 #pragma unroll
 		for (int j = 0; j < kRowBatch; ++j) {
 			pass[j] = mask != 0u;
-			rows[j] = pass[j] ? static_cast<uint32_t>(__ffs(mask)) - 1u : 0u;
+			rows[j] = pass[j] ? static_cast<uint32_t>(__ffs(mask)) - 1u : idle;
 			mask &= mask - 1u;
 #pragma unroll
 			for (int k = 0; k < FLS_MAX_GROUP_KEYS; ++k) { kv[k][j] = 0; }
@@ -769,6 +808,7 @@ struct ProbeBody {
 
 	__device__ __forceinline__ void operator()(const Vec<Q>& V, uint64_t v, uint32_t lane) {
 		uint32_t mask = valid_rows(P.S, Q::kLayout, v, lane);
+		if constexpr (Q::kHalf) { mask &= V.h ? 0xffff0000u : 0x0000ffffu; }
 		int      f0   = Q::kNP;
 		dense_probes<Q, 0>(P, tables, V, lane, mask, f0);
 		if (!__any_sync(0xffffffffu, mask)) { return; }
@@ -857,10 +897,42 @@ __device__ __forceinline__ void lane_column(uint32_t lane, uint32_t& vw, uint32_
 	}
 }
 
-// Issue tile t into a stage: lane c copies column c (k vectors, contiguous).
+// Word rows of column `lane` in a half-vector tile: its words, its stage
+// offset, the words it skips in half 1, and its words per vector.
+template <class Q, int C>
+__device__ __forceinline__ void lane_half_column(uint32_t lane, uint32_t& hw, uint32_t& pre, uint32_t& skip,
+                                                 uint32_t& vw) {
+	if constexpr (C < Q::kNS) {
+		if (lane == C) {
+			hw   = Q::half_words(C);
+			pre  = Q::half_prefix(C);
+			skip = Q::half_skip(C);
+			vw   = Q::vec_words(C);
+		}
+		lane_half_column<Q, C + 1>(lane, hw, pre, skip, vw);
+	}
+}
+
+// Issue tile t into a stage: lane c copies column c (k vectors, contiguous;
+// or, for half-vector tiles, the word rows of half t mod 2 of vector t / 2).
 template <class Q>
 __device__ __forceinline__ void issue(const StageParams& S, uint32_t* stage, uint64_t* bar, uint64_t t, uint32_t lane,
                                       uint64_t pol) {
+	if constexpr (Q::kHalf) {
+		if (lane < static_cast<uint32_t>(Q::kNS)) {
+			uint32_t hw = 0, pre = 0, skip = 0, vw = 0;
+			lane_half_column<Q, 0>(lane, hw, pre, skip, vw);
+			const uint64_t v = t >> 1;
+			if (hw) {
+				dev::mbar_expect_tx(bar, 4u * hw);
+				dev::bulk_g2s(stage + pre, S.data[lane] + v * vw + ((t & 1u) ? skip : 0u), 4u * hw, bar, pol);
+			}
+		}
+		__syncwarp();
+		if (lane == 0) { dev::mbar_arrive(bar); }
+		__syncwarp();
+		return;
+	}
 	const uint64_t v0 = t * S.tile;
 	const uint64_t kk = S.n_vec - v0 < S.tile ? S.n_vec - v0 : S.tile;
 	if (lane < static_cast<uint32_t>(Q::kNS)) {
@@ -916,9 +988,13 @@ __device__ __forceinline__ void run(const StageParams& S, Body& body) {
 			}
 			break;
 		}
-		const uint64_t v0 = t * S.tile;
-		const uint32_t kk = static_cast<uint32_t>(S.n_vec - v0 < S.tile ? S.n_vec - v0 : S.tile);
-		for (uint32_t i = 0; i < kk; ++i) { body(Vec<Q> {base + st * S.stage_words, S.tile, i}, v0 + i, lane); }
+		if constexpr (Q::kHalf) {
+			body(Vec<Q> {base + st * S.stage_words, 1u, 0u, static_cast<uint32_t>(t & 1u)}, t >> 1, lane);
+		} else {
+			const uint64_t v0 = t * S.tile;
+			const uint32_t kk = static_cast<uint32_t>(S.n_vec - v0 < S.tile ? S.n_vec - v0 : S.tile);
+			for (uint32_t i = 0; i < kk; ++i) { body(Vec<Q> {base + st * S.stage_words, S.tile, i, 0u}, v0 + i, lane); }
+		}
 		__syncwarp();
 		if (next < S.n_tiles) {
 			dev::fence_proxy_async_smem();

@@ -178,11 +178,15 @@ Entry& compiled_entry(const std::string& key) {
 // the filter and decode kernels keep the launch configuration's (16 by
 // default: measured faster for them).
 fls_status plan_fixed(const DeviceInfo& di, const fls_column* sc, uint32_t n, uint32_t cta_words,
-                      fixed::StageParams& S, uint32_t& grid, size_t& smem, bool join = false) {
+                      fixed::StageParams& S, uint32_t& grid, size_t& smem, bool join = false, bool half = false) {
 	fls_status st       = FLS_OK;
 	uint32_t   W0 = 0, S0 = 0, ctas = 0, tile_bytes = 0;
 	fls_get_launch_config(&W0, &S0, &ctas, &tile_bytes);
-	if (join) { W0 = jit_max_warps(); }
+	if (join) {
+		// half-vector stages fit about twice the warps; registers allow 28
+		W0 = jit_max_warps();
+		if (half && W0 == kJitDefaultWarps) { W0 = kJitHalfWarps; }
+	}
 	std::memset(&S, 0, sizeof(S));
 	uint32_t sum_vec = 0;
 	for (uint32_t c = 0; c < n; ++c) {
@@ -190,13 +194,14 @@ fls_status plan_fixed(const DeviceInfo& di, const fls_column* sc, uint32_t n, ui
 		if ((st = make_devcol(sc[c], d)) != FLS_OK) { return st; }
 		if (sc[c].n_values != sc[0].n_values) { return set_error(FLS_ERR_INVALID_ARG, "columns differ in length"); }
 		S.data[c] = sc[c].data;
-		sum_vec += 32u * sc[c].bw;
+		// half-vector tiles: ceil(bw/2) word rows of each column
+		sum_vec += half ? 32u * ((sc[c].bw + 1u) / 2u) : 32u * sc[c].bw;
 	}
 	S.n_values = sc[0].n_values;
 	S.n_vec    = (S.n_values + 1023u) / 1024u;
 	const uint64_t total_warps = static_cast<uint64_t>(di.sms) * ctas * W0;
 	uint32_t       k = sum_vec ? std::max<uint32_t>(1u, tile_bytes / (4u * sum_vec)) : kMaxTile;
-	k                = std::min<uint32_t>(k, kMaxTile);
+	k                = half ? 1u : std::min<uint32_t>(k, kMaxTile);
 	while (k > 1 && (S.n_vec + k - 1) / k < 4 * total_warps) { k /= 2; }
 	const uint32_t avail = static_cast<uint32_t>(di.max_smem) / 4u;
 	auto warp_words = [&](uint32_t stages_) { return (stages_ * k * sum_vec + fixed::kSlack + 2u * stages_ + 3u) & ~3u; };
@@ -224,7 +229,7 @@ fls_status plan_fixed(const DeviceInfo& di, const fls_column* sc, uint32_t n, ui
 	}
 	if (W == 0) { return set_error(FLS_ERR_CAPACITY, "vectors and tables too large for shared memory"); }
 	S.tile            = k;
-	S.n_tiles         = (S.n_vec + k - 1) / k;
+	S.n_tiles         = half ? 2u * S.n_vec : (S.n_vec + k - 1) / k;
 	S.stages          = stages;
 	S.warps           = W;
 	S.stage_words     = k * sum_vec;
@@ -497,10 +502,11 @@ bool jit_probe_shape(const fls_join_groupby_desc* d, JitProbeShape& sh) {
 	for (uint32_t i = 0; i < sh.n_staged + sh.n_global; ++i) { sc[i] = d->cols[sh.staged[i]]; }
 	int kp[FLS_MAX_GROUP_KEYS] = {-1, -1, -1};
 	for (uint32_t k = 0; k < d->n_keys; ++k) { kp[k] = d->key_probe[k]; }
+	sh.half = tuning_half_vectors() != 0;
 	char head[160];
-	std::snprintf(head, sizeof(head), "%u, %u, %d, %d, %u, %d, %d, %d, %u, %u, %u, %u, %d, %u",
+	std::snprintf(head, sizeof(head), "%u, %u, %d, %d, %u, %d, %d, %d, %u, %u, %u, %u, %d, %d, %u",
 	              static_cast<unsigned>(sc[0].layout), d->n_probes, sh.agg, sh.sub, d->n_keys, kp[0], kp[1], kp[2], kinds,
-	              in_smem, pbit, direct, sh.gsm ? 1 : 0, sh.n_staged);
+	              in_smem, pbit, direct, sh.gsm ? 1 : 0, sh.half ? 1 : 0, sh.n_staged);
 	sh.key = key_args(sc, sh.n_staged + sh.n_global, head);
 	return true;
 }
@@ -513,7 +519,7 @@ bool jit_compile(const fls_join_groupby_desc* d, const JitProbeShape& sh) {
 	fixed::StageParams S;
 	uint32_t           grid;
 	size_t             smem;
-	if (plan_fixed(di, sc, sh.n_staged, sh.cta_words, S, grid, smem, true) != FLS_OK) { return false; }
+	if (plan_fixed(di, sc, sh.n_staged, sh.cta_words, S, grid, smem, true, sh.half) != FLS_OK) { return false; }
 	std::lock_guard<std::mutex> lk(g_mu);
 	return compiled_entry(make_key('P', S.warps, sh.key)).state > 0;
 }
@@ -540,7 +546,7 @@ fls_status jit_probe_groupby(const fls_join_groupby_desc* d, int32_t* d_res, int
 	DeviceInfo         di;
 	fls_status         s = device_info(di);
 	if (s != FLS_OK) { return s; }
-	if ((s = plan_fixed(di, sc, sh.n_staged, sh.cta_words, P.S, grid, smem, true)) != FLS_OK) { return s; }
+	if ((s = plan_fixed(di, sc, sh.n_staged, sh.cta_words, P.S, grid, smem, true, sh.half)) != FLS_OK) { return s; }
 	P.S.err = device_error_word(stream);
 	for (uint32_t i = 0; i < sh.n_staged + sh.n_global; ++i) {
 		P.base[i] = static_cast<uint32_t>(d->cols[sh.staged[i]].base);

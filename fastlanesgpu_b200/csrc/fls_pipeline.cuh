@@ -38,6 +38,9 @@ constexpr uint32_t kMaxWarps   = 16;       // warps per CTA (general kernels)
 // tables leave room for more than 16 warps run faster with them (the filter
 // and decode kernels measured faster at 16).
 constexpr uint32_t kJitDefaultWarps = 20;
+// With half-vector stages (FLS_TUNE_HALF_VECTORS): 28 warps fit at the
+// joins' 66-72 registers per thread.
+constexpr uint32_t kJitHalfWarps = 28;
 constexpr uint32_t kWaitPolls  = 1u << 17; // bounded mbarrier waits (x <= 20 us each)
 constexpr uint32_t kDictWords  = 1024;     // per-warp dictionary scratch
 constexpr uint32_t kTBufWords  = 33 * 32;  // per-warp transpose buffer
@@ -302,6 +305,7 @@ int        tuning_sparse_rows();
 int        tuning_jit();
 int        tuning_group_smem();
 int        tuning_late_measure();
+int        tuning_half_vectors();
 uint32_t   tuning_table_words(); // table budget in 4-byte words
 uint32_t   jit_max_warps(); // most warps per CTA of the specialised join kernels
 
@@ -348,6 +352,7 @@ struct JitProbeShape {
 	uint32_t    bitmaps      = 0;  // probes whose presence bitmap is staged
 	uint32_t    n_global     = 0;     // measure columns left in global memory (after the staged ones)
 	bool        gsm          = false; // group sums in shared memory
+	bool        half         = false; // half-vector tiles
 	uint32_t    gslots       = 0;     // their slots (a power of two)
 	uint32_t    gsum_off     = 0;     // their offset (words) in the CTA scratch
 	std::string key;

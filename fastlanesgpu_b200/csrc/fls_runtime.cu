@@ -69,6 +69,7 @@ std::atomic<int> g_sparse_rows {kDefaultSparseRows};
 std::atomic<int> g_jit {1};
 std::atomic<int> g_group_smem {1};
 std::atomic<int> g_late_measure {0};
+std::atomic<int> g_half_vectors {0};
 std::atomic<int> g_table_kb {kJitTableKB};
 } // namespace
 
@@ -76,6 +77,7 @@ int tuning_sparse_rows() { return g_sparse_rows.load(std::memory_order_relaxed);
 int tuning_jit() { return g_jit.load(std::memory_order_relaxed); }
 int tuning_group_smem() { return g_group_smem.load(std::memory_order_relaxed); }
 int tuning_late_measure() { return g_late_measure.load(std::memory_order_relaxed); }
+int tuning_half_vectors() { return g_half_vectors.load(std::memory_order_relaxed); }
 uint32_t tuning_table_words() { return static_cast<uint32_t>(g_table_kb.load(std::memory_order_relaxed)) * 256u; }
 
 fls_status cuda_check(cudaError_t e, const char* what) {
@@ -402,6 +404,10 @@ fls_status fls_set_tuning(uint32_t param, int64_t value) {
 		}
 		g_table_kb.store(value ? static_cast<int>(value) : static_cast<int>(kJitTableKB));
 		return FLS_OK;
+	case FLS_TUNE_HALF_VECTORS:
+		if (value != 0 && value != 1) { return set_error(FLS_ERR_INVALID_ARG, "half vectors must be 0 or 1"); }
+		g_half_vectors.store(static_cast<int>(value));
+		return FLS_OK;
 	default: return set_error(FLS_ERR_INVALID_ARG, "unknown tuning parameter");
 	}
 }
@@ -414,6 +420,7 @@ fls_status fls_get_tuning(uint32_t param, int64_t* value) {
 	case FLS_TUNE_GROUP_SMEM: *value = tuning_group_smem(); return FLS_OK;
 	case FLS_TUNE_LATE_MEASURE: *value = tuning_late_measure(); return FLS_OK;
 	case FLS_TUNE_TABLE_KB: *value = g_table_kb.load(); return FLS_OK;
+	case FLS_TUNE_HALF_VECTORS: *value = tuning_half_vectors(); return FLS_OK;
 	default: return set_error(FLS_ERR_INVALID_ARG, "unknown tuning parameter");
 	}
 }

@@ -568,7 +568,13 @@ typedef enum fls_tune_param {
 	 * staged vectors, so fewer warps per CTA.  Default 72; 0 restores it; at
 	 * most 144.  fls_join_workspace_bytes depends on it.  Results are
 	 * identical either way. */
-	FLS_TUNE_TABLE_KB = 4
+	FLS_TUNE_TABLE_KB = 4,
+	/* 1: the specialised join kernels stage half vectors (rows 0..15 or
+	 * 16..31 of every lane, half of each column's words) instead of whole
+	 * ones, so that a stage takes half the shared memory and about twice the
+	 * warps fit beside the hash tables; 0 (default): whole vectors.  Results
+	 * are identical either way. */
+	FLS_TUNE_HALF_VECTORS = 5
 } fls_tune_param;
 fls_status fls_set_tuning(uint32_t param, int64_t value);
 fls_status fls_get_tuning(uint32_t param, int64_t* value);

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from fastlanesgpu_b200 import EncodedColumn, datagen, ops
-from fastlanesgpu_b200._lib import TUNE_JIT, TUNE_LATE_MEASURE, TUNE_TABLE_KB
+from fastlanesgpu_b200._lib import TUNE_HALF_VECTORS, TUNE_JIT, TUNE_LATE_MEASURE, TUNE_TABLE_KB
 
 pytestmark = pytest.mark.gpu
 
@@ -61,10 +61,12 @@ def test_ssb_query_against_oracle(ssb_data, oracle, name):
     t, dcols = ssb_data
     want, tables = ssb_want(oracle, name, t)
     try:
-        for jit, late, table_kb in ((1, 0, 0), (1, 1, 0), (1, 0, 144), (1, 1, 144), (0, 0, 0)):
+        for jit, late, table_kb, half in ((1, 0, 0, 0), (1, 1, 0, 0), (1, 0, 144, 0), (1, 1, 144, 0), (1, 0, 0, 1),
+                                          (1, 1, 0, 1), (1, 0, 144, 1), (0, 0, 0, 0)):
             ops.set_tuning(TUNE_JIT, jit)
             ops.set_tuning(TUNE_LATE_MEASURE, late)
             ops.set_tuning(TUNE_TABLE_KB, table_kb)
+            ops.set_tuning(TUNE_HALF_VECTORS, half)
             before = ops.jit_stats()["launches"]
             got, dq = ssb_run(name, t, dcols)
             assert ops.jit_stats()["launches"] - before == jit, (name, jit)
@@ -78,4 +80,5 @@ def test_ssb_query_against_oracle(ssb_data, oracle, name):
         ops.set_tuning(TUNE_JIT, 1)
         ops.set_tuning(TUNE_LATE_MEASURE, 0)
         ops.set_tuning(TUNE_TABLE_KB, 0)
+        ops.set_tuning(TUNE_HALF_VECTORS, 0)
     assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()

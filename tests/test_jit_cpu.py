@@ -61,15 +61,34 @@ def test_precompile_q21_probe_shape():
     ([(1, 0x200000, 70000, 0, 1), (0, 0x400000, 3000, 0, 2)], 2),       # global bitmap probe, smem PHT_2
     ([(0, 0x200000, 10, 0, 2), (1, 0x400000, 20, 1, 2), (2, 0x800000, 30, 2, 1), (3, 0xA00000, 40, 3, 2)], 4),
 ])
-def test_precompile_probe_edge_shapes(probes, agg):
+@pytest.mark.parametrize("half", [0, 1])
+def test_precompile_probe_edge_shapes(probes, agg, half):
+    """Probe shapes over bit widths 17, 3, 32, 0 and 9, with whole-vector and
+    half-vector tiles (FLS_TUNE_HALF_VECTORS)."""
+    from fastlanesgpu_b200._lib import TUNE_HALF_VECTORS
     cols = [_col(bw) for bw in (17, 3, 32, 0, 9)]
     ka = next(i for i, p in enumerate(probes) if p[4] == 2)
-    ops.jit_precompile_probe(cols, probes, agg, ka, ka, 3, 1, 100)
+    try:
+        ops.set_tuning(TUNE_HALF_VECTORS, half)
+        ops.jit_precompile_probe(cols, probes, agg, ka, ka, 3, 1, 100)
+    finally:
+        ops.set_tuning(TUNE_HALF_VECTORS, 0)
     assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
 
 
+def test_half_vector_tuning():
+    """FLS_TUNE_HALF_VECTORS accepts 0 and 1 only and defaults to 0."""
+    from fastlanesgpu_b200._lib import TUNE_HALF_VECTORS
+    assert ops.get_tuning(TUNE_HALF_VECTORS) == 0
+    for bad in (-1, 2):
+        with pytest.raises(FlsError):
+            ops.set_tuning(TUNE_HALF_VECTORS, bad)
+    assert ops.get_tuning(TUNE_HALF_VECTORS) == 0
+
+
+@pytest.mark.parametrize("half", [0, 1])
 @pytest.mark.parametrize("query", ["q31", "q41"])
-def test_precompile_ssb_join_shapes(query):
+def test_precompile_ssb_join_shapes(query, half):
     if query == "q31":
         bits = datagen.Q31_BITS
         cols = [_col(bits[k]) for k in ("lo_suppkey", "lo_custkey", "lo_orderdate", "lo_revenue")]
@@ -84,7 +103,12 @@ def test_precompile_ssb_join_shapes(query):
                   (3, 0x800000, datagen.N_DAYS, 0, 2)]
         kw = dict(agg_col=4, keys=[(1, 7, 1), (3, 1, 0)], group_sub=1992, n_groups=175, res_stride=4, sum_slot=2,
                   agg_sub_col=5)
-    ops.jit_precompile_join(cols, probes, **kw)
+    from fastlanesgpu_b200._lib import TUNE_HALF_VECTORS
+    try:
+        ops.set_tuning(TUNE_HALF_VECTORS, half)
+        ops.jit_precompile_join(cols, probes, **kw)
+    finally:
+        ops.set_tuning(TUNE_HALF_VECTORS, 0)
     assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
 
 
