@@ -29,6 +29,8 @@ constexpr int      kDenseAggRows  = 16; // above this many rows in some lane, ag
 constexpr int      kRowBatch      = 4;  // selected rows per lane whose table reads are in flight together
 constexpr uint32_t kFreeSlot      = 0xffffffffu; // tag of an unclaimed group-sum slot
 constexpr int      kMaxDenseProbes = 2; // probes compiled for whole-vector evaluation (each unrolls 32 rows)
+constexpr uint32_t kRowList       = 256; // entries of a join warp's list of selected rows (16 bits each)
+constexpr uint32_t kRowListWords  = kRowList / 2;
 
 // The staged pipeline's parameters (shared by both operators).
 struct StageParams {
@@ -36,8 +38,8 @@ struct StageParams {
 	uint64_t        n_values, n_vec, n_tiles;
 	uint32_t        tile, stages, warps, warp_smem_words, stage_words, bar_off;
 	uint32_t*       err;
-	uint32_t        cta_off; // words: CTA-wide scratch (hash tables) after the warps' areas
-	uint32_t        pad_;
+	uint32_t        cta_off;  // words: CTA-wide scratch (hash tables) after the warps' areas
+	uint32_t        list_off; // words into a warp's area: its row list (join kernels), after the barriers
 };
 
 struct FilterParams {
@@ -546,7 +548,7 @@ __device__ __forceinline__ void dense_probes(const ProbeParams& P, const uint32_
 // Probe q of a batch of selected rows: hit test and group-key payload.
 template <class Q, int q>
 __device__ __forceinline__ void probe_rows_one(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
-                                               uint32_t lane, const uint32_t (&rows)[kRowBatch],
+                                               const uint32_t (&src)[kRowBatch], const uint32_t (&rows)[kRowBatch],
                                                bool (&pass)[kRowBatch], int32_t (&kv)[FLS_MAX_GROUP_KEYS][kRowBatch],
                                                int rem) {
 	const uint32_t kb  = P.base[q] - static_cast<uint32_t>(P.kmin[q]);
@@ -556,7 +558,7 @@ __device__ __forceinline__ void probe_rows_one(const ProbeParams& P, const uint3
 	for (int j = 0; j < kRowBatch; ++j) {
 		e[j] = make_uint2(0u, 0u);
 		if (j < rem) {
-			const uint32_t d = row_field<Q::bw(q)>(V.template col<q>(), lane, rows[j]) + kb;
+			const uint32_t d = row_field<Q::bw(q)>(V.template col<q>(), src[j], rows[j]) + kb;
 			uint32_t       h;
 			if (pass[j] && hash_slot<Q::direct(q)>(d, len, h, P.S.err)) {
 				e[j] = table_entry<Q, q>(P, tables, h);
@@ -573,23 +575,24 @@ __device__ __forceinline__ void probe_rows_one(const ProbeParams& P, const uint3
 	}
 }
 
-// Probes of a batch of selected rows: those from f0 on (warp-uniform), and
-// the group-key probes before f0 for their payloads (a row selected there
-// hits that table already, so testing it again changes nothing).  The table
-// reads of all rows of the batch are issued before any is consumed.  One
-// instance serves every f0, which keeps the kernel small enough for the
-// instruction cache.
+// Probes of a batch of selected rows (row rows[j] of lane src[j]): those
+// from f0 on (warp-uniform), and the group-key probes before f0 for their
+// payloads (a row selected there hits that table already, so testing it again
+// changes nothing).  The table reads of all rows of the batch are issued
+// before any is consumed.  One instance serves every f0, which keeps the
+// kernel small enough for the instruction cache.
 template <class Q, int q>
 __device__ __forceinline__ void probe_rows(const ProbeParams& P, const uint32_t* tables, const Vec<Q>& V,
-                                           uint32_t lane, const uint32_t (&rows)[kRowBatch], bool (&pass)[kRowBatch],
-                                           int32_t (&kv)[FLS_MAX_GROUP_KEYS][kRowBatch], int rem, int f0) {
+                                           const uint32_t (&src)[kRowBatch], const uint32_t (&rows)[kRowBatch],
+                                           bool (&pass)[kRowBatch], int32_t (&kv)[FLS_MAX_GROUP_KEYS][kRowBatch],
+                                           int rem, int f0) {
 	if constexpr (q < Q::kNP) {
 		constexpr bool key = (Q::key_probe(0) == q && Q::kNK > 0) || (Q::key_probe(1) == q && Q::kNK > 1) ||
 		                     (Q::key_probe(2) == q && Q::kNK > 2);
 		if (key || q >= f0) {
-			probe_rows_one<Q, q>(P, tables, V, lane, rows, pass, kv, rem);
+			probe_rows_one<Q, q>(P, tables, V, src, rows, pass, kv, rem);
 		}
-		probe_rows<Q, q + 1>(P, tables, V, lane, rows, pass, kv, rem, f0);
+		probe_rows<Q, q + 1>(P, tables, V, src, rows, pass, kv, rem, f0);
 	}
 }
 
@@ -665,53 +668,108 @@ __device__ __forceinline__ uint32_t measure_value(const ProbeParams& P, const Ve
 	}
 }
 
+// One batch of selected rows (row rows[j] of lane src[j], slots j < rem):
+// the probes left, then each passing row's measure into its group.
 template <class Q>
-__device__ __forceinline__ void row_phase(const ProbeParams& P, uint32_t* tables, const Vec<Q>& V, uint64_t v,
-                                          uint32_t lane, uint32_t mask, int f0) {
+__device__ __forceinline__ void row_batch(const ProbeParams& P, uint32_t* tables, const Vec<Q>& V, uint64_t v,
+                                          const uint32_t (&src)[kRowBatch], const uint32_t (&rows)[kRowBatch],
+                                          bool (&pass)[kRowBatch], int rem, int f0) {
+	int32_t kv[FLS_MAX_GROUP_KEYS][kRowBatch];
+#pragma unroll
+	for (int j = 0; j < kRowBatch; ++j) {
+#pragma unroll
+		for (int k = 0; k < FLS_MAX_GROUP_KEYS; ++k) { kv[k][j] = 0; }
+	}
+	probe_rows<Q, 0>(P, tables, V, src, rows, pass, kv, rem, f0);
+	if constexpr (Q::kAgg >= Q::kNS || Q::kSub >= Q::kNS) {
+		// measures in global memory: the batch's reads first, all in flight
+		uint32_t m[kRowBatch];
+#pragma unroll
+		for (int j = 0; j < kRowBatch; ++j) {
+			m[j] = 0u;
+			if (j < rem && pass[j]) {
+				m[j] = measure_value<Q, Q::kAgg>(P, V, v, src[j], rows[j]);
+				if constexpr (Q::kSub >= 0) { m[j] -= measure_value<Q, Q::kSub>(P, V, v, src[j], rows[j]); }
+			}
+		}
+#pragma unroll
+		for (int j = 0; j < kRowBatch; ++j) {
+			if (j < rem && pass[j]) { emit<Q>(P, tables, kv, j, static_cast<int32_t>(m[j])); }
+		}
+	} else {
+#pragma unroll
+		for (int j = 0; j < kRowBatch; ++j) {
+			if (j < rem && pass[j]) {
+				uint32_t m = static_cast<uint32_t>(row_value<Q, Q::kAgg>(P.base, V, src[j], rows[j]));
+				if constexpr (Q::kSub >= 0) {
+					m -= static_cast<uint32_t>(row_value<Q, Q::kSub>(P.base, V, src[j], rows[j]));
+				}
+				emit<Q>(P, tables, kv, j, static_cast<int32_t>(m));
+			}
+		}
+	}
+}
+
+// The rows that passed the dense probes.  Each lane holds its own rows, and
+// a warp-uniform loop over them runs as many times as the busiest lane has
+// rows.  When the warp's rows are few and unevenly spread, they go to the
+// warp's row list first (entry = lane * 32 + row, in lane order) and every
+// lane takes the list's entries 32 apart: ceil(rows / 32) slots per lane
+// instead of the busiest lane's count.  Any lane may read any lane's fields,
+// since the whole tile is staged.
+template <class Q>
+__device__ __forceinline__ void row_phase(const ProbeParams& P, uint32_t* tables, uint16_t* list, const Vec<Q>& V,
+                                          uint64_t v, uint32_t lane, uint32_t mask, int f0) {
 	const int n_it = max_rows(mask);
 	// A slot without a row reads the tile's first row (its fields are staged).
 	const uint32_t idle = Q::kHalf ? 16u * V.h : 0u;
+	const uint32_t cnt  = static_cast<uint32_t>(__popc(mask));
+	uint32_t       incl = cnt;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+		if (lane >= static_cast<uint32_t>(o)) { incl += x; }
+	}
+	const uint32_t total  = __shfl_sync(0xffffffffu, incl, 31);
+	const int      n_comp = static_cast<int>((total + 31u) / 32u);
+	if (total <= kRowList && n_comp < n_it) { // warp-uniform
+		uint32_t pos = incl - cnt, m = mask;
+		for (int it = 0; it < n_it; ++it) {
+			if (m != 0u) {
+				list[pos++] = static_cast<uint16_t>((lane << 5) | (static_cast<uint32_t>(__ffs(m)) - 1u));
+				m &= m - 1u;
+			}
+		}
+		__syncwarp();
+		for (int it0 = 0; it0 < n_comp; it0 += kRowBatch) {
+			const int rem = n_comp - it0; // warp-uniform
+			uint32_t  src[kRowBatch], rows[kRowBatch];
+			bool      pass[kRowBatch];
+#pragma unroll
+			for (int j = 0; j < kRowBatch; ++j) {
+				const uint32_t k = static_cast<uint32_t>(it0 + j) * 32u + lane;
+				pass[j]          = k < total;
+				const uint32_t e = pass[j] ? list[k] : ((lane << 5) | idle);
+				src[j]           = e >> 5;
+				rows[j]          = e & 31u;
+			}
+			row_batch<Q>(P, tables, V, v, src, rows, pass, rem, f0);
+		}
+		__syncwarp(); // the list is read before the next tile writes it
+		return;
+	}
 	for (int it0 = 0; it0 < n_it; it0 += kRowBatch) {
 		const int rem = n_it - it0; // warp-uniform
-		uint32_t  rows[kRowBatch];
+		uint32_t  src[kRowBatch], rows[kRowBatch];
 		bool      pass[kRowBatch];
-		int32_t   kv[FLS_MAX_GROUP_KEYS][kRowBatch];
 #pragma unroll
 		for (int j = 0; j < kRowBatch; ++j) {
+			src[j]  = lane;
 			pass[j] = mask != 0u;
 			rows[j] = pass[j] ? static_cast<uint32_t>(__ffs(mask)) - 1u : idle;
 			mask &= mask - 1u;
-#pragma unroll
-			for (int k = 0; k < FLS_MAX_GROUP_KEYS; ++k) { kv[k][j] = 0; }
 		}
-		probe_rows<Q, 0>(P, tables, V, lane, rows, pass, kv, rem, f0);
-		if constexpr (Q::kAgg >= Q::kNS || Q::kSub >= Q::kNS) {
-			// measures in global memory: the batch's reads first, all in flight
-			uint32_t m[kRowBatch];
-#pragma unroll
-			for (int j = 0; j < kRowBatch; ++j) {
-				m[j] = 0u;
-				if (j < rem && pass[j]) {
-					m[j] = measure_value<Q, Q::kAgg>(P, V, v, lane, rows[j]);
-					if constexpr (Q::kSub >= 0) { m[j] -= measure_value<Q, Q::kSub>(P, V, v, lane, rows[j]); }
-				}
-			}
-#pragma unroll
-			for (int j = 0; j < kRowBatch; ++j) {
-				if (j < rem && pass[j]) { emit<Q>(P, tables, kv, j, static_cast<int32_t>(m[j])); }
-			}
-		} else {
-#pragma unroll
-			for (int j = 0; j < kRowBatch; ++j) {
-				if (j < rem && pass[j]) {
-					uint32_t m = static_cast<uint32_t>(row_value<Q, Q::kAgg>(P.base, V, lane, rows[j]));
-					if constexpr (Q::kSub >= 0) {
-						m -= static_cast<uint32_t>(row_value<Q, Q::kSub>(P.base, V, lane, rows[j]));
-					}
-					emit<Q>(P, tables, kv, j, static_cast<int32_t>(m));
-				}
-			}
-		}
+		row_batch<Q>(P, tables, V, v, src, rows, pass, rem, f0);
 	}
 }
 
@@ -720,6 +778,7 @@ struct ProbeBody {
 	static constexpr bool kCtaSetup = true;
 	const ProbeParams&    P;
 	uint32_t*             tables = nullptr;
+	uint16_t*             list   = nullptr; // this warp's row list
 
 	// Shared-memory tables, staged once per CTA by all its threads: presence
 	// bitmaps (of PHT_1 tables, whose probe only tests slot != 0, crystal-opt/
@@ -729,7 +788,9 @@ struct ProbeBody {
 	// small PHT_2 tables verbatim.  GSM: every slot of the group-sum cache
 	// starts free.
 	__device__ void cta_setup(uint32_t* cta) {
+		extern __shared__ __align__(128) uint32_t smem[];
 		tables = cta;
+		list   = reinterpret_cast<uint16_t*>(smem + (threadIdx.x >> 5) * P.S.warp_smem_words + P.S.list_off);
 #pragma unroll 1
 		for (int q = 0; q < Q::kNP; ++q) {
 			if (!Q::in_smem(q) && !Q::pbit(q)) { continue; }
@@ -812,7 +873,7 @@ struct ProbeBody {
 		int      f0   = Q::kNP;
 		dense_probes<Q, 0>(P, tables, V, lane, mask, f0);
 		if (!__any_sync(0xffffffffu, mask)) { return; }
-		row_phase<Q>(P, tables, V, v, lane, mask, f0);
+		row_phase<Q>(P, tables, list, V, v, lane, mask, f0);
 	}
 
 	// GSM: once every warp of the CTA is done, the CTA adds each claimed

@@ -204,7 +204,12 @@ fls_status plan_fixed(const DeviceInfo& di, const fls_column* sc, uint32_t n, ui
 	k                = half ? 1u : std::min<uint32_t>(k, kMaxTile);
 	while (k > 1 && (S.n_vec + k - 1) / k < 4 * total_warps) { k /= 2; }
 	const uint32_t avail = static_cast<uint32_t>(di.max_smem) / 4u;
-	auto warp_words = [&](uint32_t stages_) { return (stages_ * k * sum_vec + fixed::kSlack + 2u * stages_ + 3u) & ~3u; };
+	// a warp's area: its stages, the slack, one barrier per stage and (join
+	// kernels) its row list
+	const uint32_t list_words = join ? fixed::kRowListWords : 0u;
+	auto warp_words = [&](uint32_t stages_) {
+		return (stages_ * k * sum_vec + fixed::kSlack + 2u * stages_ + list_words + 3u) & ~3u;
+	};
 	auto warps_for  = [&](uint32_t per_) {
 		return avail > cta_words ? std::min<uint32_t>(W0, (avail - cta_words) / per_) : 0u;
 	};
@@ -234,6 +239,7 @@ fls_status plan_fixed(const DeviceInfo& di, const fls_column* sc, uint32_t n, ui
 	S.warps           = W;
 	S.stage_words     = k * sum_vec;
 	S.bar_off         = stages * S.stage_words + fixed::kSlack;
+	S.list_off        = S.bar_off + 2u * stages;
 	S.warp_smem_words = per;
 	S.cta_off         = W * per;
 	smem              = 4ull * (static_cast<size_t>(S.cta_off) + cta_words);
