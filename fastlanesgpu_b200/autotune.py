@@ -122,7 +122,7 @@ def tune(signature: str, fn, space: dict | None = None, iters: int = 10, use_cac
 
 
 # The library's defaults for the JOIN_SPACE variants.
-JOIN_DEFAULT = {"late_measure": 0, "group_smem": 1, "table_kb": 72}
+JOIN_DEFAULT = {"late_measure": 1, "group_smem": 1, "table_kb": 72}
 
 
 def reset() -> None:
@@ -130,5 +130,6 @@ def reset() -> None:
     ops.set_launch_config(0, 0, 0, 0)
     ops.set_tuning(0, 0)
     ops.set_tuning(2, 1)
-    ops.set_tuning(3, 0)
+    ops.set_tuning(3, 1)
     ops.set_tuning(4, 0)
+    ops.set_tuning(5, 0)

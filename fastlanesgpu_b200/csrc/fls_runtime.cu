@@ -68,7 +68,7 @@ constexpr int    kDefaultSparseRows = 4;
 std::atomic<int> g_sparse_rows {kDefaultSparseRows};
 std::atomic<int> g_jit {1};
 std::atomic<int> g_group_smem {1};
-std::atomic<int> g_late_measure {0};
+std::atomic<int> g_late_measure {1};
 std::atomic<int> g_half_vectors {0};
 std::atomic<int> g_table_kb {kJitTableKB};
 } // namespace

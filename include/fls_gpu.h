@@ -556,10 +556,10 @@ typedef enum fls_tune_param {
 	 * atomic per selected row (few live groups make those atomics contend).
 	 * 0: one global atomic per row.  Results are identical either way. */
 	FLS_TUNE_GROUP_SMEM = 2,
-	/* 1: the specialised join + group-by kernels leave the measure columns
-	 * (aggregated and subtracted) in global memory and read their fields for
-	 * the selected rows only, instead of staging them whole with the probe
-	 * columns.  0 (default): staged.  Results are identical either way. */
+	/* 1 (default): the specialised join + group-by kernels leave the measure
+	 * columns (aggregated and subtracted) in global memory and read their
+	 * fields for the selected rows only; 0: they stage them whole with the
+	 * probe columns.  Results are identical either way. */
 	FLS_TUNE_LATE_MEASURE = 3,
 	/* Shared-memory budget, in KB, of the specialised join kernels' hash
 	 * tables (PHT_1 as bitmaps, PHT_2 verbatim or as presence bitmaps, placed

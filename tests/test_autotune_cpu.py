@@ -66,18 +66,18 @@ def test_prefer_retimed_with_leaders(fake):
 def test_reset_restores_every_default():
     """reset() puts back the library defaults of everything apply() can set:
     launch shape, sparse-row threshold, group sums per CTA, late measures,
-    table budget (host-side settings, no GPU needed)."""
+    table budget, half-vector stages (host-side settings, no GPU needed)."""
     from fastlanesgpu_b200 import ops
-    before = (ops.get_launch_config(), [ops.get_tuning(p) for p in (0, 2, 3, 4)])
+    before = (ops.get_launch_config(), [ops.get_tuning(p) for p in (0, 2, 3, 4, 5)])
     try:
         autotune.apply({"warps": 8, "stages": 3, "tile_bytes": 2048, "sparse_rows": 12, "group_smem": 0,
-                        "late_measure": 1, "table_kb": 144})
+                        "late_measure": 0, "table_kb": 144, "half_vectors": 1})
         assert ops.get_launch_config()[0] == 8 and ops.get_launch_config()[1] == 3
-        assert [ops.get_tuning(p) for p in (0, 2, 3, 4)] == [12, 0, 1, 144]
+        assert [ops.get_tuning(p) for p in (0, 2, 3, 4, 5)] == [12, 0, 0, 144, 1]
         autotune.apply({"table_kb": 100})  # a partial configuration leaves the rest
-        assert [ops.get_tuning(p) for p in (0, 2, 3, 4)] == [12, 0, 1, 100]
+        assert [ops.get_tuning(p) for p in (0, 2, 3, 4, 5)] == [12, 0, 0, 100, 1]
         autotune.reset()
-        assert [ops.get_tuning(p) for p in (0, 2, 3, 4)] == [4, 1, 0, 72]
-        assert (ops.get_launch_config(), [ops.get_tuning(p) for p in (0, 2, 3, 4)]) == before
+        assert [ops.get_tuning(p) for p in (0, 2, 3, 4, 5)] == [4, 1, 1, 72, 0]
+        assert (ops.get_launch_config(), [ops.get_tuning(p) for p in (0, 2, 3, 4, 5)]) == before
     finally:
         autotune.reset()

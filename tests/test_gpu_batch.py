@@ -129,7 +129,7 @@ def test_autotuner_join_space(cuda, oracle, tmp_path):
         kept = autotune.tune("q43-keep", run, space=autotune.JOIN_SPACE, iters=2, use_cache=False,
                              prefer=autotune.JOIN_DEFAULT, margin=1.0, retime=2)
         assert kept["config"] == autotune.JOIN_DEFAULT and len(kept["candidates"]) == 8
-        assert ops.get_tuning(3) == 0 and ops.get_tuning(2) == 1 and ops.get_tuning(4) == 72
+        assert ops.get_tuning(3) == 1 and ops.get_tuning(2) == 1 and ops.get_tuning(4) == 72
         assert all(np.array_equal(g.cpu().numpy(), want) for g in got)
     finally:
         autotune.reset()

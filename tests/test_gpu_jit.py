@@ -259,7 +259,7 @@ def late_measure(request):
     from fastlanesgpu_b200._lib import TUNE_LATE_MEASURE
     ops.set_tuning(TUNE_LATE_MEASURE, request.param)
     yield request.param
-    ops.set_tuning(TUNE_LATE_MEASURE, 0)
+    ops.set_tuning(TUNE_LATE_MEASURE, 1)  # the default
 
 
 @pytest.mark.parametrize("seed", range(12))
@@ -406,7 +406,7 @@ def test_jit_row_phase_flags_only_rows_that_reach_the_probe(jit_on, late):
         assert np.array_equal(got_b, want_b)
     finally:
         ops.set_tuning(TUNE_TABLE_KB, 0)
-        ops.set_tuning(TUNE_LATE_MEASURE, 0)
+        ops.set_tuning(TUNE_LATE_MEASURE, 1)  # the default
     assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
 
 

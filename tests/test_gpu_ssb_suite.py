@@ -78,7 +78,7 @@ def test_ssb_query_against_oracle(ssb_data, oracle, name):
                 assert (want != 0).any() and np.array_equal(got, want), (name, jit)
     finally:
         ops.set_tuning(TUNE_JIT, 1)
-        ops.set_tuning(TUNE_LATE_MEASURE, 0)
+        ops.set_tuning(TUNE_LATE_MEASURE, 1)  # the default
         ops.set_tuning(TUNE_TABLE_KB, 0)
         ops.set_tuning(TUNE_HALF_VECTORS, 0)
     assert ops.jit_stats()["failures"] == 0, ops.jit_last_log()
