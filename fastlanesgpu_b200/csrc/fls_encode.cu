@@ -73,13 +73,34 @@ __device__ __forceinline__ void stage_vector(const EncParams& P, uint64_t v, int
 	const int32_t last = __ldg(P.values + (P.n - 1));
 	mn                 = INT32_MAX;
 	mx                 = INT32_MIN;
+	const uint64_t v0  = v * 1024u;
+	if (v0 + 1024u <= P.n && (reinterpret_cast<uintptr_t>(P.values) & 15u) == 0) { // warp-uniform
+		// a whole vector from a 16-byte aligned column: eight 16-byte loads
+		// per lane (values 128 k + 4 lane .. + 3), all in flight at once
+		int4 q[8];
+#pragma unroll
+		for (uint32_t k = 0; k < 8; ++k) { q[k] = __ldg(reinterpret_cast<const int4*>(P.values + v0) + 32u * k + lane); }
+		asm volatile("" ::: "memory"); // every load issued before the first store below
+#pragma unroll
+		for (uint32_t k = 0; k < 8; ++k) {
+			const uint32_t j = 128u * k + 4u * lane; // conflict-free: (j + j / 32) mod 32 differs across lanes
+			const int32_t  e[4] = {q[k].x, q[k].y, q[k].z, q[k].w};
+#pragma unroll
+			for (uint32_t t = 0; t < 4; ++t) {
+				sv[(j + t) + ((j + t) >> 5)] = e[t];
+				mn                           = min(mn, e[t]);
+				mx                           = max(mx, e[t]);
+			}
+		}
+	} else {
 #pragma unroll 4
-	for (uint32_t r = 0; r < 32; ++r) {
-		const uint64_t idx = v * 1024u + 32u * r + lane;
-		const int32_t  x   = idx < P.n ? __ldg(P.values + idx) : last;
-		sv[33u * r + lane] = x;
-		mn                 = min(mn, x);
-		mx                 = max(mx, x);
+		for (uint32_t r = 0; r < 32; ++r) {
+			const uint64_t idx = v0 + 32u * r + lane;
+			const int32_t  x   = idx < P.n ? __ldg(P.values + idx) : last;
+			sv[33u * r + lane] = x;
+			mn                 = min(mn, x);
+			mx                 = max(mx, x);
+		}
 	}
 	__syncwarp();
 	mn = __reduce_min_sync(0xffffffffu, mn);
@@ -110,26 +131,17 @@ __device__ uint32_t distinct_sorted(const int32_t* sv, int32_t* a, int32_t* u, u
 	for (uint32_t j = lane; j < 1024; j += 32) { a[j] = val_at(sv, j); }
 	__syncwarp();
 	sort1024(a, lane);
-	// lane L owns positions 32L..32L+31: local flags, then a warp scan
-	uint32_t flags = 0;
-#pragma unroll
+	// row t of the sorted values (positions 32t..32t+31, one per lane): the
+	// first of each value is kept, at the count of kept values before it
+	uint32_t       total = 0;
+	const uint32_t below = (1u << lane) - 1u;
 	for (uint32_t t = 0; t < 32; ++t) {
-		const uint32_t k = 32u * lane + t;
-		flags |= (k == 0 || a[k] != a[k ? k - 1u : 0u] ? 1u : 0u) << t;
-	}
-	const uint32_t cnt = __popc(flags);
-	uint32_t       pre = cnt;
-#pragma unroll
-	for (int o = 1; o < 32; o <<= 1) {
-		const uint32_t y = __shfl_up_sync(0xffffffffu, pre, o);
-		if (lane >= static_cast<uint32_t>(o)) { pre += y; }
-	}
-	const uint32_t total = __shfl_sync(0xffffffffu, pre, 31);
-	pre -= cnt;
-	while (flags) {
-		const uint32_t t = __ffs(flags) - 1u;
-		flags &= flags - 1u;
-		u[pre++] = a[32u * lane + t];
+		const uint32_t k    = 32u * t + lane;
+		const int32_t  x    = a[k];
+		const bool     keep = k == 0 || x != a[k ? k - 1u : 0u];
+		const uint32_t b    = __ballot_sync(0xffffffffu, keep);
+		if (keep) { u[total + static_cast<uint32_t>(__popc(b & below))] = x; }
+		total += static_cast<uint32_t>(__popc(b));
 	}
 	__syncwarp();
 	return total;

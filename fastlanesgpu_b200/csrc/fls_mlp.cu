@@ -27,10 +27,14 @@ __device__ __forceinline__ uint32_t bits32(uint32_t v) { return 32u - static_cas
 
 // ------------------------------------------------------ vector statistics
 
+// Value j of a vector staged with one pad word per 32 values: lane L's
+// chunk (values 32L..32L+31) is then read without bank conflicts.
+__device__ __forceinline__ uint32_t pad33(uint32_t j) { return j + (j >> 5); }
+
 // One warp per vector; exactly the features of vector_stats() (fls_host.cpp).
 __global__ void __launch_bounds__(256) stats_kernel(const int32_t* __restrict__ values, uint64_t n, uint64_t n_vec,
                                                     float* __restrict__ out) {
-	__shared__ int32_t  vbuf[8][1024];
+	__shared__ int32_t  vbuf[8][1056];
 	__shared__ uint32_t bmap[8][32];
 	const uint32_t lane = threadIdx.x & 31u, wi = threadIdx.x >> 5;
 	const uint64_t warps = static_cast<uint64_t>(gridDim.x) * 8u;
@@ -39,45 +43,74 @@ __global__ void __launch_bounds__(256) stats_kernel(const int32_t* __restrict__ 
 	for (uint64_t vec = static_cast<uint64_t>(blockIdx.x) * 8u + wi; vec < n_vec; vec += warps) {
 		const uint64_t start = vec * 1024u;
 		const uint32_t cnt   = static_cast<uint32_t>(n - start < 1024u ? n - start : 1024u);
-		for (uint32_t j = lane; j < 1024u; j += 32u) {
-			// a partial last vector is padded with its last value (as the encoder does)
-			v[j] = values[start + min(j, cnt - 1u)];
+		int32_t        mn = INT32_MAX, mx = INT32_MIN;
+		if (cnt == 1024u && (reinterpret_cast<uintptr_t>(values) & 15u) == 0) { // warp-uniform
+			// eight 16-byte loads per lane (values 128 k + 4 lane .. + 3), all
+			// in flight, then stored 33-padded (conflict-free: (j + j / 32)
+			// mod 32 differs across lanes)
+			int4 q[8];
+#pragma unroll
+			for (uint32_t k = 0; k < 8; ++k) { q[k] = __ldg(reinterpret_cast<const int4*>(values + start) + 32u * k + lane); }
+#pragma unroll
+			for (uint32_t k = 0; k < 8; ++k) {
+				const uint32_t j    = 128u * k + 4u * lane;
+				const int32_t  e[4] = {q[k].x, q[k].y, q[k].z, q[k].w};
+#pragma unroll
+				for (uint32_t t = 0; t < 4; ++t) {
+					v[pad33(j + t)] = e[t];
+					mn              = min(mn, e[t]);
+					mx              = max(mx, e[t]);
+				}
+			}
+		} else {
+			for (uint32_t j = lane; j < 1024u; j += 32u) {
+				// a partial last vector is padded with its last value (as the encoder does)
+				const int32_t x = values[start + min(j, cnt - 1u)];
+				v[pad33(j)]     = x;
+				mn              = min(mn, x);
+				mx              = max(mx, x);
+			}
 		}
 		bm[lane] = 0u;
 		__syncwarp();
-		int32_t mn = v[32u * lane], mx = mn;
-		for (uint32_t s = 1; s < 32; ++s) {
-			mn = min(mn, v[32u * lane + s]);
-			mx = max(mx, v[32u * lane + s]);
-		}
 		mn = __reduce_min_sync(0xffffffffu, mn);
 		mx = __reduce_max_sync(0xffffffffu, mx);
 		const uint32_t rbw = bits32(static_cast<uint32_t>(mx) - static_cast<uint32_t>(mn));
-		uint32_t       max_d = 0, runs = 0, up = 0, down = 0, eq = 0, lh = 0, lq = 0;
+		const int32_t* c   = v + 33u * lane; // this lane's chunk: values 32 lane .. 32 lane + 31
+		// u <= tm_h (tm_q): the value lies in the lower half (sixteenth) of the
+		// range's bit width; every value counts when the width is 0 (<= 4)
+		const uint32_t tm_h = rbw == 0 ? 0xffffffffu : (1u << (rbw / 2)) - 1u;
+		const uint32_t tm_q = rbw <= 4 ? 0xffffffffu : (1u << (rbw - 4)) - 1u;
+		const int32_t  c0   = c[0];
+		// the value before the chunk; the vector's first value is compared
+		// with itself (an equal pair, corrected below)
+		const int32_t  pb   = lane ? v[pad33(32u * lane - 1u)] : c0;
+		int32_t        p    = pb;
+		uint32_t       max_d = 0, up = 0, eqs = 0, lh = 0, lq = 0;
 		unsigned long long sabs = 0;
 		bool               same = true;
+#pragma unroll 8
 		for (uint32_t s = 0; s < 32; ++s) {
-			const uint32_t j = 32u * lane + s;
-			const int32_t  x = v[j];
+			const int32_t  x = c[s];
 			const uint32_t u = static_cast<uint32_t>(x) - static_cast<uint32_t>(mn);
-			lh += (rbw == 0 || u < (1u << (rbw / 2))) ? 1u : 0u;
-			lq += (rbw <= 4 || u < (1u << (rbw - 4))) ? 1u : 0u;
+			lh += u <= tm_h ? 1u : 0u;
+			lq += u <= tm_q ? 1u : 0u;
 			const uint32_t h = (static_cast<uint32_t>(x) * 0x9e3779b1u) >> 22;
 			atomicOr(&bm[h >> 5], 1u << (h & 31u));
-			same = same && x == v[32u * lane];
-			if (j == 0) {
-				++runs;
-				continue;
-			}
-			const int32_t   p  = v[j - 1];
-			const long long dd = static_cast<long long>(x) - static_cast<long long>(p);
-			sabs += static_cast<unsigned long long>(dd < 0 ? -dd : dd);
-			up += dd > 0;
-			down += dd < 0;
-			eq += dd == 0;
+			same = same && x == c0;
+			sabs += static_cast<uint32_t>(max(x, p)) - static_cast<uint32_t>(min(x, p));
+			up += x > p ? 1u : 0u;
+			eqs += x == p ? 1u : 0u;
 			if (s != 0) { max_d = max(max_d, static_cast<uint32_t>(x) - static_cast<uint32_t>(p)); }
-			runs += ((j & 255u) == 0 || dd != 0) ? 1u : 0u;
+			p = x;
 		}
+		// deltas of the lane: 32 (31 for lane 0, whose first value has no
+		// predecessor); runs (rle.hpp): a change of value, or every 256 values
+		// (the chunks of lanes 0, 8, 16, 24 open one whether or not the value
+		// changes, lane 0's first value included)
+		uint32_t       eq   = eqs - (lane == 0 ? 1u : 0u);
+		uint32_t       down = 32u - up - eqs;
+		uint32_t       runs = 32u - eqs + (((lane & 7u) == 0 && c0 == pb) ? 1u : 0u);
 		__syncwarp();
 		const uint32_t occ = __reduce_add_sync(0xffffffffu, static_cast<uint32_t>(__popc(bm[lane])));
 		max_d              = __reduce_max_sync(0xffffffffu, max_d);
@@ -160,20 +193,40 @@ __device__ __forceinline__ void forward_one(const float* __restrict__ P, const f
 	float xin[kIn];
 #pragma unroll
 	for (int i = 0; i < kIn; ++i) { xin[i] = x[i]; }
+	// P is 16-byte aligned and every weight row starts at a multiple of four
+	// floats (kW1 = 0, kW2 = 1088): rows are read four weights per load
+	static_assert(kW1 % 4 == 0 && kW2 % 4 == 0 && kIn % 4 == 0 && kH % 4 == 0, "float4 weight rows");
 #pragma unroll
 	for (int j = 0; j < kH; ++j) {
-		float a = P[kB1 + j];
+		const float4* w = reinterpret_cast<const float4*>(P + kW1 + j * kIn);
+		float         a = P[kB1 + j];
 #pragma unroll
-		for (int i = 0; i < kIn; ++i) { a = fmaf(P[kW1 + j * kIn + i], xin[i], a); }
+		for (int i4 = 0; i4 < kIn / 4; ++i4) {
+			const float4 q = w[i4];
+			a = fmaf(q.x, xin[4 * i4], a);
+			a = fmaf(q.y, xin[4 * i4 + 1], a);
+			a = fmaf(q.z, xin[4 * i4 + 2], a);
+			a = fmaf(q.w, xin[4 * i4 + 3], a);
+		}
 		h1[j] = fmaxf(a, 0.0f);
 	}
 #pragma unroll
 	for (int k = 0; k < kOut; ++k) { z[k] = P[kB3 + k]; }
 #pragma unroll 1
 	for (int j = 0; j < kH; ++j) {
-		float a = P[kB2 + j];
+		// four partial sums: four independent FMA chains of 16 instead of one
+		// of 64 (the sum's rounding is that of this order, fixed)
+		const float4* w     = reinterpret_cast<const float4*>(P + kW2 + j * kH);
+		float         a4[4] = {P[kB2 + j], 0.0f, 0.0f, 0.0f};
 #pragma unroll
-		for (int i = 0; i < kH; ++i) { a = fmaf(P[kW2 + j * kH + i], h1[i], a); }
+		for (int i4 = 0; i4 < kH / 4; ++i4) {
+			const float4 q = w[i4];
+			a4[0]          = fmaf(q.x, h1[4 * i4], a4[0]);
+			a4[1]          = fmaf(q.y, h1[4 * i4 + 1], a4[1]);
+			a4[2]          = fmaf(q.z, h1[4 * i4 + 2], a4[2]);
+			a4[3]          = fmaf(q.w, h1[4 * i4 + 3], a4[3]);
+		}
+		float a = (a4[0] + a4[1]) + (a4[2] + a4[3]);
 		a = fmaxf(a, 0.0f);
 		if (h2_out) { h2_out[j] = a; }
 #pragma unroll
@@ -196,12 +249,13 @@ __device__ __forceinline__ void softmax5(float (&z)[kOut]) {
 	for (int k = 0; k < kOut; ++k) { z[k] *= inv; }
 }
 
-__global__ void __launch_bounds__(256) mlp_infer_kernel(const float* __restrict__ params, const float* __restrict__ x,
+__global__ void __launch_bounds__(256, 2) mlp_infer_kernel(const float* __restrict__ params, const float* __restrict__ x,
                                                         uint64_t n, float* __restrict__ probs, uint8_t* __restrict__ best,
                                                         float* __restrict__ conf) {
 	// One sample per thread and no sample loop, so the compiler has no reason to
-	// hoist the shared-memory weights into registers.
-	__shared__ float P[kNP];
+	// hoist the shared-memory weights into registers.  Every thread reads the
+	// same weight at the same time: shared-memory broadcasts.
+	__shared__ __align__(16) float P[kNP];
 	load_params(params, P);
 	const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
 	if (i < n) {
@@ -232,7 +286,7 @@ __global__ void __launch_bounds__(256) mlp_train_fwd_kernel(const float* __restr
                                                             const float* __restrict__ x, const uint8_t* __restrict__ y,
                                                             uint32_t B, float* __restrict__ H1, float* __restrict__ H2,
                                                             float* __restrict__ dZ, float* __restrict__ loss) {
-	__shared__ float P[kNP];
+	__shared__ __align__(16) float P[kNP];
 	load_params(params, P);
 	const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
 	float          l = 0.0f;
@@ -257,7 +311,7 @@ __global__ void __launch_bounds__(256) mlp_train_bwd_kernel(const float* __restr
                                                             const float* __restrict__ H1, const float* __restrict__ H2,
                                                             const float* __restrict__ dZ, float* __restrict__ dH1,
                                                             float* __restrict__ dH2) {
-	__shared__ float P[kNP];
+	__shared__ __align__(16) float P[kNP];
 	load_params(params, P);
 	const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
 	if (b >= B) { return; }
@@ -491,7 +545,7 @@ fls_status fls_mlp_infer(const float* d_params, const float* d_x, uint64_t n, fl
 	DeviceInfo di;
 	fls_status s = device_info(di);
 	if (s != FLS_OK) { return s; }
-	if (n > (static_cast<uint64_t>(1) << 38)) { return set_error(FLS_ERR_CAPACITY, "fls_mlp_infer: too many samples"); }
+	if (n > (static_cast<uint64_t>(1) << 36)) { return set_error(FLS_ERR_CAPACITY, "fls_mlp_infer: too many samples"); }
 	const uint32_t grid = static_cast<uint32_t>((n + 255u) / 256u);
 	mlp_infer_kernel<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(d_params, d_x, n, d_probs, d_best,
 	                                                                          d_conf);
