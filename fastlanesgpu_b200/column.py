@@ -288,7 +288,7 @@ def encode_column_learned_gpu(values, params, threshold: float = 0.9, kappa: flo
     bound = int(lib().fls_encode_bound_words(n))
     out = torch.empty(bound + 4, dtype=torch.int32, device=dev)
     meta = torch.empty(nv * 4, dtype=torch.int32, device=dev)
-    info = torch.zeros(4, dtype=torch.int64, device=dev)
+    info = torch.empty(4, dtype=torch.int64, device=dev)  # the call sets all four words
     schemes = torch.empty(nv, dtype=torch.uint8, device=dev)
     ws_bytes = int(lib().fls_encode_learned_workspace_bytes(n))
     ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)

@@ -417,6 +417,12 @@ __global__ void enc_scan_blocks_kernel(const __grid_constant__ EncParams P, uint
 	P.info[0] = run;
 }
 
+// A column of one scan block: offsets and total in one launch.
+__global__ void __launch_bounds__(256) enc_scan_single_kernel(const __grid_constant__ EncParams P) {
+	const uint64_t total = block_scan(P, 0, true, 0);
+	if (threadIdx.x == 0) { P.info[0] = total; }
+}
+
 __global__ void __launch_bounds__(256) enc_scan_offsets_kernel(const __grid_constant__ EncParams P) {
 	block_scan(P, blockIdx.x, true, P.bsum[blockIdx.x]);
 }
@@ -590,11 +596,15 @@ fls_status fls_encode_column_gpu(const int32_t* d_values, uint64_t n, const uint
 	const uint32_t grid = static_cast<uint32_t>(
 	    std::min<uint64_t>((n_vec + kEncWarps - 1) / kEncWarps, static_cast<uint64_t>(di.sms) * 8u));
 	enc_plan_kernel<<<grid, kEncWarps * 32, smem, st>>>(P);
-	enc_scan_sums_kernel<<<static_cast<uint32_t>(n_blocks), 256, 0, st>>>(P);
-	enc_scan_blocks_kernel<<<1, 32, 0, st>>>(P, n_blocks);
-	enc_scan_offsets_kernel<<<static_cast<uint32_t>(n_blocks), 256, 0, st>>>(P);
+	if (n_blocks == 1) {
+		enc_scan_single_kernel<<<1, 256, 0, st>>>(P);
+	} else {
+		enc_scan_sums_kernel<<<static_cast<uint32_t>(n_blocks), 256, 0, st>>>(P);
+		enc_scan_blocks_kernel<<<1, 32, 0, st>>>(P, n_blocks);
+		enc_scan_offsets_kernel<<<static_cast<uint32_t>(n_blocks), 256, 0, st>>>(P);
+	}
 	enc_write_kernel<<<grid, kEncWarps * 32, smem, st>>>(P);
-	count_launch(5);
+	count_launch(n_blocks == 1 ? 3 : 5);
 	return cuda_check(cudaGetLastError(), "encode kernels launch");
 }
 
