@@ -837,15 +837,20 @@ def run_mixed(a, dist: Dist):
     # (fls_encode_learned_gpu: statistics, MLP, exhaustive choice on the device
     # for low-confidence vectors, encode), and the same call with every vector
     # sent to the device's exhaustive choice
+    enc_streams = [torch.cuda.Stream() for _ in range(4)]
+
     def one_call(threshold):
-        # every column's call enqueued back to back; the encoders' info words
-        # are read once all have run (no host round trip per column)
+        # every column's call enqueued back to back, round robin over four
+        # streams so that small columns run beside large ones; the encoders'
+        # info words are read once all have run (no host round trip per column)
         torch.cuda.synchronize()
         t0_ = time.perf_counter()
-        pend = [encode_column_learned_gpu(cat_dev[vstart[i] * 1024: vstart[i] * 1024 + lens[i]], sel.params,
-                                          threshold=threshold, kappa=a.decode_kappa, layout=LAYOUT_TRANSPOSED,
-                                          compact=False, defer=True)
-                for i in range(len(cols))]
+        pend = []
+        for i in range(len(cols)):
+            with torch.cuda.stream(enc_streams[i % len(enc_streams)]):
+                pend.append(encode_column_learned_gpu(cat_dev[vstart[i] * 1024: vstart[i] * 1024 + lens[i]],
+                                                      sel.params, threshold=threshold, kappa=a.decode_kappa,
+                                                      layout=LAYOUT_TRANSPOSED, compact=False, defer=True))
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0_
         return [p.finish() for p in pend], dt
@@ -974,7 +979,8 @@ def run_mixed(a, dist: Dist):
                         "total_s": ln_upload_s + ln_select_s + ln_encode_s,
                         "parts_s": {k: v for k, v in info.items() if k.endswith("_s")}},
             "exhaustive_select_then_gpu_encode_s": ex_select_s + ex_gpu_encode_s,
-            "device_one_call": {"where": "fls_encode_learned_gpu per column, columns already on the GPU",
+            "device_one_call": {"where": "fls_encode_learned_gpu per column, columns already on the GPU, "
+                                         "round robin over 4 streams",
                                 "learned_s": ln1_s, "bytes_learned": size_ln1,
                                 "same_schemes_as_select_device": one_call_same,
                                 "exhaustive_on_device_s": exd_s, "bytes_exhaustive_on_device": size_exd},
