@@ -504,6 +504,26 @@ __device__ __forceinline__ bool table_hit(const ProbeParams& P, const uint32_t* 
 	}
 }
 
+// Hit bits of this lane's rows `far` (slot key - keys_min >= len) for probe
+// q: the remainder (crystal-opt/join.cuh:26), a negative one flagged and
+// missing.  Out of line: such keys are rare.
+template <class Q, int q>
+__device__ __noinline__ uint32_t far_hits(const ProbeParams& P, const uint32_t* tables, const Vec<Q> V, uint32_t lane,
+                                          uint32_t far) {
+	const uint32_t kb = P.base[q] - static_cast<uint32_t>(P.kmin[q]);
+	uint32_t       hits = 0;
+	while (far) {
+		const uint32_t r = static_cast<uint32_t>(__ffs(far)) - 1u;
+		far &= far - 1u;
+		uint32_t h;
+		if (hash_slot<false>(row_field<Q::bw(q)>(V.template col<q>(), lane, r) + kb, P.len[q], h, P.S.err) &&
+		    table_hit<Q, q>(P, tables, h)) {
+			hits |= 1u << r;
+		}
+	}
+	return hits;
+}
+
 // Dense probes q, q+1, ... over the whole vector (probes whose hit test reads
 // shared memory: PHT_1 bitmaps, PHT_2 tables or their presence bitmaps) while
 // some lane keeps more than sparse_rows rows; f0 receives the first probe left
@@ -531,12 +551,27 @@ __device__ __forceinline__ void dense_probes(const ProbeParams& P, const uint32_
 				hit[r & 3] |= (__funnelshift_r(bm[h >> 5], 0u, h) << r) & (1u << r);
 			});
 		} else {
+			// Keys past the table (slot key - keys_min >= len) take the
+			// remainder, rarely: they are collected in `far` and tested after
+			// the unrolled rows, out of line, so that the hot loop holds no
+			// call of the remainder (32 call sites per probe overflowed the
+			// instruction cache on SSB's own data, whose probes are not direct).
+			uint32_t far = 0;
 			unpack_tile_rows<Q, q>(V, lane, [&](int r, uint32_t x) {
-				uint32_t   h;
-				const bool ok = hash_slot<Q::direct(q)>(x + kb, len, h, P.S.err);
-				const bool b  = ok & table_hit<Q, q>(P, tables, h);
+				const uint32_t d = x + kb;
+				bool           b;
+				if constexpr (Q::direct(q)) {
+					b = table_hit<Q, q>(P, tables, d);
+				} else {
+					const bool in = d < static_cast<uint32_t>(len);
+					b             = in && table_hit<Q, q>(P, tables, in ? d : 0u);
+					far |= (in ? 0u : 1u) << r;
+				}
 				hit[r & 3] |= (b ? 1u : 0u) << r;
 			});
+			if constexpr (!Q::direct(q)) {
+				if (far) { hit[0] |= far_hits<Q, q>(P, tables, V, lane, far); }
+			}
 		}
 		mask &= (hit[0] | hit[1]) | (hit[2] | hit[3]);
 		dense_probes<Q, q + 1>(P, tables, V, lane, mask, f0);
