@@ -132,6 +132,25 @@ __device__ __forceinline__ unsigned long long delta_lane_sum(const uint32_t* __r
 	return acc;
 }
 
+// The rows `rows` of a column's last, partial vector, any code width (one
+// vector per column: a plain loop).
+__device__ __noinline__ unsigned long long dict_lane_sum_rows(const uint32_t* __restrict__ s,
+                                                             const uint32_t* __restrict__ dict, uint32_t lane,
+                                                             uint32_t cbw, uint32_t rows) {
+	unsigned long long acc = 0;
+	const uint32_t     m   = cbw >= 32 ? 0xffffffffu : ((1u << cbw) - 1u);
+	for (uint32_t r = 0; r < 32; ++r) {
+		if (cbw == 0 || !((rows >> r) & 1u)) {
+			acc += ((rows >> r) & 1u) ? dict[0] : 0u;
+			continue;
+		}
+		const uint32_t bit = r * cbw, w = bit >> 5, sh = bit & 31u;
+		const uint32_t lo = s[32u * w + lane], hi = sh + cbw > 32u ? s[32u * (w + 1u) + lane] : 0u;
+		acc += dict[(__funnelshift_r(lo, hi, sh) & m) & 1023u];
+	}
+	return acc;
+}
+
 // True when every value of the vector (base + a bw-bit field) is below 2^27.
 __device__ __forceinline__ bool small_values(const VecInfo& m) {
 	const uint64_t top = static_cast<uint64_t>(static_cast<uint32_t>(m.base)) +
@@ -139,7 +158,9 @@ __device__ __forceinline__ bool small_values(const VecInfo& m) {
 	return top < (1ull << 27);
 }
 
-template <bool Small>
+// FULL: every row of the lane holds a value (all vectors but a column's
+// last), so no row is tested.
+template <bool Small, bool FULL>
 __device__ __forceinline__ unsigned long long rle_lane_sum(const uint32_t* __restrict__ s,
                                                            const uint32_t* __restrict__ dict, uint32_t lane,
                                                            uint32_t rows) {
@@ -151,7 +172,7 @@ __device__ __forceinline__ unsigned long long rle_lane_sum(const uint32_t* __res
 	for (int st = 0; st < 32; ++st) {
 		const int r = static_cast<int>(dev::rsum_row(st));
 		idx += (bits >> r) & 1u;
-		const uint32_t v = ((rows >> r) & 1u) ? dict[idx & 1023u] : 0u;
+		const uint32_t v = (FULL || ((rows >> r) & 1u)) ? dict[idx & 1023u] : 0u;
 		if constexpr (Small) {
 			s32 += v;
 		} else {
@@ -161,17 +182,17 @@ __device__ __forceinline__ unsigned long long rle_lane_sum(const uint32_t* __res
 	return Small ? static_cast<unsigned long long>(s32) : s64;
 }
 
+// A whole vector (every row holds a value) at code width CBW.
 template <int CBW, bool Small>
 __device__ __forceinline__ unsigned long long dict_lane_sum(const uint32_t* __restrict__ s,
-                                                            const uint32_t* __restrict__ dict, uint32_t lane,
-                                                            uint32_t rows) {
+                                                            const uint32_t* __restrict__ dict, uint32_t lane) {
 	dev::LaneWords<CBW> lw;
 	dev::load_words<CBW>(s, lane, lw);
 	uint32_t           s32 = 0;
 	unsigned long long s64 = 0;
 #pragma unroll
 	for (int r = 0; r < 32; ++r) {
-		const uint32_t v = ((rows >> r) & 1u) ? dict[dev::extract<CBW>(lw, r) & 1023u] : 0u;
+		const uint32_t v = dict[dev::extract<CBW>(lw, r) & 1023u];
 		if constexpr (Small) {
 			s32 += v;
 		} else {
@@ -237,22 +258,29 @@ struct SchemeSumOp {
 		} else if constexpr (SCHEME == FLS_SCHEME_RLE) {
 			uint32_t* dict = ws.dict();
 			unpack_dict_any(sv.s + 48, sv.vi.aux, sv.vi.bw, sv.vi.base, dict, lane);
-			S.acc += small_values(sv.vi) ? rle_lane_sum<true>(sv.s, dict, lane, rows)
-			                             : rle_lane_sum<false>(sv.s, dict, lane, rows);
+			if (__all_sync(0xffffffffu, rows == 0xffffffffu)) {
+				S.acc += small_values(sv.vi) ? rle_lane_sum<true, true>(sv.s, dict, lane, rows)
+				                             : rle_lane_sum<false, true>(sv.s, dict, lane, rows);
+			} else {
+				S.acc += small_values(sv.vi) ? rle_lane_sum<true, false>(sv.s, dict, lane, rows)
+				                             : rle_lane_sum<false, false>(sv.s, dict, lane, rows);
+			}
 			__syncwarp();
 		} else {
 			uint32_t*      dict = ws.dict();
 			const uint32_t cbw  = dev::bits_of(sv.vi.aux - 1u);
 			unpack_dict_any(sv.s + 32u * cbw, sv.vi.aux, sv.vi.bw, sv.vi.base, dict, lane);
 			const bool small = small_values(sv.vi);
-			switch (cbw) {
+			if (!__all_sync(0xffffffffu, rows == 0xffffffffu)) {
+				S.acc += dict_lane_sum_rows(sv.s, dict, lane, cbw, rows);
+			} else {
+				switch (cbw) {
 #define FLS_DICT_SUM(B)                                                                                                \
-	case B:                                                                                                            \
-		S.acc += small ? dict_lane_sum<B, true>(sv.s, dict, lane, rows) : dict_lane_sum<B, false>(sv.s, dict, lane, rows); \
-		break;
-				FLS_BW_CASES_0_10(FLS_DICT_SUM)
+	case B: S.acc += small ? dict_lane_sum<B, true>(sv.s, dict, lane) : dict_lane_sum<B, false>(sv.s, dict, lane); break;
+					FLS_BW_CASES_0_10(FLS_DICT_SUM)
 #undef FLS_DICT_SUM
-			default: break;
+				default: break;
+				}
 			}
 			__syncwarp();
 		}
