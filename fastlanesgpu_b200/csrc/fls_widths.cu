@@ -43,9 +43,12 @@ __device__ __forceinline__ uint32_t lane_sum(uint32_t x) {
 
 // One vector of 8/16-bit lanes: row r of the 32/B lanes of thread word t.
 // OUT / SUM: write the values / add them to part; TAIL: the column's last,
-// partial vector (rem values).  Branch-free per row, so the loads of all rows
-// can issue before the first is used.
-template <int B, bool OUT, bool SUM, bool TAIL>
+// partial vector (rem values).  NOWRAP (sum only, whole vectors): the host
+// proved base + 2^bw - 1 < 2^B, so no value wraps and the packed fields are
+// summed in 2B-bit halves with the base added once per thread (32 values).
+// Branch-free per row, so the loads of all rows can issue before the first
+// is used.
+template <int B, bool OUT, bool SUM, bool TAIL, bool NOWRAP = false>
 __device__ __forceinline__ void narrow_vector(const uint32_t* __restrict src, uint32_t* __restrict dst, uint32_t bw,
                                               uint32_t vm, uint32_t base_rep, uint32_t t, uint64_t rem,
                                               uint32_t& part) {
@@ -53,6 +56,8 @@ __device__ __forceinline__ void narrow_vector(const uint32_t* __restrict src, ui
 	constexpr uint32_t L = 32u / B;   // lanes per thread word
 	constexpr uint32_t S = 1024u / B; // lanes per vector
 	const uint32_t     last = bw ? bw - 1u : 0u;
+	static_assert(!NOWRAP || (SUM && !OUT && !TAIL), "NOWRAP sums whole vectors only");
+	uint32_t           ev = 0, od = 0; // NOWRAP: even and odd lanes' fields, 2B-bit sums
 #pragma unroll
 	for (uint32_t r = 0; r < static_cast<uint32_t>(B); ++r) {
 		// the second word row is read unconditionally, clamped inside the vector
@@ -62,6 +67,17 @@ __device__ __forceinline__ void narrow_vector(const uint32_t* __restrict src, ui
 		const uint32_t hi      = (hi_word << (B - s)) & (((N::kLow << (B - s)) & N::kLow) * N::kRep);
 		const uint32_t x       = (((lo_word >> s) & ((N::kLow >> s) * N::kRep)) |
 		                    (s + bw > static_cast<uint32_t>(B) ? hi : 0u)) & vm;
+		if constexpr (NOWRAP) {
+			// at most 8 (B = 8) or 16 (B = 16) rows of B-bit fields per half
+			if constexpr (B == 8) {
+				ev += x & 0x00ff00ffu;
+				od += (x >> 8) & 0x00ff00ffu;
+			} else {
+				ev += x & 0xffffu;
+				od += x >> 16;
+			}
+			continue;
+		}
 		const uint32_t y = ((x & ~N::kHigh) + (base_rep & ~N::kHigh)) ^ ((x ^ base_rep) & N::kHigh);
 		if constexpr (OUT) { __stcs(dst + 32u * r + t, y); }
 		if constexpr (SUM) {
@@ -75,6 +91,14 @@ __device__ __forceinline__ void narrow_vector(const uint32_t* __restrict src, ui
 			}
 			part += lane_sum<B>(keep);
 		}
+	}
+	if constexpr (NOWRAP) {
+		if constexpr (B == 8) {
+			part += (ev & 0xffffu) + (ev >> 16) + (od & 0xffffu) + (od >> 16);
+		} else {
+			part += ev + od;
+		}
+		part += 32u * (base_rep & N::kLow); // the thread's 32 values
 	}
 }
 
@@ -90,7 +114,7 @@ constexpr int narrow_min_blocks() {
 template <int B, bool OUT, bool SUM>
 __global__ void __launch_bounds__(256, narrow_min_blocks<B, OUT, SUM>()) decode_narrow_kernel(const uint32_t* __restrict in, uint64_t n, uint64_t n_vec,
                                                             uint32_t bw, uint32_t base_rep, uint32_t* __restrict out,
-                                                            unsigned long long* sum) {
+                                                            unsigned long long* sum, bool nowrap) {
 	using N                = Narrow<B>;
 	const uint32_t     t   = threadIdx.x & 31u;
 	const uint64_t     wg  = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -112,7 +136,15 @@ __global__ void __launch_bounds__(256, narrow_min_blocks<B, OUT, SUM>()) decode_
 				if (t == 0) { acc += cnt * (base_rep & N::kLow); }
 			}
 		} else if (rem >= 1024u) {
-			narrow_vector<B, OUT, SUM, false>(src, dst, bw, vm, base_rep, t, rem, part);
+			if constexpr (SUM && !OUT) {
+				if (nowrap) {
+					narrow_vector<B, OUT, SUM, false, true>(src, dst, bw, vm, base_rep, t, rem, part);
+				} else {
+					narrow_vector<B, OUT, SUM, false>(src, dst, bw, vm, base_rep, t, rem, part);
+				}
+			} else {
+				narrow_vector<B, OUT, SUM, false>(src, dst, bw, vm, base_rep, t, rem, part);
+			}
 		} else {
 			narrow_vector<B, OUT, SUM, true>(src, dst, bw, vm, base_rep, t, rem, part);
 		}
@@ -212,15 +244,17 @@ fls_status launch_decode(uint32_t bits, const void* d_in, uint64_t n, uint8_t bw
 	} else {
 		const uint32_t rep  = bits == 8 ? static_cast<uint32_t>(base & 0xffu) * 0x01010101u
 		                                : static_cast<uint32_t>(base & 0xffffu) * 0x00010001u;
+		// no decoded value wraps: base + 2^bw - 1 < 2^bits
+		const bool nowrap = (base & ((1ull << bits) - 1u)) + ((1ull << bw) - 1u) < (1ull << bits);
 		const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>((n_vec + 7u) / 8u, static_cast<uint64_t>(di.sms) * 16u));
 		launch_mode(d_out != nullptr, d_sum != nullptr, [&](auto mode) {
 			constexpr int M = decltype(mode)::value;
 			if (bits == 8) {
 				decode_narrow_kernel<8, (M & 1) != 0, (M & 2) != 0><<<grid, 256, 0, st>>>(
-				    static_cast<const uint32_t*>(d_in), n, n_vec, bw, rep, static_cast<uint32_t*>(d_out), sum);
+				    static_cast<const uint32_t*>(d_in), n, n_vec, bw, rep, static_cast<uint32_t*>(d_out), sum, nowrap);
 			} else {
 				decode_narrow_kernel<16, (M & 1) != 0, (M & 2) != 0><<<grid, 256, 0, st>>>(
-				    static_cast<const uint32_t*>(d_in), n, n_vec, bw, rep, static_cast<uint32_t*>(d_out), sum);
+				    static_cast<const uint32_t*>(d_in), n, n_vec, bw, rep, static_cast<uint32_t*>(d_out), sum, nowrap);
 			}
 		});
 	}

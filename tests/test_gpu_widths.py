@@ -60,3 +60,17 @@ def test_full_size_sums(cuda, bits, dt):
     v = _column(g, dt, bits, bw, n, 1)
     _, total = _run(v, dt, bits, bw, 1, want_out=False)
     assert total == int(v.astype(np.uint64).sum(dtype=np.uint64))
+
+
+@pytest.mark.parametrize("bits,dt", WIDTHS[:2])
+def test_sum_only_every_bit_width(cuda, bits, dt):
+    """The sum alone, at every bit width, with a base whose values do not wrap
+    (summed without the per-value base) and one whose values do."""
+    g = np.random.default_rng(300 + bits)
+    n = 5 * 1024 + 77
+    for bw in range(0, bits + 1):
+        top = (1 << bits) - (1 << bw)  # the largest base with no wrap
+        for base in sorted({0, top, min(top + 1, (1 << bits) - 1), int(g.integers(0, 1 << bits))}):
+            v = _column(g, dt, bits, bw, n, base)
+            _, total = _run(v, dt, bits, bw, base, want_out=False)
+            assert total == int(v.astype(np.uint64).sum(dtype=np.uint64)), (bw, base)
