@@ -165,7 +165,8 @@ __global__ void __launch_bounds__(256, 3) decode_u64_kernel(const uint64_t* __re
 	const uint32_t     i   = threadIdx.x & 15u; // lane of the vector
 	const uint64_t     h0  = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 4;
 	const uint64_t     nh  = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 4;
-	const uint64_t     m   = bw >= 64 ? ~0ull : (1ull << bw) - 1ull;
+	const uint64_t     m    = bw >= 64 ? ~0ull : (1ull << bw) - 1ull;
+	const uint32_t     m_lo = static_cast<uint32_t>(m), m_hi = static_cast<uint32_t>(m >> 32);
 	const uint32_t     last = bw ? bw - 1u : 0u;
 	unsigned long long acc = 0;
 	// every half-warp runs the same number of iterations, so full-warp
@@ -183,18 +184,34 @@ __global__ void __launch_bounds__(256, 3) decode_u64_kernel(const uint64_t* __re
 			}
 			continue;
 		}
-#pragma unroll 16
-		for (uint32_t r = 0; r < 64; ++r) {
-			// both word rows read unconditionally (the second clamped inside the
-			// vector) and combined by selection: no branch between the rows
+		// Row r's field starts at bit s of word row k.  Both word rows are
+		// read unconditionally (the second clamped inside the vector) and
+		// the field is cut from their four 32-bit halves by two 32-bit
+		// funnel shifts; bits of the second row past a field that does not
+		// straddle fall under the mask.
+		auto row = [&](uint32_t r) -> uint64_t {
 			const uint32_t o = r * bw, k = o >> 6, s = o & 63u;
-			const uint64_t lo_word = __ldg(src + 16u * k + i);
-			const uint64_t hi_word = __ldg(src + 16u * min(k + 1u, last) + i);
-			const uint64_t hi      = (hi_word << 1) << (63u - s); // hi_word << (64 - s), defined for s = 0
-			const uint64_t x       = ((lo_word >> s) | (s + bw > 64u ? hi : 0ull)) & m;
-			const uint64_t y       = x + base;
-			if constexpr (OUT) { __stcs(reinterpret_cast<unsigned long long*>(out) + v * 1024u + 16u * r + i, y); }
-			if constexpr (SUM) { acc += 16u * r + i < rem ? y : 0ull; }
+			const uint2    a = __ldg(reinterpret_cast<const uint2*>(src + 16u * k + i));
+			const uint2    b = __ldg(reinterpret_cast<const uint2*>(src + 16u * min(k + 1u, last) + i));
+			const bool     up = s >= 32u;
+			const uint32_t w0 = up ? a.y : a.x, w1 = up ? b.x : a.y, w2 = up ? b.y : b.x;
+			const uint32_t xl = __funnelshift_r(w0, w1, s) & m_lo, xh = __funnelshift_r(w1, w2, s) & m_hi;
+			return ((static_cast<uint64_t>(xh) << 32) | xl) + base;
+		};
+		if (rem >= 1024u) {
+#pragma unroll 16
+			for (uint32_t r = 0; r < 64; ++r) {
+				const uint64_t y = row(r);
+				if constexpr (OUT) { __stcs(reinterpret_cast<unsigned long long*>(out) + v * 1024u + 16u * r + i, y); }
+				if constexpr (SUM) { acc += y; }
+			}
+		} else {
+#pragma unroll 4
+			for (uint32_t r = 0; r < 64; ++r) {
+				const uint64_t y = row(r);
+				if constexpr (OUT) { __stcs(reinterpret_cast<unsigned long long*>(out) + v * 1024u + 16u * r + i, y); }
+				if constexpr (SUM) { acc += 16u * r + i < rem ? y : 0ull; }
+			}
 		}
 	}
 	if constexpr (SUM) {
