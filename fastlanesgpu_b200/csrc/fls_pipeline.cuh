@@ -35,9 +35,10 @@ constexpr uint32_t kMaxTile    = 32;       // vectors per tile (one lane per vec
 constexpr uint32_t kMaxWarps   = 16;       // warps per CTA (general kernels)
 // Warps per CTA of the specialised join kernels unless the caller set a
 // launch configuration: their launch bounds follow the shape, and joins whose
-// tables leave room for more than 16 warps run faster with them (the filter
-// and decode kernels measured faster at 16).
-constexpr uint32_t kJitDefaultWarps = 20;
+// tables leave room for more than 16 warps run faster with them (Q2.1: 0.230
+// ms at 20, 0.210 ms at 24; the filter and decode kernels measured faster at
+// 16).
+constexpr uint32_t kJitDefaultWarps = 24;
 // With half-vector stages (FLS_TUNE_HALF_VECTORS): 28 warps fit at the
 // joins' 66-72 registers per thread.
 constexpr uint32_t kJitHalfWarps = 28;
